@@ -1,0 +1,276 @@
+/* tomos_b200.h -- C ABI of the B200 (sm_100a) LSQR hot path.
+ *
+ * Every entry point takes plain pointers and sizes, never throws, and
+ * returns a tomos_status (0 on success).  tomos_last_error() gives the
+ * message of the calling thread's last failure.  Device pointers are CUDA
+ * device memory on the current device; `stream` is a cudaStream_t passed as
+ * void* (NULL = the legacy default stream).  Calls are asynchronous on
+ * `stream` unless documented otherwise; tomos_sync() blocks.
+ *
+ * Enum values mirror the reference (TOMOS) so a binding can pass the
+ * reference's own enums through unchanged:
+ *   NumericType  include/core/precision.hpp:43-50 (FP32_BF16 is new, slot 5)
+ *   Layout       include/core/precision.hpp:51
+ *   TransposeType src/core/matrix/transpose.hpp
+ */
+#ifndef TOMOS_B200_H
+#define TOMOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int tomos_status;
+enum {
+    TOMOS_OK = 0,
+    TOMOS_ERR_INVALID = -1,     /* std::invalid_argument in the reference  */
+    TOMOS_ERR_UNSUPPORTED = -2, /* std::runtime_error "no kernel registered" */
+    TOMOS_ERR_CUDA = -3,        /* CUDA runtime error                       */
+    TOMOS_ERR_ALLOC = -4,       /* allocation failure                       */
+    TOMOS_ERR_NUMERIC = -5      /* singular R / non-finite data             */
+};
+
+enum tomos_numeric {
+    TOMOS_FP64 = 0, TOMOS_FP32 = 1, TOMOS_FP16 = 2, TOMOS_FP32_16 = 3,
+    TOMOS_BF16 = 4, TOMOS_FP32_BF16 = 5
+};
+enum tomos_layout { TOMOS_ROW_MAJOR = 0, TOMOS_COL_MAJOR = 1 };
+enum tomos_trans { TOMOS_NO_TRANSPOSE = 0, TOMOS_TRANSPOSE = 1 };
+
+/* Compute tier of a product with A (reference dense_registries.cpp:350-362
+ * and blas.hpp:160-172):
+ *   NATIVE   -- A's own type (FP32 / FP64 storage).
+ *   HALF     -- packed A read from its 16-bit wh plane only: FP32_16 decoded
+ *               exactly as fp32_16_half_only (the reference's "fast" tier,
+ *               fp32_16_kernels.cpp:102-123), FP32_BF16 as its bf16 word;
+ *               FP32 accumulation.
+ *   ACCURATE -- packed A reconstructed exactly from wh+wr (fp32_16_combine /
+ *               fp32_bf16_combine[_rounded]); FP64 row accumulation.
+ *   AUTO     -- the reference's default rule (blas.cpp:33-53): HALF for
+ *               packed A, NATIVE otherwise. */
+enum tomos_tier { TOMOS_TIER_AUTO = 0, TOMOS_TIER_NATIVE = 1, TOMOS_TIER_HALF = 2,
+                  TOMOS_TIER_ACCURATE = 3 };
+
+/* A strided dense matrix in device memory (non-owning; the reference's
+ * StridedView, include/core/matrix.hpp:167-177).  For the packed types
+ * `values` is the wh plane (uint16) and `values_lo` the wr plane; NULL
+ * values_lo means the reference's planar layout (fp32_16_pack.hpp:861-874):
+ * wr = wh + ld * (layout == COL_MAJOR ? cols : rows).  FP32_BF16 packs may
+ * be truncating (rounded == 0, fp32_bf16_split) or rounding (rounded == 1,
+ * fp32_bf16_split_rounded). */
+typedef struct tomos_dense {
+    int32_t numeric;
+    int32_t layout;
+    int64_t rows;
+    int64_t cols;
+    int64_t ld;
+    void* values;
+    void* values_lo;
+    int32_t rounded;
+    int32_t reserved;
+} tomos_dense;
+
+/* A CSR matrix in device memory (non-owning; CsrView, matrix.hpp:182-200).
+ * index_type 0 = int32, 1 = int64 (IntType).  Packed values as above with
+ * values_lo = values + nnz when NULL. */
+typedef struct tomos_csr {
+    int32_t numeric;
+    int32_t index_type;
+    int64_t rows;
+    int64_t cols;
+    int64_t nnz;
+    void* values;
+    void* values_lo;
+    void* row_ptrs;
+    void* col_idxs;
+    int32_t rounded;
+    int32_t reserved;
+} tomos_csr;
+
+const char* tomos_last_error(void);
+const char* tomos_version(void);
+tomos_status tomos_sync(void* stream);
+
+/* ------------------------------------------------------------------ pack */
+
+/* FP32 -> FP32_16 planes, bit-exact with fp32_16_split (the reference's
+ * split_fp32_16 -> cuda::split_dense_fp32_16, fp32_16_cuda_kernels.cu:
+ * 271-299; encoder fp32_16_pack.hpp:129-190).  src and dst share rows,
+ * cols and layout; ld_src / ld_dst are their leading dimensions.
+ * counts (device, may be NULL, 4 x uint64 accumulated into): elements
+ * encoded [0] normal, [1] extended underflow, [2] extended overflow,
+ * [3] saturated. */
+tomos_status tomos_pack_fp32_16(const float* src, int32_t layout, int64_t rows,
+                                int64_t cols, int64_t ld_src, uint16_t* wh,
+                                uint16_t* wr, int64_t ld_dst,
+                                unsigned long long* counts, void* stream);
+/* FP32_16 planes -> FP32 (fp32_16_combine; combine_fp32_16,
+ * fp32_16_registries.cpp:48-62). */
+tomos_status tomos_unpack_fp32_16(const uint16_t* wh, const uint16_t* wr,
+                                  int32_t layout, int64_t rows, int64_t cols,
+                                  int64_t ld_src, float* dst, int64_t ld_dst,
+                                  void* stream);
+/* FP32 -> FP32_BF16 planes (fp32_bf16_split / fp32_bf16_split_rounded,
+ * fp32_bf16_pack.hpp:68-73,117-145) and back (combine / combine_rounded). */
+tomos_status tomos_pack_fp32_bf16(const float* src, int32_t layout, int64_t rows,
+                                  int64_t cols, int64_t ld_src, uint16_t* wh,
+                                  uint16_t* wr, int64_t ld_dst, int32_t rounded,
+                                  void* stream);
+tomos_status tomos_unpack_fp32_bf16(const uint16_t* wh, const uint16_t* wr,
+                                    int32_t layout, int64_t rows, int64_t cols,
+                                    int64_t ld_src, float* dst, int64_t ld_dst,
+                                    int32_t rounded, void* stream);
+
+/* ------------------------------------------------------------------ GEMV */
+
+/* y = alpha * op(A) x + beta * y (FP32 x, y), the reference's mv_apply
+ * (src/core/blas/blas.cpp:23-31) resolved through dispatch::Dense::lookup_mv
+ * (dense_registries.cpp:180-189) / Fp32_16 tiers (fp32_16_registries.cpp).
+ * Deterministic: the transposed product of a row-major A (and the plain
+ * product of a column-major A) reduces per-block partials in a fixed
+ * order.  beta == 0 never reads y.  scratch: device buffer of at least
+ * tomos_gemv_scratch_bytes() bytes (may be NULL when that is 0). */
+size_t tomos_gemv_scratch_bytes(const tomos_dense* A, int32_t trans);
+tomos_status tomos_gemv(int32_t trans, double alpha, const tomos_dense* A,
+                        int32_t tier, const float* x, double beta, float* y,
+                        void* scratch, size_t scratch_bytes, void* stream);
+
+/* CSR y = alpha * op(A) x + beta * y (cuda::mv_csr, mv_cuda_kernels.cu:
+ * 2029-2058; dispatch::Sparse::lookup_mv).  FP32, FP64 and packed values.
+ * The transposed product is deterministic (no atomics). */
+size_t tomos_csr_gemv_scratch_bytes(const tomos_csr* A, int32_t trans);
+tomos_status tomos_csr_gemv(int32_t trans, double alpha, const tomos_csr* A,
+                            int32_t tier, const float* x, double beta, float* y,
+                            void* scratch, size_t scratch_bytes, void* stream);
+
+/* ----------------------------------------------------------- CountSketch */
+
+#define TOMOS_CS_BUCKET_SEED 0x12345678abcdef00ull
+#define TOMOS_CS_SIGN_SEED 0xf00dd00d42babe55ull
+
+/* Row i of A -> bucket splitmix64(i ^ bucket_seed) mod s, sign + if bit 0 of
+ * splitmix64(i ^ sign_seed) is set (countsketch_kernels.cpp:59-85,
+ * countsketch_cuda_kernels.cu:267-286).  Device outputs, m entries each. */
+tomos_status tomos_countsketch_hash(int64_t m, int64_t s, uint64_t bucket_seed,
+                                    uint64_t sign_seed, int32_t* bucket,
+                                    int8_t* sign, void* stream);
+/* SA (s x cols, column-major FP64, leading dimension ld_sa) = S * A, with
+ * S the hash CountSketch above (replaces apply_count_sketch,
+ * src/core/sketch/countsketch.cpp:20-26, whose dense-source CUDA path the
+ * reference omits, sketch_registries.cpp:29-41).  Deterministic: each
+ * bucket is summed by one owner in increasing row order, FP64
+ * accumulation.  Packed A is read at `tier` (HALF reads only wh).
+ * fro2 (device, may be NULL) receives sum(A_ij^2) of the values read. */
+size_t tomos_countsketch_scratch_bytes(int64_t m, int64_t s);
+tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t s,
+                                     uint64_t bucket_seed, uint64_t sign_seed,
+                                     double* SA, int64_t ld_sa, double* fro2,
+                                     void* scratch, size_t scratch_bytes,
+                                     void* stream);
+tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64_t s,
+                                         uint64_t bucket_seed, uint64_t sign_seed,
+                                         double* SA, int64_t ld_sa, double* fro2,
+                                         void* scratch, size_t scratch_bytes,
+                                         void* stream);
+
+/* ------------------------------------------------------------- sketch QR */
+
+/* FP64 Householder QR of the k x n (k >= n) column-major SA, then the
+ * explicit inverse of R: on return the leading n x n block of SA holds
+ * R^{-1} (upper triangular, zeros below), exactly the contract of
+ * generate_sketch_qr_precond (src/core/precond/sketch_qr.hpp:19,
+ * sketch_qr.cpp:38-64: geqrf + trtri).  R (device, may be NULL, n x n
+ * column-major, ld n) receives R itself. */
+size_t tomos_sketch_qr_scratch_bytes(int64_t k, int64_t n);
+tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64_t ld,
+                                         double* R, void* scratch,
+                                         size_t scratch_bytes, void* stream);
+
+/* ------------------------------------------------------------------ LSQR */
+
+/* Stopping rules.  RELRES is the reference's (lsqr.cpp:418-425, :723-729):
+ * stop when |phi_bar| / ||b|| < tol or < max_relres.  BACKWARD stops when
+ * the normwise backward error
+ *   eta = min( ||r|| / (||A||_F ||x|| + ||b||),  ||A^T r|| / (||A||_F ||r||) )
+ * of the current x, recomputed from an ACCURATE-tier residual at every
+ * restart boundary, is <= tol. */
+enum tomos_stop { TOMOS_STOP_RELRES = 0, TOMOS_STOP_BACKWARD = 1 };
+
+typedef struct tomos_lsqr_opts {
+    double tol;              /* lsqr_solve's tol                          */
+    int32_t max_iters;       /* iterations per restart                     */
+    int32_t restarts;        /* outer cycles (lsqr_solve's restarts)       */
+    double max_relres;       /* lsqr_solve's max_relres                    */
+    int32_t stop_rule;       /* enum tomos_stop                            */
+    int32_t iter_tier;       /* per-iteration products (Workspace::
+                                mv_compute_type_); AUTO = reference rule   */
+    int32_t implicit_duplicate; /* Workspace::use_implicit_duplicate_: the
+                                restart residual reads packed A ACCURATE    */
+    int32_t warm_start;      /* 0: x zeroed first (lsqr_registries.cpp:156) */
+    double inner_rtol;       /* BACKWARD rule: an inner cycle ends once its
+                                residual estimate fell by this factor (0 =
+                                run max_iters)                              */
+    double anorm_fro;        /* ||A||_F if already known (e.g. from
+                                tomos_countsketch_apply's fro2); 0 = the
+                                BACKWARD rule computes it (one pass)        */
+    double* history;         /* host, may be NULL: |phi_bar|/||b|| per
+                                completed iteration (residual_history)     */
+    int32_t history_cap;
+    int32_t reserved;
+} tomos_lsqr_opts;
+
+typedef struct tomos_lsqr_report {
+    int32_t iterations;      /* completed inner iterations, all restarts   */
+    int32_t restarts_used;
+    int32_t converged;
+    int32_t history_len;
+    double relres;           /* |phi_bar| / ||b|| at exit                  */
+    double rnorm;            /* last accurate ||b - A x||                   */
+    double arnorm;           /* last accurate ||A^T (b - A x)||             */
+    double anorm_fro;        /* ||A||_F                                     */
+    double xnorm;
+    double bnorm;
+    double backward_error;   /* eta of the returned x (accurate residual)   */
+    double elapsed_ms;       /* device time of the solve                    */
+    int32_t accurate_passes; /* ACCURATE-tier passes over A                 */
+    int32_t half_passes;     /* HALF-tier passes over A                     */
+} tomos_lsqr_report;
+
+typedef struct tomos_workspace tomos_workspace;
+
+/* create_lsqr_workspace (src/core/solver/lsqr.cpp:389-406,
+ * include/core/solver.hpp:15-25): owns the device arena for the m- and
+ * n-vectors, the per-block partials of the transposed products and the
+ * solver state.  value_type must be FP32; precond_type FP32 or FP64. */
+tomos_status tomos_workspace_create(int64_t m, int64_t n, int32_t value_type,
+                                    int32_t precond_type, tomos_workspace** ws);
+tomos_status tomos_workspace_destroy(tomos_workspace* ws);
+/* add_precond (include/core/workspace.hpp:112-120): attaches a non-owning
+ * n x n right preconditioner R^{-1} (FP32 or FP64 Dense, any layout); its
+ * numeric type must equal the workspace's precond_type.  NULL detaches. */
+tomos_status tomos_workspace_add_precond(tomos_workspace* ws, const tomos_dense* Rinv);
+
+/* lsqr_solve (include/core/solver.hpp:68-78; lsqr.cpp:785-801): solves
+ * min ||A x - b|| with A m x n on the device, b (m) and x (n) FP32 device
+ * vectors.  Synchronous on `stream` (the report is filled on return). */
+tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float* x,
+                                    tomos_workspace* ws, const tomos_lsqr_opts* opts,
+                                    tomos_lsqr_report* report, void* stream);
+tomos_status tomos_lsqr_solve_csr(const tomos_csr* A, const float* b, float* x,
+                                  tomos_workspace* ws, const tomos_lsqr_opts* opts,
+                                  tomos_lsqr_report* report, void* stream);
+
+/* Normwise backward error of x (FP64, ACCURATE tier): fills report's
+ * rnorm, arnorm, anorm_fro, xnorm, bnorm and backward_error.  Needs a
+ * workspace of A's shape for its partials. */
+tomos_status tomos_backward_error_dense(const tomos_dense* A, const float* b,
+                                        const float* x, tomos_workspace* ws,
+                                        tomos_lsqr_report* report, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOMOS_B200_H */

@@ -1,0 +1,88 @@
+"""CSR products, CSR CountSketch and CSR LSQR against FP64 oracles."""
+import numpy as np
+import pytest
+import torch
+
+import tomos_b200 as tb
+from gpu_util import cuda
+
+pytestmark = pytest.mark.gpu
+NT = tb.NumericType
+
+
+def random_csr(m, n, k, seed, decades=1.0):
+    rng = np.random.default_rng(seed)
+    cols = np.stack([np.sort(rng.choice(n, k, replace=False)) for _ in range(m)])
+    vals = rng.standard_normal((m, k)) * 10.0 ** rng.uniform(-decades, decades, (m, 1))
+    D = np.zeros((m, n))
+    np.put_along_axis(D, cols, vals, axis=1)
+    rp = np.arange(0, (m + 1) * k, k, dtype=np.int32)
+    return rp, cols.astype(np.int32).ravel(), vals.astype(np.float32).ravel(), D.astype(np.float32)
+
+
+def make(rp, ci, v, m, n, numeric=NT.FP32, rounded=False):
+    vals = cuda(v)
+    if numeric != NT.FP32:
+        t = tb.Dense.from_tensor(vals[None, :], tb.Layout.ROW_MAJOR)
+        P = tb.pack(t, numeric, rounded=rounded)
+        vals = P.storage  # [wh | wr] planar, nnz each
+    return tb.Csr(numeric, (m, n), cuda(rp, torch.int32), cuda(ci, torch.int32), vals, rounded)
+
+
+@pytest.mark.parametrize("numeric,tier", [(NT.FP32, tb.Tier.AUTO), (NT.FP32_16, tb.Tier.HALF),
+                                          (NT.FP32_16, tb.Tier.ACCURATE), (NT.FP32_BF16, tb.Tier.HALF)])
+def test_csr_gemv(orc, numeric, tier):
+    m, n = 3001, 517
+    rp, ci, v, D = random_csr(m, n, 9, 1)
+    A = make(rp, ci, v, m, n, numeric)
+    if numeric == NT.FP32:
+        Dd = D.astype(np.float64)
+    else:
+        wh, wr = (orc.fp32_16_split(v) if numeric == NT.FP32_16 else orc.fp32_bf16_split(v))
+        kind = "fp32_16" if numeric == NT.FP32_16 else "fp32_bf16"
+        vv = orc.decode(kind, wh, wr, "half" if tier == tb.Tier.HALF else "accurate")
+        Dd = np.zeros((m, n))
+        np.put_along_axis(Dd, ci.reshape(m, -1).astype(np.int64), vv.reshape(m, -1), axis=1)
+    rng = np.random.default_rng(2)
+    for trans, M in ((tb.NO_TRANSPOSE, Dd), (tb.TRANSPOSE, Dd.T)):
+        x = rng.standard_normal(M.shape[1]).astype(np.float32)
+        y0 = rng.standard_normal(M.shape[0]).astype(np.float32)
+        for beta in (0.0, -0.25):
+            yy = y0.copy()
+            if beta == 0.0:
+                yy[:] = np.nan
+            y = cuda(yy)
+            tb.mv_apply(tb.Device.CUDA, trans, 2.0, A, cuda(x), beta, y, tier=tier)
+            ref = 2.0 * (M @ x) + (beta * y0 if beta else 0.0)
+            scale = 2.0 * (np.abs(M) @ np.abs(x)) + abs(beta) * np.abs(y0)
+            assert np.all(np.abs(y.cpu().numpy() - ref) <= 2e-5 * scale + 1e-6 * np.abs(ref) + 1e-30)
+
+
+def test_csr_countsketch(orc):
+    m, n, s = 4000, 300, 211
+    rp, ci, v, D = random_csr(m, n, 12, 5)
+    A = make(rp, ci, v, m, n)
+    SA, fro2 = tb.apply_count_sketch(A, s)
+    ref = orc.countsketch_apply(D, s)
+    np.testing.assert_allclose(SA.view().cpu().numpy(), ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    np.testing.assert_allclose(fro2.item(), (v.astype(np.float64) ** 2).sum(), rtol=1e-12)
+
+
+@pytest.mark.parametrize("numeric", [NT.FP32, NT.FP32_16])
+def test_csr_lsqr_preconditioned(orc, numeric):
+    m, n = 20000, 400
+    rp, ci, v, D = random_csr(m, n, 20, 7, decades=2.0)
+    rng = np.random.default_rng(8)
+    xt = rng.standard_normal(n)
+    b = (D.astype(np.float64) @ xt + 1e-8 * rng.standard_normal(m)).astype(np.float32)
+    A = make(rp, ci, v, m, n, numeric)
+    SA, fro2 = tb.apply_count_sketch(A, 4 * n, tier=tb.Tier.AUTO)
+    Rinv = tb.generate_sketch_qr_precond(SA)
+    ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32, NT.FP64)
+    tb.add_precond(Rinv, ws)
+    x = torch.zeros(n, device="cuda")
+    rep = tb.lsqr_solve(None, A, cuda(b), x, ws, 1e-6, 200, 0.0, restarts=6,
+                        stop_rule=tb.StopRule.BACKWARD, inner_rtol=1e-3 if numeric != NT.FP32 else 0.0)
+    xx = x.cpu().numpy()
+    eta = orc.backward_error(D, b, xx)
+    assert rep["converged"] == 1 and eta <= 1.05e-6, (eta, rep)

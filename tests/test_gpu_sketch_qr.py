@@ -1,0 +1,103 @@
+"""CountSketch (bit-exact hash, deterministic FP64 owner sums) and the FP64
+Householder sketch QR against the oracle and the reference's outputs."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import tomos_b200 as tb
+from gpu_util import to_dense, decoded
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+pytestmark = pytest.mark.gpu
+L = tb.Layout
+NT = tb.NumericType
+
+
+@pytest.mark.parametrize("s", [1, 64, 4000])
+def test_hash_bit_exact(orc, s):
+    m = 100_003
+    b, g = tb.countsketch_hash(m, s)
+    eb, eg = orc.countsketch_hash(m, s)
+    assert np.array_equal(b.cpu().numpy(), eb) and np.array_equal(g.cpu().numpy(), eg)
+    gold = np.load(os.path.join(GOLD, "countsketch.npz"))
+    if s in (64, 4000):
+        assert np.array_equal(b[:4096].cpu().numpy(), gold[f"bucket_s{s}"])
+
+
+@pytest.mark.parametrize("numeric,tier", [(NT.FP32, tb.Tier.AUTO), (NT.FP32_16, tb.Tier.HALF),
+                                          (NT.FP32_16, tb.Tier.ACCURATE), (NT.FP32_BF16, tb.Tier.HALF)])
+@pytest.mark.parametrize("layout", [L.ROW_MAJOR, L.COL_MAJOR])
+def test_apply_vs_oracle(orc, numeric, tier, layout):
+    rng = np.random.default_rng(4)
+    m, n, s = 5003, 301, 97
+    A0 = (rng.standard_normal((m, n)) * np.logspace(-2, 2, n)).astype(np.float32)
+    A = to_dense(A0, layout, numeric, pad=3)
+    SA, fro2 = tb.apply_count_sketch(A, s, tier=tier)
+    Ad = decoded(orc, A, tier).astype(np.float32)
+    ref = orc.countsketch_apply(Ad, s, row_major=True)
+    got = SA.view().cpu().numpy()
+    if layout == L.ROW_MAJOR:
+        # one owner per bucket, rows in increasing order, FP64: same sums
+        assert np.array_equal(got, ref)
+    else:
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    np.testing.assert_allclose(fro2.item(), (Ad.astype(np.float64) ** 2).sum(), rtol=1e-12)
+
+
+def test_apply_reference_golden(orc):
+    g = np.load(os.path.join(GOLD, "countsketch.npz"))
+    A = to_dense(g["X"], L.COL_MAJOR)
+    SA, _ = tb.apply_count_sketch(A, 64)
+    np.testing.assert_allclose(SA.view().cpu().numpy(), g["Y"], rtol=1e-5, atol=1e-5)
+
+
+def test_apply_deterministic():
+    rng = np.random.default_rng(9)
+    A = to_dense(rng.standard_normal((20000, 64)).astype(np.float32), L.COL_MAJOR)
+    a, _ = tb.apply_count_sketch(A, 128)
+    b, _ = tb.apply_count_sketch(A, 128)
+    assert torch.equal(a.storage, b.storage)
+
+
+def qr_on_gpu(SA):
+    D = tb.Dense.create_strided(None, L.COL_MAJOR, NT.FP64, SA.shape)
+    D.view()[...] = torch.from_numpy(np.asarray(SA, np.float64)).cuda()
+    R = torch.zeros(SA.shape[1] * SA.shape[1], dtype=torch.float64, device="cuda")
+    Rinv = tb.generate_sketch_qr_precond(D, R_out=R)
+    return Rinv.view().cpu().numpy(), R.view(SA.shape[1], SA.shape[1]).t().cpu().numpy()
+
+
+def test_qr_reference_golden(orc):
+    g = np.load(os.path.join(GOLD, "sketch_qr.npz"))
+    Rinv, R = qr_on_gpu(g["SA"])
+    np.testing.assert_allclose(Rinv, g["Rinv"], rtol=1e-9, atol=1e-12 * np.abs(g["Rinv"]).max())
+    Ro, _ = orc.householder_qr(g["SA"])
+    np.testing.assert_allclose(R, Ro, rtol=1e-10, atol=1e-10 * np.abs(Ro).max())
+
+
+def test_qr_known_4x2():
+    A = np.array([[1.0, 2.0], [3.0, 4.0], [5.0, 6.0], [7.0, 8.0]])
+    Rinv, _ = qr_on_gpu(A)
+    assert np.allclose(np.tril(Rinv, -1), 0)
+    np.testing.assert_allclose(Rinv.T @ A.T @ A @ Rinv, np.eye(2), atol=1e-10)
+
+
+@pytest.mark.parametrize("k,n", [(64, 64), (97, 33), (700, 100), (4000, 1000)])
+def test_qr_property_and_vs_lapack(k, n):
+    rng = np.random.default_rng(k + n)
+    SA = rng.standard_normal((k, n)) * np.logspace(0, 4, n)
+    Rinv, R = qr_on_gpu(SA)
+    Rl = np.linalg.qr(SA, mode="r")
+    # same Householder sign convention as LAPACK: R agrees entry-wise
+    np.testing.assert_allclose(R, Rl, rtol=1e-8, atol=1e-9 * np.abs(Rl).max())
+    Q = SA @ Rinv
+    np.testing.assert_allclose(Q.T @ Q, np.eye(n), atol=1e-8)
+
+
+def test_qr_rejects_wide_and_singular():
+    with pytest.raises(tb.TomosError):
+        qr_on_gpu(np.ones((3, 5)))
+    with pytest.raises(tb.TomosError):
+        qr_on_gpu(np.zeros((10, 4)))

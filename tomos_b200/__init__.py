@@ -1,0 +1,477 @@
+"""tomos_b200 -- the TOMOS LSQR hot path on NVIDIA B200 (sm_100a).
+
+Python mirror of the reference's public API (include/core/*.hpp) over the
+C ABI in include/tomos_b200.h.  Names, argument meaning and error behaviour
+follow the reference: Dense / Workspace objects, create_lsqr_workspace,
+add_precond, lsqr_solve, mv_apply, split_fp32_16 / combine_fp32_16,
+apply_count_sketch, generate_sketch_qr_precond.  Device memory comes from
+torch (CUDA tensors); every product runs in the sm_100a kernels of
+libtomos_b200.so.  There is no CPU path: a CPU Context raises.
+"""
+import ctypes
+import enum
+
+import torch
+
+from . import _capi as C
+from ._capi import TomosError, CS_BUCKET_SEED, CS_SIGN_SEED
+
+__all__ = [
+    "NumericType", "Layout", "TransposeType", "Device", "Tier", "StopRule", "Context", "Dense",
+    "Csr", "Workspace", "create_lsqr_workspace", "add_precond", "lsqr_solve", "mv_apply",
+    "split_fp32_16", "combine_fp32_16", "split_fp32_bf16", "combine_fp32_bf16",
+    "countsketch_hash", "apply_count_sketch", "generate_sketch_qr_precond", "backward_error",
+    "TomosError", "CS_BUCKET_SEED", "CS_SIGN_SEED", "NO_TRANSPOSE", "TRANSPOSE",
+]
+
+
+class NumericType(enum.IntEnum):
+    """include/core/precision.hpp:43-50; FP32_BF16 takes the new slot 5."""
+    FP64 = 0
+    FP32 = 1
+    FP16 = 2
+    FP32_16 = 3
+    BF16 = 4
+    FP32_BF16 = 5
+
+
+class Layout(enum.IntEnum):
+    ROW_MAJOR = 0
+    COL_MAJOR = 1
+
+
+class TransposeType(enum.IntEnum):
+    NO_TRANSPOSE = 0
+    TRANSPOSE = 1
+
+
+NO_TRANSPOSE = TransposeType.NO_TRANSPOSE
+TRANSPOSE = TransposeType.TRANSPOSE
+
+
+class Device(enum.IntEnum):
+    CPU = 0
+    OMP = 1
+    CUDA = 2
+
+
+class Tier(enum.IntEnum):
+    AUTO = 0
+    NATIVE = 1
+    HALF = 2
+    ACCURATE = 3
+
+
+class StopRule(enum.IntEnum):
+    RELRES = 0
+    BACKWARD = 1
+
+
+PACKED = (NumericType.FP32_16, NumericType.FP32_BF16)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Context:
+    """include/core/context: only Device::CUDA is registered here."""
+
+    def __init__(self, device=Device.CUDA):
+        if Device(device) != Device.CUDA:
+            raise ValueError("tomos_b200 runs on the GPU only: Context(Device.CUDA)")
+        if not torch.cuda.is_available():
+            raise RuntimeError("Context(Device.CUDA): no CUDA device available")
+        self.device = Device.CUDA
+
+    def get_device(self):
+        return self.device
+
+
+class Dense:
+    """A strided dense matrix on the device (include/core/matrix.hpp Dense).
+
+    FP32 / FP64 storage is one buffer of ld * outer elements; FP32_16 and
+    FP32_BF16 use the reference's planar layout (fp32_16_pack.hpp:861-874):
+    a uint16 buffer of 2 * ld * outer words, wh plane first, wr plane
+    second.  outer = cols for COL_MAJOR, rows for ROW_MAJOR.
+    """
+
+    def __init__(self, numeric, layout, size, ld, storage, rounded=False):
+        self.numeric = NumericType(numeric)
+        self.layout = Layout(layout)
+        self.size = (int(size[0]), int(size[1]))
+        self.ld = int(ld)
+        self.storage = storage
+        self.rounded = bool(rounded)
+
+    # -- construction ---------------------------------------------------
+    @staticmethod
+    def _outer_inner(layout, size):
+        return (size[1], size[0]) if Layout(layout) == Layout.COL_MAJOR else (size[0], size[1])
+
+    @classmethod
+    def create_strided(cls, ctx, layout, store_type, size, lead_dim=None, rounded=False):
+        outer, inner = cls._outer_inner(layout, size)
+        ld = inner if lead_dim is None else int(lead_dim)
+        if ld < inner:
+            raise ValueError("lead_dim smaller than the contiguous extent")
+        n = ld * outer
+        st = NumericType(store_type)
+        if st == NumericType.FP32:
+            buf = torch.zeros(max(n, 1), dtype=torch.float32, device="cuda")
+        elif st == NumericType.FP64:
+            buf = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda")
+        elif st in PACKED:
+            buf = torch.zeros(max(2 * n, 2), dtype=torch.int16, device="cuda")
+        else:
+            raise TomosError(C.TOMOS_ERR_UNSUPPORTED, f"no storage registered for {st.name}")
+        return cls(st, layout, size, ld, buf, rounded)
+
+    @classmethod
+    def from_tensor(cls, t, layout=Layout.COL_MAJOR, store_type=NumericType.FP32, lead_dim=None):
+        """Copies a logical (rows x cols) tensor into a new Dense of this layout."""
+        t = torch.as_tensor(t)
+        if t.dim() == 1:
+            t = t[:, None]
+        rows, cols = t.shape
+        st = NumericType(store_type)
+        if st not in (NumericType.FP32, NumericType.FP64):
+            raise ValueError("from_tensor builds FP32/FP64 storage; pack with split_fp32_16")
+        d = cls.create_strided(None, layout, st, (rows, cols), lead_dim)
+        d.view()[...] = t.to(device="cuda", dtype=d.storage.dtype)
+        return d
+
+    # -- views ----------------------------------------------------------
+    @property
+    def outer(self):
+        return self._outer_inner(self.layout, self.size)[0]
+
+    @property
+    def inner(self):
+        return self._outer_inner(self.layout, self.size)[1]
+
+    def _plane(self, k):
+        n = self.ld * self.outer
+        return self.storage[k * n:(k + 1) * n]
+
+    def view(self, plane=0):
+        """The logical (rows x cols) view of the values (or of one packed plane)."""
+        buf = self.storage if self.numeric not in PACKED else self._plane(plane)
+        rows, cols = self.size
+        if self.outer == 0 or self.inner == 0:
+            return buf[:0].reshape(rows, cols) if rows * cols == 0 else buf
+        m = buf[: self.ld * self.outer].view(self.outer, self.ld)[:, : self.inner]
+        return m.t() if self.layout == Layout.COL_MAJOR else m
+
+    def wh(self):
+        return self.view(0)
+
+    def wr(self):
+        return self.view(1)
+
+    def get_value_type(self):
+        return self.numeric
+
+    def get_size(self):
+        return self.size
+
+    def desc(self):
+        d = C.DenseDesc()
+        d.numeric = int(self.numeric)
+        d.layout = int(self.layout)
+        d.rows, d.cols = self.size
+        d.ld = self.ld
+        d.values = self.storage.data_ptr()
+        d.values_lo = (self.storage.data_ptr() + 2 * self.ld * self.outer) if self.numeric in PACKED else None
+        d.rounded = 1 if self.rounded else 0
+        return d
+
+
+class Csr:
+    """A CSR matrix on the device (include/core/matrix.hpp Sparse)."""
+
+    def __init__(self, numeric, size, row_ptrs, col_idxs, values, rounded=False):
+        self.numeric = NumericType(numeric)
+        self.size = (int(size[0]), int(size[1]))
+        self.row_ptrs = row_ptrs
+        self.col_idxs = col_idxs
+        self.values = values
+        self.rounded = bool(rounded)
+        self.nnz = int(col_idxs.numel())
+
+    def get_value_type(self):
+        return self.numeric
+
+    def desc(self):
+        d = C.CsrDesc()
+        d.numeric = int(self.numeric)
+        d.index_type = 0 if self.col_idxs.dtype == torch.int32 else 1
+        d.rows, d.cols = self.size
+        d.nnz = self.nnz
+        d.values = self.values.data_ptr()
+        d.values_lo = (self.values.data_ptr() + 2 * self.nnz) if self.numeric in PACKED else None
+        d.row_ptrs = self.row_ptrs.data_ptr()
+        d.col_idxs = self.col_idxs.data_ptr()
+        d.rounded = 1 if self.rounded else 0
+        return d
+
+
+# ------------------------------------------------------------------ packing
+
+def split_fp32_16(source, target, counts=None, stream=None):
+    """FP32 Dense -> FP32_16 Dense (blas.hpp split_fp32_16), bit-exact with
+    the reference encoder.  counts (int64 cuda tensor of 4, optional) is
+    accumulated with [normal, extended underflow, extended overflow,
+    saturated] element counts."""
+    if source.numeric != NumericType.FP32 or target.numeric != NumericType.FP32_16:
+        raise TomosError(C.TOMOS_ERR_INVALID, "split_fp32_16: FP32 source, FP32_16 target")
+    if source.size != target.size or source.layout != target.layout:
+        raise TomosError(C.TOMOS_ERR_INVALID, "split_fp32_16: shape/layout mismatch")
+    t = target.desc()
+    C.check(C.lib().tomos_pack_fp32_16(_ptr(source.storage), int(source.layout), source.size[0],
+                                       source.size[1], source.ld, t.values, t.values_lo, target.ld,
+                                       _ptr(counts), _stream(stream)), "split_fp32_16")
+
+
+def combine_fp32_16(source, target, stream=None):
+    if source.numeric != NumericType.FP32_16 or target.numeric != NumericType.FP32:
+        raise TomosError(C.TOMOS_ERR_INVALID, "combine_fp32_16: FP32_16 source, FP32 target")
+    s = source.desc()
+    C.check(C.lib().tomos_unpack_fp32_16(s.values, s.values_lo, int(source.layout), source.size[0],
+                                         source.size[1], source.ld, _ptr(target.storage), target.ld,
+                                         _stream(stream)), "combine_fp32_16")
+
+
+def split_fp32_bf16(source, target, rounded=False, stream=None):
+    if source.numeric != NumericType.FP32 or target.numeric != NumericType.FP32_BF16:
+        raise TomosError(C.TOMOS_ERR_INVALID, "split_fp32_bf16: FP32 source, FP32_BF16 target")
+    target.rounded = bool(rounded)
+    t = target.desc()
+    C.check(C.lib().tomos_pack_fp32_bf16(_ptr(source.storage), int(source.layout), source.size[0],
+                                         source.size[1], source.ld, t.values, t.values_lo,
+                                         target.ld, int(bool(rounded)), _stream(stream)),
+            "split_fp32_bf16")
+
+
+def combine_fp32_bf16(source, target, stream=None):
+    s = source.desc()
+    C.check(C.lib().tomos_unpack_fp32_bf16(s.values, s.values_lo, int(source.layout),
+                                           source.size[0], source.size[1], source.ld,
+                                           _ptr(target.storage), target.ld, s.rounded,
+                                           _stream(stream)), "combine_fp32_bf16")
+
+
+def pack(A_fp32, store_type, rounded=False, stream=None):
+    """Convenience: a packed copy of an FP32 Dense with the same layout."""
+    P = Dense.create_strided(None, A_fp32.layout, store_type, A_fp32.size, A_fp32.ld, rounded)
+    if NumericType(store_type) == NumericType.FP32_16:
+        split_fp32_16(A_fp32, P, stream=stream)
+    else:
+        split_fp32_bf16(A_fp32, P, rounded, stream=stream)
+    return P
+
+
+# ------------------------------------------------------------------ products
+
+def _tier_of(A, compute_type):
+    """The reference's compute_type rule (blas.cpp:33-53) as a tier."""
+    if compute_type is None:
+        return Tier.AUTO
+    ct = NumericType(compute_type)
+    if A.numeric in PACKED:
+        if ct in (NumericType.FP16, NumericType.BF16):
+            return Tier.HALF
+        if ct == NumericType.FP32:
+            return Tier.ACCURATE
+    elif ct == A.numeric:
+        return Tier.NATIVE
+    raise TomosError(C.TOMOS_ERR_UNSUPPORTED,
+                     f"no mv kernel registered for {A.numeric.name} with compute {ct.name}")
+
+
+def _vec(v):
+    if isinstance(v, Dense):
+        return v.storage
+    return v
+
+
+def mv_apply(dev, transpose, alpha, A, x, beta, y, compute_type=None, tier=None, stream=None):
+    """y = alpha * op(A) x + beta * y (src/core/blas/blas.cpp:23-86).
+
+    A: Dense or Csr; x, y: FP32 Dense column vectors or float32 CUDA tensors.
+    """
+    if Device(dev) != Device.CUDA:
+        raise ValueError("mv_apply: Device.CUDA only")
+    t = _tier_of(A, compute_type) if tier is None else Tier(tier)
+    xs, ys = _vec(x), _vec(y)
+    if isinstance(A, Csr):
+        d = A.desc()
+        nb = C.lib().tomos_csr_gemv_scratch_bytes(ctypes.byref(d), int(transpose))
+        scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
+        C.check(C.lib().tomos_csr_gemv(int(transpose), float(alpha), ctypes.byref(d), int(t),
+                                       _ptr(xs), float(beta), _ptr(ys), _ptr(scratch), nb,
+                                       _stream(stream)), "mv_apply")
+        return 0
+    d = A.desc()
+    nb = C.lib().tomos_gemv_scratch_bytes(ctypes.byref(d), int(transpose))
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
+    C.check(C.lib().tomos_gemv(int(transpose), float(alpha), ctypes.byref(d), int(t), _ptr(xs),
+                               float(beta), _ptr(ys), _ptr(scratch), nb, _stream(stream)),
+            "mv_apply")
+    return 0
+
+
+# ------------------------------------------------------------------ sketch
+
+def countsketch_hash(m, s, bucket_seed=CS_BUCKET_SEED, sign_seed=CS_SIGN_SEED, stream=None):
+    """Per-row bucket and sign of the hash CountSketch (device tensors)."""
+    bucket = torch.empty(max(m, 1), dtype=torch.int32, device="cuda")
+    sign = torch.empty(max(m, 1), dtype=torch.int8, device="cuda")
+    C.check(C.lib().tomos_countsketch_hash(m, s, bucket_seed, sign_seed, _ptr(bucket), _ptr(sign),
+                                           _stream(stream)), "countsketch_hash")
+    return bucket[:m], sign[:m]
+
+
+def apply_count_sketch(A, s, tier=Tier.AUTO, bucket_seed=CS_BUCKET_SEED, sign_seed=CS_SIGN_SEED,
+                       stream=None):
+    """SA = S A (s x n, column-major FP64 Dense) and ||A||_F^2 of the values read."""
+    n = A.size[1]
+    SA = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (s, n))
+    fro2 = torch.zeros(1, dtype=torch.float64, device="cuda")
+    m = A.size[0]
+    nb = C.lib().tomos_countsketch_scratch_bytes(m, s)
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
+    d = A.desc()
+    fn = C.lib().tomos_countsketch_apply_csr if isinstance(A, Csr) else C.lib().tomos_countsketch_apply
+    C.check(fn(ctypes.byref(d), int(tier), s, bucket_seed, sign_seed, _ptr(SA.storage), s,
+               _ptr(fro2), _ptr(scratch), nb, _stream(stream)), "apply_count_sketch")
+    return SA, fro2
+
+
+def generate_sketch_qr_precond(sketched, R_out=None, stream=None):
+    """FP64 Householder QR of the k x n column-major sketched matrix; on
+    return its leading n x n block holds R^{-1} (sketch_qr.hpp:19).
+    Returns (Rinv Dense view copy, R tensor or None)."""
+    if sketched.numeric != NumericType.FP64 or sketched.layout != Layout.COL_MAJOR:
+        raise TomosError(C.TOMOS_ERR_INVALID, "generate_sketch_qr_precond: FP64 column-major input")
+    k, n = sketched.size
+    if k < n:
+        raise TomosError(C.TOMOS_ERR_INVALID,
+                         "generate_sketch_qr_precond: sketched_mtx must have at least as many "
+                         "rows as columns (k >= n).")
+    nb = C.lib().tomos_sketch_qr_scratch_bytes(k, n)
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
+    C.check(C.lib().tomos_sketch_qr_precond_f64(k, n, _ptr(sketched.storage), sketched.ld,
+                                                _ptr(R_out), _ptr(scratch), nb, _stream(stream)),
+            "generate_sketch_qr_precond")
+    Rinv = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (n, n))
+    Rinv.view()[...] = sketched.view()[:n, :n]
+    return Rinv
+
+
+# ------------------------------------------------------------------ LSQR
+
+class Workspace:
+    """include/core/workspace.hpp Workspace over a tomos_workspace*."""
+
+    def __init__(self, m, n, value_type=NumericType.FP32, precond_type=None):
+        self.size = (int(m), int(n))
+        self.value_type_ = NumericType(value_type)
+        self.precond_type_ = NumericType(value_type if precond_type is None else precond_type)
+        h = ctypes.c_void_p()
+        C.check(C.lib().tomos_workspace_create(m, n, int(self.value_type_),
+                                               int(self.precond_type_), ctypes.byref(h)),
+                "create_lsqr_workspace")
+        self._h = h
+        self.precond_ = None
+        self.use_implicit_duplicate_ = False
+        self.mv_compute_type_ = NumericType.FP16
+        self.mv_compute_type_set_ = False
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            C.lib().tomos_workspace_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def create_lsqr_workspace(ctx, size, value_type, precond_type=None):
+    return Workspace(size[0], size[1], value_type, precond_type)
+
+
+def add_precond(precond, workspace):
+    """Attaches a non-owning R^{-1} (include/core/workspace.hpp:112-120)."""
+    if precond.get_value_type() != workspace.precond_type_:
+        raise TomosError(C.TOMOS_ERR_INVALID,
+                         "add_precond: precond's NumericType doesn't match the precond_type the "
+                         "workspace was created with.")
+    d = precond.desc()
+    C.check(C.lib().tomos_workspace_add_precond(workspace.handle, ctypes.byref(d)), "add_precond")
+    workspace.precond_ = precond
+
+
+def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=None,
+               residual_history=None, restarts=1, stop_rule=StopRule.RELRES, inner_rtol=0.0,
+               anorm_fro=0.0, warm_start=False, tier=None, stream=None):
+    """include/core/solver.hpp:68-78.  A: Dense or Csr on the device; b, x:
+    FP32 Dense column vectors or float32 CUDA tensors.  iterations and
+    residual_history, when lists, receive the reference's out-parameters.
+    Returns the solver report as a dict."""
+    opts = C.LsqrOpts()
+    opts.tol = float(tol)
+    opts.max_iters = int(max_iters)
+    opts.restarts = int(restarts)
+    opts.max_relres = float(max_relres)
+    opts.stop_rule = int(stop_rule)
+    if tier is not None:
+        opts.iter_tier = int(tier)
+    elif workspace.mv_compute_type_set_:
+        opts.iter_tier = int(_tier_of(A, workspace.mv_compute_type_))
+    else:
+        opts.iter_tier = int(Tier.AUTO)
+    opts.implicit_duplicate = 1 if workspace.use_implicit_duplicate_ else 0
+    opts.warm_start = 1 if warm_start else 0
+    opts.inner_rtol = float(inner_rtol)
+    opts.anorm_fro = float(anorm_fro)
+    cap = max(1, int(max_iters) * int(restarts) + int(restarts))
+    hist = (ctypes.c_double * cap)()
+    opts.history = hist
+    opts.history_cap = cap
+    rep = C.LsqrReport()
+    d = A.desc()
+    fn = C.lib().tomos_lsqr_solve_csr if isinstance(A, Csr) else C.lib().tomos_lsqr_solve_dense
+    C.check(fn(ctypes.byref(d), _ptr(_vec(b)), _ptr(_vec(x)), workspace.handle, ctypes.byref(opts),
+               ctypes.byref(rep), _stream(stream)), "lsqr_solve")
+    out = rep.as_dict()
+    out["history"] = [hist[i] for i in range(rep.history_len)]
+    if isinstance(iterations, list):
+        iterations.append(rep.iterations)
+    if isinstance(residual_history, list):
+        residual_history.extend(out["history"])
+    return out
+
+
+def backward_error(A, b, x, workspace, stream=None):
+    """Normwise backward error of x (FP64, accurate tier)."""
+    rep = C.LsqrReport()
+    d = A.desc()
+    C.check(C.lib().tomos_backward_error_dense(ctypes.byref(d), _ptr(_vec(b)), _ptr(_vec(x)),
+                                               workspace.handle, ctypes.byref(rep),
+                                               _stream(stream)), "backward_error")
+    return rep.as_dict()

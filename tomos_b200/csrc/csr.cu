@@ -1,0 +1,514 @@
+// csr.cu -- CSR products (tomos_csr_gemv), the CSR LSQR pass
+// (tomos_lsqr_solve_csr) and the CSR CountSketch.
+//
+// The reference's CSR path (cuda::mv_csr, mv_cuda_kernels.cu:1964-2058)
+// is one thread per row for A x and an atomicAdd scatter for A^T x; it has
+// no packed (FP32_16) values (lsqr_registries.cpp:274-285).  Here values
+// may be FP32, FP32_16 or FP32_BF16 (read at a tier like the dense path),
+// indices int32, and both products are deterministic:
+//   * a warp owns a row; lanes stride its nonzeros, reading p through L1;
+//   * the transposed product accumulates into a warp-private FP32 vector
+//     in shared memory.  A CSR row has distinct column indices, so the
+//     lanes of one row never touch the same word and no atomics are
+//     needed; the CTA sums its warps' vectors in a fixed order and writes
+//     one partial row, reduced across CTAs in a fixed order later.
+// The LSQR pass fuses both: ut_i = cp (A p)_i + cu u_i, then
+// q += ut_i A[i, :] while row i is in registers -- one read of the index
+// and value arrays per iteration.
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "gemv.cuh"
+#include "lsqr.cuh"
+#include "sketch.cuh"
+
+namespace tomos_b200 {
+
+constexpr int kCsrMaxWarps = 8;
+constexpr size_t kCsrSmemBudget = 200 * 1024;
+
+struct CsrPassParams {
+    const void* hi;
+    const void* lo;
+    const int32_t* row_ptrs;
+    const int32_t* col_idxs;
+    int64_t m, n;
+    const float* p;
+    const float* u_in;
+    float* u_out;
+    const double* coef;     // device [cp, cu], or NULL: use cp_h / cu_h
+    double cp_h, cu_h;
+    float* qpart;           // gridDim.x x qstride (NULL: no transposed product)
+    int64_t qstride;
+    double* sspart;         // gridDim.x (NULL: skip)
+    const int* skip;
+    int write_u;            // 0: A p only feeds the transposed product
+};
+
+// One kernel, three uses: the fused LSQR pass (write_u, qpart, sspart),
+// the plain product (write_u only: y = cp A p + cu y) and the transposed
+// product (qpart only, with u_in as the input vector and cp = 0, cu = 1).
+template <Elem E, bool ACC64>
+__global__ void __launch_bounds__(256) csr_pass_kernel(CsrPassParams P) {
+    if (P.skip && *P.skip) return;
+    using Dot = typename std::conditional<ACC64, double, float>::type;
+    extern __shared__ __align__(16) float qacc[];  // nw x n_pad
+    __shared__ double ssw[kCsrMaxWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t npad = P.qstride;
+    double cp = P.cp_h, cu = P.cu_h;
+    if (P.coef) {
+        cp = P.coef[0];
+        cu = P.coef[1];
+    }
+    float* acc = qacc + (size_t)w * npad;
+    if (P.qpart)
+        for (int64_t j = lane; j < npad; j += 32) acc[j] = 0.0f;
+    __syncwarp();
+    const int64_t per = (P.m + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = (int64_t)blockIdx.x * per;
+    int64_t r1 = r0 + per;
+    if (r1 > P.m) r1 = P.m;
+    double ss = 0.0;
+    for (int64_t i = r0 + w; i < r1; i += nw) {
+        const int32_t k0 = P.row_ptrs[i], k1 = P.row_ptrs[i + 1];
+        double ut;
+        if (cp != 0.0) {
+            Dot d = 0;
+            for (int32_t k = k0 + lane; k < k1; k += 32)
+                d += (Dot)load_elem<E>(P.hi, P.lo, k) * (Dot)__ldg(P.p + P.col_idxs[k]);
+            d = warp_sum(d);
+            ut = cp * (double)d + cu * (double)__ldg(P.u_in + i);
+        } else {
+            ut = cu * (double)__ldg(P.u_in + i);
+        }
+        const float uf = (float)ut;
+        if (lane == 0) {
+            if (P.write_u) P.u_out[i] = uf;
+            ss += (double)uf * (double)uf;
+        }
+        if (P.qpart) {
+            for (int32_t k = k0 + lane; k < k1; k += 32) {
+                const int32_t c = P.col_idxs[k];
+                acc[c] = fmaf(load_elem<E>(P.hi, P.lo, k), uf, acc[c]);
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) ssw[w] = ss;
+    __syncthreads();
+    if (P.qpart) {
+        float* out = P.qpart + (size_t)blockIdx.x * npad;
+        for (int64_t j = threadIdx.x; j < P.n; j += blockDim.x) {
+            float s = 0.0f;
+            for (int k = 0; k < nw; ++k) s += qacc[(size_t)k * npad + j];
+            out[j] = s;
+        }
+    }
+    if (P.sspart && threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < nw; ++k) s += ssw[k];
+        P.sspart[blockIdx.x] = s;
+    }
+}
+
+// y[j] = alpha * sum_c part[c][j] + beta * y[j] (fixed order).
+__global__ void csr_trans_reduce_kernel(const float* __restrict__ part, int g, int64_t stride,
+                                        int64_t n, double alpha, double beta, float* __restrict__ y) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double s = 0.0;
+    for (int c = 0; c < g; ++c) s += (double)part[(size_t)c * stride + j];
+    double r = alpha * s;
+    if (beta != 0.0) r += beta * (double)y[j];
+    y[j] = (float)r;
+}
+
+static int csr_warps_for(int64_t n) {
+    const int64_t npad = ((n + 31) / 32) * 32;
+    int64_t w = (int64_t)(kCsrSmemBudget / (sizeof(float) * (npad > 0 ? npad : 32)));
+    if (w > kCsrMaxWarps) w = kCsrMaxWarps;
+    return (int)w;
+}
+
+template <Elem E, bool ACC64>
+static tomos_status launch_csr_t(const CsrPassParams& P, int grid, int warps, cudaStream_t st) {
+    const size_t smem = P.qpart ? (size_t)warps * P.qstride * sizeof(float) : 0;
+    if (smem > 48 * 1024)
+        TOMOS_CUDA_TRY(cudaFuncSetAttribute(csr_pass_kernel<E, ACC64>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    csr_pass_kernel<E, ACC64><<<grid, warps * 32, smem, st>>>(P);
+    TOMOS_LAUNCH_CHECK("csr_pass_kernel");
+    return TOMOS_OK;
+}
+
+static tomos_status launch_csr(Elem e, bool acc64, const CsrPassParams& P, int grid, int warps,
+                               cudaStream_t st) {
+    switch (e) {
+        case Elem::F32: return acc64 ? launch_csr_t<Elem::F32, true>(P, grid, warps, st)
+                                     : launch_csr_t<Elem::F32, false>(P, grid, warps, st);
+        case Elem::H16: return acc64 ? launch_csr_t<Elem::H16, true>(P, grid, warps, st)
+                                     : launch_csr_t<Elem::H16, false>(P, grid, warps, st);
+        case Elem::B16: return acc64 ? launch_csr_t<Elem::B16, true>(P, grid, warps, st)
+                                     : launch_csr_t<Elem::B16, false>(P, grid, warps, st);
+        case Elem::A16: return launch_csr_t<Elem::A16, true>(P, grid, warps, st);
+        case Elem::AB16: return launch_csr_t<Elem::AB16, true>(P, grid, warps, st);
+        case Elem::AB16R: return launch_csr_t<Elem::AB16R, true>(P, grid, warps, st);
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "csr: element type");
+    }
+}
+
+static const void* csr_lo(const tomos_csr* A) {
+    if (A->values_lo) return A->values_lo;
+    return static_cast<const uint16_t*>(A->values) + A->nnz;
+}
+
+static bool csr_ok(const tomos_csr* A, std::string* why) {
+    if (!A) {
+        *why = "null matrix";
+        return false;
+    }
+    if (A->rows < 0 || A->cols < 0 || A->nnz < 0) {
+        *why = "negative size";
+        return false;
+    }
+    if (A->index_type != 0) {
+        *why = "only int32 indices are registered";
+        return false;
+    }
+    if (A->rows > 0x7fffffffLL || A->nnz > 0x7fffffffLL) {
+        *why = "size exceeds int32 indexing";
+        return false;
+    }
+    if (csr_warps_for(A->cols) < 1) {
+        *why = "n too large for the shared-memory accumulators";
+        return false;
+    }
+    return true;
+}
+
+static int csr_grid(int64_t m) {
+    int64_t g = (int64_t)sm_count() * 2;
+    int64_t gr = (m + 63) / 64;
+    if (g > gr) g = gr;
+    return (int)(g < 1 ? 1 : g);
+}
+
+static int64_t csr_qstride(int64_t n) { return ((n + 31) / 32) * 32 < 32 ? 32 : ((n + 31) / 32) * 32; }
+
+// Fused LSQR pass over CSR storage.
+struct CsrPass : PassOps {
+    tomos_workspace* ws;
+    const tomos_csr* A;
+    Elem iter_e, init_e;
+    CsrPass(tomos_workspace* w, const tomos_csr* a, Elem ie, Elem ze) : ws(w), A(a), iter_e(ie), init_e(ze) {}
+    PassPlan plan(bool init) override {
+        PassPlan pl;
+        pl.fused = true;
+        pl.e = init ? init_e : iter_e;
+        pl.acc64 = init || elem_is_exact(pl.e);
+        pl.grid = csr_grid(A->rows);
+        if (pl.grid > ws->gmax) pl.grid = ws->gmax;
+        pl.gq = pl.grid;
+        pl.gs = pl.grid;
+        pl.qstride = ws->qstride;
+        pl.nch = csr_warps_for(A->cols);
+        return pl;
+    }
+    tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
+                         const int* skip, cudaStream_t st) override {
+        CsrPassParams P;
+        P.hi = A->values;
+        P.lo = elem_is_exact(pl.e) ? csr_lo(A) : nullptr;
+        P.row_ptrs = static_cast<const int32_t*>(A->row_ptrs);
+        P.col_idxs = static_cast<const int32_t*>(A->col_idxs);
+        P.m = A->rows;
+        P.n = A->cols;
+        P.p = p;
+        P.u_in = u_in;
+        P.u_out = ws->u;
+        P.coef = coef;
+        P.cp_h = 1.0;
+        P.cu_h = 0.0;
+        P.qpart = ws->qpart;
+        P.qstride = pl.qstride;
+        P.sspart = ws->sspart;
+        P.skip = skip;
+        P.write_u = 1;
+        return launch_csr(pl.e, pl.acc64, P, pl.grid, pl.nch, st);
+    }
+    tomos_status fro2(double* out, cudaStream_t st) override;
+    uint64_t key() override {
+        return reinterpret_cast<uint64_t>(A->values) ^ (reinterpret_cast<uint64_t>(A->col_idxs) << 1);
+    }
+    int64_t rows() override { return A->rows; }
+    int64_t cols() override { return A->cols; }
+};
+
+template <Elem E>
+__global__ void csr_fro2_kernel(const void* hi, const void* lo, int64_t nnz, double* part) {
+    __shared__ double sm[8];
+    double s = 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        double v = load_elem<E>(hi, lo, k);
+        s += v * v;
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sm[k];
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void csr_sum_kernel(const double* part, int np, double* out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < np; ++k) s += part[k];
+        *out = s;
+    }
+}
+
+tomos_status CsrPass::fro2(double* out, cudaStream_t st) {
+    const int g = ws->gs_max;
+    const void* lo = elem_is_exact(init_e) ? csr_lo(A) : nullptr;
+    switch (init_e) {
+        case Elem::F32: csr_fro2_kernel<Elem::F32><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
+        case Elem::H16: csr_fro2_kernel<Elem::H16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
+        case Elem::A16: csr_fro2_kernel<Elem::A16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
+        case Elem::B16: csr_fro2_kernel<Elem::B16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
+        case Elem::AB16: csr_fro2_kernel<Elem::AB16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
+        case Elem::AB16R: csr_fro2_kernel<Elem::AB16R><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "csr fro2: element type");
+    }
+    TOMOS_LAUNCH_CHECK("csr_fro2_kernel");
+    csr_sum_kernel<<<1, 32, 0, st>>>(ws->bpart, g, out);
+    TOMOS_LAUNCH_CHECK("csr_sum_kernel");
+    return TOMOS_OK;
+}
+
+// CSR CountSketch owner sums: a warp per bucket accumulates its rows into
+// a warp-private dense row (shared memory, FP64; distinct columns within a
+// row need no atomics), then writes SA row b.
+template <Elem E>
+__global__ void cs_csr_kernel(const void* hi, const void* lo, const int32_t* row_ptrs,
+                              const int32_t* col_idxs, int64_t n, int64_t s,
+                              const int32_t* offsets, const int32_t* perm, const int8_t* sign,
+                              double* SA, int64_t ld_sa, double* fro_part) {
+    extern __shared__ __align__(16) double racc[];
+    __shared__ double smf[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t b = (int64_t)blockIdx.x * nw + w;
+    double* acc = racc + (size_t)w * n;
+    double f2 = 0.0;
+    if (b < s) {
+        for (int64_t j = lane; j < n; j += 32) acc[j] = 0.0;
+        __syncwarp();
+        const int32_t o0 = offsets[b], o1 = offsets[b + 1];
+        for (int32_t q = o0; q < o1; ++q) {
+            const int32_t r = perm[q];
+            const double sg = (double)sign[r];
+            for (int32_t k = row_ptrs[r] + lane; k < row_ptrs[r + 1]; k += 32) {
+                const double a = load_elem<E>(hi, lo, k);
+                acc[col_idxs[k]] += sg * a;
+                f2 += a * a;
+            }
+            __syncwarp();
+        }
+        for (int64_t j = lane; j < n; j += 32) SA[(size_t)j * ld_sa + b] = acc[j];
+    }
+    f2 = warp_sum(f2);
+    if (lane == 0) smf[w] = f2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < nw; ++k) t += smf[k];
+        fro_part[blockIdx.x] = t;
+    }
+}
+
+__global__ void cs_csr_fro_reduce(const double* part, int64_t np, double* out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int64_t k = 0; k < np; ++k) s += part[k];
+        *out = s;
+    }
+}
+
+}  // namespace tomos_b200
+
+using namespace tomos_b200;
+
+extern "C" {
+
+size_t tomos_csr_gemv_scratch_bytes(const tomos_csr* A, int32_t trans) {
+    std::string why;
+    if (!csr_ok(A, &why) || trans != TOMOS_TRANSPOSE) return 0;
+    return (size_t)csr_grid(A->rows) * csr_qstride(A->cols) * sizeof(float);
+}
+
+tomos_status tomos_csr_gemv(int32_t trans, double alpha, const tomos_csr* A, int32_t tier,
+                            const float* x, double beta, float* y, void* scratch,
+                            size_t scratch_bytes, void* stream) {
+    std::string why;
+    if (!csr_ok(A, &why)) return fail(TOMOS_ERR_INVALID, "tomos_csr_gemv: " + why);
+    if (trans != TOMOS_NO_TRANSPOSE && trans != TOMOS_TRANSPOSE)
+        return fail(TOMOS_ERR_INVALID, "tomos_csr_gemv: bad transpose flag");
+    Elem e;
+    if (!resolve_elem_csr(A, tier, &e, &why)) return fail(TOMOS_ERR_UNSUPPORTED, "tomos_csr_gemv: " + why);
+    cudaStream_t st = as_stream(stream);
+    const int64_t ylen = trans == TOMOS_NO_TRANSPOSE ? A->rows : A->cols;
+    if (ylen == 0) return TOMOS_OK;
+    if (!y || (!x && (trans == TOMOS_NO_TRANSPOSE ? A->cols : A->rows) > 0))
+        return fail(TOMOS_ERR_INVALID, "tomos_csr_gemv: null vector");
+    CsrPassParams P;
+    P.hi = A->values;
+    P.lo = elem_is_exact(e) ? csr_lo(A) : nullptr;
+    P.row_ptrs = static_cast<const int32_t*>(A->row_ptrs);
+    P.col_idxs = static_cast<const int32_t*>(A->col_idxs);
+    P.m = A->rows;
+    P.n = A->cols;
+    P.coef = nullptr;
+    P.sspart = nullptr;
+    P.skip = nullptr;
+    P.qstride = csr_qstride(A->cols);
+    const int grid = csr_grid(A->rows);
+    if (trans == TOMOS_NO_TRANSPOSE) {
+        if (A->rows > 0 && !A->row_ptrs) return fail(TOMOS_ERR_INVALID, "tomos_csr_gemv: null row_ptrs");
+        P.p = x;
+        P.u_in = y;
+        P.u_out = y;
+        P.cp_h = alpha;
+        P.cu_h = beta;
+        P.qpart = nullptr;
+        P.write_u = 1;
+        if (beta == 0.0) {
+            // beta == 0 must not read y: run with cu = 0 on a zeroed y.
+            TOMOS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(float) * A->rows, st));
+        }
+        if (A->rows == 0) return TOMOS_OK;
+        return launch_csr(e, elem_is_exact(e), P, grid, 8, st);
+    }
+    const size_t need = (size_t)grid * P.qstride * sizeof(float);
+    if (!scratch || scratch_bytes < need)
+        return fail(TOMOS_ERR_INVALID, "tomos_csr_gemv: scratch too small (need " + std::to_string(need) + " bytes)");
+    if (A->rows == 0) {
+        csr_trans_reduce_kernel<<<(unsigned)((A->cols + 255) / 256), 256, 0, st>>>(
+            static_cast<float*>(scratch), 0, P.qstride, A->cols, alpha, beta, y);
+        TOMOS_LAUNCH_CHECK("csr_trans_reduce_kernel");
+        return TOMOS_OK;
+    }
+    P.p = nullptr;
+    P.u_in = x;
+    P.u_out = nullptr;
+    P.cp_h = 0.0;
+    P.cu_h = 1.0;
+    P.qpart = static_cast<float*>(scratch);
+    P.write_u = 0;
+    tomos_status s = launch_csr(e, elem_is_exact(e), P, grid, csr_warps_for(A->cols), st);
+    if (s) return s;
+    csr_trans_reduce_kernel<<<(unsigned)((A->cols + 255) / 256), 256, 0, st>>>(
+        P.qpart, grid, P.qstride, A->cols, alpha, beta, y);
+    TOMOS_LAUNCH_CHECK("csr_trans_reduce_kernel");
+    return TOMOS_OK;
+}
+
+tomos_status tomos_lsqr_solve_csr(const tomos_csr* A, const float* b, float* x,
+                                  tomos_workspace* ws, const tomos_lsqr_opts* opts,
+                                  tomos_lsqr_report* report, void* stream) {
+    std::string why;
+    if (!csr_ok(A, &why)) return fail(TOMOS_ERR_INVALID, "lsqr_solve: " + why);
+    if (!opts) return fail(TOMOS_ERR_INVALID, "lsqr_solve: null options");
+    tomos_status s = workspace_check(ws, A->rows, A->cols);
+    if (s) return s;
+    if (!b || !x) return fail(TOMOS_ERR_INVALID, "lsqr_solve: null pointer");
+    if (opts->implicit_duplicate && A->numeric != TOMOS_FP32_16 && A->numeric != TOMOS_FP32_BF16)
+        return fail(TOMOS_ERR_INVALID, "lsqr_solve: use_implicit_duplicate_ requires packed A");
+    Elem ie, ze;
+    if (!resolve_elem_csr(A, opts->iter_tier, &ie, &why))
+        return fail(TOMOS_ERR_UNSUPPORTED, "lsqr_solve: " + why);
+    const bool packed = A->numeric == TOMOS_FP32_16 || A->numeric == TOMOS_FP32_BF16;
+    int32_t it = opts->iter_tier == TOMOS_TIER_AUTO ? (packed ? TOMOS_TIER_HALF : TOMOS_TIER_NATIVE)
+                                                    : opts->iter_tier;
+    int32_t zt = (packed && (opts->implicit_duplicate || opts->stop_rule == TOMOS_STOP_BACKWARD))
+                     ? TOMOS_TIER_ACCURATE : it;
+    if (!resolve_elem_csr(A, zt, &ze, &why)) return fail(TOMOS_ERR_UNSUPPORTED, "lsqr_solve: " + why);
+    if (A->rows == 0 || A->cols == 0) {
+        if (A->cols > 0 && !opts->warm_start) cudaMemsetAsync(x, 0, sizeof(float) * A->cols, as_stream(stream));
+        if (report) {
+            std::memset(report, 0, sizeof(*report));
+            report->converged = 1;
+        }
+        return TOMOS_OK;
+    }
+    CsrPass ops(ws, A, ie, ze);
+    return solve_driver(ws, ops, b, x, opts, report, stream);
+}
+
+tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64_t s,
+                                         uint64_t bucket_seed, uint64_t sign_seed, double* SA,
+                                         int64_t ld_sa, double* fro2, void* scratch,
+                                         size_t scratch_bytes, void* stream) {
+    std::string why;
+    if (!csr_ok(A, &why)) return fail(TOMOS_ERR_INVALID, "countsketch_apply_csr: " + why);
+    if (s <= 0 || ld_sa < s) return fail(TOMOS_ERR_INVALID, "countsketch_apply_csr: bad s / ld_sa");
+    Elem e;
+    if (!resolve_elem_csr(A, tier, &e, &why)) return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply_csr: " + why);
+    const int64_t m = A->rows, n = A->cols;
+    cudaStream_t st = as_stream(stream);
+    if (n == 0) return TOMOS_OK;
+    if (!SA) return fail(TOMOS_ERR_INVALID, "countsketch_apply_csr: null SA");
+    // A warp needs n doubles of shared memory.
+    const int64_t wpb = (int64_t)(kCsrSmemBudget / (sizeof(double) * (size_t)n));
+    if (wpb < 1) return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply_csr: n too large");
+    const int nw = (int)(wpb > 8 ? 8 : wpb);
+    if (m == 0) {
+        for (int64_t j = 0; j < n; ++j)
+            TOMOS_CUDA_TRY(cudaMemsetAsync(SA + j * ld_sa, 0, sizeof(double) * s, st));
+        if (fro2) TOMOS_CUDA_TRY(cudaMemsetAsync(fro2, 0, sizeof(double), st));
+        return TOMOS_OK;
+    }
+    CsScratch need = cs_layout(nullptr, m, s, cs_fro_parts(m, s));
+    if (!scratch || scratch_bytes < need.bytes)
+        return fail(TOMOS_ERR_INVALID, "countsketch_apply_csr: scratch too small (need " +
+                                           std::to_string(need.bytes) + " bytes)");
+    CsScratch c = cs_layout(scratch, m, s, cs_fro_parts(m, s));
+    tomos_status rc = cs_bucketize(m, s, bucket_seed, sign_seed, c, st);
+    if (rc) return rc;
+    const void* lo = elem_is_exact(e) ? csr_lo(A) : nullptr;
+    const unsigned grid = (unsigned)((s + nw - 1) / nw);
+    const size_t smem = (size_t)nw * n * sizeof(double);
+    const int32_t* rp = static_cast<const int32_t*>(A->row_ptrs);
+    const int32_t* ci = static_cast<const int32_t*>(A->col_idxs);
+#define TOMOS_CS_CSR(EE)                                                                        \
+    do {                                                                                        \
+        if (smem > 48 * 1024)                                                                   \
+            TOMOS_CUDA_TRY(cudaFuncSetAttribute(cs_csr_kernel<EE>,                              \
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                                (int)smem));                                    \
+        cs_csr_kernel<EE><<<grid, nw * 32, smem, st>>>(A->values, lo, rp, ci, n, s, c.offsets,  \
+                                                       c.perm, c.sign, SA, ld_sa, c.fro_part); \
+    } while (0)
+    switch (e) {
+        case Elem::F32: TOMOS_CS_CSR(Elem::F32); break;
+        case Elem::H16: TOMOS_CS_CSR(Elem::H16); break;
+        case Elem::A16: TOMOS_CS_CSR(Elem::A16); break;
+        case Elem::B16: TOMOS_CS_CSR(Elem::B16); break;
+        case Elem::AB16: TOMOS_CS_CSR(Elem::AB16); break;
+        case Elem::AB16R: TOMOS_CS_CSR(Elem::AB16R); break;
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply_csr: element type");
+    }
+#undef TOMOS_CS_CSR
+    TOMOS_LAUNCH_CHECK("cs_csr_kernel");
+    if (fro2) {
+        cs_csr_fro_reduce<<<1, 32, 0, st>>>(c.fro_part, grid, fro2);
+        TOMOS_LAUNCH_CHECK("cs_csr_fro_reduce");
+    }
+    return TOMOS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1116 @@
+// lsqr.cu -- preconditioned LSQR on the device: workspace, the n-side
+// kernels of one Golub-Kahan step, and the host driver behind
+// tomos_lsqr_solve_dense / _csr and tomos_backward_error_dense.
+//
+// Algorithm: Paige-Saunders LSQR with a right preconditioner M = R^{-1}
+// (the reference's fused_lsqr_impl, src/core/solver/lsqr.cpp:432-747),
+// restarted from the current x, with two changes of formulation that
+// leave the iterates mathematically unchanged:
+//   * u is kept unnormalised: the A pass produces ut = A p - (alpha/beta) ut
+//     (p = M v), so A^T u = A^T ut / beta comes from the same pass over A
+//     (fused.cuh) instead of a second one;
+//   * w is kept in x-space (wt = M w), so x += (phi/rho) wt and
+//     wt = p - (theta/rho) wt need no third product with M per iteration.
+// Every scalar of the recurrence (alpha, beta, rho, rho_bar, phi, phi_bar,
+// c, s, theta) and every norm is FP64 and stays on the device; one
+// iteration is five kernels with no host round trip, captured once into a
+// CUDA graph and replayed.  The host only looks at the state at restart
+// boundaries and between batches of iterations.
+//
+// Per iteration:
+//   A pass   ut = A p + cu * ut, partials of A^T ut and ||ut||^2
+//   N1       beta = ||ut||, t = A^T ut / beta (fixed-order partial reduce)
+//   N2       z = M^T t, vh = z - beta v               (preconditioned only)
+//   N3       alpha = ||vh||, v = vh / alpha, p = M v, Givens, x and wt
+//   N4       state update, history, stopping rule, next cu = -alpha/beta
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "fused.cuh"
+#include "gemv.cuh"
+#include "lsqr.cuh"
+
+namespace tomos_b200 {
+
+// ------------------------------------------------------------ reductions
+
+__device__ __forceinline__ double block_sum(double v, double* sm) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < nw ? sm[lane] : 0.0;
+        r = warp_sum(r);
+        if (lane == 0) sm[0] = r;
+    }
+    __syncthreads();
+    r = sm[0];
+    __syncthreads();
+    return r;
+}
+
+// Block-wide fixed-order sum of part[0..np).
+__device__ __forceinline__ double block_sum_array(const double* part, int64_t np, double* sm) {
+    double s = 0.0;
+    for (int64_t k = threadIdx.x; k < np; k += blockDim.x) s += part[k];
+    return block_sum(s, sm);
+}
+
+__global__ void sumsq_partial_kernel(const float* __restrict__ x, int64_t n, const int* skip,
+                                     double* __restrict__ part) {
+    if (skip && *skip) return;
+    __shared__ double sm[32];
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t i0 = (int64_t)blockIdx.x * per;
+    int64_t i1 = i0 + per;
+    if (i1 > n) i1 = n;
+    double s = 0.0;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        double v = x[i];
+        s += v * v;
+    }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void sum_to_scalar_kernel(const double* __restrict__ part, int64_t np,
+                                     double* __restrict__ out) {
+    __shared__ double sm[32];
+    double s = block_sum_array(part, np, sm);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// sum of squares of every element of a strided matrix (its ||.||_F^2),
+// read at element tag E; per-block partials.
+template <Elem E>
+__global__ void fro2_partial_kernel(const void* hi, const void* lo, int64_t outer, int64_t inner,
+                                    int64_t ld, double* part) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int64_t o = blockIdx.x; o < outer; o += gridDim.x)
+        for (int64_t i = threadIdx.x; i < inner; i += blockDim.x) {
+            double v = load_elem<E>(hi, lo, (size_t)o * ld + i);
+            s += v * v;
+        }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void fill_f32_kernel(float* p, int64_t n, float v) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// FP64 column-major and row-major copies of a dense n x n preconditioner.
+__global__ void precond_copy_kernel(const void* R, int numeric, int layout, int64_t ld, int64_t n,
+                                    double* Rcm, double* Rrm) {
+    const int64_t total = n * n;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = k % n, j = k / n;  // element (i, j)
+        const size_t src = layout == TOMOS_COL_MAJOR ? (size_t)j * ld + i : (size_t)i * ld + j;
+        double v = numeric == TOMOS_FP64 ? static_cast<const double*>(R)[src]
+                                         : (double)static_cast<const float*>(R)[src];
+        Rcm[(size_t)j * n + i] = v;
+        Rrm[(size_t)i * n + j] = v;
+    }
+}
+
+// ------------------------------------------------------------- n-side
+
+struct NSide {
+    int64_t n;
+    const float* qpart;
+    int64_t qstride;
+    int gq;
+    const double* sspart;
+    int gs;
+    double* t;
+    double* vhat;
+    float* v;
+    float* wt;
+    float* p;
+    float* x;
+    double* vpart;
+    double* xpart;
+    double* qnpart;
+    const double* Rcm;
+    const double* Rrm;
+    int has_precond;
+    int init;
+    int nb1;   // N1 blocks
+    int nb3;   // N2/N3 blocks
+    double* scal;
+    LsqrDev* st;
+    const int* skip;
+};
+
+// Givens step of LSQR (lsqr.cpp:633-679), FP64.
+struct Givens {
+    double rho, c, s, theta, rho_bar, phi, phi_bar;
+};
+__device__ __forceinline__ Givens givens(double rho_bar, double phi_bar, double alpha, double beta) {
+    Givens g;
+    g.rho = hypot(rho_bar, beta);
+    const double inv = g.rho > 0.0 ? 1.0 / g.rho : 0.0;
+    g.c = rho_bar * inv;
+    g.s = beta * inv;
+    g.theta = g.s * alpha;
+    g.rho_bar = -g.c * alpha;
+    g.phi = g.c * phi_bar;
+    g.phi_bar = g.s * phi_bar;
+    return g;
+}
+
+// N1: beta and t = A^T ut / beta (no preconditioner: vh = t - beta v).
+__global__ void __launch_bounds__(256) nside_reduce_kernel(NSide S) {
+    if (S.skip && *S.skip) return;
+    __shared__ double sm[32];
+    __shared__ double smq[8][33];
+    const double beta = sqrt(block_sum_array(S.sspart, S.gs, sm));
+    const double inv = beta > 0.0 ? 1.0 / beta : 0.0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t j = (int64_t)blockIdx.x * 32 + lane;
+    double q = 0.0;
+    if (j < S.n)
+        for (int c = w; c < S.gq; c += 8) q += (double)S.qpart[(size_t)c * S.qstride + j];
+    smq[w][lane] = q;
+    __syncthreads();
+    if (w == 0) {
+        double qs = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) qs += smq[k][lane];
+        double vh2 = 0.0, qn = 0.0;
+        if (j < S.n) {
+            const double tj = qs * inv;
+            if (S.has_precond) {
+                S.t[j] = tj;
+            } else {
+                const double vh = S.init ? tj : tj - beta * (double)S.v[j];
+                S.vhat[j] = vh;
+                vh2 = vh * vh;
+            }
+            qn = qs * qs;
+        }
+        vh2 = warp_sum(vh2);
+        qn = warp_sum(qn);
+        if (lane == 0) {
+            if (!S.has_precond) S.vpart[blockIdx.x] = vh2;
+            S.qnpart[blockIdx.x] = qn;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) S.scal[0] = beta;
+}
+
+// N2: z = M^T t (M = R^{-1}), vh = z - beta v.
+__global__ void __launch_bounds__(256) nside_precond_t_kernel(NSide S) {
+    if (S.skip && *S.skip) return;
+    __shared__ double smv[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t j = (int64_t)blockIdx.x * 8 + w;
+    const double beta = S.scal[0];
+    double vh2 = 0.0;
+    if (j < S.n) {
+        const double* col = S.Rcm + (size_t)j * S.n;
+        double z = 0.0;
+        for (int64_t i = lane; i < S.n; i += 32) z += col[i] * S.t[i];
+        z = warp_sum(z);
+        const double vh = S.init ? z : z - beta * (double)S.v[j];
+        if (lane == 0) S.vhat[j] = vh;
+        vh2 = vh * vh;
+    }
+    if (lane == 0) smv[w] = vh2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += smv[k];
+        S.vpart[blockIdx.x] = s;
+    }
+}
+
+// N3: alpha, v, p = M v, and the x / wt update of the Givens step.
+__global__ void __launch_bounds__(256) nside_update_kernel(NSide S) {
+    if (S.skip && *S.skip) return;
+    __shared__ double sm[32];
+    __shared__ double smx[8];
+    const int nvp = S.has_precond ? S.nb3 : S.nb1;
+    const double alpha = sqrt(block_sum_array(S.vpart, nvp, sm));
+    const double inva = alpha > 0.0 ? 1.0 / alpha : 0.0;
+    const double beta = S.scal[0];
+    Givens g = givens(S.st->rho_bar, S.st->phi_bar, alpha, beta);
+    const double step_x = g.rho > 0.0 ? g.phi / g.rho : 0.0;
+    const double step_w = g.rho > 0.0 ? g.theta / g.rho : 0.0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t i = (int64_t)blockIdx.x * 8 + w;
+    double xs = 0.0;
+    if (i < S.n) {
+        double pi;
+        if (S.has_precond) {
+            const double* row = S.Rrm + (size_t)i * S.n;
+            double z = 0.0;
+            for (int64_t jj = lane; jj < S.n; jj += 32) z += row[jj] * S.vhat[jj];
+            pi = warp_sum(z) * inva;
+        } else {
+            pi = S.vhat[i] * inva;
+        }
+        if (lane == 0) {
+            S.v[i] = (float)(S.vhat[i] * inva);
+            double xi = (double)S.x[i];
+            if (S.init) {
+                S.wt[i] = (float)pi;
+            } else {
+                const double wi = (double)S.wt[i];
+                xi += step_x * wi;
+                S.x[i] = (float)xi;
+                S.wt[i] = (float)(pi - step_w * wi);
+            }
+            S.p[i] = (float)pi;
+            const double xf = (double)(float)xi;
+            xs = xf * xf;
+        }
+    }
+    if (lane == 0) smx[w] = xs;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += smx[k];
+        S.xpart[blockIdx.x] = s;
+        if (blockIdx.x == 0) S.scal[1] = alpha;
+    }
+}
+
+// N4: one block -- state update and the stopping rule.
+__global__ void __launch_bounds__(256) nside_finish_kernel(NSide S) {
+    if (S.skip && *S.skip) return;
+    __shared__ double sm[32];
+    const double xn = sqrt(block_sum_array(S.xpart, S.nb3, sm));
+    const double qn = S.init ? sqrt(block_sum_array(S.qnpart, S.nb1, sm)) : 0.0;
+    if (threadIdx.x != 0) return;
+    LsqrDev* st = S.st;
+    const double beta = S.scal[0], alpha = S.scal[1];
+    st->xnorm = xn;
+    st->coef[0] = 1.0;
+    st->coef[1] = beta > 0.0 ? -alpha / beta : 0.0;
+    if (S.init) {
+        st->alpha = alpha;
+        st->beta = beta;
+        st->rho_bar = alpha;
+        st->phi_bar = beta;
+        st->beta_init = beta;
+        st->arnorm = qn;
+        st->iter_restart = 0;
+        st->relres = st->rhsnorm > 0.0 ? beta / st->rhsnorm : 0.0;
+        st->done = 0;
+        st->breakdown = (alpha == 0.0 || beta == 0.0) ? 1 : 0;
+        return;
+    }
+    Givens g = givens(st->rho_bar, st->phi_bar, alpha, beta);
+    st->alpha = alpha;
+    st->beta = beta;
+    st->rho_bar = g.rho_bar;
+    st->phi_bar = g.phi_bar;
+    st->iter += 1;
+    st->iter_restart += 1;
+    const double relres = st->rhsnorm > 0.0 ? fabs(g.phi_bar) / st->rhsnorm : 0.0;
+    st->relres = relres;
+    if (st->history && st->iter - 1 < st->history_cap) st->history[st->iter - 1] = relres;
+    int stop = 0;
+    if (st->rhsnorm == 0.0) stop = 1;
+    if (st->stop_rule == TOMOS_STOP_RELRES) {
+        if (relres < st->tol || relres < st->max_relres) {
+            stop = 1;
+            st->converged = 1;
+        }
+    } else {
+        const double den = st->anorm_fro * xn + st->bnorm;
+        const double eta1 = den > 0.0 ? fabs(g.phi_bar) / den : 0.0;
+        if (eta1 <= st->tol) stop = 1;
+        if (st->inner_rtol > 0.0 && fabs(g.phi_bar) <= st->inner_rtol * st->beta_init) stop = 1;
+    }
+    if (alpha == 0.0 || beta == 0.0) {
+        stop = 1;
+        st->breakdown = 1;
+    }
+    if (st->iter_restart >= st->max_iters) stop = 1;
+    if (stop) st->done = 1;
+}
+
+// ------------------------------------------------------------ workspace
+
+static void ws_free(tomos_workspace* ws) {
+    void* ptrs[] = {ws->u,      ws->v,      ws->wt,     ws->p,    ws->qvec,   ws->t,
+                    ws->vhat,   ws->qpart,  ws->sspart, ws->vpart, ws->xpart, ws->qnpart,
+                    ws->scal,   ws->coef_init, ws->bpart, ws->fro2, ws->st,   ws->Rcm,
+                    ws->Rrm,    ws->hist,   ws->scratch};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (ws->st_host) cudaFreeHost(ws->st_host);
+    if (ws->graph) cudaGraphExecDestroy(ws->graph);
+    if (ws->ev_start) cudaEventDestroy(ws->ev_start);
+    if (ws->ev_stop) cudaEventDestroy(ws->ev_stop);
+    if (ws->ev_fence) cudaEventDestroy(ws->ev_fence);
+    if (ws->stream) cudaStreamDestroy(ws->stream);
+}
+
+template <typename T>
+static cudaError_t alloc(T** p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void**>(p), (count ? count : 1) * sizeof(T));
+}
+
+tomos_status ensure_scratch(tomos_workspace* ws, size_t bytes) {
+    if (bytes <= ws->scratch_bytes) return TOMOS_OK;
+    if (ws->scratch) cudaFree(ws->scratch);
+    ws->scratch = nullptr;
+    ws->scratch_bytes = 0;
+    cudaError_t e = cudaMalloc(&ws->scratch, bytes);
+    if (e != cudaSuccess) return fail(TOMOS_ERR_ALLOC, "workspace scratch allocation failed");
+    ws->scratch_bytes = bytes;
+    return TOMOS_OK;
+}
+
+static tomos_status ensure_history(tomos_workspace* ws, int cap) {
+    if (cap <= ws->hist_cap) return TOMOS_OK;
+    if (ws->hist) cudaFree(ws->hist);
+    ws->hist = nullptr;
+    ws->hist_cap = 0;
+    if (alloc(&ws->hist, (size_t)cap) != cudaSuccess)
+        return fail(TOMOS_ERR_ALLOC, "history allocation failed");
+    ws->hist_cap = cap;
+    return TOMOS_OK;
+}
+
+// ------------------------------------------------------------ A passes
+
+template <Elem E, int NCH, bool ACC64>
+static void launch_fused_t(const FusedParams& P, int grid, cudaStream_t st) {
+    fused_pass_kernel<E, NCH, ACC64><<<grid, kFusedThreads, 0, st>>>(P);
+}
+
+template <Elem E, bool ACC64>
+static bool launch_fused_e(const FusedParams& P, int nch, int grid, cudaStream_t st) {
+    switch (nch) {
+        case 1: launch_fused_t<E, 1, ACC64>(P, grid, st); return true;
+        case 2: launch_fused_t<E, 2, ACC64>(P, grid, st); return true;
+        case 4: launch_fused_t<E, 4, ACC64>(P, grid, st); return true;
+        case 8:
+            if constexpr (E == Elem::F32) {
+                launch_fused_t<E, 8, ACC64>(P, grid, st);
+                return true;
+            }
+            return false;
+        default: return false;
+    }
+}
+
+static bool launch_fused(Elem e, bool acc64, const FusedParams& P, int nch, int grid,
+                         cudaStream_t st) {
+    switch (e) {
+        case Elem::F32:
+            return acc64 ? launch_fused_e<Elem::F32, true>(P, nch, grid, st)
+                         : launch_fused_e<Elem::F32, false>(P, nch, grid, st);
+        case Elem::H16:
+            return acc64 ? launch_fused_e<Elem::H16, true>(P, nch, grid, st)
+                         : launch_fused_e<Elem::H16, false>(P, nch, grid, st);
+        case Elem::B16:
+            return acc64 ? launch_fused_e<Elem::B16, true>(P, nch, grid, st)
+                         : launch_fused_e<Elem::B16, false>(P, nch, grid, st);
+        case Elem::A16: return launch_fused_e<Elem::A16, true>(P, nch, grid, st);
+        case Elem::AB16: return launch_fused_e<Elem::AB16, true>(P, nch, grid, st);
+        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true>(P, nch, grid, st);
+        default: return false;
+    }
+}
+
+// Chooses the fused pass when A is row-major with 16-byte aligned rows
+// and n fits one warp's register-resident columns; otherwise the generic
+// two-kernel path.
+static PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64) {
+    PassPlan pl;
+    pl.e = e;
+    pl.acc64 = acc64 || elem_is_exact(e);
+    const int vec = (e == Elem::F32) ? 4 : 8;
+    const int wbytes = (e == Elem::F32) ? 4 : 2;
+    bool ok = A->layout == TOMOS_ROW_MAJOR && ((A->ld * wbytes) % 16 == 0) &&
+              (reinterpret_cast<uintptr_t>(A->values) % 16 == 0);
+    if (ok && elem_is_exact(e))
+        ok = reinterpret_cast<uintptr_t>(dense_lo_plane(A)) % 16 == 0;
+    int nch = 0;
+    for (int c : {1, 2, 4, 8}) {
+        if (c == 8 && e != Elem::F32) break;
+        if ((int64_t)32 * c * vec >= A->cols) {
+            nch = c;
+            break;
+        }
+    }
+    if (ok && nch > 0 && A->cols > 0) {
+        pl.fused = true;
+        pl.nch = nch;
+        int64_t g = ws->gmax;
+        int64_t min_rows_cta = 64;
+        int64_t gr = (A->rows + min_rows_cta - 1) / min_rows_cta;
+        if (g > gr) g = gr;
+        if (g < 1) g = 1;
+        pl.grid = (int)g;
+        pl.gq = pl.grid;
+        pl.gs = pl.grid;
+        pl.qstride = ws->qstride;
+    } else {
+        pl.fused = false;
+        pl.gq = 1;
+        pl.qstride = A->cols;
+        pl.gs = ws->gs_max;
+    }
+    return pl;
+}
+
+static size_t dense_pass_scratch(const tomos_dense* A) {
+    size_t a = gemv_scratch_bytes_max(A, TOMOS_NO_TRANSPOSE);
+    size_t b = gemv_scratch_bytes_max(A, TOMOS_TRANSPOSE);
+    return a > b ? a : b;
+}
+
+// Enqueues one A pass.  p: right vector; u_in: vector combined with cu;
+// coef: device [cp, cu]; skip: device stop flag (NULL for unconditional).
+static tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A,
+                                       const PassPlan& pl, const float* p, const float* u_in,
+                                       const double* coef, const int* skip, cudaStream_t st) {
+    const void* lo = elem_is_exact(pl.e) ? dense_lo_plane(A) : nullptr;
+    if (pl.fused) {
+        FusedParams P;
+        P.hi = A->values;
+        P.lo = lo;
+        P.m = A->rows;
+        P.n = A->cols;
+        P.ld = A->ld;
+        P.p = p;
+        P.u_in = u_in;
+        P.u_out = ws->u;
+        P.coef = coef;
+        P.qpart = ws->qpart;
+        P.sspart = ws->sspart;
+        P.qstride = pl.qstride;
+        P.skip = skip;
+        if (!launch_fused(pl.e, pl.acc64, P, pl.nch, pl.grid, st))
+            return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
+        TOMOS_LAUNCH_CHECK("fused_pass_kernel");
+        return TOMOS_OK;
+    }
+    // Generic path: u = cp*A p + cu*u_in (u_in copied into u first when
+    // they differ), ||u||^2, then q = A^T u.
+    if (u_in != ws->u) {
+        TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->u, u_in, sizeof(float) * A->rows,
+                                       cudaMemcpyDeviceToDevice, st));
+    }
+    GemvLaunch L;
+    std::string why;
+    if (!gemv_shape(A, TOMOS_NO_TRANSPOSE, &L.dot, &L.outer, &L.inner, &why))
+        return fail(TOMOS_ERR_INVALID, why);
+    L.hi = A->values;
+    L.lo = lo;
+    L.ld = A->ld;
+    L.x = p;
+    L.y = ws->u;
+    L.coef = coef;
+    L.skip = skip;
+    L.scratch = ws->scratch;
+    L.scratch_bytes = ws->scratch_bytes;
+    tomos_status s = gemv_launch(L, pl.e, pl.acc64, st);
+    if (s) return s;
+    sumsq_partial_kernel<<<pl.gs, 256, 0, st>>>(ws->u, A->rows, skip, ws->sspart);
+    TOMOS_LAUNCH_CHECK("sumsq_partial_kernel");
+    GemvLaunch T;
+    if (!gemv_shape(A, TOMOS_TRANSPOSE, &T.dot, &T.outer, &T.inner, &why))
+        return fail(TOMOS_ERR_INVALID, why);
+    T.hi = A->values;
+    T.lo = lo;
+    T.ld = A->ld;
+    T.x = ws->u;
+    T.y = ws->qpart;
+    T.alpha = 1.0;
+    T.beta = 0.0;
+    T.skip = skip;
+    T.scratch = ws->scratch;
+    T.scratch_bytes = ws->scratch_bytes;
+    return gemv_launch(T, pl.e, pl.acc64, st);
+}
+
+// ------------------------------------------------------------ n-side glue
+
+static NSide make_nside(tomos_workspace* ws, const PassPlan& pl, float* x, bool init,
+                        const int* skip) {
+    NSide S;
+    S.n = ws->n;
+    S.qpart = ws->qpart;
+    S.qstride = pl.qstride;
+    S.gq = pl.gq;
+    S.sspart = ws->sspart;
+    S.gs = pl.gs;
+    S.t = ws->t;
+    S.vhat = ws->vhat;
+    S.v = ws->v;
+    S.wt = ws->wt;
+    S.p = ws->p;
+    S.x = x;
+    S.vpart = ws->vpart;
+    S.xpart = ws->xpart;
+    S.qnpart = ws->qnpart;
+    S.Rcm = ws->Rcm;
+    S.Rrm = ws->Rrm;
+    S.has_precond = ws->has_precond ? 1 : 0;
+    S.init = init ? 1 : 0;
+    S.nb1 = ws->nb1;
+    S.nb3 = ws->nb3;
+    S.scal = ws->scal;
+    S.st = ws->st;
+    S.skip = skip;
+    return S;
+}
+
+static tomos_status enqueue_nside(tomos_workspace* ws, const NSide& S, cudaStream_t st) {
+    nside_reduce_kernel<<<ws->nb1, 256, 0, st>>>(S);
+    TOMOS_LAUNCH_CHECK("nside_reduce_kernel");
+    if (S.has_precond) {
+        nside_precond_t_kernel<<<ws->nb3, 256, 0, st>>>(S);
+        TOMOS_LAUNCH_CHECK("nside_precond_t_kernel");
+    }
+    nside_update_kernel<<<ws->nb3, 256, 0, st>>>(S);
+    TOMOS_LAUNCH_CHECK("nside_update_kernel");
+    nside_finish_kernel<<<1, 256, 0, st>>>(S);
+    TOMOS_LAUNCH_CHECK("nside_finish_kernel");
+    return TOMOS_OK;
+}
+
+struct DensePass : PassOps {
+    tomos_workspace* ws;
+    const tomos_dense* A;
+    Elem iter_e, init_e;
+    DensePass(tomos_workspace* w, const tomos_dense* a, Elem ie, Elem ze)
+        : ws(w), A(a), iter_e(ie), init_e(ze) {}
+    PassPlan plan(bool init) override {
+        return plan_dense_pass(ws, A, init ? init_e : iter_e, init);
+    }
+    tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
+                         const int* skip, cudaStream_t st) override {
+        return enqueue_dense_pass(ws, A, pl, p, u_in, coef, skip, st);
+    }
+    tomos_status fro2(double* out, cudaStream_t st) override {
+        bool dot;
+        int64_t outer, inner;
+        std::string why;
+        gemv_shape(A, TOMOS_NO_TRANSPOSE, &dot, &outer, &inner, &why);
+        const void* lo = elem_is_exact(init_e) ? dense_lo_plane(A) : nullptr;
+        int g = ws->gs_max;
+        switch (init_e) {
+            case Elem::F32: fro2_partial_kernel<Elem::F32><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
+            case Elem::H16: fro2_partial_kernel<Elem::H16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
+            case Elem::A16: fro2_partial_kernel<Elem::A16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
+            case Elem::B16: fro2_partial_kernel<Elem::B16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
+            case Elem::AB16: fro2_partial_kernel<Elem::AB16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
+            case Elem::AB16R: fro2_partial_kernel<Elem::AB16R><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
+            default: return fail(TOMOS_ERR_UNSUPPORTED, "fro2: element type");
+        }
+        TOMOS_LAUNCH_CHECK("fro2_partial_kernel");
+        sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, g, out);
+        TOMOS_LAUNCH_CHECK("sum_to_scalar_kernel");
+        return TOMOS_OK;
+    }
+    uint64_t key() override {
+        return reinterpret_cast<uint64_t>(A->values) ^ ((uint64_t)A->layout << 60) ^
+               ((uint64_t)A->ld << 20);
+    }
+    int64_t rows() override { return A->rows; }
+    int64_t cols() override { return A->cols; }
+};
+
+// ------------------------------------------------------------ driver
+
+static tomos_status sync_state(tomos_workspace* ws) {
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->st_host, ws->st, sizeof(LsqrDev), cudaMemcpyDeviceToHost,
+                                   ws->stream));
+    TOMOS_CUDA_TRY(cudaStreamSynchronize(ws->stream));
+    return TOMOS_OK;
+}
+
+static double eta_of(const LsqrDev& s) {
+    const double den1 = s.anorm_fro * s.xnorm + s.bnorm;
+    const double e1 = den1 > 0.0 ? s.beta / den1 : 0.0;
+    const double den2 = s.anorm_fro * s.beta;
+    const double e2 = den2 > 0.0 ? s.arnorm / den2 : 0.0;
+    return e1 < e2 ? e1 : e2;
+}
+
+tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, float* x,
+                          const tomos_lsqr_opts* o, tomos_lsqr_report* rep, void* user_stream) {
+    cudaStream_t us = as_stream(user_stream);
+    cudaStream_t st = ws->stream;
+    const int64_t m = ops.rows(), n = ops.cols();
+    tomos_lsqr_report R;
+    std::memset(&R, 0, sizeof(R));
+
+    // Order against the caller's stream.
+    TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_fence, us));
+    TOMOS_CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_fence, 0));
+    TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
+
+    const int max_iters = o->max_iters > 0 ? o->max_iters : 0;
+    const int restarts = o->restarts > 0 ? o->restarts : 1;
+    const int64_t hist_total = (int64_t)max_iters * restarts;
+    tomos_status s = ensure_history(ws, (int)(hist_total > 0 ? hist_total : 1));
+    if (s) return s;
+
+    // Precondition copies (FP64, both orientations).
+    if (ws->has_precond) {
+        precond_copy_kernel<<<ws->gs_max, 256, 0, st>>>(ws->precond.values, ws->precond.numeric,
+                                                       ws->precond.layout, ws->precond.ld, n,
+                                                       ws->Rcm, ws->Rrm);
+        TOMOS_LAUNCH_CHECK("precond_copy_kernel");
+    }
+    if (!o->warm_start) TOMOS_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(float) * n, st));
+
+    // ||b|| and, for the backward-error rule, ||A||_F.
+    sumsq_partial_kernel<<<ws->gs_max, 256, 0, st>>>(b, m, nullptr, ws->bpart);
+    TOMOS_LAUNCH_CHECK("sumsq_partial_kernel");
+    sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, ws->scal + 2);
+    TOMOS_LAUNCH_CHECK("sum_to_scalar_kernel");
+    double anorm = o->anorm_fro;
+    int extra_passes = 0;
+    if (o->stop_rule == TOMOS_STOP_BACKWARD && !(anorm > 0.0)) {
+        s = ops.fro2(ws->scal + 3, st);
+        if (s) return s;
+        extra_passes = 1;
+    }
+    double hostsc[4];
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(hostsc, ws->scal, sizeof(hostsc), cudaMemcpyDeviceToHost, st));
+    TOMOS_CUDA_TRY(cudaStreamSynchronize(st));
+    const double bnorm = std::sqrt(hostsc[2]);
+    if (o->stop_rule == TOMOS_STOP_BACKWARD && !(anorm > 0.0)) anorm = std::sqrt(hostsc[3]);
+
+    LsqrDev init_state;
+    std::memset(&init_state, 0, sizeof(init_state));
+    init_state.rhsnorm = bnorm;
+    init_state.bnorm = bnorm;
+    init_state.anorm_fro = anorm;
+    init_state.tol = o->tol;
+    init_state.max_relres = o->max_relres;
+    init_state.inner_rtol = o->stop_rule == TOMOS_STOP_BACKWARD ? o->inner_rtol : 0.0;
+    init_state.max_iters = max_iters;
+    init_state.stop_rule = o->stop_rule;
+    init_state.history = ws->hist;
+    init_state.history_cap = ws->hist_cap;
+    init_state.done = 1;
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->st, &init_state, sizeof(LsqrDev), cudaMemcpyHostToDevice, st));
+    const double coef_init[2] = {-1.0, 1.0};
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->coef_init, coef_init, sizeof(coef_init),
+                                   cudaMemcpyHostToDevice, st));
+
+    PassPlan pl_init = ops.plan(true);
+    PassPlan pl_iter = ops.plan(false);
+
+    // Capture (or reuse) the graph of one iteration.
+    std::vector<uint64_t> key = {ops.key(),
+                                 (uint64_t)pl_iter.fused,
+                                 (uint64_t)pl_iter.e,
+                                 (uint64_t)pl_iter.nch,
+                                 (uint64_t)pl_iter.grid,
+                                 reinterpret_cast<uint64_t>(x),
+                                 (uint64_t)ws->has_precond,
+                                 (uint64_t)n,
+                                 (uint64_t)m};
+    if (!ws->graph || ws->graph_key != key) {
+        if (ws->graph) cudaGraphExecDestroy(ws->graph);
+        ws->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        TOMOS_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int* skip = &ws->st->done;
+        tomos_status cs = ops.enqueue(pl_iter, ws->p, ws->u, ws->st->coef, skip, st);
+        if (!cs) cs = enqueue_nside(ws, make_nside(ws, pl_iter, x, false, skip), st);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (cs) {
+            if (g) cudaGraphDestroy(g);
+            return cs;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+        ce = cudaGraphInstantiate(&ws->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+        ws->graph_key = key;
+    }
+
+    std::vector<double> hist_host;
+    int hist_read = 0;
+    int accurate_passes = extra_passes, iter_passes = 0;
+    bool converged = false;
+    int restarts_used = 0;
+    LsqrDev& H = *ws->st_host;
+
+    for (int rs = 0; rs < restarts; ++rs) {
+        // Restart-boundary stopping check on the running estimate
+        // (check_stopping_criteria at the top of each restart, lsqr.cpp:705-708).
+        if (rs > 0 && o->stop_rule == TOMOS_STOP_RELRES && H.iter > 0) {
+            double rel = H.rhsnorm == 0.0 ? 0.0 : std::fabs(H.phi_bar) / H.rhsnorm;
+            hist_host.push_back(rel);
+            if (H.rhsnorm == 0.0 || rel < o->tol || rel < o->max_relres) {
+                converged = true;
+                break;
+            }
+        }
+        // initialize(): ut = b - A x (restarted from the current x).
+        restarts_used = rs + 1;
+        s = ops.enqueue(pl_init, x, b, ws->coef_init, nullptr, st);
+        if (s) return s;
+        s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr), st);
+        if (s) return s;
+        if (pl_init.e == Elem::A16 || pl_init.e == Elem::AB16 || pl_init.e == Elem::AB16R ||
+            pl_init.e != pl_iter.e)
+            ++accurate_passes;
+        else
+            ++iter_passes;
+        s = sync_state(ws);
+        if (s) return s;
+        if (H.rhsnorm == 0.0) {
+            converged = true;
+            break;
+        }
+        if (o->stop_rule == TOMOS_STOP_RELRES) {
+            const double true_relres = H.beta / H.rhsnorm;
+            if (true_relres < o->tol || true_relres < o->max_relres) {
+                converged = true;
+                break;
+            }
+        } else {
+            R.rnorm = H.beta;
+            R.arnorm = H.arnorm;
+            R.xnorm = H.xnorm;
+            R.backward_error = eta_of(H);
+            if (R.backward_error <= o->tol || H.beta == 0.0) {
+                converged = true;
+                break;
+            }
+        }
+        if (H.breakdown || max_iters == 0) continue;
+        // Inner iterations in batches of graph launches; the device stops
+        // doing work once its stopping rule fires.
+        int batch = 4;
+        int done_iters = 0;
+        while (done_iters < max_iters) {
+            int k = batch < max_iters - done_iters ? batch : max_iters - done_iters;
+            for (int i = 0; i < k; ++i) TOMOS_CUDA_TRY(cudaGraphLaunch(ws->graph, st));
+            s = sync_state(ws);
+            if (s) return s;
+            done_iters = H.iter_restart;
+            if (H.done) break;
+            if (batch < 32) batch *= 2;
+        }
+        iter_passes += H.iter_restart;
+        if (H.iter > hist_read) {
+            int cnt = (H.iter < ws->hist_cap ? H.iter : ws->hist_cap) - hist_read;
+            if (cnt > 0) {
+                std::vector<double> tmp(cnt);
+                TOMOS_CUDA_TRY(cudaMemcpy(tmp.data(), ws->hist + hist_read, sizeof(double) * cnt,
+                                          cudaMemcpyDeviceToHost));
+                hist_host.insert(hist_host.end(), tmp.begin(), tmp.end());
+                hist_read += cnt;
+            }
+        }
+        if (o->stop_rule == TOMOS_STOP_RELRES && H.converged) {
+            converged = true;
+            break;
+        }
+    }
+    // The backward-error rule reports the accurate eta of the returned x.
+    if (o->stop_rule == TOMOS_STOP_BACKWARD && !converged) {
+        s = ops.enqueue(pl_init, x, b, ws->coef_init, nullptr, st);
+        if (s) return s;
+        s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr), st);
+        if (s) return s;
+        ++accurate_passes;
+        s = sync_state(ws);
+        if (s) return s;
+        R.rnorm = H.beta;
+        R.arnorm = H.arnorm;
+        R.xnorm = H.xnorm;
+        R.backward_error = eta_of(H);
+        converged = R.backward_error <= o->tol;
+    }
+    TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
+    TOMOS_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop);
+    TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_fence, st));
+    TOMOS_CUDA_TRY(cudaStreamWaitEvent(us, ws->ev_fence, 0));
+
+    R.iterations = H.iter;
+    R.restarts_used = restarts_used;
+    R.converged = converged ? 1 : 0;
+    R.relres = H.relres;
+    if (o->stop_rule == TOMOS_STOP_RELRES) R.relres = H.rhsnorm > 0 ? std::fabs(H.phi_bar) / H.rhsnorm : 0.0;
+    R.anorm_fro = anorm;
+    R.bnorm = bnorm;
+    if (o->stop_rule != TOMOS_STOP_BACKWARD) R.xnorm = H.xnorm;
+    R.elapsed_ms = ms;
+    R.accurate_passes = accurate_passes;
+    R.half_passes = iter_passes;
+    if (o->history && o->history_cap > 0) {
+        int cnt = (int)hist_host.size() < o->history_cap ? (int)hist_host.size() : o->history_cap;
+        for (int i = 0; i < cnt; ++i) o->history[i] = hist_host[i];
+        R.history_len = cnt;
+    }
+    if (rep) *rep = R;
+    return TOMOS_OK;
+}
+
+tomos_status workspace_check(tomos_workspace* ws, int64_t m, int64_t n) {
+    if (!ws) return fail(TOMOS_ERR_INVALID, "lsqr_solve: null workspace");
+    if (ws->m != m || ws->n != n)
+        return fail(TOMOS_ERR_INVALID, "lsqr_solve: workspace is sized for " +
+                                           std::to_string(ws->m) + "x" + std::to_string(ws->n) +
+                                           ", matrix is " + std::to_string(m) + "x" +
+                                           std::to_string(n));
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != ws->device)
+        return fail(TOMOS_ERR_INVALID, "lsqr_solve: workspace belongs to another device");
+    return TOMOS_OK;
+}
+
+static bool opts_ok(const tomos_lsqr_opts* o, std::string* why) {
+    if (!o) {
+        *why = "null options";
+        return false;
+    }
+    if (o->stop_rule != TOMOS_STOP_RELRES && o->stop_rule != TOMOS_STOP_BACKWARD) {
+        *why = "unknown stop rule";
+        return false;
+    }
+    if (o->max_iters < 0) {
+        *why = "negative max_iters";
+        return false;
+    }
+    return true;
+}
+
+// Tier used for the restart-boundary residual.
+static int32_t init_tier_for(int32_t numeric, const tomos_lsqr_opts* o, int32_t iter_tier) {
+    const bool packed = numeric == TOMOS_FP32_16 || numeric == TOMOS_FP32_BF16;
+    if (packed && (o->implicit_duplicate || o->stop_rule == TOMOS_STOP_BACKWARD))
+        return TOMOS_TIER_ACCURATE;
+    return iter_tier;
+}
+
+}  // namespace tomos_b200
+
+using namespace tomos_b200;
+
+extern "C" {
+
+tomos_status tomos_workspace_create(int64_t m, int64_t n, int32_t value_type,
+                                    int32_t precond_type, tomos_workspace** out) {
+    if (!out) return fail(TOMOS_ERR_INVALID, "tomos_workspace_create: null output");
+    *out = nullptr;
+    if (m < 0 || n < 0) return fail(TOMOS_ERR_INVALID, "tomos_workspace_create: negative size");
+    if (value_type != TOMOS_FP32)
+        return fail(TOMOS_ERR_UNSUPPORTED,
+                    "tomos_workspace_create: only FP32 working vectors are registered");
+    if (precond_type != TOMOS_FP32 && precond_type != TOMOS_FP64)
+        return fail(TOMOS_ERR_UNSUPPORTED,
+                    "tomos_workspace_create: precond_type must be FP32 or FP64");
+    tomos_workspace* ws = new tomos_workspace();
+    ws->m = m;
+    ws->n = n;
+    ws->value_type = value_type;
+    ws->precond_type = precond_type;
+    cudaGetDevice(&ws->device);
+    const int sms = sm_count();
+    ws->gmax = sms * 4;
+    ws->qstride = ((n + 31) / 32) * 32;
+    if (ws->qstride < 32) ws->qstride = 32;
+    ws->nb1 = (int)((n + 31) / 32);
+    ws->nb3 = (int)((n + 7) / 8);
+    if (ws->nb1 < 1) ws->nb1 = 1;
+    if (ws->nb3 < 1) ws->nb3 = 1;
+    ws->gs_max = sms * 2;
+    bool ok = true;
+    auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
+    A(alloc(&ws->u, (size_t)m));
+    A(alloc(&ws->v, (size_t)n));
+    A(alloc(&ws->wt, (size_t)n));
+    A(alloc(&ws->p, (size_t)n));
+    A(alloc(&ws->qvec, (size_t)n));
+    A(alloc(&ws->t, (size_t)n));
+    A(alloc(&ws->vhat, (size_t)n));
+    size_t qp = (size_t)ws->gmax * ws->qstride;
+    if (qp < (size_t)n) qp = n;
+    A(alloc(&ws->qpart, qp));
+    size_t sp = (size_t)(ws->gmax > ws->gs_max ? ws->gmax : ws->gs_max);
+    A(alloc(&ws->sspart, sp));
+    A(alloc(&ws->vpart, (size_t)(ws->nb1 > ws->nb3 ? ws->nb1 : ws->nb3)));
+    A(alloc(&ws->xpart, (size_t)ws->nb3));
+    A(alloc(&ws->qnpart, (size_t)ws->nb1));
+    A(alloc(&ws->scal, 8));
+    A(alloc(&ws->coef_init, 2));
+    A(alloc(&ws->bpart, (size_t)ws->gs_max));
+    A(alloc(&ws->fro2, 1));
+    A(alloc(&ws->st, 1));
+    A(cudaMallocHost(reinterpret_cast<void**>(&ws->st_host), sizeof(LsqrDev)));
+    A(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+    A(cudaEventCreate(&ws->ev_start));
+    A(cudaEventCreate(&ws->ev_stop));
+    A(cudaEventCreateWithFlags(&ws->ev_fence, cudaEventDisableTiming));
+    if (!ok) {
+        ws_free(ws);
+        delete ws;
+        return fail(TOMOS_ERR_ALLOC, "tomos_workspace_create: device allocation failed");
+    }
+    std::memset(ws->st_host, 0, sizeof(LsqrDev));
+    *out = ws;
+    return TOMOS_OK;
+}
+
+tomos_status tomos_workspace_destroy(tomos_workspace* ws) {
+    if (!ws) return TOMOS_OK;
+    cudaStreamSynchronize(ws->stream);
+    ws_free(ws);
+    delete ws;
+    return TOMOS_OK;
+}
+
+tomos_status tomos_workspace_add_precond(tomos_workspace* ws, const tomos_dense* Rinv) {
+    if (!ws) return fail(TOMOS_ERR_INVALID, "add_precond: null workspace");
+    if (!Rinv) {
+        ws->has_precond = false;
+        return TOMOS_OK;
+    }
+    if (Rinv->numeric != ws->precond_type)
+        return fail(TOMOS_ERR_INVALID,
+                    "add_precond: precond's NumericType doesn't match the precond_type the "
+                    "workspace was created with.");
+    if (Rinv->rows != ws->n || Rinv->cols != ws->n)
+        return fail(TOMOS_ERR_INVALID, "add_precond: preconditioner must be n x n");
+    if (Rinv->layout != TOMOS_ROW_MAJOR && Rinv->layout != TOMOS_COL_MAJOR)
+        return fail(TOMOS_ERR_INVALID, "add_precond: bad layout");
+    if (Rinv->ld < ws->n) return fail(TOMOS_ERR_INVALID, "add_precond: bad leading dimension");
+    if (!ws->Rcm) {
+        bool ok = alloc(&ws->Rcm, (size_t)ws->n * ws->n) == cudaSuccess &&
+                  alloc(&ws->Rrm, (size_t)ws->n * ws->n) == cudaSuccess;
+        if (!ok) return fail(TOMOS_ERR_ALLOC, "add_precond: allocation failed");
+    }
+    ws->precond = *Rinv;
+    ws->has_precond = true;
+    return TOMOS_OK;
+}
+
+tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float* x,
+                                    tomos_workspace* ws, const tomos_lsqr_opts* opts,
+                                    tomos_lsqr_report* report, void* stream) {
+    std::string why;
+    bool dot;
+    int64_t outer, inner;
+    if (!gemv_shape(A, TOMOS_NO_TRANSPOSE, &dot, &outer, &inner, &why))
+        return fail(TOMOS_ERR_INVALID, "lsqr_solve: " + why);
+    if (!opts_ok(opts, &why)) return fail(TOMOS_ERR_INVALID, "lsqr_solve: " + why);
+    tomos_status s = workspace_check(ws, A->rows, A->cols);
+    if (s) return s;
+    if (!b || !x || (!A->values && A->rows * A->cols > 0))
+        return fail(TOMOS_ERR_INVALID, "lsqr_solve: null pointer");
+    if (opts->implicit_duplicate && A->numeric != TOMOS_FP32_16 && A->numeric != TOMOS_FP32_BF16)
+        return fail(TOMOS_ERR_INVALID,
+                    "lsqr_solve: Workspace::use_implicit_duplicate_ requires A to be stored "
+                    "packed (FP32_16 or FP32_BF16).");
+    Elem ie, ze;
+    if (!resolve_elem(A, opts->iter_tier, &ie, &why))
+        return fail(TOMOS_ERR_UNSUPPORTED, "lsqr_solve: " + why);
+    int32_t it = opts->iter_tier == TOMOS_TIER_AUTO
+                     ? ((A->numeric == TOMOS_FP32) ? TOMOS_TIER_NATIVE : TOMOS_TIER_HALF)
+                     : opts->iter_tier;
+    if (!resolve_elem(A, init_tier_for(A->numeric, opts, it), &ze, &why))
+        return fail(TOMOS_ERR_UNSUPPORTED, "lsqr_solve: " + why);
+    if (A->rows == 0 || A->cols == 0) {
+        if (A->cols > 0 && !opts->warm_start) cudaMemsetAsync(x, 0, sizeof(float) * A->cols, as_stream(stream));
+        if (report) std::memset(report, 0, sizeof(*report));
+        if (report) report->converged = 1;
+        return TOMOS_OK;
+    }
+    DensePass ops(ws, A, ie, ze);
+    PassPlan a = ops.plan(true), b2 = ops.plan(false);
+    if (!a.fused || !b2.fused) {
+        s = ensure_scratch(ws, dense_pass_scratch(A));
+        if (s) return s;
+    }
+    return solve_driver(ws, ops, b, x, opts, report, stream);
+}
+
+tomos_status tomos_backward_error_dense(const tomos_dense* A, const float* b, const float* x,
+                                        tomos_workspace* ws, tomos_lsqr_report* report,
+                                        void* stream) {
+    std::string why;
+    bool dot;
+    int64_t outer, inner;
+    if (!gemv_shape(A, TOMOS_NO_TRANSPOSE, &dot, &outer, &inner, &why))
+        return fail(TOMOS_ERR_INVALID, "backward_error: " + why);
+    tomos_status s = workspace_check(ws, A->rows, A->cols);
+    if (s) return s;
+    if (!report) return fail(TOMOS_ERR_INVALID, "backward_error: null report");
+    Elem ze;
+    int32_t tier = (A->numeric == TOMOS_FP32) ? TOMOS_TIER_NATIVE : TOMOS_TIER_ACCURATE;
+    if (!resolve_elem(A, tier, &ze, &why)) return fail(TOMOS_ERR_UNSUPPORTED, why);
+    DensePass ops(ws, A, ze, ze);
+    PassPlan pl = ops.plan(true);
+    if (!pl.fused) {
+        s = ensure_scratch(ws, dense_pass_scratch(A));
+        if (s) return s;
+    }
+    cudaStream_t us = as_stream(stream), st = ws->stream;
+    TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_fence, us));
+    TOMOS_CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_fence, 0));
+    const double coef_init[2] = {-1.0, 1.0};
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->coef_init, coef_init, sizeof(coef_init),
+                                   cudaMemcpyHostToDevice, st));
+    s = ops.enqueue(pl, x, b, ws->coef_init, nullptr, st);
+    if (s) return s;
+    // beta = ||r|| and ||A^T r|| through N1 (no preconditioner, init mode).
+    bool had = ws->has_precond;
+    ws->has_precond = false;
+    NSide S = make_nside(ws, pl, nullptr, true, nullptr);
+    ws->has_precond = had;
+    nside_reduce_kernel<<<ws->nb1, 256, 0, st>>>(S);
+    TOMOS_LAUNCH_CHECK("nside_reduce_kernel");
+    sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->qnpart, ws->nb1, ws->scal + 4);
+    sumsq_partial_kernel<<<ws->gs_max, 256, 0, st>>>(b, A->rows, nullptr, ws->bpart);
+    sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, ws->scal + 2);
+    sumsq_partial_kernel<<<1, 256, 0, st>>>(x, A->cols, nullptr, ws->xpart);
+    sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->xpart, 1, ws->scal + 5);
+    s = ops.fro2(ws->scal + 3, st);
+    if (s) return s;
+    TOMOS_LAUNCH_CHECK("backward_error reductions");
+    double h[6];
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(h, ws->scal, sizeof(h), cudaMemcpyDeviceToHost, st));
+    TOMOS_CUDA_TRY(cudaStreamSynchronize(st));
+    TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_fence, st));
+    TOMOS_CUDA_TRY(cudaStreamWaitEvent(us, ws->ev_fence, 0));
+    LsqrDev L;
+    std::memset(&L, 0, sizeof(L));
+    L.beta = h[0];
+    L.bnorm = std::sqrt(h[2]);
+    L.anorm_fro = std::sqrt(h[3]);
+    L.arnorm = std::sqrt(h[4]);
+    L.xnorm = std::sqrt(h[5]);
+    std::memset(report, 0, sizeof(*report));
+    report->rnorm = L.beta;
+    report->arnorm = L.arnorm;
+    report->anorm_fro = L.anorm_fro;
+    report->xnorm = L.xnorm;
+    report->bnorm = L.bnorm;
+    report->backward_error = eta_of(L);
+    report->accurate_passes = 2;
+    return TOMOS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+// lsqr.cuh -- internal interface of the LSQR driver (lsqr.cu): the device
+// state of the recurrence, the workspace, and the "A pass" abstraction that
+// lets dense and CSR storage share one driver.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace tomos_b200 {
+
+// Device-resident LSQR state.  All scalars FP64.
+struct LsqrDev {
+    double alpha, beta, rho_bar, phi_bar;
+    double rhsnorm;      // ||b|| (the reference's relres denominator)
+    double beta_init;    // beta at the start of the current restart
+    double xnorm;        // ||x|| after the last update
+    double relres;       // |phi_bar| / ||b||
+    double coef[2];      // [cp, cu] of the next A pass
+    double arnorm;       // ||A^T r|| from the last restart pass
+    double anorm_fro, bnorm;
+    double tol, max_relres, inner_rtol;
+    double* history;     // device, |phi_bar|/||b|| per iteration
+    int iter;            // completed iterations, all restarts
+    int iter_restart;    // completed iterations in this restart
+    int max_iters;       // per restart
+    int done;            // nonzero: kernels of an iteration return at once
+    int converged;       // RELRES rule satisfied
+    int breakdown;       // alpha or beta reached zero
+    int stop_rule;
+    int history_cap;
+};
+
+// How one pass over A is run.
+struct PassPlan {
+    bool fused = false;
+    Elem e = Elem::F32;
+    bool acc64 = false;
+    int grid = 0;    // fused CTAs
+    int nch = 0;     // fused chunks per lane
+    int gq = 1;      // rows of A^T partials
+    int gs = 1;      // ||ut||^2 partials
+    int64_t qstride = 0;
+};
+
+// One pass over A producing ut = cp*A p + cu*u_in in the workspace's u,
+// ||ut||^2 partials (sspart, gs of them) and A^T ut partials (qpart, gq
+// rows of stride qstride).
+struct PassOps {
+    virtual ~PassOps() = default;
+    virtual PassPlan plan(bool init) = 0;
+    virtual tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in,
+                                 const double* coef, const int* skip, cudaStream_t st) = 0;
+    virtual tomos_status fro2(double* out_dev, cudaStream_t st) = 0;
+    virtual uint64_t key() = 0;
+    virtual int64_t rows() = 0;
+    virtual int64_t cols() = 0;
+};
+
+tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, float* x,
+                          const tomos_lsqr_opts* o, tomos_lsqr_report* rep, void* user_stream);
+tomos_status workspace_check(tomos_workspace* ws, int64_t m, int64_t n);
+tomos_status ensure_scratch(tomos_workspace* ws, size_t bytes);
+
+}  // namespace tomos_b200
+
+struct tomos_workspace {
+    int64_t m = 0, n = 0;
+    int32_t value_type = TOMOS_FP32, precond_type = TOMOS_FP32;
+    int device = 0;
+    int gmax = 0;          // max CTAs of the fused pass
+    int64_t qstride = 0;   // row stride of the A^T partials
+    int nb1 = 0, nb3 = 0;  // n-side block counts
+    int gs_max = 0;        // sum-of-squares partial blocks
+
+    float* u = nullptr;     // m: unnormalised u
+    float* v = nullptr;     // n
+    float* wt = nullptr;    // n: M w
+    float* p = nullptr;     // n: M v, the right vector of the next pass
+    float* qvec = nullptr;  // n
+    double* t = nullptr;    // n: A^T u
+    double* vhat = nullptr; // n
+    float* qpart = nullptr;
+    double* sspart = nullptr;
+    double* vpart = nullptr;
+    double* xpart = nullptr;
+    double* qnpart = nullptr;
+    double* scal = nullptr;
+    double* coef_init = nullptr;
+    double* bpart = nullptr;
+    double* fro2 = nullptr;
+    tomos_b200::LsqrDev* st = nullptr;
+    double* Rcm = nullptr;  // FP64 copy of M, column-major
+    double* Rrm = nullptr;  // FP64 copy of M, row-major
+    double* hist = nullptr;
+    int hist_cap = 0;
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+
+    bool has_precond = false;
+    tomos_dense precond{};
+
+    tomos_b200::LsqrDev* st_host = nullptr;  // pinned mirror of *st
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_fence = nullptr;
+
+    cudaGraphExec_t graph = nullptr;
+    std::vector<uint64_t> graph_key;
+};

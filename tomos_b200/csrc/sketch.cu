@@ -1,0 +1,383 @@
+// sketch.cu -- hash CountSketch SA = S A (tomos_countsketch_*).
+//
+// S is the reference's hash sketch (countsketch_kernels.cpp:59-85,
+// countsketch_cuda_kernels.cu:267-286): row i of A is added, with sign
+// +1 if bit 0 of splitmix64(i ^ sign_seed) is set and -1 otherwise, into
+// row splitmix64(i ^ bucket_seed) mod s of SA.  Integer hashing is
+// bit-exact with the reference.  Unlike the reference (atomicAdd scatter,
+// order-dependent float sums), every bucket here is summed by one owner in
+// increasing row order, in FP64, so SA is deterministic:
+//   1. hash + bucket histogram       (integer atomics: order-free)
+//   2. exclusive scan of the counts  (one block)
+//   3. scatter row ids to buckets    (arbitrary order within a bucket)
+//   4. sort each bucket's row ids    (one warp per bucket)
+//   5. owner sums                    (row-major: a warp per bucket walks
+//                                     whole rows; column-major: a warp
+//                                     per (column, bucket) gathers down a
+//                                     contiguous column)
+// The sum of squares of the values read (||A||_F^2) falls out of step 5.
+#include <string>
+
+#include "common.cuh"
+#include "sketch.cuh"
+
+namespace tomos_b200 {
+
+__global__ void cs_hash_kernel(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed,
+                               int32_t* __restrict__ bucket, int8_t* __restrict__ sign,
+                               int32_t* __restrict__ counts) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = (int32_t)(splitmix64((uint64_t)i ^ bseed) % (uint64_t)s);
+        bucket[i] = b;
+        sign[i] = (splitmix64((uint64_t)i ^ sseed) & 1ull) ? (int8_t)1 : (int8_t)-1;
+        if (counts) atomicAdd(&counts[b], 1);
+    }
+}
+
+// Exclusive scan of counts[0..s) into offsets[0..s], one block.
+__global__ void cs_scan_kernel(const int32_t* __restrict__ counts, int64_t s,
+                               int32_t* __restrict__ offsets) {
+    __shared__ int32_t carry;
+    __shared__ int32_t wsum[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t base = 0; base < s; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        int32_t v = i < s ? counts[i] : 0;
+        int32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int32_t t = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            wsum[lane] = t;
+        }
+        __syncthreads();
+        const int32_t before = carry + (w > 0 ? wsum[w - 1] : 0) + x - v;
+        if (i < s) offsets[i] = before;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = before + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) offsets[s] = carry;
+}
+
+__global__ void cs_scatter_kernel(int64_t m, const int32_t* __restrict__ bucket,
+                                  const int32_t* __restrict__ offsets, int32_t* __restrict__ cursor,
+                                  int32_t* __restrict__ perm) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = bucket[i];
+        perm[offsets[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
+    }
+}
+
+// Sorts each bucket's row ids ascending (odd-even transposition by a warp;
+// buckets hold about m/s rows).
+__global__ void cs_sort_kernel(int64_t s, const int32_t* __restrict__ offsets,
+                               int32_t* __restrict__ perm) {
+    const int lane = threadIdx.x & 31;
+    const int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (b >= s) return;
+    const int32_t o0 = offsets[b], o1 = offsets[b + 1];
+    const int32_t len = o1 - o0;
+    int32_t* seg = perm + o0;
+    for (int32_t pass = 0; pass < len; ++pass) {
+        const int32_t start = pass & 1;
+        for (int32_t k = start + 2 * lane; k + 1 < len; k += 64) {
+            int32_t a = seg[k], c = seg[k + 1];
+            if (a > c) {
+                seg[k] = c;
+                seg[k + 1] = a;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Row-major owner sums: warp per bucket, lanes over columns of a panel of
+// 32 * KC columns (grid.y walks the panels).
+template <Elem E, int KC>
+__global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void* lo, int64_t n,
+                                                      int64_t ld, int64_t s,
+                                                      const int32_t* __restrict__ offsets,
+                                                      const int32_t* __restrict__ perm,
+                                                      const int8_t* __restrict__ sign,
+                                                      double* __restrict__ SA, int64_t ld_sa,
+                                                      double* __restrict__ fro_part) {
+    __shared__ double smf[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t b = (int64_t)blockIdx.x * 8 + w;
+    const int64_t c0 = (int64_t)blockIdx.y * 32 * KC;
+    double acc[KC];
+#pragma unroll
+    for (int k = 0; k < KC; ++k) acc[k] = 0.0;
+    double f2 = 0.0;
+    if (b < s) {
+        const int32_t o0 = offsets[b], o1 = offsets[b + 1];
+        for (int32_t q = o0; q < o1; ++q) {
+            const int32_t r = perm[q];
+            const double sg = (double)sign[r];
+            const size_t base = (size_t)r * ld;
+#pragma unroll
+            for (int k = 0; k < KC; ++k) {
+                const int64_t j = c0 + k * 32 + lane;
+                if (j < n) {
+                    const double a = (double)load_elem<E>(hi, lo, base + j);
+                    acc[k] += sg * a;
+                    f2 += a * a;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+            const int64_t j = c0 + k * 32 + lane;
+            if (j < n) SA[(size_t)j * ld_sa + b] = acc[k];
+        }
+    }
+    f2 = warp_sum(f2);
+    if (lane == 0) smf[w] = f2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t += smf[k];
+        fro_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// Column-major owner sums: block per column, warps over buckets, lanes
+// over the bucket's rows (gathered down the contiguous column).
+template <Elem E>
+__global__ void __launch_bounds__(256) cs_cols_kernel(const void* hi, const void* lo, int64_t n,
+                                                      int64_t ld, int64_t s,
+                                                      const int32_t* __restrict__ offsets,
+                                                      const int32_t* __restrict__ perm,
+                                                      const int8_t* __restrict__ sign,
+                                                      double* __restrict__ SA, int64_t ld_sa,
+                                                      double* __restrict__ fro_part) {
+    __shared__ double smf[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t j = blockIdx.x;
+    const size_t cbase = (size_t)j * ld;
+    double f2 = 0.0;
+    for (int64_t b = w; b < s; b += 8) {
+        const int32_t o0 = offsets[b], o1 = offsets[b + 1];
+        double acc = 0.0;
+        for (int32_t q = o0 + lane; q < o1; q += 32) {
+            const int32_t r = perm[q];
+            const double a = (double)load_elem<E>(hi, lo, cbase + r);
+            acc += (double)sign[r] * a;
+            f2 += a * a;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) SA[(size_t)j * ld_sa + b] = acc;
+    }
+    f2 = warp_sum(f2);
+    if (lane == 0) smf[w] = f2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t += smf[k];
+        fro_part[blockIdx.x] = t;
+    }
+}
+
+__global__ void cs_fro_reduce_kernel(const double* __restrict__ part, int64_t np,
+                                     double* __restrict__ out) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int64_t k = threadIdx.x; k < np; k += blockDim.x) s += part[k];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) *out = t;
+    }
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+CsScratch cs_layout(void* base, int64_t m, int64_t s, int64_t fro_parts) {
+    CsScratch c;
+    size_t off = 0;
+    char* p = static_cast<char*>(base);
+    auto take = [&](size_t bytes) {
+        char* q = p ? p + off : nullptr;
+        off += align256(bytes);
+        return q;
+    };
+    c.bucket = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (m > 0 ? m : 1)));
+    c.sign = reinterpret_cast<int8_t*>(take(m > 0 ? m : 1));
+    c.counts = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (s + 1)));
+    c.offsets = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (s + 1)));
+    c.cursor = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (s + 1)));
+    c.perm = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (m > 0 ? m : 1)));
+    c.fro_part = reinterpret_cast<double*>(take(sizeof(double) * (fro_parts > 0 ? fro_parts : 1)));
+    c.bytes = off;
+    return c;
+}
+
+// Upper bound of the owner-sum partial count over both layouts and the
+// CSR path, so one size query serves all callers.
+int64_t cs_fro_parts(int64_t m, int64_t s) {
+    (void)m;
+    const int64_t rows = ((s + 7) / 8) * 64;  // row-major: blocks x panels (n <= 64 panels cap)
+    const int64_t csr = (s + 7) / 8;
+    int64_t v = rows > csr ? rows : csr;
+    return v < 65536 ? 65536 : v;  // column-major: one per column (n <= 65536)
+}
+
+static bool cs_grid(int64_t m, int* g) {
+    int64_t b = (m + 255) / 256;
+    int64_t cap = (int64_t)sm_count() * 8;
+    if (b > cap) b = cap;
+    *g = (int)(b < 1 ? 1 : b);
+    return true;
+}
+
+// Steps 1-4 (shared by the dense and CSR owner sums).
+tomos_status cs_bucketize(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed, const CsScratch& c,
+                          cudaStream_t st) {
+    int g;
+    cs_grid(m, &g);
+    TOMOS_CUDA_TRY(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * (s + 1), st));
+    TOMOS_CUDA_TRY(cudaMemsetAsync(c.cursor, 0, sizeof(int32_t) * (s + 1), st));
+    cs_hash_kernel<<<g, 256, 0, st>>>(m, s, bseed, sseed, c.bucket, c.sign, c.counts);
+    TOMOS_LAUNCH_CHECK("cs_hash_kernel");
+    cs_scan_kernel<<<1, 1024, 0, st>>>(c.counts, s, c.offsets);
+    TOMOS_LAUNCH_CHECK("cs_scan_kernel");
+    cs_scatter_kernel<<<g, 256, 0, st>>>(m, c.bucket, c.offsets, c.cursor, c.perm);
+    TOMOS_LAUNCH_CHECK("cs_scatter_kernel");
+    cs_sort_kernel<<<(unsigned)((s + 7) / 8), 256, 0, st>>>(s, c.offsets, c.perm);
+    TOMOS_LAUNCH_CHECK("cs_sort_kernel");
+    return TOMOS_OK;
+}
+
+template <Elem E>
+static void launch_rows(const tomos_dense* A, const void* lo, int64_t s, const CsScratch& c,
+                        double* SA, int64_t ld_sa, unsigned gx, unsigned panels, cudaStream_t st) {
+    dim3 grid(gx, panels);
+    cs_rows_kernel<E, 8><<<grid, 256, 0, st>>>(A->values, lo, A->cols, A->ld, s, c.offsets, c.perm,
+                                               c.sign, SA, ld_sa, c.fro_part);
+}
+
+template <Elem E>
+static void launch_cols(const tomos_dense* A, const void* lo, int64_t s, const CsScratch& c,
+                        double* SA, int64_t ld_sa, cudaStream_t st) {
+    cs_cols_kernel<E><<<(unsigned)A->cols, 256, 0, st>>>(A->values, lo, A->cols, A->ld, s, c.offsets,
+                                                         c.perm, c.sign, SA, ld_sa, c.fro_part);
+}
+
+}  // namespace tomos_b200
+
+using namespace tomos_b200;
+
+extern "C" {
+
+tomos_status tomos_countsketch_hash(int64_t m, int64_t s, uint64_t bucket_seed, uint64_t sign_seed,
+                                    int32_t* bucket, int8_t* sign, void* stream) {
+    if (m < 0 || s <= 0) return fail(TOMOS_ERR_INVALID, "countsketch_hash: need m >= 0, s > 0");
+    if (m == 0) return TOMOS_OK;
+    if (m > 0x7fffffffLL) return fail(TOMOS_ERR_INVALID, "countsketch_hash: m exceeds int32");
+    if (!bucket || !sign) return fail(TOMOS_ERR_INVALID, "countsketch_hash: null output");
+    int g;
+    cs_grid(m, &g);
+    cs_hash_kernel<<<g, 256, 0, as_stream(stream)>>>(m, s, bucket_seed, sign_seed, bucket, sign,
+                                                     nullptr);
+    TOMOS_LAUNCH_CHECK("cs_hash_kernel");
+    return TOMOS_OK;
+}
+
+size_t tomos_countsketch_scratch_bytes(int64_t m, int64_t s) {
+    if (m < 0 || s <= 0) return 0;
+    return cs_layout(nullptr, m, s, cs_fro_parts(m, s)).bytes;
+}
+
+tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t s,
+                                     uint64_t bucket_seed, uint64_t sign_seed, double* SA,
+                                     int64_t ld_sa, double* fro2, void* scratch,
+                                     size_t scratch_bytes, void* stream) {
+    if (!A || s <= 0) return fail(TOMOS_ERR_INVALID, "countsketch_apply: need A and s > 0");
+    if (A->layout != TOMOS_ROW_MAJOR && A->layout != TOMOS_COL_MAJOR)
+        return fail(TOMOS_ERR_INVALID, "countsketch_apply: bad layout");
+    const int64_t m = A->rows, n = A->cols;
+    if (m < 0 || n < 0) return fail(TOMOS_ERR_INVALID, "countsketch_apply: negative size");
+    if (m > 0x7fffffffLL) return fail(TOMOS_ERR_INVALID, "countsketch_apply: m exceeds int32");
+    if (ld_sa < s) return fail(TOMOS_ERR_INVALID, "countsketch_apply: ld_sa < s");
+    const int64_t inner = A->layout == TOMOS_ROW_MAJOR ? n : m;
+    if (A->ld < inner) return fail(TOMOS_ERR_INVALID, "countsketch_apply: bad leading dimension");
+    if (A->layout == TOMOS_COL_MAJOR && n > 65536)
+        return fail(TOMOS_ERR_INVALID, "countsketch_apply: column-major n > 65536");
+    if (A->layout == TOMOS_ROW_MAJOR && n > 64 * 256)
+        return fail(TOMOS_ERR_INVALID, "countsketch_apply: row-major n > 16384");
+    Elem e;
+    std::string why;
+    if (!resolve_elem(A, tier, &e, &why)) return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply: " + why);
+    cudaStream_t st = as_stream(stream);
+    if (n == 0) return TOMOS_OK;
+    if (!SA) return fail(TOMOS_ERR_INVALID, "countsketch_apply: null SA");
+    if (m == 0) {
+        for (int64_t j = 0; j < n; ++j)
+            TOMOS_CUDA_TRY(cudaMemsetAsync(SA + j * ld_sa, 0, sizeof(double) * s, st));
+        if (fro2) TOMOS_CUDA_TRY(cudaMemsetAsync(fro2, 0, sizeof(double), st));
+        return TOMOS_OK;
+    }
+    CsScratch need = cs_layout(nullptr, m, s, cs_fro_parts(m, s));
+    if (!scratch || scratch_bytes < need.bytes)
+        return fail(TOMOS_ERR_INVALID, "countsketch_apply: scratch too small (need " +
+                                           std::to_string(need.bytes) + " bytes)");
+    CsScratch c = cs_layout(scratch, m, s, cs_fro_parts(m, s));
+    tomos_status rc = cs_bucketize(m, s, bucket_seed, sign_seed, c, st);
+    if (rc) return rc;
+    const void* lo = (e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R) ? dense_lo_plane(A)
+                                                                             : nullptr;
+    int64_t nparts;
+    if (A->layout == TOMOS_ROW_MAJOR) {
+        const unsigned gx = (unsigned)((s + 7) / 8);
+        const unsigned panels = (unsigned)((n + 255) / 256);
+        switch (e) {
+            case Elem::F32: launch_rows<Elem::F32>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
+            case Elem::H16: launch_rows<Elem::H16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
+            case Elem::A16: launch_rows<Elem::A16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
+            case Elem::B16: launch_rows<Elem::B16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
+            case Elem::AB16: launch_rows<Elem::AB16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
+            case Elem::AB16R: launch_rows<Elem::AB16R>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
+            default: return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply: element type");
+        }
+        nparts = (int64_t)gx * panels;
+    } else {
+        switch (e) {
+            case Elem::F32: launch_cols<Elem::F32>(A, lo, s, c, SA, ld_sa, st); break;
+            case Elem::H16: launch_cols<Elem::H16>(A, lo, s, c, SA, ld_sa, st); break;
+            case Elem::A16: launch_cols<Elem::A16>(A, lo, s, c, SA, ld_sa, st); break;
+            case Elem::B16: launch_cols<Elem::B16>(A, lo, s, c, SA, ld_sa, st); break;
+            case Elem::AB16: launch_cols<Elem::AB16>(A, lo, s, c, SA, ld_sa, st); break;
+            case Elem::AB16R: launch_cols<Elem::AB16R>(A, lo, s, c, SA, ld_sa, st); break;
+            default: return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply: element type");
+        }
+        nparts = n;
+    }
+    TOMOS_LAUNCH_CHECK("countsketch owner sums");
+    if (fro2) {
+        cs_fro_reduce_kernel<<<1, 256, 0, st>>>(c.fro_part, nparts, fro2);
+        TOMOS_LAUNCH_CHECK("cs_fro_reduce_kernel");
+    }
+    return TOMOS_OK;
+}
+
+}  // extern "C"
