@@ -163,18 +163,20 @@ tomos_status tomos_countsketch_hash(int64_t m, int64_t s, uint64_t bucket_seed,
  * reference omits, sketch_registries.cpp:29-41).  Deterministic: each
  * bucket is summed by one owner in increasing row order, FP64
  * accumulation.  Packed A is read at `tier` (HALF reads only wh).
- * fro2 (device, may be NULL) receives sum(A_ij^2) of the values read. */
-size_t tomos_countsketch_scratch_bytes(int64_t m, int64_t s);
+ * fro2 (device, may be NULL) receives sum(A_ij^2) of the values read and
+ * colsq (device, may be NULL, cols entries) the sum of squares of every
+ * column, both in the same pass. */
+size_t tomos_countsketch_scratch_bytes(int64_t m, int64_t cols, int64_t s);
 tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t s,
                                      uint64_t bucket_seed, uint64_t sign_seed,
                                      double* SA, int64_t ld_sa, double* fro2,
-                                     void* scratch, size_t scratch_bytes,
-                                     void* stream);
+                                     double* colsq, void* scratch,
+                                     size_t scratch_bytes, void* stream);
 tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64_t s,
                                          uint64_t bucket_seed, uint64_t sign_seed,
                                          double* SA, int64_t ld_sa, double* fro2,
-                                         void* scratch, size_t scratch_bytes,
-                                         void* stream);
+                                         double* colsq, void* scratch,
+                                         size_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------- sketch QR */
 
@@ -196,7 +198,12 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
  * the normwise backward error
  *   eta = min( ||r|| / (||A||_F ||x|| + ||b||),  ||A^T r|| / (||A||_F ||r||) )
  * of the current x, recomputed from an ACCURATE-tier residual at every
- * restart boundary, is <= tol. */
+ * restart boundary, is <= tol.  With a column scale D (opts.col_scale) the
+ * same quantity is taken for the column-scaled problem (A D^{-1}, b, D x):
+ *   eta_D = min( ||r|| / (||A D^{-1}||_F ||D x|| + ||b||),
+ *                ||D^{-1} A^T r|| / (||A D^{-1}||_F ||r||) ),
+ * which is invariant to the scaling of A's columns; with D the column
+ * norms it is the backward error of the equilibrated problem. */
 enum tomos_stop { TOMOS_STOP_RELRES = 0, TOMOS_STOP_BACKWARD = 1 };
 
 typedef struct tomos_lsqr_opts {
@@ -213,13 +220,20 @@ typedef struct tomos_lsqr_opts {
     double inner_rtol;       /* BACKWARD rule: an inner cycle ends once its
                                 residual estimate fell by this factor (0 =
                                 run max_iters)                              */
-    double anorm_fro;        /* ||A||_F if already known (e.g. from
-                                tomos_countsketch_apply's fro2); 0 = the
-                                BACKWARD rule computes it (one pass)        */
+    double anorm_fro;        /* ||A||_F (||A D^{-1}||_F with a column
+                                scale) if already known, e.g. from
+                                tomos_countsketch_apply; 0 = the BACKWARD
+                                rule computes it (one pass)                  */
+    const double* col_scale; /* device, n entries, may be NULL: the column
+                                scale D of the BACKWARD rule                 */
     double* history;         /* host, may be NULL: |phi_bar|/||b|| per
                                 completed iteration (residual_history)     */
     int32_t history_cap;
-    int32_t reserved;
+    int32_t profile;         /* nonzero: time every pass over A with CUDA
+                                events on the solver stream (the reference's
+                                TOMOS_LSQR_TIMING buckets, lsqr.cpp:85-166);
+                                iterations then run as plain launches
+                                instead of graph replays                    */
 } tomos_lsqr_opts;
 
 typedef struct tomos_lsqr_report {
@@ -235,8 +249,16 @@ typedef struct tomos_lsqr_report {
     double bnorm;
     double backward_error;   /* eta of the returned x (accurate residual)   */
     double elapsed_ms;       /* device time of the solve                    */
-    int32_t accurate_passes; /* ACCURATE-tier passes over A                 */
-    int32_t half_passes;     /* HALF-tier passes over A                     */
+    int32_t accurate_passes; /* restart-boundary passes over A              */
+    int32_t half_passes;     /* per-iteration passes over A                 */
+    double iter_pass_ms;     /* profile: total device time of the
+                                per-iteration passes over A                 */
+    double init_pass_ms;     /* profile: same for the restart passes        */
+    int32_t iter_pass_count;
+    int32_t init_pass_count;
+    int32_t kernel_launches; /* kernels the solve enqueued (graph replays
+                                counted per kernel)                          */
+    int32_t reserved;
 } tomos_lsqr_report;
 
 typedef struct tomos_workspace tomos_workspace;
@@ -264,11 +286,13 @@ tomos_status tomos_lsqr_solve_csr(const tomos_csr* A, const float* b, float* x,
                                   tomos_lsqr_report* report, void* stream);
 
 /* Normwise backward error of x (FP64, ACCURATE tier): fills report's
- * rnorm, arnorm, anorm_fro, xnorm, bnorm and backward_error.  Needs a
+ * rnorm, arnorm, anorm_fro, xnorm, bnorm and backward_error.  col_scale
+ * (device, may be NULL) selects eta_D (see the stopping rules).  Needs a
  * workspace of A's shape for its partials. */
 tomos_status tomos_backward_error_dense(const tomos_dense* A, const float* b,
-                                        const float* x, tomos_workspace* ws,
-                                        tomos_lsqr_report* report, void* stream);
+                                        const float* x, const double* col_scale,
+                                        tomos_workspace* ws, tomos_lsqr_report* report,
+                                        void* stream);
 
 #ifdef __cplusplus
 }

@@ -229,6 +229,16 @@ def backward_error(A, b, x):
     return min(e1, e2)
 
 
+def backward_error_scaled(A, b, x, d=None):
+    """eta_D: the backward error of the column-scaled problem (A D^{-1}, b,
+    D x), D = column norms of A by default (FP64)."""
+    A = np.asarray(A, np.float64)
+    if d is None:
+        d = np.linalg.norm(A, axis=0)
+        d = np.where(d > 0, d, 1.0)
+    return backward_error(A / d, b, np.asarray(x, np.float64) * d)
+
+
 def lsqr_f32(A, b, Rinv=None, tol=1e-6, max_iters=400, max_relres=1e-6, restarts=1):
     """Plain FP32 LSQR restated from the reference (oracle.c or_lsqr_f32).
     Returns (x, iterations, history)."""

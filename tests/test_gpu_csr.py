@@ -62,7 +62,8 @@ def test_csr_countsketch(orc):
     m, n, s = 4000, 300, 211
     rp, ci, v, D = random_csr(m, n, 12, 5)
     A = make(rp, ci, v, m, n)
-    SA, fro2 = tb.apply_count_sketch(A, s)
+    SA, fro2, colsq = tb.apply_count_sketch(A, s, with_colsq=True)
+    np.testing.assert_allclose(colsq.cpu().numpy(), (D.astype(np.float64) ** 2).sum(0), rtol=1e-12)
     ref = orc.countsketch_apply(D, s)
     np.testing.assert_allclose(SA.view().cpu().numpy(), ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
     np.testing.assert_allclose(fro2.item(), (v.astype(np.float64) ** 2).sum(), rtol=1e-12)
@@ -76,13 +77,16 @@ def test_csr_lsqr_preconditioned(orc, numeric):
     xt = rng.standard_normal(n)
     b = (D.astype(np.float64) @ xt + 1e-8 * rng.standard_normal(m)).astype(np.float32)
     A = make(rp, ci, v, m, n, numeric)
-    SA, fro2 = tb.apply_count_sketch(A, 4 * n, tier=tb.Tier.AUTO)
+    SA, fro2, colsq = tb.apply_count_sketch(A, 4 * n, tier=tb.Tier.AUTO, with_colsq=True)
     Rinv = tb.generate_sketch_qr_precond(SA)
+    d, an = tb.column_scale(colsq)
     ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32, NT.FP64)
     tb.add_precond(Rinv, ws)
     x = torch.zeros(n, device="cuda")
     rep = tb.lsqr_solve(None, A, cuda(b), x, ws, 1e-6, 200, 0.0, restarts=6,
-                        stop_rule=tb.StopRule.BACKWARD, inner_rtol=1e-3 if numeric != NT.FP32 else 0.0)
+                        stop_rule=tb.StopRule.BACKWARD, inner_rtol=1e-3 if numeric != NT.FP32 else 0.0,
+                        col_scale=d, anorm_fro=an)
     xx = x.cpu().numpy()
-    eta = orc.backward_error(D, b, xx)
+    eta = orc.backward_error_scaled(D, b, xx)
     assert rep["converged"] == 1 and eta <= 1.05e-6, (eta, rep)
+    assert orc.backward_error(D, b, xx) <= eta * 1.01

@@ -8,7 +8,7 @@ import pytest
 import torch
 
 import tomos_b200 as tb
-from gpu_util import to_dense, cuda
+from gpu_util import to_dense, cuda, decoded
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 pytestmark = pytest.mark.gpu
@@ -89,9 +89,10 @@ def test_known_systems():
     np.testing.assert_allclose(x, [3.5, 1.4], atol=1e-5)
 
 
-def gpu_precond(A, s, seed_shift=0):
-    SA, fro2 = tb.apply_count_sketch(A, s, tier=tb.Tier.AUTO)
-    return tb.generate_sketch_qr_precond(SA), fro2.item()
+def gpu_precond(A, s):
+    SA, fro2, colsq = tb.apply_count_sketch(A, s, tier=tb.Tier.AUTO, with_colsq=True)
+    d, an = tb.column_scale(colsq)
+    return tb.generate_sketch_qr_precond(SA), d, an
 
 
 def scaled_problem(m, n, seed, decades=2.0):
@@ -105,19 +106,42 @@ def scaled_problem(m, n, seed, decades=2.0):
 @pytest.mark.parametrize("numeric", [NT.FP32, NT.FP32_16, NT.FP32_BF16])
 @pytest.mark.parametrize("layout", [L.ROW_MAJOR, L.COL_MAJOR])
 def test_preconditioned_backward_error(orc, numeric, layout):
-    """Sketch-preconditioned LSQR to normwise backward error 1e-6 (FP64
-    oracle check), with FP32 residual refinement for packed storage."""
+    """Sketch-preconditioned LSQR to backward error 1e-6 of the
+    column-scaled problem (FP64 oracle check), with FP32 residual
+    refinement for packed storage; the plain normwise backward error is
+    then below it too."""
     A0, b = scaled_problem(30000, 250, 3)
     A = to_dense(A0, layout, numeric)
-    Rinv, fro2 = gpu_precond(A, 1000)
+    Rinv, d, an = gpu_precond(A, 1000)
     x, rep = solve(A, b, Rinv, tol=1e-6, max_iters=100, restarts=6,
-                   stop_rule=tb.StopRule.BACKWARD, inner_rtol=1e-3 if numeric != NT.FP32 else 0.0)
-    eta = orc.backward_error(A0, b, x)
+                   stop_rule=tb.StopRule.BACKWARD, inner_rtol=1e-3 if numeric != NT.FP32 else 0.0,
+                   col_scale=d, anorm_fro=an)
+    eta = orc.backward_error_scaled(A0, b, x)
     assert rep["converged"] == 1, rep
     assert eta <= 1.05e-6, (eta, rep)
     assert abs(rep["backward_error"] - eta) <= 0.05 * eta + 1e-9
+    assert orc.backward_error(A0, b, x) <= eta * 1.01
     xs = orc.lstsq_f64(A0, b)
     assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-2
+
+
+@pytest.mark.parametrize("numeric", [NT.FP32, NT.FP32_16, NT.FP32_BF16])
+@pytest.mark.parametrize("n,ld", [(257, 264), (1000, 1000), (1001, 1008), (500, 512)])
+def test_fused_pass_matches_oracle_lsqr(orc, numeric, n, ld):
+    """The TMA-staged fused pass (row-major, one CTA per SM) against the
+    oracle's LSQR on the values the tier reads: the same 6 iterations give
+    the same x (FP32 arithmetic in both, different summation order)."""
+    m = 6000
+    rng = np.random.default_rng(n)
+    A0 = (rng.standard_normal((m, n)) * np.where(rng.random((m, n)) < 0.02, 1e-6, 1.0)).astype(np.float32)
+    b = rng.standard_normal(m).astype(np.float32)
+    A = to_dense(A0, L.ROW_MAJOR, numeric, pad=ld - n)
+    Ad = decoded(orc, A, tb.Tier.HALF if numeric != NT.FP32 else tb.Tier.AUTO).astype(np.float32)
+    x_ref, it_ref, h_ref = orc.lsqr_f32(Ad, b, None, 0.0, 6, 0.0, 1)
+    x, rep = solve(A, b, tol=0.0, max_iters=6, max_relres=0.0)
+    assert rep["iterations"] == it_ref == 6
+    np.testing.assert_allclose(rep["history"][:6], h_ref[:6], rtol=1e-4)
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-4
 
 
 def test_backward_error_entry(orc):
@@ -127,6 +151,9 @@ def test_backward_error_entry(orc):
     ws = tb.create_lsqr_workspace(None, A.size, NT.FP32)
     rep = tb.backward_error(A, cuda(b), cuda(x), ws)
     np.testing.assert_allclose(rep["backward_error"], orc.backward_error(A0, b, x), rtol=1e-6)
+    d = np.linalg.norm(A0.astype(np.float64), axis=0)
+    rep = tb.backward_error(A, cuda(b), cuda(x), ws, col_scale=cuda(d, torch.float64))
+    np.testing.assert_allclose(rep["backward_error"], orc.backward_error_scaled(A0, b, x), rtol=1e-6)
 
 
 def test_errors():

@@ -34,8 +34,9 @@ def test_apply_vs_oracle(orc, numeric, tier, layout):
     m, n, s = 5003, 301, 97
     A0 = (rng.standard_normal((m, n)) * np.logspace(-2, 2, n)).astype(np.float32)
     A = to_dense(A0, layout, numeric, pad=3)
-    SA, fro2 = tb.apply_count_sketch(A, s, tier=tier)
+    SA, fro2, colsq = tb.apply_count_sketch(A, s, tier=tier, with_colsq=True)
     Ad = decoded(orc, A, tier).astype(np.float32)
+    np.testing.assert_allclose(colsq.cpu().numpy(), (Ad.astype(np.float64) ** 2).sum(0), rtol=1e-12)
     ref = orc.countsketch_apply(Ad, s, row_major=True)
     got = SA.view().cpu().numpy()
     if layout == L.ROW_MAJOR:

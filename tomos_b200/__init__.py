@@ -21,6 +21,7 @@ __all__ = [
     "Csr", "Workspace", "create_lsqr_workspace", "add_precond", "lsqr_solve", "mv_apply",
     "split_fp32_16", "combine_fp32_16", "split_fp32_bf16", "combine_fp32_bf16",
     "countsketch_hash", "apply_count_sketch", "generate_sketch_qr_precond", "backward_error",
+    "column_scale",
     "TomosError", "CS_BUCKET_SEED", "CS_SIGN_SEED", "NO_TRANSPOSE", "TRANSPOSE",
 ]
 
@@ -340,18 +341,22 @@ def countsketch_hash(m, s, bucket_seed=CS_BUCKET_SEED, sign_seed=CS_SIGN_SEED, s
 
 
 def apply_count_sketch(A, s, tier=Tier.AUTO, bucket_seed=CS_BUCKET_SEED, sign_seed=CS_SIGN_SEED,
-                       stream=None):
-    """SA = S A (s x n, column-major FP64 Dense) and ||A||_F^2 of the values read."""
+                       with_colsq=False, stream=None):
+    """SA = S A (s x n, column-major FP64 Dense) and ||A||_F^2 of the values
+    read; with_colsq also returns the column sums of squares (same pass)."""
     n = A.size[1]
     SA = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (s, n))
     fro2 = torch.zeros(1, dtype=torch.float64, device="cuda")
+    colsq = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda") if with_colsq else None
     m = A.size[0]
-    nb = C.lib().tomos_countsketch_scratch_bytes(m, s)
+    nb = C.lib().tomos_countsketch_scratch_bytes(m, n, s)
     scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
     d = A.desc()
     fn = C.lib().tomos_countsketch_apply_csr if isinstance(A, Csr) else C.lib().tomos_countsketch_apply
     C.check(fn(ctypes.byref(d), int(tier), s, bucket_seed, sign_seed, _ptr(SA.storage), s,
-               _ptr(fro2), _ptr(scratch), nb, _stream(stream)), "apply_count_sketch")
+               _ptr(fro2), _ptr(colsq), _ptr(scratch), nb, _stream(stream)), "apply_count_sketch")
+    if with_colsq:
+        return SA, fro2, colsq[:n]
     return SA, fro2
 
 
@@ -428,7 +433,8 @@ def add_precond(precond, workspace):
 
 def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=None,
                residual_history=None, restarts=1, stop_rule=StopRule.RELRES, inner_rtol=0.0,
-               anorm_fro=0.0, warm_start=False, tier=None, stream=None):
+               anorm_fro=0.0, warm_start=False, tier=None, profile=False, col_scale=None,
+               stream=None):
     """include/core/solver.hpp:68-78.  A: Dense or Csr on the device; b, x:
     FP32 Dense column vectors or float32 CUDA tensors.  iterations and
     residual_history, when lists, receive the reference's out-parameters.
@@ -449,6 +455,8 @@ def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=N
     opts.warm_start = 1 if warm_start else 0
     opts.inner_rtol = float(inner_rtol)
     opts.anorm_fro = float(anorm_fro)
+    opts.profile = 1 if profile else 0
+    opts.col_scale = col_scale.data_ptr() if col_scale is not None else None
     cap = max(1, int(max_iters) * int(restarts) + int(restarts))
     hist = (ctypes.c_double * cap)()
     opts.history = hist
@@ -467,11 +475,22 @@ def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=N
     return out
 
 
-def backward_error(A, b, x, workspace, stream=None):
-    """Normwise backward error of x (FP64, accurate tier)."""
+def backward_error(A, b, x, workspace, col_scale=None, stream=None):
+    """Normwise backward error of x (FP64, accurate tier); with col_scale D
+    (float64 CUDA tensor) the backward error of the column-scaled problem."""
     rep = C.LsqrReport()
     d = A.desc()
     C.check(C.lib().tomos_backward_error_dense(ctypes.byref(d), _ptr(_vec(b)), _ptr(_vec(x)),
-                                               workspace.handle, ctypes.byref(rep),
-                                               _stream(stream)), "backward_error")
+                                               _ptr(col_scale), workspace.handle,
+                                               ctypes.byref(rep), _stream(stream)),
+            "backward_error")
     return rep.as_dict()
+
+
+def column_scale(colsq):
+    """D = column norms from column sums of squares (zero columns -> 1), and
+    ||A D^{-1}||_F for it."""
+    d = torch.sqrt(colsq.double())
+    nz = d > 0
+    d = torch.where(nz, d, torch.ones_like(d))
+    return d, float(torch.sqrt(nz.sum().double()).item())

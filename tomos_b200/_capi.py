@@ -44,8 +44,8 @@ class LsqrOpts(ctypes.Structure):
     _fields_ = [("tol", c_dbl), ("max_iters", c_i32), ("restarts", c_i32),
                 ("max_relres", c_dbl), ("stop_rule", c_i32), ("iter_tier", c_i32),
                 ("implicit_duplicate", c_i32), ("warm_start", c_i32), ("inner_rtol", c_dbl),
-                ("anorm_fro", c_dbl), ("history", ctypes.POINTER(c_dbl)),
-                ("history_cap", c_i32), ("reserved", c_i32)]
+                ("anorm_fro", c_dbl), ("col_scale", c_vp), ("history", ctypes.POINTER(c_dbl)),
+                ("history_cap", c_i32), ("profile", c_i32)]
 
 
 class LsqrReport(ctypes.Structure):
@@ -53,7 +53,9 @@ class LsqrReport(ctypes.Structure):
                 ("history_len", c_i32), ("relres", c_dbl), ("rnorm", c_dbl), ("arnorm", c_dbl),
                 ("anorm_fro", c_dbl), ("xnorm", c_dbl), ("bnorm", c_dbl),
                 ("backward_error", c_dbl), ("elapsed_ms", c_dbl), ("accurate_passes", c_i32),
-                ("half_passes", c_i32)]
+                ("half_passes", c_i32), ("iter_pass_ms", c_dbl), ("init_pass_ms", c_dbl),
+                ("iter_pass_count", c_i32), ("init_pass_count", c_i32),
+                ("kernel_launches", c_i32), ("reserved", c_i32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -78,11 +80,11 @@ SIGNATURES = {
     "tomos_csr_gemv": (c_i32, [c_i32, c_dbl, ctypes.POINTER(CsrDesc), c_i32, c_vp, c_dbl, c_vp,
                                c_vp, c_sz, c_vp]),
     "tomos_countsketch_hash": (c_i32, [c_i64, c_i64, c_u64, c_u64, c_vp, c_vp, c_vp]),
-    "tomos_countsketch_scratch_bytes": (c_sz, [c_i64, c_i64]),
+    "tomos_countsketch_scratch_bytes": (c_sz, [c_i64, c_i64, c_i64]),
     "tomos_countsketch_apply": (c_i32, [ctypes.POINTER(DenseDesc), c_i32, c_i64, c_u64, c_u64,
-                                        c_vp, c_i64, c_vp, c_vp, c_sz, c_vp]),
+                                        c_vp, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
     "tomos_countsketch_apply_csr": (c_i32, [ctypes.POINTER(CsrDesc), c_i32, c_i64, c_u64, c_u64,
-                                            c_vp, c_i64, c_vp, c_vp, c_sz, c_vp]),
+                                            c_vp, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
     "tomos_sketch_qr_scratch_bytes": (c_sz, [c_i64, c_i64]),
     "tomos_sketch_qr_precond_f64": (c_i32, [c_i64, c_i64, c_vp, c_i64, c_vp, c_vp, c_sz, c_vp]),
     "tomos_workspace_create": (c_i32, [c_i64, c_i64, c_i32, c_i32, ctypes.POINTER(c_vp)]),
@@ -93,7 +95,7 @@ SIGNATURES = {
                                        c_vp]),
     "tomos_lsqr_solve_csr": (c_i32, [ctypes.POINTER(CsrDesc), c_vp, c_vp, c_vp,
                                      ctypes.POINTER(LsqrOpts), ctypes.POINTER(LsqrReport), c_vp]),
-    "tomos_backward_error_dense": (c_i32, [ctypes.POINTER(DenseDesc), c_vp, c_vp, c_vp,
+    "tomos_backward_error_dense": (c_i32, [ctypes.POINTER(DenseDesc), c_vp, c_vp, c_vp, c_vp,
                                            ctypes.POINTER(LsqrReport), c_vp]),
 }
 

@@ -236,9 +236,10 @@ struct CsrPass : PassOps {
         P.sspart = ws->sspart;
         P.skip = skip;
         P.write_u = 1;
+        ws->launches += 1;
         return launch_csr(pl.e, pl.acc64, P, pl.grid, pl.nch, st);
     }
-    tomos_status fro2(double* out, cudaStream_t st) override;
+    tomos_status fro2(double* out, const double* d, cudaStream_t st) override;
     uint64_t key() override {
         return reinterpret_cast<uint64_t>(A->values) ^ (reinterpret_cast<uint64_t>(A->col_idxs) << 1);
     }
@@ -247,12 +248,14 @@ struct CsrPass : PassOps {
 };
 
 template <Elem E>
-__global__ void csr_fro2_kernel(const void* hi, const void* lo, int64_t nnz, double* part) {
+__global__ void csr_fro2_kernel(const void* hi, const void* lo, const int32_t* col_idxs,
+                                const double* d, int64_t nnz, double* part) {
     __shared__ double sm[8];
     double s = 0.0;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
          k += (int64_t)gridDim.x * blockDim.x) {
         double v = load_elem<E>(hi, lo, k);
+        if (d) v /= d[col_idxs[k]];
         s += v * v;
     }
     s = warp_sum(s);
@@ -273,18 +276,21 @@ __global__ void csr_sum_kernel(const double* part, int np, double* out) {
     }
 }
 
-tomos_status CsrPass::fro2(double* out, cudaStream_t st) {
+tomos_status CsrPass::fro2(double* out, const double* d, cudaStream_t st) {
     const int g = ws->gs_max;
     const void* lo = elem_is_exact(init_e) ? csr_lo(A) : nullptr;
+    const int32_t* ci = static_cast<const int32_t*>(A->col_idxs);
+#define TOMOS_CFRO(EE) csr_fro2_kernel<EE><<<g, 256, 0, st>>>(A->values, lo, ci, d, A->nnz, ws->bpart)
     switch (init_e) {
-        case Elem::F32: csr_fro2_kernel<Elem::F32><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
-        case Elem::H16: csr_fro2_kernel<Elem::H16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
-        case Elem::A16: csr_fro2_kernel<Elem::A16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
-        case Elem::B16: csr_fro2_kernel<Elem::B16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
-        case Elem::AB16: csr_fro2_kernel<Elem::AB16><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
-        case Elem::AB16R: csr_fro2_kernel<Elem::AB16R><<<g, 256, 0, st>>>(A->values, lo, A->nnz, ws->bpart); break;
+        case Elem::F32: TOMOS_CFRO(Elem::F32); break;
+        case Elem::H16: TOMOS_CFRO(Elem::H16); break;
+        case Elem::A16: TOMOS_CFRO(Elem::A16); break;
+        case Elem::B16: TOMOS_CFRO(Elem::B16); break;
+        case Elem::AB16: TOMOS_CFRO(Elem::AB16); break;
+        case Elem::AB16R: TOMOS_CFRO(Elem::AB16R); break;
         default: return fail(TOMOS_ERR_UNSUPPORTED, "csr fro2: element type");
     }
+#undef TOMOS_CFRO
     TOMOS_LAUNCH_CHECK("csr_fro2_kernel");
     csr_sum_kernel<<<1, 32, 0, st>>>(ws->bpart, g, out);
     TOMOS_LAUNCH_CHECK("csr_sum_kernel");
@@ -329,6 +335,43 @@ __global__ void cs_csr_kernel(const void* hi, const void* lo, const int32_t* row
         for (int k = 0; k < nw; ++k) t += smf[k];
         fro_part[blockIdx.x] = t;
     }
+}
+
+// Column sums of squares of a CSR matrix: CTAs own row chunks, warps
+// accumulate into private FP64 rows in shared memory (distinct columns per
+// row, no atomics), the CTA writes one partial row.
+template <Elem E>
+__global__ void csr_colsq_kernel(const void* hi, const void* lo, const int32_t* row_ptrs,
+                                 const int32_t* col_idxs, int64_t m, int64_t n, double* col_part) {
+    extern __shared__ __align__(16) double cacc[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double* acc = cacc + (size_t)w * n;
+    for (int64_t j = lane; j < n; j += 32) acc[j] = 0.0;
+    __syncwarp();
+    const int64_t per = (m + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = (int64_t)blockIdx.x * per;
+    const int64_t r1 = r0 + per < m ? r0 + per : m;
+    for (int64_t i = r0 + w; i < r1; i += nw) {
+        for (int32_t k = row_ptrs[i] + lane; k < row_ptrs[i + 1]; k += 32) {
+            const double a = load_elem<E>(hi, lo, k);
+            acc[col_idxs[k]] += a * a;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        double t = 0.0;
+        for (int k = 0; k < nw; ++k) t += cacc[(size_t)k * n + j];
+        col_part[(size_t)blockIdx.x * n + j] = t;
+    }
+}
+
+__global__ void csr_col_reduce_kernel(const double* part, int64_t nparts, int64_t n, double* colsq) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double t = 0.0;
+    for (int64_t r = 0; r < nparts; ++r) t += part[(size_t)r * n + j];
+    colsq[j] = t;
 }
 
 __global__ void cs_csr_fro_reduce(const double* part, int64_t np, double* out) {
@@ -451,7 +494,7 @@ tomos_status tomos_lsqr_solve_csr(const tomos_csr* A, const float* b, float* x,
 
 tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64_t s,
                                          uint64_t bucket_seed, uint64_t sign_seed, double* SA,
-                                         int64_t ld_sa, double* fro2, void* scratch,
+                                         int64_t ld_sa, double* fro2, double* colsq, void* scratch,
                                          size_t scratch_bytes, void* stream) {
     std::string why;
     if (!csr_ok(A, &why)) return fail(TOMOS_ERR_INVALID, "countsketch_apply_csr: " + why);
@@ -470,13 +513,15 @@ tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64
         for (int64_t j = 0; j < n; ++j)
             TOMOS_CUDA_TRY(cudaMemsetAsync(SA + j * ld_sa, 0, sizeof(double) * s, st));
         if (fro2) TOMOS_CUDA_TRY(cudaMemsetAsync(fro2, 0, sizeof(double), st));
+        if (colsq) TOMOS_CUDA_TRY(cudaMemsetAsync(colsq, 0, sizeof(double) * n, st));
         return TOMOS_OK;
     }
-    CsScratch need = cs_layout(nullptr, m, s, cs_fro_parts(m, s));
+    const int64_t col_parts = cs_col_part_rows(m, s) * n;
+    CsScratch need = cs_layout(nullptr, m, s, cs_fro_parts(m, s), col_parts);
     if (!scratch || scratch_bytes < need.bytes)
         return fail(TOMOS_ERR_INVALID, "countsketch_apply_csr: scratch too small (need " +
                                            std::to_string(need.bytes) + " bytes)");
-    CsScratch c = cs_layout(scratch, m, s, cs_fro_parts(m, s));
+    CsScratch c = cs_layout(scratch, m, s, cs_fro_parts(m, s), col_parts);
     tomos_status rc = cs_bucketize(m, s, bucket_seed, sign_seed, c, st);
     if (rc) return rc;
     const void* lo = elem_is_exact(e) ? csr_lo(A) : nullptr;
@@ -507,6 +552,33 @@ tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64
     if (fro2) {
         cs_csr_fro_reduce<<<1, 32, 0, st>>>(c.fro_part, grid, fro2);
         TOMOS_LAUNCH_CHECK("cs_csr_fro_reduce");
+    }
+    if (colsq) {
+        const int cg = csr_grid(m);
+        const int64_t cw = (int64_t)(kCsrSmemBudget / (sizeof(double) * (size_t)n));
+        const int cnw = (int)(cw > 8 ? 8 : cw);
+        const size_t csm = (size_t)cnw * n * sizeof(double);
+#define TOMOS_CSR_COLSQ(EE)                                                                      \
+    do {                                                                                         \
+        if (csm > 48 * 1024)                                                                     \
+            TOMOS_CUDA_TRY(cudaFuncSetAttribute(csr_colsq_kernel<EE>,                            \
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                                (int)csm));                                      \
+        csr_colsq_kernel<EE><<<cg, cnw * 32, csm, st>>>(A->values, lo, rp, ci, m, n, c.col_part); \
+    } while (0)
+        switch (e) {
+            case Elem::F32: TOMOS_CSR_COLSQ(Elem::F32); break;
+            case Elem::H16: TOMOS_CSR_COLSQ(Elem::H16); break;
+            case Elem::A16: TOMOS_CSR_COLSQ(Elem::A16); break;
+            case Elem::B16: TOMOS_CSR_COLSQ(Elem::B16); break;
+            case Elem::AB16: TOMOS_CSR_COLSQ(Elem::AB16); break;
+            case Elem::AB16R: TOMOS_CSR_COLSQ(Elem::AB16R); break;
+            default: break;
+        }
+#undef TOMOS_CSR_COLSQ
+        TOMOS_LAUNCH_CHECK("csr_colsq_kernel");
+        csr_col_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c.col_part, cg, n, colsq);
+        TOMOS_LAUNCH_CHECK("csr_col_reduce_kernel");
     }
     return TOMOS_OK;
 }

@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include "fused.cuh"
+#include "fused_tma.cuh"
 #include "gemv.cuh"
 #include "lsqr.cuh"
 
@@ -90,12 +91,14 @@ __global__ void sum_to_scalar_kernel(const double* __restrict__ part, int64_t np
 // read at element tag E; per-block partials.
 template <Elem E>
 __global__ void fro2_partial_kernel(const void* hi, const void* lo, int64_t outer, int64_t inner,
-                                    int64_t ld, double* part) {
+                                    int64_t ld, const double* dscale, int col_is_inner,
+                                    double* part) {
     __shared__ double sm[32];
     double s = 0.0;
     for (int64_t o = blockIdx.x; o < outer; o += gridDim.x)
         for (int64_t i = threadIdx.x; i < inner; i += blockDim.x) {
             double v = load_elem<E>(hi, lo, (size_t)o * ld + i);
+            if (dscale) v /= dscale[col_is_inner ? i : o];
             s += v * v;
         }
     s = block_sum(s, sm);
@@ -105,6 +108,19 @@ __global__ void fro2_partial_kernel(const void* hi, const void* lo, int64_t oute
 __global__ void fill_f32_kernel(float* p, int64_t n, float v) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
+}
+
+// sum of (d_i x_i)^2 (d may be NULL), one block.
+__global__ void scaled_sumsq_kernel(const float* __restrict__ x, const double* __restrict__ d,
+                                    int64_t n, double* __restrict__ out) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = (double)x[i] * (d ? d[i] : 1.0);
+        s += v * v;
+    }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) *out = s;
 }
 
 // FP64 column-major and row-major copies of a dense n x n preconditioner.
@@ -149,6 +165,7 @@ struct NSide {
     double* scal;
     LsqrDev* st;
     const int* skip;
+    const double* dscale;  // column scale D of the backward-error rule, or NULL
 };
 
 // Givens step of LSQR (lsqr.cpp:633-679), FP64.
@@ -196,7 +213,8 @@ __global__ void __launch_bounds__(256) nside_reduce_kernel(NSide S) {
                 S.vhat[j] = vh;
                 vh2 = vh * vh;
             }
-            qn = qs * qs;
+            const double qd = S.dscale ? qs / S.dscale[j] : qs;
+            qn = qd * qd;
         }
         vh2 = warp_sum(vh2);
         qn = warp_sum(qn);
@@ -272,7 +290,7 @@ __global__ void __launch_bounds__(256) nside_update_kernel(NSide S) {
                 S.wt[i] = (float)(pi - step_w * wi);
             }
             S.p[i] = (float)pi;
-            const double xf = (double)(float)xi;
+            const double xf = (double)(float)xi * (S.dscale ? S.dscale[i] : 1.0);
             xs = xf * xf;
         }
     }
@@ -357,6 +375,8 @@ static void ws_free(tomos_workspace* ws) {
     if (ws->ev_start) cudaEventDestroy(ws->ev_start);
     if (ws->ev_stop) cudaEventDestroy(ws->ev_stop);
     if (ws->ev_fence) cudaEventDestroy(ws->ev_fence);
+    if (ws->ev_pa) cudaEventDestroy(ws->ev_pa);
+    if (ws->ev_pb) cudaEventDestroy(ws->ev_pb);
     if (ws->stream) cudaStreamDestroy(ws->stream);
 }
 
@@ -390,42 +410,57 @@ static tomos_status ensure_history(tomos_workspace* ws, int cap) {
 // ------------------------------------------------------------ A passes
 
 template <Elem E, int NCH, bool ACC64>
-static void launch_fused_t(const FusedParams& P, int grid, cudaStream_t st) {
-    fused_pass_kernel<E, NCH, ACC64><<<grid, kFusedThreads, 0, st>>>(P);
+static tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
+    constexpr int VEC = ChunkElems<E>::value;
+    const int esz = (E == Elem::F32) ? 4 : 2;
+    TmaParams T;
+    T.f = P;
+    T.err = err;
+    T.copy_bytes = (int)((((int64_t)P.n * esz) + 15) / 16 * 16);
+    const size_t stage = (size_t)kTmaRows * T.copy_bytes * SmemChunk<E>::planes;
+    int ns = (int)(kTmaSmemBudget / stage);
+    if (ns > kTmaMaxStages) ns = kTmaMaxStages;
+    if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
+    T.nstage = ns;
+    const size_t smem = fused_tma_smem<E, NCH>(ns, T.copy_bytes);
+    static_assert(VEC > 0, "");
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(fused_tma_kernel<E, NCH, ACC64>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fused_tma_kernel<E, NCH, ACC64><<<grid, kTmaThreads, smem, st>>>(T);
+    TOMOS_LAUNCH_CHECK("fused_tma_kernel");
+    return TOMOS_OK;
 }
 
 template <Elem E, bool ACC64>
-static bool launch_fused_e(const FusedParams& P, int nch, int grid, cudaStream_t st) {
+static tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int grid,
+                                   cudaStream_t st) {
     switch (nch) {
-        case 1: launch_fused_t<E, 1, ACC64>(P, grid, st); return true;
-        case 2: launch_fused_t<E, 2, ACC64>(P, grid, st); return true;
-        case 4: launch_fused_t<E, 4, ACC64>(P, grid, st); return true;
+        case 1: return launch_fused_t<E, 1, ACC64>(P, err, grid, st);
+        case 2: return launch_fused_t<E, 2, ACC64>(P, err, grid, st);
+        case 4: return launch_fused_t<E, 4, ACC64>(P, err, grid, st);
         case 8:
-            if constexpr (E == Elem::F32) {
-                launch_fused_t<E, 8, ACC64>(P, grid, st);
-                return true;
-            }
-            return false;
-        default: return false;
+            if constexpr (E == Elem::F32) return launch_fused_t<E, 8, ACC64>(P, err, grid, st);
+            return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
     }
 }
 
-static bool launch_fused(Elem e, bool acc64, const FusedParams& P, int nch, int grid,
-                         cudaStream_t st) {
+static tomos_status launch_fused(Elem e, bool acc64, const FusedParams& P, int* err, int nch,
+                                 int grid, cudaStream_t st) {
     switch (e) {
         case Elem::F32:
-            return acc64 ? launch_fused_e<Elem::F32, true>(P, nch, grid, st)
-                         : launch_fused_e<Elem::F32, false>(P, nch, grid, st);
+            return acc64 ? launch_fused_e<Elem::F32, true>(P, err, nch, grid, st)
+                         : launch_fused_e<Elem::F32, false>(P, err, nch, grid, st);
         case Elem::H16:
-            return acc64 ? launch_fused_e<Elem::H16, true>(P, nch, grid, st)
-                         : launch_fused_e<Elem::H16, false>(P, nch, grid, st);
+            return acc64 ? launch_fused_e<Elem::H16, true>(P, err, nch, grid, st)
+                         : launch_fused_e<Elem::H16, false>(P, err, nch, grid, st);
         case Elem::B16:
-            return acc64 ? launch_fused_e<Elem::B16, true>(P, nch, grid, st)
-                         : launch_fused_e<Elem::B16, false>(P, nch, grid, st);
-        case Elem::A16: return launch_fused_e<Elem::A16, true>(P, nch, grid, st);
-        case Elem::AB16: return launch_fused_e<Elem::AB16, true>(P, nch, grid, st);
-        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true>(P, nch, grid, st);
-        default: return false;
+            return acc64 ? launch_fused_e<Elem::B16, true>(P, err, nch, grid, st)
+                         : launch_fused_e<Elem::B16, false>(P, err, nch, grid, st);
+        case Elem::A16: return launch_fused_e<Elem::A16, true>(P, err, nch, grid, st);
+        case Elem::AB16: return launch_fused_e<Elem::AB16, true>(P, err, nch, grid, st);
+        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true>(P, err, nch, grid, st);
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: element type");
     }
 }
 
@@ -453,7 +488,7 @@ static PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem 
     if (ok && nch > 0 && A->cols > 0) {
         pl.fused = true;
         pl.nch = nch;
-        int64_t g = ws->gmax;
+        int64_t g = sm_count();
         int64_t min_rows_cta = 64;
         int64_t gr = (A->rows + min_rows_cta - 1) / min_rows_cta;
         if (g > gr) g = gr;
@@ -498,9 +533,9 @@ static tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A
         P.sspart = ws->sspart;
         P.qstride = pl.qstride;
         P.skip = skip;
-        if (!launch_fused(pl.e, pl.acc64, P, pl.nch, pl.grid, st))
-            return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
-        TOMOS_LAUNCH_CHECK("fused_pass_kernel");
+        tomos_status ls = launch_fused(pl.e, pl.acc64, P, &ws->st->pipe_err, pl.nch, pl.grid, st);
+        if (ls) return ls;
+        ws->launches += 1;
         return TOMOS_OK;
     }
     // Generic path: u = cp*A p + cu*u_in (u_in copied into u first when
@@ -524,6 +559,7 @@ static tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A
     L.scratch_bytes = ws->scratch_bytes;
     tomos_status s = gemv_launch(L, pl.e, pl.acc64, st);
     if (s) return s;
+    ws->launches += (L.dot ? 1 : 2) + 1 + 2;
     sumsq_partial_kernel<<<pl.gs, 256, 0, st>>>(ws->u, A->rows, skip, ws->sspart);
     TOMOS_LAUNCH_CHECK("sumsq_partial_kernel");
     GemvLaunch T;
@@ -545,8 +581,9 @@ static tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A
 // ------------------------------------------------------------ n-side glue
 
 static NSide make_nside(tomos_workspace* ws, const PassPlan& pl, float* x, bool init,
-                        const int* skip) {
+                        const int* skip, const double* dscale = nullptr) {
     NSide S;
+    S.dscale = dscale;
     S.n = ws->n;
     S.qpart = ws->qpart;
     S.qstride = pl.qstride;
@@ -585,6 +622,7 @@ static tomos_status enqueue_nside(tomos_workspace* ws, const NSide& S, cudaStrea
     TOMOS_LAUNCH_CHECK("nside_update_kernel");
     nside_finish_kernel<<<1, 256, 0, st>>>(S);
     TOMOS_LAUNCH_CHECK("nside_finish_kernel");
+    ws->launches += S.has_precond ? 4 : 3;
     return TOMOS_OK;
 }
 
@@ -601,22 +639,25 @@ struct DensePass : PassOps {
                          const int* skip, cudaStream_t st) override {
         return enqueue_dense_pass(ws, A, pl, p, u_in, coef, skip, st);
     }
-    tomos_status fro2(double* out, cudaStream_t st) override {
+    tomos_status fro2(double* out, const double* d, cudaStream_t st) override {
         bool dot;
         int64_t outer, inner;
         std::string why;
         gemv_shape(A, TOMOS_NO_TRANSPOSE, &dot, &outer, &inner, &why);
         const void* lo = elem_is_exact(init_e) ? dense_lo_plane(A) : nullptr;
-        int g = ws->gs_max;
+        const int g = ws->gs_max;
+        const int ci = A->layout == TOMOS_ROW_MAJOR ? 1 : 0;
+#define TOMOS_FRO2(EE) fro2_partial_kernel<EE><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, d, ci, ws->bpart)
         switch (init_e) {
-            case Elem::F32: fro2_partial_kernel<Elem::F32><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
-            case Elem::H16: fro2_partial_kernel<Elem::H16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
-            case Elem::A16: fro2_partial_kernel<Elem::A16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
-            case Elem::B16: fro2_partial_kernel<Elem::B16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
-            case Elem::AB16: fro2_partial_kernel<Elem::AB16><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
-            case Elem::AB16R: fro2_partial_kernel<Elem::AB16R><<<g, 256, 0, st>>>(A->values, lo, outer, inner, A->ld, ws->bpart); break;
+            case Elem::F32: TOMOS_FRO2(Elem::F32); break;
+            case Elem::H16: TOMOS_FRO2(Elem::H16); break;
+            case Elem::A16: TOMOS_FRO2(Elem::A16); break;
+            case Elem::B16: TOMOS_FRO2(Elem::B16); break;
+            case Elem::AB16: TOMOS_FRO2(Elem::AB16); break;
+            case Elem::AB16R: TOMOS_FRO2(Elem::AB16R); break;
             default: return fail(TOMOS_ERR_UNSUPPORTED, "fro2: element type");
         }
+#undef TOMOS_FRO2
         TOMOS_LAUNCH_CHECK("fro2_partial_kernel");
         sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, g, out);
         TOMOS_LAUNCH_CHECK("sum_to_scalar_kernel");
@@ -636,6 +677,9 @@ static tomos_status sync_state(tomos_workspace* ws) {
     TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->st_host, ws->st, sizeof(LsqrDev), cudaMemcpyDeviceToHost,
                                    ws->stream));
     TOMOS_CUDA_TRY(cudaStreamSynchronize(ws->stream));
+    if (ws->st_host->pipe_err)
+        return fail(TOMOS_ERR_CUDA, "A pass: a bounded pipeline wait expired (code " +
+                                        std::to_string(ws->st_host->pipe_err) + ")");
     return TOMOS_OK;
 }
 
@@ -660,6 +704,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     TOMOS_CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_fence, 0));
     TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
 
+    const int64_t launches0 = ws->launches;
     const int max_iters = o->max_iters > 0 ? o->max_iters : 0;
     const int restarts = o->restarts > 0 ? o->restarts : 1;
     const int64_t hist_total = (int64_t)max_iters * restarts;
@@ -672,6 +717,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
                                                        ws->precond.layout, ws->precond.ld, n,
                                                        ws->Rcm, ws->Rrm);
         TOMOS_LAUNCH_CHECK("precond_copy_kernel");
+        ws->launches += 1;
     }
     if (!o->warm_start) TOMOS_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(float) * n, st));
 
@@ -680,12 +726,15 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     TOMOS_LAUNCH_CHECK("sumsq_partial_kernel");
     sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, ws->scal + 2);
     TOMOS_LAUNCH_CHECK("sum_to_scalar_kernel");
+    ws->launches += 2;
     double anorm = o->anorm_fro;
     int extra_passes = 0;
+    const double* dsc = o->stop_rule == TOMOS_STOP_BACKWARD ? o->col_scale : nullptr;
     if (o->stop_rule == TOMOS_STOP_BACKWARD && !(anorm > 0.0)) {
-        s = ops.fro2(ws->scal + 3, st);
+        s = ops.fro2(ws->scal + 3, dsc, st);
         if (s) return s;
         extra_passes = 1;
+        ws->launches += 2;
     }
     double hostsc[4];
     TOMOS_CUDA_TRY(cudaMemcpyAsync(hostsc, ws->scal, sizeof(hostsc), cudaMemcpyDeviceToHost, st));
@@ -728,10 +777,11 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         if (ws->graph) cudaGraphExecDestroy(ws->graph);
         ws->graph = nullptr;
         cudaGraph_t g = nullptr;
+        const int64_t before = ws->launches;
         TOMOS_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         const int* skip = &ws->st->done;
         tomos_status cs = ops.enqueue(pl_iter, ws->p, ws->u, ws->st->coef, skip, st);
-        if (!cs) cs = enqueue_nside(ws, make_nside(ws, pl_iter, x, false, skip), st);
+        if (!cs) cs = enqueue_nside(ws, make_nside(ws, pl_iter, x, false, skip, dsc), st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         if (cs) {
             if (g) cudaGraphDestroy(g);
@@ -742,6 +792,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
         ws->graph_key = key;
+        ws->graph_kernels = ws->launches - before;
     }
 
     std::vector<double> hist_host;
@@ -764,9 +815,11 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         }
         // initialize(): ut = b - A x (restarted from the current x).
         restarts_used = rs + 1;
+        if (o->profile) TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pa, st));
         s = ops.enqueue(pl_init, x, b, ws->coef_init, nullptr, st);
         if (s) return s;
-        s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr), st);
+        if (o->profile) TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pb, st));
+        s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr, dsc), st);
         if (s) return s;
         if (pl_init.e == Elem::A16 || pl_init.e == Elem::AB16 || pl_init.e == Elem::AB16R ||
             pl_init.e != pl_iter.e)
@@ -775,6 +828,12 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
             ++iter_passes;
         s = sync_state(ws);
         if (s) return s;
+        if (o->profile) {
+            float pm = 0.0f;
+            TOMOS_CUDA_TRY(cudaEventElapsedTime(&pm, ws->ev_pa, ws->ev_pb));
+            R.init_pass_ms += pm;
+            R.init_pass_count += 1;
+        }
         if (H.rhsnorm == 0.0) {
             converged = true;
             break;
@@ -797,12 +856,31 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         }
         if (H.breakdown || max_iters == 0) continue;
         // Inner iterations in batches of graph launches; the device stops
-        // doing work once its stopping rule fires.
+        // doing work once its stopping rule fires.  The profiling mode
+        // launches each iteration directly and times its pass over A.
         int batch = 4;
         int done_iters = 0;
-        while (done_iters < max_iters) {
+        while (o->profile && done_iters < max_iters) {
+            const int* skip = &ws->st->done;
+            TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pa, st));
+            s = ops.enqueue(pl_iter, ws->p, ws->u, ws->st->coef, skip, st);
+            if (s) return s;
+            TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pb, st));
+            s = enqueue_nside(ws, make_nside(ws, pl_iter, x, false, skip, dsc), st);
+            if (s) return s;
+            s = sync_state(ws);
+            if (s) return s;
+            float pm = 0.0f;
+            TOMOS_CUDA_TRY(cudaEventElapsedTime(&pm, ws->ev_pa, ws->ev_pb));
+            R.iter_pass_ms += pm;
+            R.iter_pass_count += 1;
+            done_iters = H.iter_restart;
+            if (H.done) break;
+        }
+        while (!o->profile && done_iters < max_iters) {
             int k = batch < max_iters - done_iters ? batch : max_iters - done_iters;
             for (int i = 0; i < k; ++i) TOMOS_CUDA_TRY(cudaGraphLaunch(ws->graph, st));
+            ws->launches += (int64_t)k * ws->graph_kernels;
             s = sync_state(ws);
             if (s) return s;
             done_iters = H.iter_restart;
@@ -829,7 +907,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     if (o->stop_rule == TOMOS_STOP_BACKWARD && !converged) {
         s = ops.enqueue(pl_init, x, b, ws->coef_init, nullptr, st);
         if (s) return s;
-        s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr), st);
+        s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr, dsc), st);
         if (s) return s;
         ++accurate_passes;
         s = sync_state(ws);
@@ -858,6 +936,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     R.elapsed_ms = ms;
     R.accurate_passes = accurate_passes;
     R.half_passes = iter_passes;
+    R.kernel_launches = (int32_t)(ws->launches - launches0);
     if (o->history && o->history_cap > 0) {
         int cnt = (int)hist_host.size() < o->history_cap ? (int)hist_host.size() : o->history_cap;
         for (int i = 0; i < cnt; ++i) o->history[i] = hist_host[i];
@@ -963,6 +1042,8 @@ tomos_status tomos_workspace_create(int64_t m, int64_t n, int32_t value_type,
     A(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
     A(cudaEventCreate(&ws->ev_start));
     A(cudaEventCreate(&ws->ev_stop));
+    A(cudaEventCreate(&ws->ev_pa));
+    A(cudaEventCreate(&ws->ev_pb));
     A(cudaEventCreateWithFlags(&ws->ev_fence, cudaEventDisableTiming));
     if (!ok) {
         ws_free(ws);
@@ -970,6 +1051,7 @@ tomos_status tomos_workspace_create(int64_t m, int64_t n, int32_t value_type,
         return fail(TOMOS_ERR_ALLOC, "tomos_workspace_create: device allocation failed");
     }
     std::memset(ws->st_host, 0, sizeof(LsqrDev));
+    cudaMemset(ws->st, 0, sizeof(LsqrDev));
     *out = ws;
     return TOMOS_OK;
 }
@@ -1048,8 +1130,8 @@ tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float*
 }
 
 tomos_status tomos_backward_error_dense(const tomos_dense* A, const float* b, const float* x,
-                                        tomos_workspace* ws, tomos_lsqr_report* report,
-                                        void* stream) {
+                                        const double* col_scale, tomos_workspace* ws,
+                                        tomos_lsqr_report* report, void* stream) {
     std::string why;
     bool dot;
     int64_t outer, inner;
@@ -1078,16 +1160,15 @@ tomos_status tomos_backward_error_dense(const tomos_dense* A, const float* b, co
     // beta = ||r|| and ||A^T r|| through N1 (no preconditioner, init mode).
     bool had = ws->has_precond;
     ws->has_precond = false;
-    NSide S = make_nside(ws, pl, nullptr, true, nullptr);
+    NSide S = make_nside(ws, pl, nullptr, true, nullptr, col_scale);
     ws->has_precond = had;
     nside_reduce_kernel<<<ws->nb1, 256, 0, st>>>(S);
     TOMOS_LAUNCH_CHECK("nside_reduce_kernel");
     sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->qnpart, ws->nb1, ws->scal + 4);
     sumsq_partial_kernel<<<ws->gs_max, 256, 0, st>>>(b, A->rows, nullptr, ws->bpart);
     sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, ws->scal + 2);
-    sumsq_partial_kernel<<<1, 256, 0, st>>>(x, A->cols, nullptr, ws->xpart);
-    sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->xpart, 1, ws->scal + 5);
-    s = ops.fro2(ws->scal + 3, st);
+    scaled_sumsq_kernel<<<1, 256, 0, st>>>(x, col_scale, A->cols, ws->scal + 5);
+    s = ops.fro2(ws->scal + 3, col_scale, st);
     if (s) return s;
     TOMOS_LAUNCH_CHECK("backward_error reductions");
     double h[6];

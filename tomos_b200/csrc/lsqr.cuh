@@ -31,6 +31,8 @@ struct LsqrDev {
     int breakdown;       // alpha or beta reached zero
     int stop_rule;
     int history_cap;
+    int pipe_err;        // nonzero: a bounded pipeline wait expired in an A pass
+    int pad_;
 };
 
 // How one pass over A is run.
@@ -53,7 +55,8 @@ struct PassOps {
     virtual PassPlan plan(bool init) = 0;
     virtual tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in,
                                  const double* coef, const int* skip, cudaStream_t st) = 0;
-    virtual tomos_status fro2(double* out_dev, cudaStream_t st) = 0;
+    // sum of squares of A's elements divided by d[column] (d may be NULL)
+    virtual tomos_status fro2(double* out_dev, const double* d, cudaStream_t st) = 0;
     virtual uint64_t key() = 0;
     virtual int64_t rows() = 0;
     virtual int64_t cols() = 0;
@@ -105,7 +108,10 @@ struct tomos_workspace {
     tomos_b200::LsqrDev* st_host = nullptr;  // pinned mirror of *st
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_fence = nullptr;
+    cudaEvent_t ev_pa = nullptr, ev_pb = nullptr;  // profiling: one pass over A
 
     cudaGraphExec_t graph = nullptr;
+    int64_t launches = 0;        // kernels enqueued by the driver (graph replays included)
+    int64_t graph_kernels = 0;   // kernels in one replay of `graph`
     std::vector<uint64_t> graph_key;
 };

@@ -107,6 +107,8 @@ __global__ void __cluster_dims__(kQrCluster, 1, 1) __launch_bounds__(kQrThreads)
     __shared__ double taul[kQrMaxNb];
     __shared__ double gsum[kQrMaxNb * kQrMaxNb];
     __shared__ double tmat[kQrMaxNb * kQrMaxNb];
+    __shared__ double gath[2 * kQrCluster];
+    __shared__ double wgath[kQrCluster][kQrMaxNb];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -147,13 +149,18 @@ __global__ void __cluster_dims__(kQrCluster, 1, 1) __launch_bounds__(kQrThreads)
             X.norm[par][1] = owner ? pan[(size_t)j * rpc + lp] : 0.0;
         }
         cluster.sync();
-        // 2. every CTA forms the same reflector from the 8 partials.
+        // 2. every CTA forms the same reflector from the 8 partials
+        //    (one distributed-shared-memory read per partial, in parallel).
+        if (tid < 2 * kQrCluster) {
+            const PanelXch* rx = cluster.map_shared_rank(&X, tid >> 1);
+            gath[tid] = rx->norm[par][tid & 1];
+        }
+        __syncthreads();
         if (tid == 0) {
             double xn2 = 0.0, alpha = 0.0;
             for (int c = 0; c < kQrCluster; ++c) {
-                const PanelXch* rx = cluster.map_shared_rank(&X, c);
-                xn2 += rx->norm[par][0];
-                alpha += rx->norm[par][1];
+                xn2 += gath[2 * c];
+                alpha += gath[2 * c + 1];
             }
             double tau = 0.0, beta = alpha, scal = 0.0;
             if (xn2 > 0.0) {
@@ -187,10 +194,15 @@ __global__ void __cluster_dims__(kQrCluster, 1, 1) __launch_bounds__(kQrThreads)
             if (lane == 0) X.w[par][c] = w;
         }
         cluster.sync();
-        // 4. a_c -= tau * w_c * v.
+        // 4. a_c -= tau * w_c * v, w_c summed over the cluster in a fixed order.
+        for (int e = tid; e < kQrCluster * nb; e += kQrThreads) {
+            const int q = e / nb, c = e % nb;
+            if (c > j) wgath[q][c] = cluster.map_shared_rank(&X, q)->w[par][c];
+        }
+        __syncthreads();
         for (int c = j + 1 + warp; c < nb; c += kQrThreads / 32) {
             double w = 0.0;
-            for (int q = 0; q < kQrCluster; ++q) w += cluster.map_shared_rank(&X, q)->w[par][c];
+            for (int q = 0; q < kQrCluster; ++q) w += wgath[q][c];
             const double tw = tau * w;
             for (int64_t r = lane; r < nrows; r += 32) {
                 const int64_t g = row0 + r;
@@ -204,19 +216,20 @@ __global__ void __cluster_dims__(kQrCluster, 1, 1) __launch_bounds__(kQrThreads)
     }
 
     // Gram matrix G = V^T V of the panel's reflectors (unit diagonal,
-    // zeros above), partial per CTA.
-    for (int e = tid; e < nb * nb; e += kQrThreads) {
+    // zeros above), partial per CTA: a warp per (a < b) pair, lanes over rows.
+    for (int e = warp; e < nb * nb; e += kQrThreads / 32) {
         const int a = e % nb, b = e / nb;
         double g = 0.0;
         if (a < b) {
-            for (int64_t r = 0; r < nrows; ++r) {
+            for (int64_t r = lane; r < nrows; r += 32) {
                 const int64_t row = row0 + r;
                 const double va = row > P.j0 + a ? pan[(size_t)a * rpc + r] : (row == P.j0 + a ? 1.0 : 0.0);
                 const double vb = row > P.j0 + b ? pan[(size_t)b * rpc + r] : (row == P.j0 + b ? 1.0 : 0.0);
                 g += va * vb;
             }
+            g = warp_sum(g);
         }
-        X.gram[e] = g;
+        if (lane == 0) X.gram[e] = g;
     }
     cluster.sync();
     if (rank == 0) {
@@ -224,8 +237,12 @@ __global__ void __cluster_dims__(kQrCluster, 1, 1) __launch_bounds__(kQrThreads)
         // column-major): T_jj = tau_j, T(0:j, j) = -tau_j T(0:j, 0:j) G(0:j, j)
         // (LAPACK dlarft, forward / columnwise).
         for (int e = tid; e < nb * nb; e += kQrThreads) {
+            double gq[kQrCluster];
+#pragma unroll
+            for (int q = 0; q < kQrCluster; ++q) gq[q] = cluster.map_shared_rank(&X, q)->gram[e];
             double g = 0.0;
-            for (int q = 0; q < kQrCluster; ++q) g += cluster.map_shared_rank(&X, q)->gram[e];
+#pragma unroll
+            for (int q = 0; q < kQrCluster; ++q) g += gq[q];
             gsum[e] = g;
         }
         __syncthreads();
@@ -303,27 +320,46 @@ __global__ void __launch_bounds__(kQrThreads) qr_w_partial_kernel(const double* 
     }
 }
 
-// W2(:, c) = T^T * sum_chunks Wp(:, :, c).
-__global__ void qr_w_reduce_kernel(const double* Wp, int64_t chunks, int64_t nc, int nb,
-                                   const double* T, double* W2) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    double w[kQrMaxNb];
-#pragma unroll
-    for (int a = 0; a < kQrMaxNb; ++a) {
-        double s = 0.0;
-        if (a < nb)
-            for (int64_t q = 0; q < chunks; ++q) s += Wp[((size_t)q * kQrMaxNb + a) * (size_t)nc + c];
-        w[a] = s;
+// W2(:, c) = T^T * sum_chunks Wp(:, :, c): a block per 32 trailing
+// columns, threads over (row of W, column) pairs, coalesced along columns.
+__global__ void __launch_bounds__(256) qr_w_reduce_kernel(const double* Wp, int64_t chunks,
+                                                          int64_t nc, int nb, const double* T,
+                                                          double* W2) {
+    __shared__ double Ws[kQrMaxNb][kQrTile + 1];
+    __shared__ double Ts[kQrMaxNb][kQrMaxNb + 1];
+    const int64_t c0 = (int64_t)blockIdx.x * kQrTile;
+    for (int e = threadIdx.x; e < kQrMaxNb * kQrMaxNb; e += blockDim.x) {
+        const int a = e % kQrMaxNb, b = e / kQrMaxNb;
+        Ts[a][b] = (a < nb && b < nb) ? T[b * nb + a] : 0.0;  // T(a, b)
     }
-#pragma unroll
-    for (int b = 0; b < kQrMaxNb; ++b) {
-        if (b >= nb) break;
-        double s = 0.0;
-#pragma unroll
-        for (int a = 0; a < kQrMaxNb; ++a)
-            if (a <= b) s += T[b * nb + a] * w[a];
-        W2[(size_t)b * nc + c] = s;
+    for (int e = threadIdx.x; e < kQrMaxNb * kQrTile; e += blockDim.x) {
+        const int a = e / kQrTile, cc = e % kQrTile;
+        const int64_t col = c0 + cc;
+        double sum = 0.0;
+        if (a < nb && col < nc) {
+            const double* p = Wp + (size_t)a * nc + col;
+            const size_t stride = (size_t)kQrMaxNb * nc;
+            int64_t q = 0;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            for (; q + 3 < chunks; q += 4) {
+                s0 += p[(size_t)q * stride];
+                s1 += p[(size_t)(q + 1) * stride];
+                s2 += p[(size_t)(q + 2) * stride];
+                s3 += p[(size_t)(q + 3) * stride];
+            }
+            for (; q < chunks; ++q) s0 += p[(size_t)q * stride];
+            sum = (s0 + s1) + (s2 + s3);
+        }
+        Ws[a][cc] = sum;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kQrMaxNb * kQrTile; e += blockDim.x) {
+        const int b = e / kQrTile, cc = e % kQrTile;
+        const int64_t col = c0 + cc;
+        if (b >= nb || col >= nc) continue;
+        double sum = 0.0;
+        for (int a = 0; a <= b; ++a) sum += Ts[a][b] * Ws[a][cc];
+        W2[(size_t)b * nc + col] = sum;
     }
 }
 
@@ -371,26 +407,67 @@ __global__ void qr_extract_kernel(const double* A, int64_t ld, int64_t n, double
     }
 }
 
-// Column j of R^{-1} by back substitution (warp per column), written into
-// the leading n x n block of A with zeros below the diagonal.
-__global__ void __launch_bounds__(256) qr_trtri_kernel(const double* Rt, int64_t n, double* A,
-                                                       int64_t ld) {
-    extern __shared__ double xs[];  // 8 warps x n
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t j = (int64_t)blockIdx.x * 8 + w;
-    if (j >= n) return;
-    double* x = xs + (size_t)w * n;
-    if (lane == 0) x[j] = 1.0 / Rt[(size_t)j * n + j];
-    __syncwarp();
-    for (int64_t i = j - 1; i >= 0; --i) {
-        const double* row = Rt + (size_t)i * n;
-        double s = 0.0;
-        for (int64_t k = i + 1 + lane; k <= j; k += 32) s += row[k] * x[k];
-        s = warp_sum(s);
-        if (lane == 0) x[i] = -s / row[i];
-        __syncwarp();
+__global__ void qr_zero_lower_kernel(double* A, int64_t ld, int64_t n) {
+    const int64_t total = n * n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, j = e / n;
+        if (i > j) A[(size_t)j * ld + i] = 0.0;
     }
-    for (int64_t i = lane; i < n; i += 32) A[(size_t)j * ld + i] = i <= j ? x[i] : 0.0;
+}
+
+// R^{-1} in 32 x 32 blocks, written into the leading n x n block of A
+// (whose strictly lower part qr_extract_kernel has zeroed).
+// Diagonal blocks: a warp per block, lane j back-substitutes column j.
+__global__ void __launch_bounds__(32) qr_trtri_diag_kernel(const double* Rt, int64_t n, double* A,
+                                                           int64_t ld) {
+    __shared__ double Rb[32][33];
+    __shared__ double Xb[32][33];
+    const int lane = threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.x * 32;
+    const int bs = (int)(n - i0 < 32 ? n - i0 : 32);
+    for (int r = 0; r < 32; ++r)
+        Rb[r][lane] = (r < bs && lane < bs && lane >= r) ? Rt[(size_t)(i0 + r) * n + i0 + lane] : 0.0;
+    __syncwarp();
+    const int j = lane;
+    if (j < bs) {
+        Xb[j][j] = 1.0 / Rb[j][j];
+        for (int i = j - 1; i >= 0; --i) {
+            double sum = 0.0;
+            for (int k = i + 1; k <= j; ++k) sum += Rb[i][k] * Xb[k][j];
+            Xb[i][j] = -sum / Rb[i][i];
+        }
+        for (int i = 0; i < bs; ++i) A[(size_t)(i0 + j) * ld + i0 + i] = i <= j ? Xb[i][j] : 0.0;
+    }
+}
+
+// Off-diagonal blocks of block column J (8 columns per CTA):
+// X_IJ = -X_II * sum_{K=I+1..J} R_IK X_KJ for I = J-1 down to 0.
+__global__ void __launch_bounds__(256) qr_trtri_off_kernel(const double* Rt, int64_t n, double* A,
+                                                           int64_t ld) {
+    __shared__ double tmp[32][9];
+    const int J = blockIdx.x;
+    const int64_t j0 = (int64_t)J * 32 + blockIdx.y * 8;
+    const int i = threadIdx.x / 8, jj = threadIdx.x % 8;
+    const int64_t col = j0 + jj;
+    const bool cv = col < n && blockIdx.y * 8 + jj < 32;
+    for (int I = J - 1; I >= 0; --I) {
+        const int64_t i0 = (int64_t)I * 32;
+        double sum = 0.0;
+        if (cv) {
+            const double* rrow = Rt + (size_t)(i0 + i) * n;
+            const double* xcol = A + (size_t)col * ld;
+            for (int64_t k = i0 + 32; k <= col; ++k) sum += rrow[k] * xcol[k];
+        }
+        tmp[i][jj] = sum;
+        __syncthreads();
+        if (cv) {
+            double out = 0.0;
+            for (int l = i; l < 32; ++l) out += A[(size_t)(i0 + l) * ld + i0 + i] * tmp[l][jj];
+            A[(size_t)col * ld + i0 + i] = -out;
+        }
+        __syncthreads();
+    }
 }
 
 }  // namespace tomos_b200
@@ -444,8 +521,8 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
         dim3 g1((unsigned)((nc + kQrTile - 1) / kQrTile), (unsigned)chunks);
         qr_w_partial_kernel<<<g1, kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb, q.Wp);
         TOMOS_LAUNCH_CHECK("qr_w_partial_kernel");
-        qr_w_reduce_kernel<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(q.Wp, chunks, nc, nb, q.T,
-                                                                          q.W2);
+        qr_w_reduce_kernel<<<(unsigned)((nc + kQrTile - 1) / kQrTile), 256, 0, st>>>(
+            q.Wp, chunks, nc, nb, q.T, q.W2);
         TOMOS_LAUNCH_CHECK("qr_w_reduce_kernel");
         qr_update_kernel<<<g1, kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb, q.W2);
         TOMOS_LAUNCH_CHECK("qr_update_kernel");
@@ -459,13 +536,16 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     if (flag)
         return fail(TOMOS_ERR_NUMERIC,
                     "generate_sketch_qr_precond: trtri failed -- R is singular.");
-    const size_t tsmem = (size_t)8 * n * sizeof(double);
-    if (tsmem > 48 * 1024)
-        TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_trtri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)tsmem));
-    if (tsmem > 227 * 1024) return fail(TOMOS_ERR_UNSUPPORTED, "sketch_qr: n too large for trtri");
-    qr_trtri_kernel<<<(unsigned)((n + 7) / 8), 256, tsmem, st>>>(q.Rt, n, SA, ld);
-    TOMOS_LAUNCH_CHECK("qr_trtri_kernel");
+    const int64_t nbk = (n + 31) / 32;
+    qr_zero_lower_kernel<<<(unsigned)((n * n + 255) / 256 < 4096 ? (n * n + 255) / 256 : 4096), 256, 0,
+                           st>>>(SA, ld, n);
+    TOMOS_LAUNCH_CHECK("qr_zero_lower_kernel");
+    qr_trtri_diag_kernel<<<(unsigned)nbk, 32, 0, st>>>(q.Rt, n, SA, ld);
+    TOMOS_LAUNCH_CHECK("qr_trtri_diag_kernel");
+    if (nbk > 1) {
+        qr_trtri_off_kernel<<<dim3((unsigned)nbk, 4), 256, 0, st>>>(q.Rt, n, SA, ld);
+    }
+    TOMOS_LAUNCH_CHECK("qr_trtri_off_kernel");
     return TOMOS_OK;
 }
 

@@ -19,6 +19,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "fused.cuh"
 #include "sketch.cuh"
 
 namespace tomos_b200 {
@@ -115,14 +116,16 @@ __global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void
                                                       const int32_t* __restrict__ perm,
                                                       const int8_t* __restrict__ sign,
                                                       double* __restrict__ SA, int64_t ld_sa,
-                                                      double* __restrict__ fro_part) {
+                                                      double* __restrict__ fro_part,
+                                                      double* __restrict__ col_part) {
     __shared__ double smf[8];
+    __shared__ double smc[8][32 * KC];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t b = (int64_t)blockIdx.x * 8 + w;
     const int64_t c0 = (int64_t)blockIdx.y * 32 * KC;
-    double acc[KC];
+    double acc[KC], csq[KC];
 #pragma unroll
-    for (int k = 0; k < KC; ++k) acc[k] = 0.0;
+    for (int k = 0; k < KC; ++k) acc[k] = csq[k] = 0.0;
     double f2 = 0.0;
     if (b < s) {
         const int32_t o0 = offsets[b], o1 = offsets[b + 1];
@@ -136,7 +139,7 @@ __global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void
                 if (j < n) {
                     const double a = (double)load_elem<E>(hi, lo, base + j);
                     acc[k] += sg * a;
-                    f2 += a * a;
+                    csq[k] += a * a;
                 }
             }
         }
@@ -144,8 +147,11 @@ __global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void
         for (int k = 0; k < KC; ++k) {
             const int64_t j = c0 + k * 32 + lane;
             if (j < n) SA[(size_t)j * ld_sa + b] = acc[k];
+            f2 += csq[k];
         }
     }
+#pragma unroll
+    for (int k = 0; k < KC; ++k) smc[w][k * 32 + lane] = csq[k];
     f2 = warp_sum(f2);
     if (lane == 0) smf[w] = f2;
     __syncthreads();
@@ -154,6 +160,134 @@ __global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void
 #pragma unroll
         for (int k = 0; k < 8; ++k) t += smf[k];
         fro_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+    }
+    if (col_part) {
+        for (int e = threadIdx.x; e < 32 * KC; e += blockDim.x) {
+            const int64_t j = c0 + e;
+            if (j >= n) continue;
+            double t = 0.0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) t += smc[k][e];
+            col_part[(size_t)blockIdx.x * n + j] = t;
+        }
+    }
+}
+
+// colsq[j] = sum over nparts rows of part[r][j] (fixed order).
+__global__ void cs_col_reduce_kernel(const double* __restrict__ part, int64_t nparts, int64_t n,
+                                     double* __restrict__ colsq) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double t = 0.0;
+    for (int64_t r = 0; r < nparts; ++r) t += part[(size_t)r * n + j];
+    colsq[j] = t;
+}
+
+// Row-major owner sums with 16-byte chunk loads: a warp per (bucket,
+// panel); lane l owns chunks l, l+32, ... (KCH of them, VEC columns each)
+// of the panel, and walks the bucket's rows four at a time.  Needs
+// 16-byte aligned rows (ld * element bytes a multiple of 16).
+template <Elem E, int KCH>
+__global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const void* lo, int64_t n,
+                                                          int64_t ld, int64_t s,
+                                                          const int32_t* __restrict__ offsets,
+                                                          const int32_t* __restrict__ perm,
+                                                          const int8_t* __restrict__ sign,
+                                                          double* __restrict__ SA, int64_t ld_sa,
+                                                          double* __restrict__ fro_part,
+                                                          double* __restrict__ col_part) {
+    constexpr int VEC = ChunkElems<E>::value;
+    constexpr int PW = 32 * KCH * VEC;  // columns per panel
+    constexpr bool TWO = (E == Elem::A16 || E == Elem::AB16 || E == Elem::AB16R);
+    constexpr int esz = (E == Elem::F32) ? 4 : 2;
+    __shared__ double smf[8];
+    __shared__ double smc[8][PW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t b = (int64_t)blockIdx.x * 8 + w;
+    const int64_t c0 = (int64_t)blockIdx.y * PW;
+    const int64_t nch = (n + VEC - 1) / VEC;
+    double acc[KCH][VEC], csq[KCH][VEC];
+#pragma unroll
+    for (int k = 0; k < KCH; ++k)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) acc[k][e] = csq[k][e] = 0.0;
+    bool live[KCH];
+#pragma unroll
+    for (int k = 0; k < KCH; ++k) live[k] = (c0 / VEC + k * 32 + lane) < nch;
+    const bool ragged = (n % VEC) != 0;
+    if (b < s) {
+        const int32_t o0 = offsets[b], o1 = offsets[b + 1];
+        for (int32_t q = o0; q < o1; q += 4) {
+            int32_t r[4];
+            double sg[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                r[u] = q + u < o1 ? perm[q + u] : -1;
+                sg[u] = r[u] >= 0 ? (double)sign[r[u]] : 0.0;
+            }
+            uint4 h[4][KCH], l[4][KCH];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int k = 0; k < KCH; ++k) {
+                    h[u][k] = l[u][k] = make_uint4(0, 0, 0, 0);
+                    if (r[u] >= 0 && live[k]) {
+                        const size_t off = (size_t)r[u] * ld * esz + (size_t)(c0 + (k * 32 + lane) * VEC) * esz;
+                        h[u][k] = __ldcs(reinterpret_cast<const uint4*>(static_cast<const uint8_t*>(hi) + off));
+                        if (TWO) l[u][k] = __ldcs(reinterpret_cast<const uint4*>(static_cast<const uint8_t*>(lo) + off));
+                    }
+                }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int k = 0; k < KCH; ++k) {
+                    if (r[u] < 0 || !live[k]) continue;
+                    float f[VEC];
+                    ChunkDecoder<E>::decode(h[u][k], l[u][k], f);
+                    const int64_t cbase = c0 + (int64_t)(k * 32 + lane) * VEC;
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) {
+                        if (ragged && cbase + e >= n) continue;
+                        const double a = (double)f[e];
+                        acc[k][e] = fma(sg[u], a, acc[k][e]);
+                        csq[k][e] = fma(a, a, csq[k][e]);
+                    }
+                }
+        }
+#pragma unroll
+        for (int k = 0; k < KCH; ++k) {
+            const int64_t cbase = c0 + (int64_t)(k * 32 + lane) * VEC;
+#pragma unroll
+            for (int e = 0; e < VEC; ++e)
+                if (live[k] && cbase + e < n) SA[(size_t)(cbase + e) * ld_sa + b] = acc[k][e];
+        }
+    }
+    double f2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < KCH; ++k)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) {
+            smc[w][(k * 32 + lane) * VEC + e] = csq[k][e];
+            f2 += csq[k][e];
+        }
+    f2 = warp_sum(f2);
+    if (lane == 0) smf[w] = f2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t += smf[k];
+        fro_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+    }
+    if (col_part) {
+        for (int e = threadIdx.x; e < PW; e += blockDim.x) {
+            const int64_t j = c0 + e;
+            if (j >= n) continue;
+            double t = 0.0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) t += smc[k][e];
+            col_part[(size_t)blockIdx.x * n + j] = t;
+        }
     }
 }
 
@@ -166,7 +300,8 @@ __global__ void __launch_bounds__(256) cs_cols_kernel(const void* hi, const void
                                                       const int32_t* __restrict__ perm,
                                                       const int8_t* __restrict__ sign,
                                                       double* __restrict__ SA, int64_t ld_sa,
-                                                      double* __restrict__ fro_part) {
+                                                      double* __restrict__ fro_part,
+                                                      double* __restrict__ colsq) {
     __shared__ double smf[8];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t j = blockIdx.x;
@@ -192,6 +327,7 @@ __global__ void __launch_bounds__(256) cs_cols_kernel(const void* hi, const void
 #pragma unroll
         for (int k = 0; k < 8; ++k) t += smf[k];
         fro_part[blockIdx.x] = t;
+        if (colsq) colsq[blockIdx.x] = t;
     }
 }
 
@@ -212,7 +348,7 @@ __global__ void cs_fro_reduce_kernel(const double* __restrict__ part, int64_t np
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-CsScratch cs_layout(void* base, int64_t m, int64_t s, int64_t fro_parts) {
+CsScratch cs_layout(void* base, int64_t m, int64_t s, int64_t fro_parts, int64_t col_parts) {
     CsScratch c;
     size_t off = 0;
     char* p = static_cast<char*>(base);
@@ -228,8 +364,17 @@ CsScratch cs_layout(void* base, int64_t m, int64_t s, int64_t fro_parts) {
     c.cursor = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (s + 1)));
     c.perm = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (m > 0 ? m : 1)));
     c.fro_part = reinterpret_cast<double*>(take(sizeof(double) * (fro_parts > 0 ? fro_parts : 1)));
+    c.col_part = reinterpret_cast<double*>(take(sizeof(double) * (col_parts > 0 ? col_parts : 1)));
     c.bytes = off;
     return c;
+}
+
+int64_t cs_col_part_rows(int64_t m, int64_t s) {
+    const int64_t rows = (s + 7) / 8;                  // row-major owner blocks
+    int64_t csr = (int64_t)sm_count() * 2;             // CSR row-chunk blocks
+    const int64_t cm = (m + 63) / 64;
+    if (csr > cm) csr = cm;
+    return rows > csr ? rows : csr;
 }
 
 // Upper bound of the owner-sum partial count over both layouts and the
@@ -268,19 +413,38 @@ tomos_status cs_bucketize(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed, 
     return TOMOS_OK;
 }
 
+// Panel width of the row-major owner sums for an element type.
 template <Elem E>
-static void launch_rows(const tomos_dense* A, const void* lo, int64_t s, const CsScratch& c,
-                        double* SA, int64_t ld_sa, unsigned gx, unsigned panels, cudaStream_t st) {
-    dim3 grid(gx, panels);
-    cs_rows_kernel<E, 8><<<grid, 256, 0, st>>>(A->values, lo, A->cols, A->ld, s, c.offsets, c.perm,
-                                               c.sign, SA, ld_sa, c.fro_part);
+static int rows_vec_panel() {
+    return 32 * 2 * ChunkElems<E>::value;
+}
+
+template <Elem E>
+static unsigned launch_rows(const tomos_dense* A, const void* lo, int64_t s, const CsScratch& c,
+                            double* SA, int64_t ld_sa, bool want_cols, unsigned gx,
+                            cudaStream_t st) {
+    const int esz = (E == Elem::F32) ? 4 : 2;
+    bool vec = ((A->ld * esz) % 16 == 0) && (reinterpret_cast<uintptr_t>(A->values) % 16 == 0);
+    if (vec && lo) vec = reinterpret_cast<uintptr_t>(lo) % 16 == 0;
+    if (vec) {
+        const unsigned panels = (unsigned)((A->cols + rows_vec_panel<E>() - 1) / rows_vec_panel<E>());
+        cs_rows_vec_kernel<E, 2><<<dim3(gx, panels), 256, 0, st>>>(
+            A->values, lo, A->cols, A->ld, s, c.offsets, c.perm, c.sign, SA, ld_sa, c.fro_part,
+            want_cols ? c.col_part : nullptr);
+        return panels;
+    }
+    const unsigned panels = (unsigned)((A->cols + 255) / 256);
+    cs_rows_kernel<E, 8><<<dim3(gx, panels), 256, 0, st>>>(A->values, lo, A->cols, A->ld, s, c.offsets,
+                                                           c.perm, c.sign, SA, ld_sa, c.fro_part,
+                                                           want_cols ? c.col_part : nullptr);
+    return panels;
 }
 
 template <Elem E>
 static void launch_cols(const tomos_dense* A, const void* lo, int64_t s, const CsScratch& c,
-                        double* SA, int64_t ld_sa, cudaStream_t st) {
+                        double* SA, int64_t ld_sa, double* colsq, cudaStream_t st) {
     cs_cols_kernel<E><<<(unsigned)A->cols, 256, 0, st>>>(A->values, lo, A->cols, A->ld, s, c.offsets,
-                                                         c.perm, c.sign, SA, ld_sa, c.fro_part);
+                                                         c.perm, c.sign, SA, ld_sa, c.fro_part, colsq);
 }
 
 }  // namespace tomos_b200
@@ -303,14 +467,14 @@ tomos_status tomos_countsketch_hash(int64_t m, int64_t s, uint64_t bucket_seed, 
     return TOMOS_OK;
 }
 
-size_t tomos_countsketch_scratch_bytes(int64_t m, int64_t s) {
-    if (m < 0 || s <= 0) return 0;
-    return cs_layout(nullptr, m, s, cs_fro_parts(m, s)).bytes;
+size_t tomos_countsketch_scratch_bytes(int64_t m, int64_t cols, int64_t s) {
+    if (m < 0 || s <= 0 || cols < 0) return 0;
+    return cs_layout(nullptr, m, s, cs_fro_parts(m, s), cs_col_part_rows(m, s) * cols).bytes;
 }
 
 tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t s,
                                      uint64_t bucket_seed, uint64_t sign_seed, double* SA,
-                                     int64_t ld_sa, double* fro2, void* scratch,
+                                     int64_t ld_sa, double* fro2, double* colsq, void* scratch,
                                      size_t scratch_bytes, void* stream) {
     if (!A || s <= 0) return fail(TOMOS_ERR_INVALID, "countsketch_apply: need A and s > 0");
     if (A->layout != TOMOS_ROW_MAJOR && A->layout != TOMOS_COL_MAJOR)
@@ -335,13 +499,15 @@ tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t
         for (int64_t j = 0; j < n; ++j)
             TOMOS_CUDA_TRY(cudaMemsetAsync(SA + j * ld_sa, 0, sizeof(double) * s, st));
         if (fro2) TOMOS_CUDA_TRY(cudaMemsetAsync(fro2, 0, sizeof(double), st));
+        if (colsq) TOMOS_CUDA_TRY(cudaMemsetAsync(colsq, 0, sizeof(double) * n, st));
         return TOMOS_OK;
     }
-    CsScratch need = cs_layout(nullptr, m, s, cs_fro_parts(m, s));
+    const int64_t col_parts = cs_col_part_rows(m, s) * n;
+    CsScratch need = cs_layout(nullptr, m, s, cs_fro_parts(m, s), col_parts);
     if (!scratch || scratch_bytes < need.bytes)
         return fail(TOMOS_ERR_INVALID, "countsketch_apply: scratch too small (need " +
                                            std::to_string(need.bytes) + " bytes)");
-    CsScratch c = cs_layout(scratch, m, s, cs_fro_parts(m, s));
+    CsScratch c = cs_layout(scratch, m, s, cs_fro_parts(m, s), col_parts);
     tomos_status rc = cs_bucketize(m, s, bucket_seed, sign_seed, c, st);
     if (rc) return rc;
     const void* lo = (e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R) ? dense_lo_plane(A)
@@ -349,25 +515,29 @@ tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t
     int64_t nparts;
     if (A->layout == TOMOS_ROW_MAJOR) {
         const unsigned gx = (unsigned)((s + 7) / 8);
-        const unsigned panels = (unsigned)((n + 255) / 256);
+        unsigned panels = 0;
         switch (e) {
-            case Elem::F32: launch_rows<Elem::F32>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
-            case Elem::H16: launch_rows<Elem::H16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
-            case Elem::A16: launch_rows<Elem::A16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
-            case Elem::B16: launch_rows<Elem::B16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
-            case Elem::AB16: launch_rows<Elem::AB16>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
-            case Elem::AB16R: launch_rows<Elem::AB16R>(A, lo, s, c, SA, ld_sa, gx, panels, st); break;
+            case Elem::F32: panels = launch_rows<Elem::F32>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
+            case Elem::H16: panels = launch_rows<Elem::H16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
+            case Elem::A16: panels = launch_rows<Elem::A16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
+            case Elem::B16: panels = launch_rows<Elem::B16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
+            case Elem::AB16: panels = launch_rows<Elem::AB16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
+            case Elem::AB16R: panels = launch_rows<Elem::AB16R>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
             default: return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply: element type");
         }
         nparts = (int64_t)gx * panels;
+        if (colsq) {
+            TOMOS_LAUNCH_CHECK("countsketch owner sums");
+            cs_col_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c.col_part, gx, n, colsq);
+        }
     } else {
         switch (e) {
-            case Elem::F32: launch_cols<Elem::F32>(A, lo, s, c, SA, ld_sa, st); break;
-            case Elem::H16: launch_cols<Elem::H16>(A, lo, s, c, SA, ld_sa, st); break;
-            case Elem::A16: launch_cols<Elem::A16>(A, lo, s, c, SA, ld_sa, st); break;
-            case Elem::B16: launch_cols<Elem::B16>(A, lo, s, c, SA, ld_sa, st); break;
-            case Elem::AB16: launch_cols<Elem::AB16>(A, lo, s, c, SA, ld_sa, st); break;
-            case Elem::AB16R: launch_cols<Elem::AB16R>(A, lo, s, c, SA, ld_sa, st); break;
+            case Elem::F32: launch_cols<Elem::F32>(A, lo, s, c, SA, ld_sa, colsq, st); break;
+            case Elem::H16: launch_cols<Elem::H16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
+            case Elem::A16: launch_cols<Elem::A16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
+            case Elem::B16: launch_cols<Elem::B16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
+            case Elem::AB16: launch_cols<Elem::AB16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
+            case Elem::AB16R: launch_cols<Elem::AB16R>(A, lo, s, c, SA, ld_sa, colsq, st); break;
             default: return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply: element type");
         }
         nparts = n;

@@ -23,10 +23,13 @@ struct CsScratch {
     int32_t* cursor;    // s + 1
     int32_t* perm;      // m: row ids grouped by bucket, ascending within a bucket
     double* fro_part;   // owner-sum partials of sum(A_ij^2)
+    double* col_part;   // per-block partial column sums of squares
     size_t bytes;
 };
 
-CsScratch cs_layout(void* base, int64_t m, int64_t s, int64_t fro_parts);
+CsScratch cs_layout(void* base, int64_t m, int64_t s, int64_t fro_parts, int64_t col_parts);
+// Rows of col_part any caller may need (times the column count).
+int64_t cs_col_part_rows(int64_t m, int64_t s);
 int64_t cs_fro_parts(int64_t m, int64_t s);
 tomos_status cs_bucketize(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed, const CsScratch& c,
                           cudaStream_t st);
