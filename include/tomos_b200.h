@@ -138,6 +138,23 @@ tomos_status tomos_gemv(int32_t trans, double alpha, const tomos_dense* A,
                         int32_t tier, const float* x, double beta, float* y,
                         void* scratch, size_t scratch_bytes, void* stream);
 
+/* tomos_gemv without caller scratch and without allocating anything.  No
+ * reference counterpart: the reference's mv_apply takes its workspace from
+ * the caller or allocates it.  This entry is for callers that cannot
+ * allocate device memory at call time -- a loop that runs under a device
+ * memory budget fixed in advance, or code that must not risk the device-wide
+ * synchronisation that cudaMalloc/cudaFree can cause.  Its scratch is one
+ * 16 MiB buffer per device, built into the library; a product whose
+ * tomos_gemv_scratch_bytes() exceeds 16 MiB (16777216) is rejected with
+ * TOMOS_ERR_INVALID.  The first call made with a device current looks up that
+ * device's buffer address, so make it before any stream capture.  All calls
+ * on a device share the buffer: two calls that can overlap on the GPU (other
+ * streams, or other host threads) race and may return wrong results; order
+ * them on one stream or with events.  Results equal tomos_gemv's. */
+tomos_status tomos_gemv_no_alloc(int32_t trans, double alpha, const tomos_dense* A,
+                                 int32_t tier, const float* x, double beta, float* y,
+                                 void* stream);
+
 /* CSR y = alpha * op(A) x + beta * y (cuda::mv_csr, mv_cuda_kernels.cu:
  * 2029-2058; dispatch::Sparse::lookup_mv).  FP32, FP64 and packed values.
  * The transposed product is deterministic (no atomics). */

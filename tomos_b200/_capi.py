@@ -76,6 +76,8 @@ SIGNATURES = {
     "tomos_gemv_scratch_bytes": (c_sz, [ctypes.POINTER(DenseDesc), c_i32]),
     "tomos_gemv": (c_i32, [c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32, c_vp, c_dbl, c_vp,
                            c_vp, c_sz, c_vp]),
+    "tomos_gemv_no_alloc": (c_i32, [c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32, c_vp, c_dbl,
+                                    c_vp, c_vp]),
     "tomos_csr_gemv_scratch_bytes": (c_sz, [ctypes.POINTER(CsrDesc), c_i32]),
     "tomos_csr_gemv": (c_i32, [c_i32, c_dbl, ctypes.POINTER(CsrDesc), c_i32, c_vp, c_dbl, c_vp,
                                c_vp, c_sz, c_vp]),

@@ -16,6 +16,7 @@
 // HALF-tier and FP32 products accumulate in FP32, ACCURATE-tier in FP64.
 // The LSQR iteration uses the fused row-major pass in fused.cuh instead;
 // these kernels serve tomos_gemv and the shapes that pass does not cover.
+#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -239,11 +240,59 @@ tomos_status gemv_dispatch(int32_t trans, double alpha, const tomos_dense* A, in
     return gemv_launch(L, e, elem_is_exact(e), st);
 }
 
+// Fixed scratch for tomos_gemv_no_alloc: the per-chunk partials of a
+// line-sum product live in this module-scope buffer instead of caller
+// memory.  The line-sum kernel writes every partial it later reduces, so
+// nothing in it has to start at zero.
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_gemv_static_scratch[kNoAllocScratchBytes / sizeof(double)];
+
+// Device address of g_gemv_static_scratch on the current device, looked up
+// on the first call made with that device current and cached afterwards.
+static tomos_status no_alloc_scratch(void** out) {
+    static std::mutex mu;
+    static void* addr[kNoAllocMaxDevices] = {};
+    int dev = 0;
+    TOMOS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(TOMOS_ERR_UNSUPPORTED, "tomos_gemv_no_alloc: device ordinal " +
+                                               std::to_string(dev) + " out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_gemv_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(gemv static scratch)");
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return TOMOS_OK;
+}
+
+tomos_status gemv_no_alloc(int32_t trans, double alpha, const tomos_dense* A, int32_t tier,
+                           const float* x, double beta, float* y, cudaStream_t st) {
+    const size_t need = gemv_scratch_bytes_max(A, trans);
+    if (need > kNoAllocScratchBytes)
+        return fail(TOMOS_ERR_INVALID,
+                    "tomos_gemv_no_alloc: this product needs " + std::to_string(need) +
+                        " bytes of scratch; the fixed buffer holds " +
+                        std::to_string(kNoAllocScratchBytes) + " (use tomos_gemv)");
+    void* scratch = nullptr;
+    tomos_status s = no_alloc_scratch(&scratch);
+    if (s) return s;
+    return gemv_dispatch(trans, alpha, A, tier, x, beta, y, scratch, kNoAllocScratchBytes, st);
+}
+
 }  // namespace tomos_b200
 
 using namespace tomos_b200;
 
 extern "C" {
+
+tomos_status tomos_gemv_no_alloc(int32_t trans, double alpha, const tomos_dense* A, int32_t tier,
+                                 const float* x, double beta, float* y, void* stream) {
+    return gemv_no_alloc(trans, alpha, A, tier, x, beta, y, as_stream(stream));
+}
 
 size_t tomos_gemv_scratch_bytes(const tomos_dense* A, int32_t trans) {
     // Sized for the widest (FP64-accumulating) tier so one buffer serves all.
