@@ -134,9 +134,16 @@ def gpu_solve(tb, torch, A, b, s):
     backward error of the column-scaled problem is <= 1e-6.  Returns (x, report)."""
     packed = A.numeric in (tb.NumericType.FP32_16, tb.NumericType.FP32_BF16)
     m, n = A.size
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if gpu_solve.profile else None
+    if ev:
+        ev[0].record()
     SA, fro2, colsq = tb.apply_count_sketch(A, s, tier=tb.Tier.HALF if packed else tb.Tier.AUTO,
                                             with_colsq=True)
+    if ev:
+        ev[1].record()
     Rinv = tb.generate_sketch_qr_precond(SA)
+    if ev:
+        ev[2].record()
     d, anorm = tb.column_scale(colsq)
     gpu_solve.last_scale = d
     ws = gpu_solve.ws.get((m, n))
@@ -148,6 +155,12 @@ def gpu_solve(tb, torch, A, b, s):
     rep = tb.lsqr_solve(None, A, b, x, ws, TOL, 200, 0.0, restarts=8,
                         stop_rule=tb.StopRule.BACKWARD, inner_rtol=2e-3 if packed else 0.0,
                         anorm_fro=anorm, col_scale=d, profile=gpu_solve.profile)
+    if ev:
+        ev[3].record()
+        torch.cuda.synchronize()
+        rep = dict(rep)
+        rep["phase_ms"] = {"sketch": ev[0].elapsed_time(ev[1]), "qr": ev[1].elapsed_time(ev[2]),
+                           "solve": ev[2].elapsed_time(ev[3])}
     return x, rep
 
 
@@ -197,12 +210,17 @@ def run_ours(args):
     # timed region: packed 16-bit (the headline), then FP32 storage
     barrier()
     sampler = ClockSampler(local)
+    nvtx = torch.cuda.nvtx
     with sampler:
+        nvtx.range_push("packed_solve")
         ms_packed, (xp, rep_p) = time_steps(torch, lambda: gpu_solve(tb, torch, Ap, b, s),
                                             args.steps, args.warmup)
+        nvtx.range_pop()
         barrier()
+        nvtx.range_push("fp32_solve")
         ms_fp32, (xf, rep_f) = time_steps(torch, lambda: gpu_solve(tb, torch, Af, b, s),
                                           args.steps, args.warmup)
+        nvtx.range_pop()
     barrier()
     if world > 1:
         t = torch.tensor([ms_packed, ms_fp32], device="cuda")
@@ -256,7 +274,9 @@ def run_ours(args):
             return x.cpu()
 
         barrier()
-        e2e_ms, _ = time_steps(torch, e2e_step, args.e2e_steps, 1)
+        nvtx.range_push("e2e")
+        e2e_ms, _ = time_steps(torch, e2e_step, args.e2e_steps, args.warmup)
+        nvtx.range_pop()
         barrier()
         if world > 1:
             t = torch.tensor([e2e_ms], device="cuda")
@@ -293,12 +313,15 @@ def run_ours(args):
             "backward_error": {"measure": "eta_D: backward error of (A D^-1, b, D x), D = column norms",
                                "packed": be_p, "fp32": be_f, "packed_plain_eta": be_p_plain,
                                "fp32_plain_eta": be_f_plain, "x_rel_err_vs_xtrue": rel_x},
+            "phase_ms": {"packed": prof_p.get("phase_ms"), "fp32": prof_f.get("phase_ms"),
+                         "packed_restart_pass_ms": init_ms,
+                         "note": "one profiled solve each (passes timed one by one)"},
             "gemv_gbs": {"fused_pass_fp32_16_half": ach, "fused_pass_fp32": ach_f,
                          "fused_pass_fp32_16_exact_fp64acc": ach_init,
                          "pass_ms_half": pass_ms, "pass_ms_fp32": pass_ms_f},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
-                         "kernel": "fused_pass_kernel<H16> (one LSQR iteration's A and A^T)",
+                         "kernel": "fused_tma_kernel<H16> (one LSQR iteration's A and A^T)",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "traffic": ncu_traffic("fused_pass_h16_1e6x1000")},
             "cpu_baseline": cpu,

@@ -270,7 +270,9 @@ typedef struct tomos_lsqr_report {
     int32_t half_passes;     /* per-iteration passes over A                 */
     double iter_pass_ms;     /* profile: total device time of the
                                 per-iteration passes over A                 */
-    double init_pass_ms;     /* profile: same for the restart passes        */
+    double init_pass_ms;     /* profile: same for the accurate-tier restart
+                                passes (the first pass from x = 0 runs at
+                                the iteration tier and is not counted)      */
     int32_t iter_pass_count;
     int32_t init_pass_count;
     int32_t kernel_launches; /* kernels the solve enqueued (graph replays
@@ -294,7 +296,11 @@ tomos_status tomos_workspace_add_precond(tomos_workspace* ws, const tomos_dense*
 
 /* lsqr_solve (include/core/solver.hpp:68-78; lsqr.cpp:785-801): solves
  * min ||A x - b|| with A m x n on the device, b (m) and x (n) FP32 device
- * vectors.  Synchronous on `stream` (the report is filled on return). */
+ * vectors.  Synchronous on `stream` (the report is filled on return).
+ * HALF-tier iterations over a row-major FP32_16 A stream an fp16 copy of
+ * its wh plane that the solve writes into the workspace first (2 bytes per
+ * element, allocated by the first such solve and kept); if that allocation
+ * fails the iterations read A directly. */
 tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float* x,
                                     tomos_workspace* ws, const tomos_lsqr_opts* opts,
                                     tomos_lsqr_report* report, void* stream);
@@ -310,6 +316,34 @@ tomos_status tomos_backward_error_dense(const tomos_dense* A, const float* b,
                                         const float* x, const double* col_scale,
                                         tomos_workspace* ws, tomos_lsqr_report* report,
                                         void* stream);
+
+/* --------------------------------------------------------------- adjoint */
+
+/* Adjoint of x* = argmin ||A x - b|| (no reference counterpart: the
+ * reference has no differentiation).  For a loss L with g = dL/dx*:
+ *   lambda = (A^T A)^{-1} g,  dL/db = A lambda,
+ *   dL/dA = r lambda^T - (A lambda) x*^T  with r = b - A x*.
+ * tomos_lsqr_adjoint_dense: lambda (n, FP32 device) by preconditioned
+ * conjugate gradients on R^{-T} A^T A R^{-1} (the normal-equations form of
+ * LSQR) with the workspace's R^{-1} (tomos_workspace_add_precond; none means
+ * plain CG), one pass over A per iteration.  opts: tol (stop when
+ * ||g - A^T A lambda|| <= tol ||g||), max_iters, iter_tier (AUTO = the exact
+ * values of a packed A).  report: iterations, converged, relres (the final
+ * relative residual), elapsed_ms, kernel_launches.  Synchronous on stream. */
+tomos_status tomos_lsqr_adjoint_dense(const tomos_dense* A, const float* g, float* lambda,
+                                      tomos_workspace* ws, const tomos_lsqr_opts* opts,
+                                      tomos_lsqr_report* report, void* stream);
+/* The gradients for K right-hand sides in one pass over a row-major A:
+ * B (m x K), X = x*_k (n x K), Lam = lambda_k (n x K), column-major with
+ * leading dimensions ldb, ldx, ldl.  gradB (m x K, ld ldgb) = A Lam;
+ * gradA (m x n row-major, ld ldga; may be NULL) = sum_k r_k lambda_k^T -
+ * (A lambda_k) x_k^T.  Packed A is read at its exact values.  n * min(K, 8)
+ * must fit 25600 (X and Lam staged in shared memory). */
+tomos_status tomos_lsqr_adjoint_grad_dense(const tomos_dense* A, int64_t K, const float* B,
+                                           int64_t ldb, const float* X, int64_t ldx,
+                                           const float* Lam, int64_t ldl, float* gradB,
+                                           int64_t ldgb, float* gradA, int64_t ldga,
+                                           void* stream);
 
 #ifdef __cplusplus
 }

@@ -52,6 +52,7 @@ def lib():
         L.or_splitmix64.argtypes = [_u64]
         L.or_countsketch_hash.argtypes = [_sz, _sz, _u64, _u64, _vp, _vp]
         L.or_countsketch_apply_f64.argtypes = [_sz, _sz, _vp, _sz, _i32, _sz, _u64, _u64, _vp]
+        L.or_countsketch_apply_f32.argtypes = [_sz, _sz, _vp, _sz, _i32, _sz, _u64, _u64, _vp]
         L.or_householder_qr_f64.argtypes = [_sz, _sz, _vp, _sz, _vp]
         L.or_trtri_upper_f64.argtypes = [_sz, _vp, _sz, _vp, _sz]
         L.or_lsqr_f32.argtypes = [_sz, _sz, _vp, _sz, _vp, _vp, _vp, _dbl, _i32, _dbl, _i32, _vp, _vp]
@@ -168,15 +169,18 @@ def countsketch_hash(m, s, bucket_seed=BUCKET_SEED, sign_seed=SIGN_SEED):
     return b, g
 
 
-def countsketch_apply(A, s, row_major=True, bucket_seed=BUCKET_SEED, sign_seed=SIGN_SEED):
-    """SA (s x n, FP64) = S A for a float32 (m x n) array."""
+def countsketch_apply(A, s, row_major=True, bucket_seed=BUCKET_SEED, sign_seed=SIGN_SEED,
+                      acc="f64"):
+    """SA (s x n, returned as FP64) = S A for a float32 (m x n) array,
+    accumulated in FP64 (acc="f64") or, as the reference's float path, in
+    FP32 in increasing row order (acc="f32")."""
     A = np.asarray(A, np.float32)
     m, n = A.shape
     src = np.ascontiguousarray(A) if row_major else np.asfortranarray(A)
     ld = n if row_major else m
     SA = np.zeros((s, n), np.float64, order="F")
-    lib().or_countsketch_apply_f64(m, n, _P(src), ld, 1 if row_major else 0, s, bucket_seed,
-                                   sign_seed, _P(SA))
+    fn = lib().or_countsketch_apply_f32 if acc == "f32" else lib().or_countsketch_apply_f64
+    fn(m, n, _P(src), ld, 1 if row_major else 0, s, bucket_seed, sign_seed, _P(SA))
     return SA
 
 
@@ -237,6 +241,57 @@ def backward_error_scaled(A, b, x, d=None):
         d = np.linalg.norm(A, axis=0)
         d = np.where(d > 0, d, 1.0)
     return backward_error(A / d, b, np.asarray(x, np.float64) * d)
+
+
+def lstsq_grads_f64(A, B, G):
+    """FP64 normal-equations reference for the adjoint of X = argmin
+    ||A X - B|| (columnwise) and the loss sum_k <G_k, X_k>:
+    Lam = (A^T A)^{-1} G, dL/dB = A Lam, dL/dA = R Lam^T - (A Lam) X^T with
+    R = B - A X.  Returns (X, Lam, gradA, gradB)."""
+    A = np.asarray(A, np.float64)
+    B = np.asarray(B, np.float64).reshape(A.shape[0], -1)
+    G = np.asarray(G, np.float64).reshape(A.shape[1], -1)
+    N = A.T @ A
+    X = np.linalg.solve(N, A.T @ B)
+    Lam = np.linalg.solve(N, G)
+    R = B - A @ X
+    W = A @ Lam
+    return X, Lam, R @ Lam.T - W @ X.T, W
+
+
+def lstsq_loss_f64(A, B, G):
+    """sum_k <G_k, argmin ||A x - B_k||> in FP64 (Householder QR)."""
+    A = np.asarray(A, np.float64)
+    B = np.asarray(B, np.float64).reshape(A.shape[0], -1)
+    G = np.asarray(G, np.float64).reshape(A.shape[1], -1)
+    Q, R = np.linalg.qr(A)
+    X = np.linalg.solve(R, Q.T @ B)
+    return float(np.sum(G * X))
+
+
+def lstsq_fd_f64(A, B, G, entries_A, entries_B, h=1e-6):
+    """Central finite differences of lstsq_loss_f64 at the given (i, j)
+    entries of A and of B, step h."""
+    A = np.array(A, np.float64)
+    B = np.array(B, np.float64).reshape(A.shape[0], -1)
+    dA, dB = [], []
+    for (i, j) in entries_A:
+        a0 = A[i, j]
+        A[i, j] = a0 + h
+        lp = lstsq_loss_f64(A, B, G)
+        A[i, j] = a0 - h
+        lm = lstsq_loss_f64(A, B, G)
+        A[i, j] = a0
+        dA.append((lp - lm) / (2 * h))
+    for (i, k) in entries_B:
+        b0 = B[i, k]
+        B[i, k] = b0 + h
+        lp = lstsq_loss_f64(A, B, G)
+        B[i, k] = b0 - h
+        lm = lstsq_loss_f64(A, B, G)
+        B[i, k] = b0
+        dB.append((lp - lm) / (2 * h))
+    return np.array(dA), np.array(dB)
 
 
 def lsqr_f32(A, b, Rinv=None, tol=1e-6, max_iters=400, max_relres=1e-6, restarts=1):

@@ -184,6 +184,25 @@ void or_countsketch_apply_f64(size_t m, size_t n, const float* A, size_t ld,
     }
 }
 
+/* The reference's own float path (countsketch_kernels.cpp:70-83,
+ * countsketch_apply_impl<float>): Y[bucket] += sign * x in FP32, rows in
+ * increasing order.  SA is returned widened to FP64. */
+void or_countsketch_apply_f32(size_t m, size_t n, const float* A, size_t ld,
+                              int row_major, size_t s, uint64_t bucket_seed,
+                              uint64_t sign_seed, double* SA) {
+    float* acc = (float*)calloc(s * n, sizeof(float));
+    for (size_t i = 0; i < m; ++i) {
+        size_t bkt = (size_t)(or_splitmix64((uint64_t)i ^ bucket_seed) % (uint64_t)s);
+        float sg = (or_splitmix64((uint64_t)i ^ sign_seed) & 1ull) ? 1.0f : -1.0f;
+        for (size_t j = 0; j < n; ++j) {
+            float a = row_major ? A[i * ld + j] : A[i + j * ld];
+            acc[bkt + j * s] += sg * a;
+        }
+    }
+    for (size_t e = 0; e < s * n; ++e) SA[e] = (double)acc[e];
+    free(acc);
+}
+
 /* ---------------------------------------------------------------------
  * Householder QR, LAPACK dgeqr2/dlarfg convention (the reference calls
  * LAPACKE_dgeqrf at src/core/precond/sketch_qr.cpp:20-22,48): reflector

@@ -38,6 +38,9 @@ void or_countsketch_hash(size_t nrows, size_t s, uint64_t bucket_seed,
                          uint64_t sign_seed, int32_t* bucket, int8_t* sign);
 /* SA (s x n, col-major, zeroed by the caller) += S * A, FP64 accumulate.
  * A is m x n with leading dimension ld, column-major or row-major. */
+void or_countsketch_apply_f32(size_t m, size_t n, const float* A, size_t ld,
+                              int row_major, size_t s, uint64_t bucket_seed,
+                              uint64_t sign_seed, double* SA);
 void or_countsketch_apply_f64(size_t m, size_t n, const float* A, size_t ld,
                               int row_major, size_t s, uint64_t bucket_seed,
                               uint64_t sign_seed, double* SA);

@@ -125,20 +125,27 @@ def test_preconditioned_backward_error(orc, numeric, layout):
     assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-2
 
 
+@pytest.mark.parametrize("tier", [tb.Tier.AUTO, tb.Tier.ACCURATE])
 @pytest.mark.parametrize("numeric", [NT.FP32, NT.FP32_16, NT.FP32_BF16])
-@pytest.mark.parametrize("n,ld", [(257, 264), (1000, 1000), (1001, 1008), (500, 512)])
-def test_fused_pass_matches_oracle_lsqr(orc, numeric, n, ld):
-    """The TMA-staged fused pass (row-major, one CTA per SM) against the
-    oracle's LSQR on the values the tier reads: the same 6 iterations give
-    the same x (FP32 arithmetic in both, different summation order)."""
+@pytest.mark.parametrize("n,ld", [(257, 264), (1000, 1000), (1001, 1008), (500, 512),
+                                  (1500, 1504), (2000, 2000), (3001, 3008)])
+def test_fused_pass_matches_oracle_lsqr(orc, numeric, n, ld, tier):
+    """The staged fused pass (row-major, one CTA per SM; one warp per row
+    up to 1024 columns, 2 or 4 beyond) against the oracle's LSQR on the
+    values the tier reads: the same 6 iterations give the same x (FP32
+    arithmetic in both, different summation order).  ACCURATE runs the
+    iterations on the exact (wh + wr) values with FP64 chunk sums."""
+    if tier == tb.Tier.ACCURATE and numeric == NT.FP32:
+        pytest.skip("FP32 storage has one tier")
     m = 6000
     rng = np.random.default_rng(n)
     A0 = (rng.standard_normal((m, n)) * np.where(rng.random((m, n)) < 0.02, 1e-6, 1.0)).astype(np.float32)
     b = rng.standard_normal(m).astype(np.float32)
     A = to_dense(A0, L.ROW_MAJOR, numeric, pad=ld - n)
-    Ad = decoded(orc, A, tb.Tier.HALF if numeric != NT.FP32 else tb.Tier.AUTO).astype(np.float32)
+    read = tb.Tier.AUTO if numeric == NT.FP32 else (tb.Tier.HALF if tier == tb.Tier.AUTO else tier)
+    Ad = decoded(orc, A, read).astype(np.float32)
     x_ref, it_ref, h_ref = orc.lsqr_f32(Ad, b, None, 0.0, 6, 0.0, 1)
-    x, rep = solve(A, b, tol=0.0, max_iters=6, max_relres=0.0)
+    x, rep = solve(A, b, tol=0.0, max_iters=6, max_relres=0.0, tier=tier)
     assert rep["iterations"] == it_ref == 6
     np.testing.assert_allclose(rep["history"][:6], h_ref[:6], rtol=1e-4)
     assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-4

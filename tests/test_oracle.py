@@ -93,6 +93,23 @@ def test_countsketch_hash_golden(orc):
         assert np.array_equal(b, g[f"bucket_s{s}"]) and np.array_equal(sg, g[f"sign_s{s}"])
     SA = orc.countsketch_apply(g["X"], 64, row_major=False)
     np.testing.assert_allclose(SA, g["Y"], rtol=1e-5, atol=1e-5)
+    # the float restatement is the reference's float path bit for bit
+    SA32 = orc.countsketch_apply(g["X"], 64, row_major=False, acc="f32")
+    assert np.array_equal(SA32.astype(np.float32), g["Y"])
+
+
+def test_countsketch_f32_matches_reference_build(orc):
+    if not orc.ref_available():
+        pytest.skip("reference CPU build not present")
+    import ctypes
+    rng = np.random.default_rng(12)
+    X = np.asfortranarray((rng.standard_normal((3001, 17)) * np.logspace(-3, 3, 17)).astype(np.float32))
+    Y = np.zeros((97, 17), np.float32, order="F")
+    sz = ctypes.c_size_t
+    orc.ref().ref_countsketch_apply_f32(sz(3001), sz(17), X.ctypes.data_as(ctypes.c_void_p), sz(3001),
+                                       sz(97), Y.ctypes.data_as(ctypes.c_void_p), sz(97))
+    SA = orc.countsketch_apply(X, 97, row_major=False, acc="f32")
+    assert np.array_equal(SA.astype(np.float32), Y)
 
 
 def test_countsketch_linear_and_norm_unbiased(orc):

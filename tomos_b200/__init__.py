@@ -487,6 +487,44 @@ def backward_error(A, b, x, workspace, col_scale=None, stream=None):
     return rep.as_dict()
 
 
+def lsqr_adjoint(A, g, workspace, tol=1e-7, max_iters=500, tier=None, stream=None):
+    """lambda = (A^T A)^{-1} g by preconditioned CG with the workspace's
+    R^{-1} (tomos_lsqr_adjoint_dense).  g: float32 CUDA tensor (n).
+    Returns (lambda, report)."""
+    opts = C.LsqrOpts()
+    opts.tol = float(tol)
+    opts.max_iters = int(max_iters)
+    opts.restarts = 1
+    opts.iter_tier = int(Tier.AUTO if tier is None else Tier(tier))
+    lam = torch.empty(A.size[1], dtype=torch.float32, device="cuda")
+    rep = C.LsqrReport()
+    d = A.desc()
+    C.check(C.lib().tomos_lsqr_adjoint_dense(ctypes.byref(d), _ptr(_vec(g)), _ptr(lam),
+                                             workspace.handle, ctypes.byref(opts),
+                                             ctypes.byref(rep), _stream(stream)),
+            "lsqr_adjoint")
+    return lam, rep.as_dict()
+
+
+def lsqr_adjoint_grad(A, B, X, Lam, want_grad_a=True, stream=None):
+    """dL/dB = A Lam and dL/dA = (B - A X) Lam^T - (A Lam) X^T in one pass
+    over the row-major A (tomos_lsqr_adjoint_grad_dense).  B: (m, K), X and
+    Lam: (n, K) float32 CUDA tensors.  Returns (gradA or None, gradB)."""
+    m, n = A.size
+    K = B.shape[1]
+    Bc = B.t().contiguous()  # column-major (m x K)
+    Xc = X.t().contiguous()
+    Lc = Lam.t().contiguous()
+    gB = torch.empty((K, m), dtype=torch.float32, device="cuda")
+    gA = torch.empty((m, n), dtype=torch.float32, device="cuda") if want_grad_a else None
+    d = A.desc()
+    C.check(C.lib().tomos_lsqr_adjoint_grad_dense(ctypes.byref(d), K, _ptr(Bc), m, _ptr(Xc), n,
+                                                  _ptr(Lc), n, _ptr(gB), m, _ptr(gA), n,
+                                                  _stream(stream)),
+            "lsqr_adjoint_grad")
+    return gA, gB.t()
+
+
 def column_scale(colsq):
     """D = column norms from column sums of squares (zero columns -> 1), and
     ||A D^{-1}||_F for it."""

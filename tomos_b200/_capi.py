@@ -99,6 +99,11 @@ SIGNATURES = {
                                      ctypes.POINTER(LsqrOpts), ctypes.POINTER(LsqrReport), c_vp]),
     "tomos_backward_error_dense": (c_i32, [ctypes.POINTER(DenseDesc), c_vp, c_vp, c_vp, c_vp,
                                            ctypes.POINTER(LsqrReport), c_vp]),
+    "tomos_lsqr_adjoint_dense": (c_i32, [ctypes.POINTER(DenseDesc), c_vp, c_vp, c_vp,
+                                         ctypes.POINTER(LsqrOpts), ctypes.POINTER(LsqrReport),
+                                         c_vp]),
+    "tomos_lsqr_adjoint_grad_dense": (c_i32, [ctypes.POINTER(DenseDesc), c_i64, c_vp, c_i64, c_vp,
+                                              c_i64, c_vp, c_i64, c_vp, c_i64, c_vp, c_i64, c_vp]),
 }
 
 

@@ -185,7 +185,9 @@ enum class Elem : int {
     A16 = 3,       // FP32_16, wh + wr exact
     B16 = 4,       // FP32_BF16, wh plane only (bf16 value)
     AB16 = 5,      // FP32_BF16 truncating, wh + wr exact
-    AB16R = 6      // FP32_BF16 rounded, wh + wr (combine_rounded)
+    AB16R = 6,     // FP32_BF16 rounded, wh + wr (combine_rounded)
+    F16 = 7        // IEEE fp16 (the solver's staged copy of an FP32_16 wh
+                   // plane, control words already decoded)
 };
 
 // Scalar element decode at flat index idx (generic kernels).
@@ -238,7 +240,7 @@ inline int elem_bytes(Elem e) {
     switch (e) {
         case Elem::F32: return 4;
         case Elem::F64: return 8;
-        case Elem::H16: case Elem::B16: return 2;
+        case Elem::H16: case Elem::B16: case Elem::F16: return 2;
         default: return 4;  // wh + wr
     }
 }

@@ -8,7 +8,7 @@
 // leave the iterates mathematically unchanged:
 //   * u is kept unnormalised: the A pass produces ut = A p - (alpha/beta) ut
 //     (p = M v), so A^T u = A^T ut / beta comes from the same pass over A
-//     (fused.cuh) instead of a second one;
+//     (rowpass.cuh) instead of a second one;
 //   * w is kept in x-space (wt = M w), so x += (phi/rho) wt and
 //     wt = p - (theta/rho) wt need no third product with M per iteration.
 // Every scalar of the recurrence (alpha, beta, rho, rho_bar, phi, phi_bar,
@@ -30,38 +30,13 @@
 
 #include "common.cuh"
 #include "fused.cuh"
-#include "fused_tma.cuh"
 #include "gemv.cuh"
 #include "lsqr.cuh"
+#include "rowpass.cuh"
 
 namespace tomos_b200 {
 
 // ------------------------------------------------------------ reductions
-
-__device__ __forceinline__ double block_sum(double v, double* sm) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    v = warp_sum(v);
-    __syncthreads();
-    if (lane == 0) sm[w] = v;
-    __syncthreads();
-    double r = 0.0;
-    if (w == 0) {
-        r = lane < nw ? sm[lane] : 0.0;
-        r = warp_sum(r);
-        if (lane == 0) sm[0] = r;
-    }
-    __syncthreads();
-    r = sm[0];
-    __syncthreads();
-    return r;
-}
-
-// Block-wide fixed-order sum of part[0..np).
-__device__ __forceinline__ double block_sum_array(const double* part, int64_t np, double* sm) {
-    double s = 0.0;
-    for (int64_t k = threadIdx.x; k < np; k += blockDim.x) s += part[k];
-    return block_sum(s, sm);
-}
 
 __global__ void sumsq_partial_kernel(const float* __restrict__ x, int64_t n, const int* skip,
                                      double* __restrict__ part) {
@@ -367,7 +342,7 @@ static void ws_free(tomos_workspace* ws) {
     void* ptrs[] = {ws->u,      ws->v,      ws->wt,     ws->p,    ws->qvec,   ws->t,
                     ws->vhat,   ws->qpart,  ws->sspart, ws->vpart, ws->xpart, ws->qnpart,
                     ws->scal,   ws->coef_init, ws->bpart, ws->fro2, ws->st,   ws->Rcm,
-                    ws->Rrm,    ws->hist,   ws->scratch};
+                    ws->Rrm,    ws->hist,   ws->scratch, ws->h16, ws->adj};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (ws->st_host) cudaFreeHost(ws->st_host);
@@ -409,65 +384,117 @@ static tomos_status ensure_history(tomos_workspace* ws, int cap) {
 
 // ------------------------------------------------------------ A passes
 
-template <Elem E, int NCH, bool ACC64>
+template <Elem E, int NCH, int G, bool ACC64>
 static tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
-    constexpr int VEC = ChunkElems<E>::value;
-    const int esz = (E == Elem::F32) ? 4 : 2;
-    TmaParams T;
+    constexpr int ESZ = (E == Elem::F32) ? 4 : 2;
+    constexpr int RS = kRowWarps / G;
+    RowPassParams T;
     T.f = P;
     T.err = err;
-    T.copy_bytes = (int)((((int64_t)P.n * esz) + 15) / 16 * 16);
-    const size_t stage = (size_t)kTmaRows * T.copy_bytes * SmemChunk<E>::planes;
-    int ns = (int)(kTmaSmemBudget / stage);
-    if (ns > kTmaMaxStages) ns = kTmaMaxStages;
+    T.copy_bytes = (int)((((int64_t)P.n * ESZ) + 15) / 16 * 16);
+    const size_t stage = (size_t)RS * T.copy_bytes * RowPlanes<E>::value;
+    int ns = (int)(kRowSmemBudget / stage);
+    if (ns > kRowMaxStages) ns = kRowMaxStages;
     if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
     T.nstage = ns;
-    const size_t smem = fused_tma_smem<E, NCH>(ns, T.copy_bytes);
-    static_assert(VEC > 0, "");
-    TOMOS_CUDA_TRY(cudaFuncSetAttribute(fused_tma_kernel<E, NCH, ACC64>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    fused_tma_kernel<E, NCH, ACC64><<<grid, kTmaThreads, smem, st>>>(T);
-    TOMOS_LAUNCH_CHECK("fused_tma_kernel");
+    const size_t smem = fused_rows_smem<E, NCH>(ns, RS, T.copy_bytes);
+    auto kern = fused_rows_kernel<E, NCH, G, ACC64>;
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, kRowThreads, smem, st>>>(T);
+    TOMOS_LAUNCH_CHECK("fused_rows_kernel");
     return TOMOS_OK;
 }
 
+// Columns one consumer warp covers at its widest: 32 lanes x 16-byte
+// chunks x (4, 16-bit storage / 8, FP32) -- halved for ACC64, whose p is
+// held in FP64 registers.
+static int fused_nch_max(Elem e, bool acc64) {
+    const int nmax = (e == Elem::F32) ? 8 : 4;
+    return acc64 ? nmax / 2 : nmax;
+}
+
+// (nch, g) pairs with an instantiation: one warp per row with 1..NCHMAX
+// chunks per lane, or G = 2, 3, 4, 6, 12 warps per row at NCHMAX.
 template <Elem E, bool ACC64>
-static tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int grid,
+static tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int g, int grid,
                                    cudaStream_t st) {
-    switch (nch) {
-        case 1: return launch_fused_t<E, 1, ACC64>(P, err, grid, st);
-        case 2: return launch_fused_t<E, 2, ACC64>(P, err, grid, st);
-        case 4: return launch_fused_t<E, 4, ACC64>(P, err, grid, st);
-        case 8:
-            if constexpr (E == Elem::F32) return launch_fused_t<E, 8, ACC64>(P, err, grid, st);
-            return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
-        default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
+    constexpr int NMAX = ((E == Elem::F32) ? 8 : 4) / (ACC64 ? 2 : 1);
+    if (g == 1) {
+        switch (nch) {
+            case 1: return launch_fused_t<E, 1, 1, ACC64>(P, err, grid, st);
+            case 2: return launch_fused_t<E, 2, 1, ACC64>(P, err, grid, st);
+            case 4:
+                if constexpr (NMAX >= 4) return launch_fused_t<E, 4, 1, ACC64>(P, err, grid, st);
+                break;
+            case 8:
+                if constexpr (NMAX == 8) return launch_fused_t<E, 8, 1, ACC64>(P, err, grid, st);
+                break;
+            default: break;
+        }
+    } else if (nch == NMAX) {
+        switch (g) {
+            case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
+            case 3: return launch_fused_t<E, NMAX, 3, ACC64>(P, err, grid, st);
+            case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
+            case 6: return launch_fused_t<E, NMAX, 6, ACC64>(P, err, grid, st);
+            case 12: return launch_fused_t<E, NMAX, 12, ACC64>(P, err, grid, st);
+            default: break;
+        }
     }
+    return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
 }
 
 static tomos_status launch_fused(Elem e, bool acc64, const FusedParams& P, int* err, int nch,
-                                 int grid, cudaStream_t st) {
+                                 int g, int grid, cudaStream_t st) {
     switch (e) {
         case Elem::F32:
-            return acc64 ? launch_fused_e<Elem::F32, true>(P, err, nch, grid, st)
-                         : launch_fused_e<Elem::F32, false>(P, err, nch, grid, st);
+            return acc64 ? launch_fused_e<Elem::F32, true>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::F32, false>(P, err, nch, g, grid, st);
         case Elem::H16:
-            return acc64 ? launch_fused_e<Elem::H16, true>(P, err, nch, grid, st)
-                         : launch_fused_e<Elem::H16, false>(P, err, nch, grid, st);
+            return acc64 ? launch_fused_e<Elem::H16, true>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::H16, false>(P, err, nch, g, grid, st);
         case Elem::B16:
-            return acc64 ? launch_fused_e<Elem::B16, true>(P, err, nch, grid, st)
-                         : launch_fused_e<Elem::B16, false>(P, err, nch, grid, st);
-        case Elem::A16: return launch_fused_e<Elem::A16, true>(P, err, nch, grid, st);
-        case Elem::AB16: return launch_fused_e<Elem::AB16, true>(P, err, nch, grid, st);
-        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true>(P, err, nch, grid, st);
+            return acc64 ? launch_fused_e<Elem::B16, true>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::B16, false>(P, err, nch, g, grid, st);
+        case Elem::F16:
+            return acc64 ? launch_fused_e<Elem::F16, true>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::F16, false>(P, err, nch, g, grid, st);
+        case Elem::A16: return launch_fused_e<Elem::A16, true>(P, err, nch, g, grid, st);
+        case Elem::AB16: return launch_fused_e<Elem::AB16, true>(P, err, nch, g, grid, st);
+        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true>(P, err, nch, g, grid, st);
         default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: element type");
     }
 }
 
+// wh plane of a row-major FP32_16 A -> IEEE fp16 words with the
+// fp32_16_half_only values (fp32_16_pack.hpp:553-571), rows of ldh words;
+// a block per row, a thread per 16-byte chunk.  Control-bit words are
+// rare and scattered: here a chunk holding one costs that one thread a few
+// instructions, where inside the LSQR pass the whole warp would wait on
+// it every iteration.
+__global__ void __launch_bounds__(128) stage_half_kernel(const uint16_t* __restrict__ wh,
+                                                         int64_t m, int64_t ld, int64_t nch,
+                                                         uint16_t* __restrict__ h16, int64_t ldh) {
+    for (int64_t r = blockIdx.x; r < m; r += gridDim.x) {
+        const uint4* src = reinterpret_cast<const uint4*>(wh + (size_t)r * ld);
+        uint4* dst = reinterpret_cast<uint4*>(h16 + (size_t)r * ldh);
+        for (int64_t c = threadIdx.x; c < nch; c += blockDim.x) {
+            uint4 w = __ldcs(src + c);
+            if ((w.x | w.y | w.z | w.w) & 0x00010001u) {
+                if (w.x & 0x00010001u) w.x = fix_half_pair(w.x);
+                if (w.y & 0x00010001u) w.y = fix_half_pair(w.y);
+                if (w.z & 0x00010001u) w.z = fix_half_pair(w.z);
+                if (w.w & 0x00010001u) w.w = fix_half_pair(w.w);
+            }
+            dst[c] = w;
+        }
+    }
+}
+
 // Chooses the fused pass when A is row-major with 16-byte aligned rows
-// and n fits one warp's register-resident columns; otherwise the generic
-// two-kernel path.
-static PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64) {
+// and n fits 12 consumer warps (12288 columns, 6144 for ACC64); otherwise
+// the generic two-kernel path.
+PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64) {
     PassPlan pl;
     pl.e = e;
     pl.acc64 = acc64 || elem_is_exact(e);
@@ -477,23 +504,34 @@ static PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem 
               (reinterpret_cast<uintptr_t>(A->values) % 16 == 0);
     if (ok && elem_is_exact(e))
         ok = reinterpret_cast<uintptr_t>(dense_lo_plane(A)) % 16 == 0;
-    int nch = 0;
+    int nch = 0, g = 1;
+    const int nmax = fused_nch_max(e, pl.acc64);
     for (int c : {1, 2, 4, 8}) {
-        if (c == 8 && e != Elem::F32) break;
+        if (c > nmax) break;
         if ((int64_t)32 * c * vec >= A->cols) {
             nch = c;
             break;
         }
     }
+    if (nch == 0) {
+        for (int gg : {2, 3, 4, 6, 12}) {
+            if ((int64_t)gg * 32 * nmax * vec >= A->cols) {
+                nch = nmax;
+                g = gg;
+                break;
+            }
+        }
+    }
     if (ok && nch > 0 && A->cols > 0) {
         pl.fused = true;
         pl.nch = nch;
-        int64_t g = sm_count();
-        int64_t min_rows_cta = 64;
-        int64_t gr = (A->rows + min_rows_cta - 1) / min_rows_cta;
-        if (g > gr) g = gr;
-        if (g < 1) g = 1;
-        pl.grid = (int)g;
+        pl.g = g;
+        int64_t grid = sm_count();
+        const int64_t min_rows_cta = 64;
+        const int64_t gr = (A->rows + min_rows_cta - 1) / min_rows_cta;
+        if (grid > gr) grid = gr;
+        if (grid < 1) grid = 1;
+        pl.grid = (int)grid;
         pl.gq = pl.grid;
         pl.gs = pl.grid;
         pl.qstride = ws->qstride;
@@ -506,7 +544,7 @@ static PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem 
     return pl;
 }
 
-static size_t dense_pass_scratch(const tomos_dense* A) {
+size_t dense_pass_scratch(const tomos_dense* A) {
     size_t a = gemv_scratch_bytes_max(A, TOMOS_NO_TRANSPOSE);
     size_t b = gemv_scratch_bytes_max(A, TOMOS_TRANSPOSE);
     return a > b ? a : b;
@@ -514,7 +552,7 @@ static size_t dense_pass_scratch(const tomos_dense* A) {
 
 // Enqueues one A pass.  p: right vector; u_in: vector combined with cu;
 // coef: device [cp, cu]; skip: device stop flag (NULL for unconditional).
-static tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A,
+tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A,
                                        const PassPlan& pl, const float* p, const float* u_in,
                                        const double* coef, const int* skip, cudaStream_t st) {
     const void* lo = elem_is_exact(pl.e) ? dense_lo_plane(A) : nullptr;
@@ -533,7 +571,7 @@ static tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A
         P.sspart = ws->sspart;
         P.qstride = pl.qstride;
         P.skip = skip;
-        tomos_status ls = launch_fused(pl.e, pl.acc64, P, &ws->st->pipe_err, pl.nch, pl.grid, st);
+        tomos_status ls = launch_fused(pl.e, pl.acc64, P, &ws->st->pipe_err, pl.nch, pl.g, pl.grid, st);
         if (ls) return ls;
         ws->launches += 1;
         return TOMOS_OK;
@@ -626,18 +664,58 @@ static tomos_status enqueue_nside(tomos_workspace* ws, const NSide& S, cudaStrea
     return TOMOS_OK;
 }
 
+// HALF-tier iterations over a row-major FP32_16 A read a staged fp16 copy
+// of its wh plane (one conversion per solve, in the workspace); the
+// restart passes read A itself.
 struct DensePass : PassOps {
     tomos_workspace* ws;
     const tomos_dense* A;
     Elem iter_e, init_e;
+    bool stage = false;
+    tomos_dense staged{};
     DensePass(tomos_workspace* w, const tomos_dense* a, Elem ie, Elem ze)
-        : ws(w), A(a), iter_e(ie), init_e(ze) {}
+        : ws(w), A(a), iter_e(ie), init_e(ze) {
+        stage = ie == Elem::H16 && plan_dense_pass(ws, A, ie, false).fused;
+        staged = *A;  // values set by prepare()
+        staged.values_lo = nullptr;
+        staged.ld = (A->cols + 7) / 8 * 8;
+    }
+    tomos_status prepare(cudaStream_t st) override {
+        if (!stage) return TOMOS_OK;
+        const int64_t m = A->rows, n = A->cols, ldh = (n + 7) / 8 * 8;
+        const size_t bytes = (size_t)m * ldh * sizeof(uint16_t);
+        if (bytes > ws->h16_bytes) {
+            if (ws->h16) cudaFree(ws->h16);
+            ws->h16 = nullptr;
+            ws->h16_bytes = 0;
+            if (cudaMalloc(&ws->h16, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                stage = false;  // not enough memory: iterate on A itself
+                return TOMOS_OK;
+            }
+            ws->h16_bytes = bytes;
+        }
+        staged = *A;
+        staged.values = ws->h16;
+        staged.values_lo = nullptr;
+        staged.ld = ldh;
+        int64_t grid = (int64_t)sm_count() * 16;
+        if (grid > m) grid = m;
+        if (grid < 1) grid = 1;
+        stage_half_kernel<<<(unsigned)grid, 128, 0, st>>>(static_cast<const uint16_t*>(A->values), m,
+                                                          A->ld, ldh / 8, static_cast<uint16_t*>(ws->h16),
+                                                          ldh);
+        TOMOS_LAUNCH_CHECK("stage_half_kernel");
+        ws->launches += 1;
+        return TOMOS_OK;
+    }
     PassPlan plan(bool init) override {
+        if (!init && stage) return plan_dense_pass(ws, &staged, Elem::F16, false);
         return plan_dense_pass(ws, A, init ? init_e : iter_e, init);
     }
     tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
                          const int* skip, cudaStream_t st) override {
-        return enqueue_dense_pass(ws, A, pl, p, u_in, coef, skip, st);
+        return enqueue_dense_pass(ws, pl.e == Elem::F16 ? &staged : A, pl, p, u_in, coef, skip, st);
     }
     tomos_status fro2(double* out, const double* d, cudaStream_t st) override {
         bool dot;
@@ -665,13 +743,23 @@ struct DensePass : PassOps {
     }
     uint64_t key() override {
         return reinterpret_cast<uint64_t>(A->values) ^ ((uint64_t)A->layout << 60) ^
-               ((uint64_t)A->ld << 20);
+               ((uint64_t)A->ld << 20) ^ (stage ? reinterpret_cast<uint64_t>(ws->h16) * 31 : 0);
     }
     int64_t rows() override { return A->rows; }
     int64_t cols() override { return A->cols; }
 };
 
 // ------------------------------------------------------------ driver
+
+tomos_status refresh_precond(tomos_workspace* ws, cudaStream_t st) {
+    if (!ws->has_precond) return TOMOS_OK;
+    precond_copy_kernel<<<ws->gs_max, 256, 0, st>>>(ws->precond.values, ws->precond.numeric,
+                                                   ws->precond.layout, ws->precond.ld, ws->n,
+                                                   ws->Rcm, ws->Rrm);
+    TOMOS_LAUNCH_CHECK("precond_copy_kernel");
+    ws->launches += 1;
+    return TOMOS_OK;
+}
 
 static tomos_status sync_state(tomos_workspace* ws) {
     TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->st_host, ws->st, sizeof(LsqrDev), cudaMemcpyDeviceToHost,
@@ -712,14 +800,11 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     if (s) return s;
 
     // Precondition copies (FP64, both orientations).
-    if (ws->has_precond) {
-        precond_copy_kernel<<<ws->gs_max, 256, 0, st>>>(ws->precond.values, ws->precond.numeric,
-                                                       ws->precond.layout, ws->precond.ld, n,
-                                                       ws->Rcm, ws->Rrm);
-        TOMOS_LAUNCH_CHECK("precond_copy_kernel");
-        ws->launches += 1;
-    }
+    s = refresh_precond(ws, st);
+    if (s) return s;
     if (!o->warm_start) TOMOS_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(float) * n, st));
+    s = ops.prepare(st);
+    if (s) return s;
 
     // ||b|| and, for the backward-error rule, ||A||_F.
     sumsq_partial_kernel<<<ws->gs_max, 256, 0, st>>>(b, m, nullptr, ws->bpart);
@@ -768,6 +853,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
                                  (uint64_t)pl_iter.fused,
                                  (uint64_t)pl_iter.e,
                                  (uint64_t)pl_iter.nch,
+                                 (uint64_t)pl_iter.g,
                                  (uint64_t)pl_iter.grid,
                                  reinterpret_cast<uint64_t>(x),
                                  (uint64_t)ws->has_precond,
@@ -813,26 +899,33 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
                 break;
             }
         }
-        // initialize(): ut = b - A x (restarted from the current x).
+        // initialize(): ut = b - A x (restarted from the current x).  From
+        // x = 0 the pass only forms A^T b, so it runs at the iteration tier
+        // (the operator the inner iterations then use); later restarts
+        // need the residual of the accurate A.
         restarts_used = rs + 1;
+        const PassPlan& pz = (rs == 0 && !o->warm_start) ? pl_iter : pl_init;
         if (o->profile) TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pa, st));
-        s = ops.enqueue(pl_init, x, b, ws->coef_init, nullptr, st);
+        s = ops.enqueue(pz, x, b, ws->coef_init, nullptr, st);
         if (s) return s;
         if (o->profile) TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pb, st));
-        s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr, dsc), st);
+        s = enqueue_nside(ws, make_nside(ws, pz, x, true, nullptr, dsc), st);
         if (s) return s;
-        if (pl_init.e == Elem::A16 || pl_init.e == Elem::AB16 || pl_init.e == Elem::AB16R ||
-            pl_init.e != pl_iter.e)
+        if (&pz == &pl_init && (elem_is_exact(pz.e) || pz.e != pl_iter.e || pz.acc64 != pl_iter.acc64))
             ++accurate_passes;
         else
             ++iter_passes;
         s = sync_state(ws);
         if (s) return s;
         if (o->profile) {
+            // restart passes at the accurate tier only (the x = 0 pass is
+            // an iteration-tier pass)
             float pm = 0.0f;
             TOMOS_CUDA_TRY(cudaEventElapsedTime(&pm, ws->ev_pa, ws->ev_pb));
-            R.init_pass_ms += pm;
-            R.init_pass_count += 1;
+            if (&pz == &pl_init) {
+                R.init_pass_ms += pm;
+                R.init_pass_count += 1;
+            }
         }
         if (H.rhsnorm == 0.0) {
             converged = true;

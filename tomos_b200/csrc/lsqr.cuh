@@ -42,6 +42,7 @@ struct PassPlan {
     bool acc64 = false;
     int grid = 0;    // fused CTAs
     int nch = 0;     // fused chunks per lane
+    int g = 1;       // fused consumer warps per row
     int gq = 1;      // rows of A^T partials
     int gs = 1;      // ||ut||^2 partials
     int64_t qstride = 0;
@@ -60,7 +61,46 @@ struct PassOps {
     virtual uint64_t key() = 0;
     virtual int64_t rows() = 0;
     virtual int64_t cols() = 0;
+    // Work done once per solve before the first pass (e.g. staging).
+    virtual tomos_status prepare(cudaStream_t) { return TOMOS_OK; }
 };
+
+// Block-wide sums (every thread gets the result), fixed order.
+__device__ __forceinline__ double block_sum(double v, double* sm) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < nw ? sm[lane] : 0.0;
+        r = warp_sum(r);
+        if (lane == 0) sm[0] = r;
+    }
+    __syncthreads();
+    r = sm[0];
+    __syncthreads();
+    return r;
+}
+
+// Block-wide fixed-order sum of part[0..np).
+__device__ __forceinline__ double block_sum_array(const double* part, int64_t np, double* sm) {
+    double s = 0.0;
+    for (int64_t k = threadIdx.x; k < np; k += blockDim.x) s += part[k];
+    return block_sum(s, sm);
+}
+
+// One pass over a dense A (the fused kernel when pl.fused, else the
+// generic two-kernel path): ut = cp A p + cu u_in into ws->u, the
+// partials of A^T ut into ws->qpart and of ||ut||^2 into ws->sspart.
+PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64);
+tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A, const PassPlan& pl,
+                                const float* p, const float* u_in, const double* coef,
+                                const int* skip, cudaStream_t st);
+size_t dense_pass_scratch(const tomos_dense* A);
+// FP64 row- and column-major copies of the attached R^{-1} (Rrm, Rcm).
+tomos_status refresh_precond(tomos_workspace* ws, cudaStream_t st);
 
 tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, float* x,
                           const tomos_lsqr_opts* o, tomos_lsqr_report* rep, void* user_stream);
@@ -101,6 +141,13 @@ struct tomos_workspace {
     int hist_cap = 0;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
+    // fp16 copy of an FP32_16 wh plane for HALF-tier iterations (row-major,
+    // ld a multiple of 8), allocated on the first solve that stages one.
+    void* h16 = nullptr;
+    size_t h16_bytes = 0;
+    // adjoint solve (adjoint.cu): FP64 n-vectors and its device state,
+    // allocated by the first adjoint call.
+    void* adj = nullptr;
 
     bool has_precond = false;
     tomos_dense precond{};

@@ -8,47 +8,50 @@
 // dgeqr2/dlarfg convention, H_j = I - tau_j v_j v_j^T with v_j(0) = 1 and
 // R_jj = -sign(a_jj) ||a_j||, so R matches the reference's R to rounding.
 //
-// Blocked right-looking algorithm, panel width nb (32 when it fits):
-//   panel    one 8-CTA thread-block cluster factors the (k-j0) x nb panel
-//            held in the CTAs' shared memory (row blocks); the two
-//            reductions of each column step (the norm below the diagonal
-//            and the reflector's inner products with the later panel
-//            columns) are exchanged through distributed shared memory
-//            with cluster barriers.  The cluster also forms the compact-WY
-//            factor T (H_1...H_nb = I - V T V^T).
-//   update   C <- (I - V T^T V^T) C on the trailing columns in three
-//            kernels: W = V^T C partials per row chunk, W <- T^T (sum),
-//            C -= V W.
-// R^{-1} is then formed column by column (a warp per column, back
-// substitution on a transposed copy of R).
-#include <cooperative_groups.h>
-
+// Blocked right-looking algorithm with 32-column panels:
+//   panel    Cholesky QR twice and Householder reconstruction
+//            (qr_panel.cuh): three row-parallel passes give the panel's
+//            reflectors V, the compact-WY factor T (H_1...H_nb = I - V T V^T),
+//            tau and R, in the layout dgeqrf leaves them.
+//   update   C <- (I - V T^T V^T) C on the trailing columns in two kernels:
+//            W = V^T C partials per row chunk (qr_w_part_kernel), then per
+//            tile the fixed-order sum of the partials, W' = T^T W and
+//            C -= V W' (qr_apply_kernel).  The tiles holding the next
+//            panel's columns also leave that panel's Gram partials.
+// R^{-1} is then formed recursively: 32 x 32 diagonal blocks by back
+// substitution, then levels of X_IJ = -X_II R_IJ X_JJ with doubling block
+// size, each two batched FP64 products.
 #include <string>
 
 #include "common.cuh"
-
-namespace cg = cooperative_groups;
+#include "qr_panel.cuh"
 
 namespace tomos_b200 {
 
-constexpr int kQrCluster = 8;
 constexpr int kQrThreads = 256;
-constexpr int kQrChunk = 64;      // rows per trailing-update block
-constexpr int kQrTile = 32;       // columns per trailing-update block
-constexpr int kQrMaxNb = 32;
-constexpr size_t kQrPanelSmem = 196 * 1024;
+constexpr int kQrNb = 32;        // panel width
+constexpr int kQrWc = 64;        // trailing columns per update tile
+constexpr int kQrChunks = 8;     // row chunks of the W partials
+constexpr int kQrRowTile = 256;  // rows per apply tile (and per Gram partial)
+constexpr int kQrPanelCtas = 16; // CTAs of the panel passes
 
 struct QrScratch {
     double* tau;    // n
-    double* T;      // kQrMaxNb^2
-    double* Wp;     // chunks x nb x n   (W partials)
-    double* W2;     // nb x n
+    double* T;      // 32 x 32
+    double* R1;     // 32 x 32
+    double* Gp;     // Gram partials of the next panel (k / 256 tiles)
+    double* G2p;    // Gram partials of Q1 (kQrPanelCtas)
+    double* Qs;     // Q1 of the current panel, k x 32 column-major
+    double* Wp;     // kQrChunks x 32 x n  (W partials)
     double* Rt;     // n x n  (R transposed: row i of R contiguous)
-    int* flag;      // singular-R flag
+    double* Tb;     // products of one level of the recursive inversion
+    int* flag;      // [0] singular R, [1] panel fallback
     size_t bytes;
 };
 
 static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int64_t qr_row_tiles(int64_t rows) { return (rows + kQrRowTile - 1) / kQrRowTile; }
 
 static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
     QrScratch q;
@@ -59,337 +62,222 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
         off += a256(b);
         return r;
     };
-    const int64_t chunks = (k + kQrChunk - 1) / kQrChunk;
-    q.tau = reinterpret_cast<double*>(take(sizeof(double) * (n > 0 ? n : 1)));
-    q.T = reinterpret_cast<double*>(take(sizeof(double) * kQrMaxNb * kQrMaxNb));
-    q.Wp = reinterpret_cast<double*>(take(sizeof(double) * (chunks > 0 ? chunks : 1) * kQrMaxNb *
-                                          (n > 0 ? n : 1)));
-    q.W2 = reinterpret_cast<double*>(take(sizeof(double) * kQrMaxNb * (n > 0 ? n : 1)));
-    q.Rt = reinterpret_cast<double*>(take(sizeof(double) * (n > 0 ? n * n : 1)));
+    const size_t nn = n > 0 ? (size_t)n : 1, kk = k > 0 ? (size_t)k : 1;
+    const size_t tiles = (size_t)qr_row_tiles(k > 0 ? k : 1);
+    q.tau = reinterpret_cast<double*>(take(sizeof(double) * nn));
+    q.T = reinterpret_cast<double*>(take(sizeof(double) * kHB * kHB));
+    q.R1 = reinterpret_cast<double*>(take(sizeof(double) * kHB * kHB));
+    q.Gp = reinterpret_cast<double*>(take(sizeof(double) * tiles * kHB * kHB));
+    q.G2p = reinterpret_cast<double*>(take(sizeof(double) * kQrPanelCtas * kHB * kHB));
+    q.Qs = reinterpret_cast<double*>(take(sizeof(double) * kk * kHB));
+    q.Wp = reinterpret_cast<double*>(take(sizeof(double) * kQrChunks * kHB * nn));
+    q.Rt = reinterpret_cast<double*>(take(sizeof(double) * nn * nn));
+    size_t tb = 1;  // the largest level of the recursive inversion
+    for (int64_t b = 32; b < n; b *= 2) {
+        const size_t pairs = (size_t)((n - b + 2 * b - 1) / (2 * b));
+        if (pairs * b * b > tb) tb = pairs * b * b;
+    }
+    q.Tb = reinterpret_cast<double*>(take(sizeof(double) * tb));
     q.flag = reinterpret_cast<int*>(take(sizeof(int) * 4));
     q.bytes = off;
     return q;
 }
 
-// Panel width: the largest power of two <= 32 whose per-CTA share of the
-// panel (rows_per_cta x nb doubles) fits the shared-memory budget.
-static int qr_panel_nb(int64_t rows) {
-    const int64_t rpc = (rows + kQrCluster - 1) / kQrCluster;
-    int nb = kQrMaxNb;
-    while (nb > 1 && (size_t)rpc * nb * sizeof(double) > kQrPanelSmem) nb >>= 1;
-    if ((size_t)rpc * nb * sizeof(double) > kQrPanelSmem) return 0;
-    return nb;
-}
-
-struct PanelArgs {
-    double* A;
-    int64_t ld, m, j0;
-    int nb;
-    int64_t rpc;     // rows per CTA
-    double* tau;     // global, indexed by column
-    double* T;       // nb x nb, column-major
-};
-
-// Shared memory of one panel CTA: the panel slice (column-major, rpc rows
-// per column), then the exchange slots.
-struct PanelXch {
-    double norm[2][2];               // [parity][0 = sum sq below pivot, 1 = pivot value]
-    double w[2][kQrMaxNb];           // [parity][column] partial V^T C
-    double gram[kQrMaxNb * kQrMaxNb];
-};
-
-__global__ void __cluster_dims__(kQrCluster, 1, 1) __launch_bounds__(kQrThreads)
-    qr_panel_kernel(PanelArgs P) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ PanelXch X;
-    __shared__ double red[kQrThreads / 32];
-    __shared__ double bcast[4];
-    __shared__ double taul[kQrMaxNb];
-    __shared__ double gsum[kQrMaxNb * kQrMaxNb];
-    __shared__ double tmat[kQrMaxNb * kQrMaxNb];
-    __shared__ double gath[2 * kQrCluster];
-    __shared__ double wgath[kQrCluster][kQrMaxNb];
-    cg::cluster_group cluster = cg::this_cluster();
-    const int rank = (int)cluster.block_rank();
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nb = P.nb;
-    const int64_t rpc = P.rpc;
-    const int64_t row0 = P.j0 + rank * rpc;  // first global row of this CTA
-    int64_t nrows = P.m - row0;
-    if (nrows > rpc) nrows = rpc;
-    if (nrows < 0) nrows = 0;
-    double* pan = smem;  // pan[c * rpc + r]
-
-    for (int64_t idx = tid; idx < (int64_t)nb * rpc; idx += kQrThreads) {
-        const int c = (int)(idx / rpc);
-        const int64_t r = idx % rpc;
-        pan[idx] = r < nrows ? P.A[(size_t)(P.j0 + c) * P.ld + row0 + r] : 0.0;
-    }
-    cluster.sync();
-
-    for (int j = 0; j < nb; ++j) {
-        const int par = j & 1;
-        const int64_t piv = P.j0 + j;           // global pivot row
-        const int64_t lp = piv - row0;          // local index of the pivot row
-        const bool owner = lp >= 0 && lp < nrows;
-        // 1. partial ||a_j below pivot||^2 and the pivot value.
-        double ss = 0.0;
-        for (int64_t r = tid; r < nrows; r += kQrThreads)
-            if (row0 + r > piv) {
-                const double a = pan[(size_t)j * rpc + r];
-                ss += a * a;
-            }
-        ss = warp_sum(ss);
-        if (lane == 0) red[warp] = ss;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int k = 0; k < kQrThreads / 32; ++k) t += red[k];
-            X.norm[par][0] = t;
-            X.norm[par][1] = owner ? pan[(size_t)j * rpc + lp] : 0.0;
-        }
-        cluster.sync();
-        // 2. every CTA forms the same reflector from the 8 partials
-        //    (one distributed-shared-memory read per partial, in parallel).
-        if (tid < 2 * kQrCluster) {
-            const PanelXch* rx = cluster.map_shared_rank(&X, tid >> 1);
-            gath[tid] = rx->norm[par][tid & 1];
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double xn2 = 0.0, alpha = 0.0;
-            for (int c = 0; c < kQrCluster; ++c) {
-                xn2 += gath[2 * c];
-                alpha += gath[2 * c + 1];
-            }
-            double tau = 0.0, beta = alpha, scal = 0.0;
-            if (xn2 > 0.0) {
-                beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-                tau = (beta - alpha) / beta;
-                scal = 1.0 / (alpha - beta);
-            }
-            bcast[0] = tau;
-            bcast[1] = beta;
-            bcast[2] = scal;
-        }
-        __syncthreads();
-        const double tau = bcast[0], beta = bcast[1], scal = bcast[2];
-        for (int64_t r = tid; r < nrows; r += kQrThreads)
-            if (row0 + r > piv) pan[(size_t)j * rpc + r] *= scal;
-        if (owner && tid == 0) pan[(size_t)j * rpc + lp] = beta;
-        if (tid == 0) taul[j] = tau;
-        if (rank == 0 && tid == 0) P.tau[piv] = tau;
-        __syncthreads();
-        // 3. partial w_c = v^T a_c for the later panel columns.
-        for (int c = j + 1 + warp; c < nb; c += kQrThreads / 32) {
-            double w = 0.0;
-            for (int64_t r = lane; r < nrows; r += 32) {
-                const int64_t g = row0 + r;
-                if (g > piv)
-                    w += pan[(size_t)j * rpc + r] * pan[(size_t)c * rpc + r];
-                else if (g == piv)
-                    w += pan[(size_t)c * rpc + r];
-            }
-            w = warp_sum(w);
-            if (lane == 0) X.w[par][c] = w;
-        }
-        cluster.sync();
-        // 4. a_c -= tau * w_c * v, w_c summed over the cluster in a fixed order.
-        for (int e = tid; e < kQrCluster * nb; e += kQrThreads) {
-            const int q = e / nb, c = e % nb;
-            if (c > j) wgath[q][c] = cluster.map_shared_rank(&X, q)->w[par][c];
-        }
-        __syncthreads();
-        for (int c = j + 1 + warp; c < nb; c += kQrThreads / 32) {
-            double w = 0.0;
-            for (int q = 0; q < kQrCluster; ++q) w += wgath[q][c];
-            const double tw = tau * w;
-            for (int64_t r = lane; r < nrows; r += 32) {
-                const int64_t g = row0 + r;
-                if (g > piv)
-                    pan[(size_t)c * rpc + r] -= tw * pan[(size_t)j * rpc + r];
-                else if (g == piv)
-                    pan[(size_t)c * rpc + r] -= tw;
-            }
-        }
-        __syncthreads();
-    }
-
-    // Gram matrix G = V^T V of the panel's reflectors (unit diagonal,
-    // zeros above), partial per CTA: a warp per (a < b) pair, lanes over rows.
-    for (int e = warp; e < nb * nb; e += kQrThreads / 32) {
-        const int a = e % nb, b = e / nb;
-        double g = 0.0;
-        if (a < b) {
-            for (int64_t r = lane; r < nrows; r += 32) {
-                const int64_t row = row0 + r;
-                const double va = row > P.j0 + a ? pan[(size_t)a * rpc + r] : (row == P.j0 + a ? 1.0 : 0.0);
-                const double vb = row > P.j0 + b ? pan[(size_t)b * rpc + r] : (row == P.j0 + b ? 1.0 : 0.0);
-                g += va * vb;
-            }
-            g = warp_sum(g);
-        }
-        if (lane == 0) X.gram[e] = g;
-    }
-    cluster.sync();
-    if (rank == 0) {
-        // Sum the Gram partials locally, then T (upper triangular,
-        // column-major): T_jj = tau_j, T(0:j, j) = -tau_j T(0:j, 0:j) G(0:j, j)
-        // (LAPACK dlarft, forward / columnwise).
-        for (int e = tid; e < nb * nb; e += kQrThreads) {
-            double gq[kQrCluster];
-#pragma unroll
-            for (int q = 0; q < kQrCluster; ++q) gq[q] = cluster.map_shared_rank(&X, q)->gram[e];
-            double g = 0.0;
-#pragma unroll
-            for (int q = 0; q < kQrCluster; ++q) g += gq[q];
-            gsum[e] = g;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            for (int j = 0; j < nb; ++j) {
-                // lane i computes T(i, j) for i < j from column-j inputs.
-                double tij = 0.0;
-                if (lane < j) {
-                    double s2 = 0.0;
-                    for (int l = lane; l < j; ++l) s2 += tmat[l * kQrMaxNb + lane] * gsum[j * nb + l];
-                    tij = -taul[j] * s2;
-                }
-                __syncwarp();
-                if (lane < j) tmat[j * kQrMaxNb + lane] = tij;
-                if (lane == j) tmat[j * kQrMaxNb + j] = taul[j];
-                __syncwarp();
-            }
-            for (int e = lane; e < kQrMaxNb * kQrMaxNb; e += 32) {
-                const int i = e % kQrMaxNb, j = e / kQrMaxNb;
-                P.T[j * nb + i] = (i < nb && j < nb) ? tmat[e] : 0.0;
-            }
-        }
-    }
-    for (int64_t idx = tid; idx < (int64_t)nb * rpc; idx += kQrThreads) {
-        const int c = (int)(idx / rpc);
-        const int64_t r = idx % rpc;
-        if (r < nrows) P.A[(size_t)(P.j0 + c) * P.ld + row0 + r] = pan[idx];
-    }
-    cluster.sync();  // keep every CTA's shared memory alive until all reads are done
-}
-
-// V(i, a) of the panel starting at column j0 (i, a relative to j0).
+// V(i, a) of the panel starting at column j0 (i, a relative to j0): unit
+// diagonal, zeros above, the stored reflector below.
 __device__ __forceinline__ double vref(const double* A, int64_t ld, int64_t j0, int64_t i, int a) {
     if (i > a) return A[(size_t)(j0 + a) * ld + j0 + i];
     return i == a ? 1.0 : 0.0;
 }
 
-// W partials: Wp[chunk][a][c] = sum over the chunk's rows of V(i,a) C(i,c).
-__global__ void __launch_bounds__(kQrThreads) qr_w_partial_kernel(const double* A, int64_t ld,
-                                                                  int64_t m, int64_t n, int64_t j0,
-                                                                  int nb, double* Wp) {
-    __shared__ double Vs[kQrChunk][kQrMaxNb + 1];
-    __shared__ double Cs[kQrChunk][kQrTile + 1];
-    const int64_t c0 = j0 + nb + (int64_t)blockIdx.x * kQrTile;  // global column
-    const int64_t i0 = (int64_t)blockIdx.y * kQrChunk;           // row relative to j0
-    const int64_t rows = m - j0;
-    for (int e = threadIdx.x; e < kQrChunk * kQrMaxNb; e += kQrThreads) {
-        const int r = e / kQrMaxNb, a = e % kQrMaxNb;
-        const int64_t i = i0 + r;
-        Vs[r][a] = (a < nb && i < rows) ? vref(A, ld, j0, i, a) : 0.0;
-    }
-    for (int e = threadIdx.x; e < kQrChunk * kQrTile; e += kQrThreads) {
-        const int r = e % kQrChunk, c = e / kQrChunk;
-        const int64_t i = i0 + r, col = c0 + c;
-        Cs[r][c] = (i < rows && col < n) ? A[(size_t)col * ld + j0 + i] : 0.0;
-    }
-    __syncthreads();
-    const int a = threadIdx.x / 8, cq = (threadIdx.x % 8) * 4;
-    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    for (int r = 0; r < kQrChunk; ++r) {
-        const double v = Vs[r][a];
-        s0 += v * Cs[r][cq];
-        s1 += v * Cs[r][cq + 1];
-        s2 += v * Cs[r][cq + 2];
-        s3 += v * Cs[r][cq + 3];
-    }
-    if (a < nb) {
-        const int64_t nc = n - j0 - nb;
-        double* out = Wp + ((size_t)blockIdx.y * kQrMaxNb + a) * (size_t)nc;
-        const int64_t cc = (int64_t)blockIdx.x * kQrTile + cq;
-        if (cc < nc) out[cc] = s0;
-        if (cc + 1 < nc) out[cc + 1] = s1;
-        if (cc + 2 < nc) out[cc + 2] = s2;
-        if (cc + 3 < nc) out[cc + 3] = s3;
-    }
-}
-
-// W2(:, c) = T^T * sum_chunks Wp(:, :, c): a block per 32 trailing
-// columns, threads over (row of W, column) pairs, coalesced along columns.
-__global__ void __launch_bounds__(256) qr_w_reduce_kernel(const double* Wp, int64_t chunks,
-                                                          int64_t nc, int nb, const double* T,
-                                                          double* W2) {
-    __shared__ double Ws[kQrMaxNb][kQrTile + 1];
-    __shared__ double Ts[kQrMaxNb][kQrMaxNb + 1];
-    const int64_t c0 = (int64_t)blockIdx.x * kQrTile;
-    for (int e = threadIdx.x; e < kQrMaxNb * kQrMaxNb; e += blockDim.x) {
-        const int a = e % kQrMaxNb, b = e / kQrMaxNb;
-        Ts[a][b] = (a < nb && b < nb) ? T[b * nb + a] : 0.0;  // T(a, b)
-    }
-    for (int e = threadIdx.x; e < kQrMaxNb * kQrTile; e += blockDim.x) {
-        const int a = e / kQrTile, cc = e % kQrTile;
-        const int64_t col = c0 + cc;
-        double sum = 0.0;
-        if (a < nb && col < nc) {
-            const double* p = Wp + (size_t)a * nc + col;
-            const size_t stride = (size_t)kQrMaxNb * nc;
-            int64_t q = 0;
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-            for (; q + 3 < chunks; q += 4) {
-                s0 += p[(size_t)q * stride];
-                s1 += p[(size_t)(q + 1) * stride];
-                s2 += p[(size_t)(q + 2) * stride];
-                s3 += p[(size_t)(q + 3) * stride];
-            }
-            for (; q < chunks; ++q) s0 += p[(size_t)q * stride];
-            sum = (s0 + s1) + (s2 + s3);
+// Gram partials of the first panel: CTA t sums rows [256 t, 256 t + 256).
+__global__ void __launch_bounds__(kQrThreads) qr_gram_kernel(const double* A, int64_t ld, int64_t k,
+                                                             int nb, double* Gp) {
+    __shared__ double Pt[kHB][kHB + 1];
+    const int t = threadIdx.x;
+    const int a = t & 31, b0 = (t >> 5) * 4;
+    const int64_t r0 = (int64_t)blockIdx.x * kQrRowTile;
+    int64_t r1 = r0 + kQrRowTile;
+    if (r1 > k) r1 = k;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t rt = r0; rt < r1; rt += kHB) {
+        __syncthreads();
+        for (int e = t; e < kHB * kHB; e += kQrThreads) {
+            const int r = e & 31, c = e >> 5;
+            const int64_t row = rt + r;
+            Pt[r][c] = (row < r1 && c < nb) ? A[(size_t)c * ld + row] : 0.0;
         }
-        Ws[a][cc] = sum;
+        __syncthreads();
+        for (int r = 0; r < kHB; ++r) {
+            const double x = Pt[r][a];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[u] += x * Pt[r][b0 + u];
+        }
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < kQrMaxNb * kQrTile; e += blockDim.x) {
-        const int b = e / kQrTile, cc = e % kQrTile;
-        const int64_t col = c0 + cc;
-        if (b >= nb || col >= nc) continue;
-        double sum = 0.0;
-        for (int a = 0; a <= b; ++a) sum += Ts[a][b] * Ws[a][cc];
-        W2[(size_t)b * nc + col] = sum;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) Gp[(size_t)blockIdx.x * kHB * kHB + a * kHB + b0 + u] = acc[u];
+}
+
+// Shared tiles of the trailing update keep an even row stride so that
+// four consecutive doubles load as two 16-byte accesses.
+constexpr int kQrWs = kQrWc + 2;
+
+// W partials: Wp[chunk][a][c] = sum over the chunk's rows of V(i, a) C(i, c),
+// C the trailing columns j0 + nb + c.  A CTA: one row chunk x 64 columns;
+// a thread: reflectors a0 and a0 + 16 x four consecutive columns.
+__global__ void __launch_bounds__(kQrThreads) qr_w_part_kernel(const double* A, int64_t ld,
+                                                               int64_t k, int64_t n, int64_t j0,
+                                                               int nb, int64_t chunk_rows,
+                                                               double* Wp) {
+    __shared__ double Vt[kHB][kHB + 1];
+    __shared__ __align__(16) double Ct[kHB][kQrWs];
+    const int t = threadIdx.x;
+    const int a0 = t & 15, cg = (t >> 4) * 4;
+    const int64_t nc = n - j0 - nb, krem = k - j0;
+    const int64_t c0 = (int64_t)blockIdx.x * kQrWc;
+    const int64_t r0 = (int64_t)blockIdx.y * chunk_rows;
+    int64_t r1 = r0 + chunk_rows;
+    if (r1 > krem) r1 = krem;
+    double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t rt = r0; rt < r1; rt += kHB) {
+        __syncthreads();
+        for (int e = t; e < kHB * kHB; e += kQrThreads) {
+            const int r = e & 31, aa = e >> 5;
+            const int64_t row = rt + r;
+            Vt[r][aa] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
+        }
+        for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
+            const int r = e & 31, c = e >> 5;
+            const int64_t row = rt + r, col = c0 + c;
+            Ct[r][c] = (row < r1 && col < nc) ? A[(size_t)(j0 + nb + col) * ld + j0 + row] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int r = 0; r < kHB; ++r) {
+            const double v0 = Vt[r][a0], v1 = Vt[r][a0 + 16];
+            const double2 cA = *reinterpret_cast<const double2*>(&Ct[r][cg]);
+            const double2 cB = *reinterpret_cast<const double2*>(&Ct[r][cg + 2]);
+            acc0[0] += v0 * cA.x;
+            acc0[1] += v0 * cA.y;
+            acc0[2] += v0 * cB.x;
+            acc0[3] += v0 * cB.y;
+            acc1[0] += v1 * cA.x;
+            acc1[1] += v1 * cA.y;
+            acc1[2] += v1 * cB.x;
+            acc1[3] += v1 * cB.y;
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int aa = a0 + 16 * h;
+        if (aa >= nb) continue;
+        double* out = Wp + ((size_t)blockIdx.y * kHB + aa) * (size_t)nc;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t col = c0 + cg + u;
+            if (col < nc) out[col] = h ? acc1[u] : acc0[u];
+        }
     }
 }
 
-// C(i, c) -= sum_a V(i, a) W2(a, c).
-__global__ void __launch_bounds__(kQrThreads) qr_update_kernel(double* A, int64_t ld, int64_t m,
-                                                               int64_t n, int64_t j0, int nb,
-                                                               const double* W2) {
-    __shared__ double Vs[kQrChunk][kQrMaxNb + 1];
-    __shared__ double Ws[kQrMaxNb][kQrTile + 1];
-    const int64_t cc0 = (int64_t)blockIdx.x * kQrTile;  // column relative to j0+nb
-    const int64_t i0 = (int64_t)blockIdx.y * kQrChunk;
-    const int64_t rows = m - j0, nc = n - j0 - nb;
-    for (int e = threadIdx.x; e < kQrChunk * kQrMaxNb; e += kQrThreads) {
-        const int r = e / kQrMaxNb, a = e % kQrMaxNb;
-        const int64_t i = i0 + r;
-        Vs[r][a] = (a < nb && i < rows) ? vref(A, ld, j0, i, a) : 0.0;
+// C -= V (T^T W) on one tile of 256 rows x 64 trailing columns, W the
+// fixed-order sum of the chunk partials; a thread: rows r0 and r0 + 16 of
+// each 32-row step x four consecutive columns.  Tiles holding the next
+// panel's columns (blockIdx.x == 0) then write that panel's Gram partial
+// over their rows below the current panel (rows j0 + nb on).
+__global__ void __launch_bounds__(kQrThreads) qr_apply_kernel(double* A, int64_t ld, int64_t k,
+                                                              int64_t n, int64_t j0, int nb,
+                                                              int nchunks, const double* Wp,
+                                                              const double* T, int nb_next,
+                                                              double* Gp_next) {
+    // W0 and Tt are dead once Wt = T^T W0 is formed; the row loop reuses
+    // their storage for the V and Gram tiles (its first barrier orders it).
+    __shared__ __align__(16) double W0[kHB][kQrWs];
+    __shared__ __align__(16) double Wt[kHB][kQrWs];
+    __shared__ double Tt[kHB][kHB + 1];
+    double (&Vt)[kHB][kHB + 1] = Tt;
+    double (*Ct)[kQrWs] = W0;
+    const int t = threadIdx.x;
+    const int64_t nc = n - j0 - nb, krem = k - j0;
+    const int64_t c0 = (int64_t)blockIdx.x * kQrWc;
+    for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
+        const int aa = e / kQrWc, c = e % kQrWc;
+        const int64_t col = c0 + c;
+        double sum = 0.0;
+        if (aa < nb && col < nc)
+            for (int q = 0; q < nchunks; ++q) sum += Wp[((size_t)q * kHB + aa) * (size_t)nc + col];
+        W0[aa][c] = sum;
     }
-    for (int e = threadIdx.x; e < kQrMaxNb * kQrTile; e += kQrThreads) {
-        const int a = e / kQrTile, c = e % kQrTile;
-        Ws[a][c] = (a < nb && cc0 + c < nc) ? W2[(size_t)a * nc + cc0 + c] : 0.0;
+    for (int e = t; e < kHB * kHB; e += kQrThreads) {
+        const int aa = e & 31, b = e >> 5;
+        Tt[aa][b] = (aa < nb && b < nb) ? T[(size_t)b * nb + aa] : 0.0;  // T(aa, b)
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < kQrChunk * kQrTile; e += kQrThreads) {
-        const int r = e % kQrChunk, c = e / kQrChunk;
-        const int64_t i = i0 + r, cc = cc0 + c;
-        if (i >= rows || cc >= nc) continue;
-        double s = 0.0;
-#pragma unroll 8
-        for (int a = 0; a < kQrMaxNb; ++a) s += Vs[r][a] * Ws[a][c];
-        A[(size_t)(j0 + nb + cc) * ld + j0 + i] -= s;
+    for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
+        const int b = e / kQrWc, c = e % kQrWc;
+        double sum = 0.0;
+        for (int aa = 0; aa <= b; ++aa) sum += Tt[aa][b] * W0[aa][c];
+        Wt[b][c] = sum;
+    }
+    const bool gram = Gp_next != nullptr && blockIdx.x == 0;
+    const int rr0 = t & 15, cg = (t >> 4) * 4;
+    const int ga = t & 31, gb = (t >> 5) * 4;
+    double gacc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t r0 = (int64_t)blockIdx.y * kQrRowTile;
+    int64_t r1 = r0 + kQrRowTile;
+    if (r1 > krem) r1 = krem;
+    for (int64_t rt = r0; rt < r1; rt += kHB) {
+        __syncthreads();
+        for (int e = t; e < kHB * kHB; e += kQrThreads) {
+            const int rr = e & 31, aa = e >> 5;
+            const int64_t row = rt + rr;
+            Vt[rr][aa] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
+        }
+        __syncthreads();
+        double s0[4] = {0.0, 0.0, 0.0, 0.0}, s1[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+        for (int aa = 0; aa < kHB; ++aa) {
+            const double v0 = Vt[rr0][aa], v1 = Vt[rr0 + 16][aa];
+            const double2 wA = *reinterpret_cast<const double2*>(&Wt[aa][cg]);
+            const double2 wB = *reinterpret_cast<const double2*>(&Wt[aa][cg + 2]);
+            s0[0] += v0 * wA.x;
+            s0[1] += v0 * wA.y;
+            s0[2] += v0 * wB.x;
+            s0[3] += v0 * wB.y;
+            s1[0] += v1 * wA.x;
+            s1[1] += v1 * wA.y;
+            s1[2] += v1 * wB.x;
+            s1[3] += v1 * wB.y;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int rr = rr0 + 16 * h;
+            const int64_t row = rt + rr;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t col = c0 + cg + u;
+                double nv = 0.0;
+                if (row < r1 && col < nc) {
+                    double* ap = A + (size_t)(j0 + nb + col) * ld + j0 + row;
+                    nv = *ap - (h ? s1[u] : s0[u]);
+                    *ap = nv;
+                }
+                if (gram && cg + u < kHB) Ct[rr][cg + u] = (row >= nb && cg + u < nb_next) ? nv : 0.0;
+            }
+        }
+        if (gram) {
+            __syncthreads();
+            for (int q = 0; q < kHB; ++q) {
+                const double x = Ct[q][ga];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) gacc[u] += x * Ct[q][gb + u];
+            }
+        }
+    }
+    if (gram) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            Gp_next[(size_t)blockIdx.y * kHB * kHB + ga * kHB + gb + u] = gacc[u];
     }
 }
 
@@ -441,33 +329,78 @@ __global__ void __launch_bounds__(32) qr_trtri_diag_kernel(const double* Rt, int
     }
 }
 
-// Off-diagonal blocks of block column J (8 columns per CTA):
-// X_IJ = -X_II * sum_{K=I+1..J} R_IK X_KJ for I = J-1 down to 0.
-__global__ void __launch_bounds__(256) qr_trtri_off_kernel(const double* Rt, int64_t n, double* A,
-                                                           int64_t ld) {
-    __shared__ double tmp[32][9];
-    const int J = blockIdx.x;
-    const int64_t j0 = (int64_t)J * 32 + blockIdx.y * 8;
-    const int i = threadIdx.x / 8, jj = threadIdx.x % 8;
-    const int64_t col = j0 + jj;
-    const bool cv = col < n && blockIdx.y * 8 + jj < 32;
-    for (int I = J - 1; I >= 0; --I) {
-        const int64_t i0 = (int64_t)I * 32;
-        double sum = 0.0;
-        if (cv) {
-            const double* rrow = Rt + (size_t)(i0 + i) * n;
-            const double* xcol = A + (size_t)col * ld;
-            for (int64_t k = i0 + 32; k <= col; ++k) sum += rrow[k] * xcol[k];
-        }
-        tmp[i][jj] = sum;
+// One level of the recursive inversion X = R^{-1}: for every pair p of
+// diagonal blocks I = [2bp, 2bp + b), J = [2bp + b, 2bp + 2b) (J clipped
+// at n), X_IJ = -X_II R_IJ X_JJ, in two batched products
+//   mode 0:  T_p  = R_IJ X_JJ      (R from Rt, row-major)
+//   mode 1:  X_IJ = -X_II T_p
+// X_II and X_JJ come from the previous level.  64 x 64 output tiles,
+// k-steps of 16 through shared memory, 4 x 4 outputs per thread.
+__global__ void __launch_bounds__(256) trtri_level_kernel(const double* Rt, int64_t n, double* X,
+                                                          int64_t ldx, double* Tb, int64_t b,
+                                                          int mode) {
+    __shared__ double As[16][64 + 1];
+    __shared__ double Bs[16][64 + 1];
+    const int64_t p = blockIdx.z;
+    const int64_t I0 = 2 * b * p, J0 = I0 + b;
+    const int64_t Jn = n - J0 < b ? n - J0 : b;
+    if (Jn <= 0) return;
+    const int64_t M = b, N = Jn, K = mode == 0 ? Jn : b;
+    const int64_t row0 = (int64_t)blockIdx.y * 64, col0 = (int64_t)blockIdx.x * 64;
+    if (row0 >= M || col0 >= N) return;
+    double* T = Tb + (size_t)p * b * b;  // b x Jn, column-major, ld b
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    double acc[4][4] = {};
+    for (int64_t k0 = 0; k0 < K; k0 += 16) {
         __syncthreads();
-        if (cv) {
-            double out = 0.0;
-            for (int l = i; l < 32; ++l) out += A[(size_t)(i0 + l) * ld + i0 + i] * tmp[l][jj];
-            A[(size_t)col * ld + i0 + i] = -out;
+        for (int e = t; e < 64 * 16; e += 256) {
+            int i, kk;
+            double v = 0.0;
+            if (mode == 0) {  // R row-major: consecutive threads along k
+                i = e / 16;
+                kk = e % 16;
+                if (row0 + i < M && k0 + kk < K) v = Rt[(size_t)(I0 + row0 + i) * n + J0 + k0 + kk];
+            } else {          // X column-major: consecutive threads along rows
+                i = e % 64;
+                kk = e / 64;
+                if (row0 + i < M && k0 + kk < K) v = X[(size_t)(I0 + k0 + kk) * ldx + I0 + row0 + i];
+            }
+            As[kk][i] = v;
+        }
+        for (int e = t; e < 64 * 16; e += 256) {
+            const int kk = e % 16, j = e / 16;
+            double v = 0.0;
+            if (k0 + kk < K && col0 + j < N)
+                v = mode == 0 ? X[(size_t)(J0 + col0 + j) * ldx + J0 + k0 + kk]
+                              : T[(size_t)(col0 + j) * b + k0 + kk];
+            Bs[kk][j] = v;
         }
         __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            double a[4], bb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a[u] = As[kk][ty * 4 + u];
+                bb[u] = Bs[kk][tx * 4 + u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * bb[v];
+        }
     }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int64_t i = row0 + ty * 4 + u, j = col0 + tx * 4 + v;
+            if (i >= M || j >= N) continue;
+            if (mode == 0)
+                T[(size_t)j * b + i] = acc[u][v];
+            else
+                X[(size_t)(J0 + j) * ldx + I0 + i] = -acc[u][v];
+        }
 }
 
 }  // namespace tomos_b200
@@ -496,36 +429,55 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
                     "sketch_qr: scratch too small (need " + std::to_string(need.bytes) + " bytes)");
     QrScratch q = qr_layout(scratch, k, n);
     cudaStream_t st = as_stream(stream);
-    const int nb_max = qr_panel_nb(k);
-    if (nb_max == 0) return fail(TOMOS_ERR_UNSUPPORTED, "sketch_qr: k too large for the panel");
-    TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kQrPanelSmem));
-    TOMOS_CUDA_TRY(cudaMemsetAsync(q.flag, 0, sizeof(int), st));
-    for (int64_t j0 = 0; j0 < n; j0 += nb_max) {
-        const int nb = (int)(n - j0 < nb_max ? n - j0 : nb_max);
-        PanelArgs P;
-        P.A = SA;
-        P.ld = ld;
-        P.m = k;
-        P.j0 = j0;
-        P.nb = nb;
-        P.rpc = (k - j0 + kQrCluster - 1) / kQrCluster;
-        P.tau = q.tau;
-        P.T = q.T;
-        const size_t smem = (size_t)P.rpc * nb * sizeof(double);
-        qr_panel_kernel<<<kQrCluster, kQrThreads, smem, st>>>(P);
-        TOMOS_LAUNCH_CHECK("qr_panel_kernel");
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_hr_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)hr_v_smem()));
+    TOMOS_CUDA_TRY(cudaMemsetAsync(q.flag, 0, sizeof(int) * 4, st));
+    {
+        const int nb0 = (int)(n < kQrNb ? n : kQrNb);
+        qr_gram_kernel<<<(unsigned)qr_row_tiles(k), kQrThreads, 0, st>>>(SA, ld, k, nb0, q.Gp);
+        TOMOS_LAUNCH_CHECK("qr_gram_kernel");
+    }
+    int ngp = (int)qr_row_tiles(k);
+    for (int64_t j0 = 0; j0 < n; j0 += kQrNb) {
+        const int nb = (int)(n - j0 < kQrNb ? n - j0 : kQrNb);
+        const int64_t krem = k - j0;
+        int gp = (int)((krem + kQrRowTile - 1) / kQrRowTile);
+        if (gp > kQrPanelCtas) gp = kQrPanelCtas;
+        if (gp < 1) gp = 1;
+        HrArgs H;
+        H.A = SA;
+        H.ld = ld;
+        H.k = k;
+        H.j0 = j0;
+        H.nb = nb;
+        H.rpc = ((krem + gp - 1) / gp + kHB - 1) / kHB * kHB;
+        H.Gp = q.Gp;
+        H.ngp = ngp;
+        H.Qs = q.Qs;
+        H.kq = k;
+        H.G2p = q.G2p;
+        H.R1 = q.R1;
+        H.fail = q.flag + 1;
+        H.T = q.T;
+        H.tau = q.tau;
+        qr_hr_q1_kernel<<<(unsigned)gp, kQrThreads, hr_q1_smem(), st>>>(H);
+        TOMOS_LAUNCH_CHECK("qr_hr_q1_kernel");
+        qr_hr_v_kernel<<<(unsigned)gp, kQrThreads, hr_v_smem(), st>>>(H);
+        TOMOS_LAUNCH_CHECK("qr_hr_v_kernel");
         const int64_t nc = n - j0 - nb;
         if (nc <= 0) continue;
-        const int64_t chunks = (k - j0 + kQrChunk - 1) / kQrChunk;
-        dim3 g1((unsigned)((nc + kQrTile - 1) / kQrTile), (unsigned)chunks);
-        qr_w_partial_kernel<<<g1, kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb, q.Wp);
-        TOMOS_LAUNCH_CHECK("qr_w_partial_kernel");
-        qr_w_reduce_kernel<<<(unsigned)((nc + kQrTile - 1) / kQrTile), 256, 0, st>>>(
-            q.Wp, chunks, nc, nb, q.T, q.W2);
-        TOMOS_LAUNCH_CHECK("qr_w_reduce_kernel");
-        qr_update_kernel<<<g1, kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb, q.W2);
-        TOMOS_LAUNCH_CHECK("qr_update_kernel");
+        const int64_t chunk_rows = ((krem + kQrChunks - 1) / kQrChunks + kHB - 1) / kHB * kHB;
+        const int nchunks = (int)((krem + chunk_rows - 1) / chunk_rows);
+        const unsigned ctiles = (unsigned)((nc + kQrWc - 1) / kQrWc);
+        qr_w_part_kernel<<<dim3(ctiles, (unsigned)nchunks), kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb,
+                                                                                 chunk_rows, q.Wp);
+        TOMOS_LAUNCH_CHECK("qr_w_part_kernel");
+        const int nb_next = (int)(nc < kQrNb ? nc : kQrNb);
+        const unsigned rtiles = (unsigned)qr_row_tiles(krem);
+        qr_apply_kernel<<<dim3(ctiles, rtiles), kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb, nchunks, q.Wp,
+                                                                     q.T, nb_next, q.Gp);
+        TOMOS_LAUNCH_CHECK("qr_apply_kernel");
+        ngp = (int)rtiles;
     }
     qr_extract_kernel<<<(unsigned)((n * n + 255) / 256 < 4096 ? (n * n + 255) / 256 : 4096), 256, 0,
                         st>>>(SA, ld, n, q.Rt, R, q.flag);
@@ -542,10 +494,14 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     TOMOS_LAUNCH_CHECK("qr_zero_lower_kernel");
     qr_trtri_diag_kernel<<<(unsigned)nbk, 32, 0, st>>>(q.Rt, n, SA, ld);
     TOMOS_LAUNCH_CHECK("qr_trtri_diag_kernel");
-    if (nbk > 1) {
-        qr_trtri_off_kernel<<<dim3((unsigned)nbk, 4), 256, 0, st>>>(q.Rt, n, SA, ld);
+    for (int64_t b = 32; b < n; b *= 2) {
+        const int64_t pairs = (n - b + 2 * b - 1) / (2 * b);
+        const dim3 g((unsigned)((b + 63) / 64), (unsigned)((b + 63) / 64), (unsigned)pairs);
+        trtri_level_kernel<<<g, 256, 0, st>>>(q.Rt, n, SA, ld, q.Tb, b, 0);
+        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
+        trtri_level_kernel<<<g, 256, 0, st>>>(q.Rt, n, SA, ld, q.Tb, b, 1);
+        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
     }
-    TOMOS_LAUNCH_CHECK("qr_trtri_off_kernel");
     return TOMOS_OK;
 }
 

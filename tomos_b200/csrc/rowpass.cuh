@@ -1,0 +1,412 @@
+// rowpass.cuh -- the fused Golub-Kahan pass over a row-major A, staged
+// through shared memory by bulk asynchronous copies (cp.async.bulk).
+//
+// Per row i of A (same arithmetic as fused.cuh):
+//     ut_i = cp (A p)_i + cu u_i            written to u_out
+//     q   += ut_i A[i, :]                   per-CTA partial of A^T ut
+//     ss  += ut_i^2                         per-CTA partial, FP64
+// so the two products of an LSQR iteration cost one read of A.
+//
+// Roles (one CTA per SM, 13 warps):
+//   producer (warp 12, lane 0)           consumers (warps 0..11)
+//   wait empty[s]                        wait full[s]
+//   expect_tx(full[s], bytes)            copy its row part to registers,
+//   cp.async.bulk per plane (one per       decode, arrive empty[s]
+//   stage when rows are contiguous,
+//   else one per row)
+//                                        dot with p (packed FP32x2 FMAs),
+//                                        shuffle reduce, ut,
+//                                        q += ut * row (packed FMAs)
+// A stage holds RS = 12 / G rows.  G consumer warps share a row when n is
+// wider than one warp's columns (1024, or 512 for ACC64; G divides 12);
+// their partial dots meet in shared memory behind a named barrier per row.  Lane l of part g
+// owns the 16-byte chunks g*32*NCH + k*32 + l (k < NCH) of its row, so p
+// and the q accumulators live in registers and every shared-memory read
+// is a conflict-free 16-byte access.
+//
+// FP32_16 wh words with the control bit set (values outside the fp16
+// range) are rare; one OR over a row's words tests for them and only then
+// takes the exact fp32_16_half_only decode.
+//
+// ACC64 (the exact tiers, restart residuals, backward errors) forms every
+// product exactly and sums it in FP64, as the reference's accurate tier
+// does: p is held in FP64 registers, so an element costs one conversion
+// and one DFMA.  To stay within the register budget an ACC64 warp covers
+// half as many columns (16 per lane) and rows are split over G = 2..12
+// warps sooner.  HALF-tier and FP32 passes accumulate in FP32.
+//
+// Every mbarrier wait is bounded.  A consumer whose wait expires records
+// the failure in *err and stops waiting (it still runs the remaining
+// named barriers, so its row partners never block); the producer stops
+// issuing and drains what it issued (bounded again).  The results of such
+// a launch are garbage and the host reports the error.
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "common.cuh"
+#include "fused.cuh"
+#include "mbarrier.cuh"
+
+namespace tomos_b200 {
+
+constexpr int kRowWarps = 12;  // 13 warps with the producer: up to 128 registers
+constexpr int kRowThreads = (kRowWarps + 1) * 32;
+constexpr int kRowMaxStages = 12;
+constexpr size_t kRowSmemBudget = 200 * 1024;
+
+template <Elem E>
+struct RowPlanes {
+    static constexpr int value = (E == Elem::A16 || E == Elem::AB16 || E == Elem::AB16R) ? 2 : 1;
+};
+
+struct RowPassParams {
+    FusedParams f;
+    int* err;        // set nonzero on a pipeline timeout
+    int nstage;
+    int copy_bytes;  // bytes copied per row and plane (16-byte multiple)
+};
+
+// fp32_16_half_only on both halves of a word (control-1 halves only).
+__device__ __forceinline__ uint32_t fix_half_pair(uint32_t w) {
+    uint32_t lo = w & 0xFFFFu, hi = w >> 16;
+    if (lo & 1u) lo = half_only_bits(lo);
+    if (hi & 1u) hi = half_only_bits(hi);
+    return lo | (hi << 16);
+}
+
+__device__ __forceinline__ uint4 lds128(const uint8_t* p) {
+    return *reinterpret_cast<const uint4*>(p);
+}
+
+__device__ __forceinline__ float2 h2f2(uint32_t w) {
+    return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+
+// Decodes this lane's NCH chunks of one row part from shared memory into
+// float pairs (the operands of the packed FMAs).  Chunks past the end of
+// the row (live bit clear) are not read and decode to zeros.
+template <Elem E, int NCH>
+__device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* lrow,
+                                           const int* coff, uint32_t live,
+                                           float2 (&a)[NCH * ChunkElems<E>::value / 2]) {
+    constexpr int VEC = ChunkElems<E>::value;
+    constexpr int HV = VEC / 2;
+    if constexpr (E == Elem::H16) {
+        uint4 h[NCH];
+        uint32_t any = 0;
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            h[k] = (live >> k) & 1u ? lds128(hrow + coff[k]) : make_uint4(0, 0, 0, 0);
+            any |= h[k].x | h[k].y | h[k].z | h[k].w;
+        }
+        if (any & 0x00010001u) {
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) {
+                h[k].x = fix_half_pair(h[k].x);
+                h[k].y = fix_half_pair(h[k].y);
+                h[k].z = fix_half_pair(h[k].z);
+                h[k].w = fix_half_pair(h[k].w);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            a[k * 4 + 0] = h2f2(h[k].x);
+            a[k * 4 + 1] = h2f2(h[k].y);
+            a[k * 4 + 2] = h2f2(h[k].z);
+            a[k * 4 + 3] = h2f2(h[k].w);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            if ((live >> k) & 1u) {
+                const uint4 h = lds128(hrow + coff[k]);
+                if constexpr (E == Elem::F16) {
+                    a[k * 4 + 0] = h2f2(h.x);
+                    a[k * 4 + 1] = h2f2(h.y);
+                    a[k * 4 + 2] = h2f2(h.z);
+                    a[k * 4 + 3] = h2f2(h.w);
+                } else if constexpr (E == Elem::F32) {
+                    a[k * 2 + 0] = make_float2(__uint_as_float(h.x), __uint_as_float(h.y));
+                    a[k * 2 + 1] = make_float2(__uint_as_float(h.z), __uint_as_float(h.w));
+                } else {
+                    uint4 r = h;
+                    if (RowPlanes<E>::value == 2) r = lds128(lrow + coff[k]);
+                    float f[VEC];
+                    ChunkDecoder<E>::decode(h, r, f);
+#pragma unroll
+                    for (int e = 0; e < HV; ++e) a[k * HV + e] = make_float2(f[2 * e], f[2 * e + 1]);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < HV; ++e) a[k * HV + e] = make_float2(0.0f, 0.0f);
+            }
+        }
+    }
+}
+
+template <Elem E, int NCH, int G, bool ACC64>
+__global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParams T) {
+    const FusedParams& P = T.f;
+    if (P.skip && *P.skip) return;
+    constexpr int VEC = ChunkElems<E>::value;
+    constexpr int PER = NCH * VEC;      // columns per lane
+    constexpr int WCOLS = 32 * PER;     // columns per consumer warp
+    constexpr int RS = kRowWarps / G;   // rows per stage
+    constexpr int PLANES = RowPlanes<E>::value;
+    constexpr int ESZ = (E == Elem::F32) ? 4 : 2;
+    static_assert(PER % 4 == 0, "pairs of pairs");
+
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[kRowMaxStages];
+    __shared__ __align__(8) uint64_t empty[kRowMaxStages];
+    __shared__ double ssw[kRowWarps];
+    __shared__ double xdot[2][kRowWarps];
+    __shared__ int abort_flag;
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nstage = T.nstage;
+    const int cb = T.copy_bytes;
+    const size_t plane_bytes = (size_t)RS * cb;
+    const size_t stage_bytes = plane_bytes * PLANES;
+
+    const int64_t rows_per_cta = (P.m + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+    int64_t r1 = r0 + rows_per_cta;
+    if (r1 > P.m) r1 = P.m;
+    const int64_t nrows = r1 > r0 ? r1 - r0 : 0;
+    const int ntiles = (int)((nrows + RS - 1) / RS);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < nstage; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kRowWarps);
+        }
+        abort_flag = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    float2 acc[PER / 2];
+#pragma unroll
+    for (int j = 0; j < PER / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
+    double ss = 0.0;
+    const int rg = warp / G;    // row of the stage
+    const int part = warp % G;  // column part of the row
+
+    if (warp == kRowWarps) {
+        // ---------------------------------------------------------- producer
+        if (lane == 0) {
+            const bool contiguous = (int64_t)P.ld * ESZ == cb;
+            int issued = 0;
+            int s = 0;
+            uint32_t ph = 0;
+            for (int t = 0; t < ntiles; ++t) {
+                if (!mbar_wait(&empty[s], ph ^ 1u)) {
+                    atomicExch(T.err, 1);
+                    break;
+                }
+                if (*(volatile int*)&abort_flag) break;
+                const int64_t i0 = r0 + (int64_t)t * RS;
+                const int rows = (int)((r1 - i0) < RS ? (r1 - i0) : RS);
+                uint8_t* st = smem + (size_t)s * stage_bytes;
+                mbar_expect_tx(&full[s], (uint32_t)(rows * cb * PLANES));
+                if (contiguous) {
+                    // rows of A are back to back: one copy per plane and stage
+                    const size_t goff = (size_t)i0 * (size_t)P.ld * ESZ;
+                    bulk_g2s(st, static_cast<const uint8_t*>(P.hi) + goff, (uint32_t)(rows * cb),
+                             &full[s]);
+                    if (PLANES == 2)
+                        bulk_g2s(st + plane_bytes, static_cast<const uint8_t*>(P.lo) + goff,
+                                 (uint32_t)(rows * cb), &full[s]);
+                } else {
+                    for (int r = 0; r < rows; ++r) {
+                        const size_t goff = (size_t)(i0 + r) * (size_t)P.ld * ESZ;
+                        bulk_g2s(st + (size_t)r * cb, static_cast<const uint8_t*>(P.hi) + goff,
+                                 (uint32_t)cb, &full[s]);
+                        if (PLANES == 2)
+                            bulk_g2s(st + plane_bytes + (size_t)r * cb,
+                                     static_cast<const uint8_t*>(P.lo) + goff, (uint32_t)cb, &full[s]);
+                    }
+                }
+                issued = t + 1;
+                if (++s == nstage) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+            }
+            // Drain: every issued stage must land before the CTA may exit.
+            for (int t = (issued > nstage ? issued - nstage : 0); t < issued; ++t) {
+                if (!mbar_wait(&full[t % nstage], (uint32_t)(t / nstage) & 1u)) {
+                    atomicExch(T.err, 2);
+                    break;
+                }
+            }
+        }
+    } else {
+        // --------------------------------------------------------- consumers
+        const double cp = P.coef[0];
+        const double cu = P.coef[1];
+        const int64_t n = P.n;
+        const int64_t nchunks = (n + VEC - 1) / VEC;
+        int coff[NCH];
+        uint32_t live = 0;
+        // p for this lane's columns: FP32 pairs, or FP64 for ACC64
+        using PT = typename std::conditional<ACC64, double, float2>::type;
+        PT pv[ACC64 ? PER : PER / 2];
+        // The lane holding the row's last, partly filled chunk zeroes the
+        // elements from zero_from on (the copy's tail past column n-1).
+        int zero_from = PER;
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            const int64_t c = (int64_t)part * 32 * NCH + (int64_t)k * 32 + lane;
+            coff[k] = (int)(c * 16);
+            if (c < nchunks) live |= 1u << k;
+            if (c == nchunks - 1 && n % VEC != 0) zero_from = k * VEC + (int)(n - c * VEC);
+#pragma unroll
+            for (int e = 0; e < VEC; e += 2) {
+                const int64_t col = c * VEC + e;
+                const float x0 = col < n ? __ldg(P.p + col) : 0.0f;
+                const float x1 = col + 1 < n ? __ldg(P.p + col + 1) : 0.0f;
+                if constexpr (ACC64) {
+                    pv[k * VEC + e] = (double)x0;
+                    pv[k * VEC + e + 1] = (double)x1;
+                } else {
+                    pv[(k * VEC + e) / 2] = make_float2(x0, x1);
+                }
+            }
+        }
+        bool failed = false;
+        // u of this warp's row, fetched two tiles ahead
+        float ua = 0.f, ub = 0.f;
+        {
+            const int64_t a0 = r0 + rg, b0 = r0 + RS + rg;
+            if (a0 < r1) ua = __ldg(P.u_in + a0);
+            if (b0 < r1) ub = __ldg(P.u_in + b0);
+        }
+        int s = 0;
+        uint32_t ph = 0;
+        for (int t = 0; t < ntiles; ++t) {
+            const int64_t i = r0 + (int64_t)t * RS + rg;
+            const bool has = i < r1;
+            const float ucur = ua;
+            ua = ub;
+            ub = (i + 2 * RS < r1) ? __ldg(P.u_in + i + 2 * RS) : 0.0f;
+            if (!failed && !mbar_wait(&full[s], ph)) {
+                atomicExch(T.err, 3);
+                abort_flag = 1;
+                failed = true;
+            }
+            const uint8_t* hrow = smem + (size_t)s * stage_bytes + (size_t)rg * cb;
+            float2 a[PER / 2];
+            if (has && !failed) {
+                decode_row<E, NCH>(hrow, hrow + plane_bytes, coff, live, a);
+                if (zero_from < PER) {
+#pragma unroll
+                    for (int e = 0; e < PER; e += 2) {
+                        if (e >= zero_from) a[e / 2].x = 0.0f;
+                        if (e + 1 >= zero_from) a[e / 2].y = 0.0f;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < PER / 2; ++e) a[e] = make_float2(0.0f, 0.0f);
+            }
+            // The stage may be refilled once every consumer warp holds its row.
+            __syncwarp();
+            if (lane == 0 && !failed) mbar_arrive(&empty[s]);
+            if (++s == nstage) {
+                s = 0;
+                ph ^= 1u;
+            }
+
+            double dsum;
+            if constexpr (ACC64) {
+                double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+                for (int j = 0; j < PER / 2; ++j) {
+                    d0 = fma((double)a[j].x, pv[2 * j], d0);
+                    d1 = fma((double)a[j].y, pv[2 * j + 1], d1);
+                }
+                double dd = d0 + d1;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(0xffffffffu, dd, o);
+                dsum = dd;
+            } else {
+                float2 d0 = make_float2(0.f, 0.f), d1 = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < PER / 2; j += 2) {
+                    d0 = __ffma2_rn(a[j], pv[j], d0);
+                    d1 = __ffma2_rn(a[j + 1], pv[j + 1], d1);
+                }
+                float d = (d0.x + d1.x) + (d0.y + d1.y);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+                dsum = (double)d;
+            }
+            if constexpr (G > 1) {
+                // partial dots of the row's G parts, summed in part order
+                if (lane == 0) xdot[t & 1][warp] = dsum;
+                named_bar_sync(1 + rg, G * 32);
+                double tot = 0.0;
+#pragma unroll
+                for (int g = 0; g < G; ++g) tot += xdot[t & 1][rg * G + g];
+                dsum = tot;
+            }
+            const float ut = has ? (float)(cp * dsum + cu * (double)ucur) : 0.0f;
+            if (lane == 0 && part == 0 && has) {
+                P.u_out[i] = ut;
+                ss += (double)ut * (double)ut;
+            }
+            const float2 ut2 = make_float2(ut, ut);
+#pragma unroll
+            for (int j = 0; j < PER / 2; ++j) acc[j] = __ffma2_rn(a[j], ut2, acc[j]);
+        }
+    }
+
+    // Epilogue: the producer waited for every copy it issued, so the stage
+    // memory can hold the cross-warp reduction.
+    __syncthreads();
+    float* red = reinterpret_cast<float*>(smem);
+    if (warp < kRowWarps) {
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            float4* dst = reinterpret_cast<float4*>(&red[(size_t)warp * WCOLS + (k * 32 + lane) * VEC]);
+#pragma unroll
+            for (int e = 0; e < VEC; e += 4) {
+                const int j = (k * VEC + e) / 2;
+                dst[e / 4] = make_float4(acc[j].x, acc[j].y, acc[j + 1].x, acc[j + 1].y);
+            }
+        }
+        if (lane == 0) ssw[warp] = ss;
+    }
+    __syncthreads();
+    float* qout = P.qpart + (size_t)blockIdx.x * P.qstride;
+    for (int64_t j = threadIdx.x; j < P.n; j += kRowThreads) {
+        const int g = (int)(j / WCOLS);
+        const int loc = (int)(j % WCOLS);
+        float sum = 0.0f;
+#pragma unroll
+        for (int r = 0; r < RS; ++r) sum += red[(size_t)(r * G + g) * WCOLS + loc];
+        qout[j] = sum;
+    }
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < kRowWarps; ++w) sum += ssw[w];
+        P.sspart[blockIdx.x] = sum;
+    }
+}
+
+// Dynamic shared memory of one launch: the stage ring, at least the
+// cross-warp reduction buffer.
+template <Elem E, int NCH>
+inline size_t fused_rows_smem(int nstage, int rows_per_stage, int copy_bytes) {
+    constexpr int VEC = ChunkElems<E>::value;
+    const size_t ring = (size_t)nstage * rows_per_stage * copy_bytes * RowPlanes<E>::value;
+    const size_t red = (size_t)kRowWarps * NCH * 32 * VEC * sizeof(float);
+    return ring > red ? ring : red;
+}
+
+}  // namespace tomos_b200

@@ -108,7 +108,10 @@ __global__ void cs_sort_kernel(int64_t s, const int32_t* __restrict__ offsets,
 }
 
 // Row-major owner sums: warp per bucket, lanes over columns of a panel of
-// 32 * KC columns (grid.y walks the panels).
+// 32 * KC columns (grid.y walks the panels).  Sums in FP32 with the rows
+// of a bucket in increasing order: bit for bit the reference's
+// countsketch_apply_impl<float> (countsketch_kernels.cpp:70-83).  The
+// column sums of squares are FP32 per bucket and FP64 across buckets.
 template <Elem E, int KC>
 __global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void* lo, int64_t n,
                                                       int64_t ld, int64_t s,
@@ -119,35 +122,35 @@ __global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void
                                                       double* __restrict__ fro_part,
                                                       double* __restrict__ col_part) {
     __shared__ double smf[8];
-    __shared__ double smc[8][32 * KC];
+    __shared__ float smc[8][32 * KC];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t b = (int64_t)blockIdx.x * 8 + w;
     const int64_t c0 = (int64_t)blockIdx.y * 32 * KC;
-    double acc[KC], csq[KC];
+    float acc[KC], csq[KC];
 #pragma unroll
-    for (int k = 0; k < KC; ++k) acc[k] = csq[k] = 0.0;
+    for (int k = 0; k < KC; ++k) acc[k] = csq[k] = 0.0f;
     double f2 = 0.0;
     if (b < s) {
         const int32_t o0 = offsets[b], o1 = offsets[b + 1];
         for (int32_t q = o0; q < o1; ++q) {
             const int32_t r = perm[q];
-            const double sg = (double)sign[r];
+            const float sg = (float)sign[r];
             const size_t base = (size_t)r * ld;
 #pragma unroll
             for (int k = 0; k < KC; ++k) {
                 const int64_t j = c0 + k * 32 + lane;
                 if (j < n) {
-                    const double a = (double)load_elem<E>(hi, lo, base + j);
-                    acc[k] += sg * a;
-                    csq[k] += a * a;
+                    const float a = load_elem<E>(hi, lo, base + j);
+                    acc[k] = fmaf(sg, a, acc[k]);
+                    csq[k] = fmaf(a, a, csq[k]);
                 }
             }
         }
 #pragma unroll
         for (int k = 0; k < KC; ++k) {
             const int64_t j = c0 + k * 32 + lane;
-            if (j < n) SA[(size_t)j * ld_sa + b] = acc[k];
-            f2 += csq[k];
+            if (j < n) SA[(size_t)j * ld_sa + b] = (double)acc[k];
+            f2 += (double)csq[k];
         }
     }
 #pragma unroll
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(256) cs_rows_kernel(const void* hi, const void
             if (j >= n) continue;
             double t = 0.0;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) t += smc[k][e];
+            for (int k = 0; k < 8; ++k) t += (double)smc[k][e];
             col_part[(size_t)blockIdx.x * n + j] = t;
         }
     }
@@ -185,8 +188,10 @@ __global__ void cs_col_reduce_kernel(const double* __restrict__ part, int64_t np
 
 // Row-major owner sums with 16-byte chunk loads: a warp per (bucket,
 // panel); lane l owns chunks l, l+32, ... (KCH of them, VEC columns each)
-// of the panel, and walks the bucket's rows four at a time.  Needs
-// 16-byte aligned rows (ld * element bytes a multiple of 16).
+// of the panel, and walks the bucket's rows four at a time, summing in
+// FP32 in increasing row order (the reference's float path, as
+// cs_rows_kernel).  Needs 16-byte aligned rows (ld * element bytes a
+// multiple of 16).
 template <Elem E, int KCH>
 __global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const void* lo, int64_t n,
                                                           int64_t ld, int64_t s,
@@ -201,16 +206,16 @@ __global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const 
     constexpr bool TWO = (E == Elem::A16 || E == Elem::AB16 || E == Elem::AB16R);
     constexpr int esz = (E == Elem::F32) ? 4 : 2;
     __shared__ double smf[8];
-    __shared__ double smc[8][PW];
+    __shared__ float smc[8][PW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t b = (int64_t)blockIdx.x * 8 + w;
     const int64_t c0 = (int64_t)blockIdx.y * PW;
     const int64_t nch = (n + VEC - 1) / VEC;
-    double acc[KCH][VEC], csq[KCH][VEC];
+    float acc[KCH][VEC], csq[KCH][VEC];
 #pragma unroll
     for (int k = 0; k < KCH; ++k)
 #pragma unroll
-        for (int e = 0; e < VEC; ++e) acc[k][e] = csq[k][e] = 0.0;
+        for (int e = 0; e < VEC; ++e) acc[k][e] = csq[k][e] = 0.0f;
     bool live[KCH];
 #pragma unroll
     for (int k = 0; k < KCH; ++k) live[k] = (c0 / VEC + k * 32 + lane) < nch;
@@ -219,11 +224,11 @@ __global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const 
         const int32_t o0 = offsets[b], o1 = offsets[b + 1];
         for (int32_t q = o0; q < o1; q += 4) {
             int32_t r[4];
-            double sg[4];
+            float sg[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 r[u] = q + u < o1 ? perm[q + u] : -1;
-                sg[u] = r[u] >= 0 ? (double)sign[r[u]] : 0.0;
+                sg[u] = r[u] >= 0 ? (float)sign[r[u]] : 0.0f;
             }
             uint4 h[4][KCH], l[4][KCH];
 #pragma unroll
@@ -248,9 +253,9 @@ __global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const 
 #pragma unroll
                     for (int e = 0; e < VEC; ++e) {
                         if (ragged && cbase + e >= n) continue;
-                        const double a = (double)f[e];
-                        acc[k][e] = fma(sg[u], a, acc[k][e]);
-                        csq[k][e] = fma(a, a, csq[k][e]);
+                        const float a = f[e];
+                        acc[k][e] = fmaf(sg[u], a, acc[k][e]);
+                        csq[k][e] = fmaf(a, a, csq[k][e]);
                     }
                 }
         }
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const 
             const int64_t cbase = c0 + (int64_t)(k * 32 + lane) * VEC;
 #pragma unroll
             for (int e = 0; e < VEC; ++e)
-                if (live[k] && cbase + e < n) SA[(size_t)(cbase + e) * ld_sa + b] = acc[k][e];
+                if (live[k] && cbase + e < n) SA[(size_t)(cbase + e) * ld_sa + b] = (double)acc[k][e];
         }
     }
     double f2 = 0.0;
@@ -268,7 +273,7 @@ __global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const 
 #pragma unroll
         for (int e = 0; e < VEC; ++e) {
             smc[w][(k * 32 + lane) * VEC + e] = csq[k][e];
-            f2 += csq[k][e];
+            f2 += (double)csq[k][e];
         }
     f2 = warp_sum(f2);
     if (lane == 0) smf[w] = f2;
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(256) cs_rows_vec_kernel(const void* hi, const 
             if (j >= n) continue;
             double t = 0.0;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) t += smc[k][e];
+            for (int k = 0; k < 8; ++k) t += (double)smc[k][e];
             col_part[(size_t)blockIdx.x * n + j] = t;
         }
     }
