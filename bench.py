@@ -73,8 +73,8 @@ def ncu_traffic(name):
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
-    return d.get(name)
+    v = json.load(open(p)).get(name)
+    return v.get("bytes_per_launch") if isinstance(v, dict) else v
 
 
 class ClockSampler:

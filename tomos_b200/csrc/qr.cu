@@ -46,12 +46,13 @@ struct QrScratch {
     double* Rt;     // n x n  (R transposed: row i of R contiguous)
     double* Tb;     // products of one level of the recursive inversion
     int* flag;      // [0] singular R, [1] panel fallback
+    void* gsync;    // grid barrier of the one-launch QR
     size_t bytes;
 };
 
 static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static int64_t qr_row_tiles(int64_t rows) { return (rows + kQrRowTile - 1) / kQrRowTile; }
+__host__ __device__ inline int64_t qr_row_tiles(int64_t rows) { return (rows + kQrRowTile - 1) / kQrRowTile; }
 
 static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
     QrScratch q;
@@ -79,6 +80,7 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
     }
     q.Tb = reinterpret_cast<double*>(take(sizeof(double) * tb));
     q.flag = reinterpret_cast<int*>(take(sizeof(int) * 4));
+    q.gsync = take(64);
     q.bytes = off;
     return q;
 }
@@ -86,17 +88,21 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
 // V(i, a) of the panel starting at column j0 (i, a relative to j0): unit
 // diagonal, zeros above, the stored reflector below.
 __device__ __forceinline__ double vref(const double* A, int64_t ld, int64_t j0, int64_t i, int a) {
-    if (i > a) return A[(size_t)(j0 + a) * ld + j0 + i];
+    if (i > a) return __ldcg(A + (size_t)(j0 + a) * ld + j0 + i);
     return i == a ? 1.0 : 0.0;
 }
 
-// Gram partials of the first panel: CTA t sums rows [256 t, 256 t + 256).
-__global__ void __launch_bounds__(kQrThreads) qr_gram_kernel(const double* A, int64_t ld, int64_t k,
-                                                             int nb, double* Gp) {
-    __shared__ double Pt[kHB][kHB + 1];
+// Gram partials of the first panel: tile `tile` sums rows [256 t, 256 t + 256).
+// Shared tiles of the phase functions below, carved from `sm` (dynamic
+// shared memory of the calling kernel, 16-byte aligned).
+constexpr int kQrTileSmemDoubles = 2 * kHB * (kQrWc + 2) + kHB * (kHB + 1);
+
+__device__ void qr_gram_tile(const double* A, int64_t ld, int64_t k, int nb, int tile, double* Gp,
+                             double* sm) {
+    double (*Pt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(sm);
     const int t = threadIdx.x;
     const int a = t & 31, b0 = (t >> 5) * 4;
-    const int64_t r0 = (int64_t)blockIdx.x * kQrRowTile;
+    const int64_t r0 = (int64_t)tile * kQrRowTile;
     int64_t r1 = r0 + kQrRowTile;
     if (r1 > k) r1 = k;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -105,7 +111,7 @@ __global__ void __launch_bounds__(kQrThreads) qr_gram_kernel(const double* A, in
         for (int e = t; e < kHB * kHB; e += kQrThreads) {
             const int r = e & 31, c = e >> 5;
             const int64_t row = rt + r;
-            Pt[r][c] = (row < r1 && c < nb) ? A[(size_t)c * ld + row] : 0.0;
+            Pt[r][c] = (row < r1 && c < nb) ? __ldcg(A + (size_t)c * ld + row) : 0.0;
         }
         __syncthreads();
         for (int r = 0; r < kHB; ++r) {
@@ -115,7 +121,14 @@ __global__ void __launch_bounds__(kQrThreads) qr_gram_kernel(const double* A, in
         }
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) Gp[(size_t)blockIdx.x * kHB * kHB + a * kHB + b0 + u] = acc[u];
+    for (int u = 0; u < 4; ++u) Gp[(size_t)tile * kHB * kHB + a * kHB + b0 + u] = acc[u];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kQrThreads) qr_gram_kernel(const double* A, int64_t ld, int64_t k,
+                                                             int nb, double* Gp) {
+    extern __shared__ __align__(16) double qsm[];
+    qr_gram_tile(A, ld, k, nb, blockIdx.x, Gp, qsm);
 }
 
 // Shared tiles of the trailing update keep an even row stride so that
@@ -125,32 +138,50 @@ constexpr int kQrWs = kQrWc + 2;
 // W partials: Wp[chunk][a][c] = sum over the chunk's rows of V(i, a) C(i, c),
 // C the trailing columns j0 + nb + c.  A CTA: one row chunk x 64 columns;
 // a thread: reflectors a0 and a0 + 16 x four consecutive columns.
-__global__ void __launch_bounds__(kQrThreads) qr_w_part_kernel(const double* A, int64_t ld,
-                                                               int64_t k, int64_t n, int64_t j0,
-                                                               int nb, int64_t chunk_rows,
-                                                               double* Wp) {
-    __shared__ double Vt[kHB][kHB + 1];
-    __shared__ __align__(16) double Ct[kHB][kQrWs];
+__device__ void qr_w_part_tile(const double* A, int64_t ld, int64_t k, int64_t n, int64_t j0, int nb,
+                               int64_t chunk_rows, double* Wp, int ct, int rc, double* sm) {
+    double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm);
+    double (*Vt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(sm + kHB * kQrWs);
     const int t = threadIdx.x;
     const int a0 = t & 15, cg = (t >> 4) * 4;
     const int64_t nc = n - j0 - nb, krem = k - j0;
-    const int64_t c0 = (int64_t)blockIdx.x * kQrWc;
-    const int64_t r0 = (int64_t)blockIdx.y * chunk_rows;
+    const int64_t c0 = (int64_t)ct * kQrWc;
+    const int64_t r0 = (int64_t)rc * chunk_rows;
     int64_t r1 = r0 + chunk_rows;
     if (r1 > krem) r1 = krem;
     double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
+    // The next 32-row sub-tile is loaded into registers while the current
+    // one is multiplied (its L2 latency hidden behind the FMAs).
+    constexpr int NV = kHB * kHB / kQrThreads, NC = kHB * kQrWc / kQrThreads;
+    double vpre[NV], cpre[NC];
+    auto fetch = [&](int64_t rt) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int e = t + i * kQrThreads, r = e & 31, aa = e >> 5;
+            const int64_t row = rt + r;
+            vpre[i] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const int e = t + i * kQrThreads, r = e & 31, c = e >> 5;
+            const int64_t row = rt + r, col = c0 + c;
+            cpre[i] = (row < r1 && col < nc) ? __ldcg(A + (size_t)(j0 + nb + col) * ld + j0 + row) : 0.0;
+        }
+    };
+    if (r0 < r1) fetch(r0);
     for (int64_t rt = r0; rt < r1; rt += kHB) {
         __syncthreads();
-        for (int e = t; e < kHB * kHB; e += kQrThreads) {
-            const int r = e & 31, aa = e >> 5;
-            const int64_t row = rt + r;
-            Vt[r][aa] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int e = t + i * kQrThreads;
+            Vt[e & 31][e >> 5] = vpre[i];
         }
-        for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
-            const int r = e & 31, c = e >> 5;
-            const int64_t row = rt + r, col = c0 + c;
-            Ct[r][c] = (row < r1 && col < nc) ? A[(size_t)(j0 + nb + col) * ld + j0 + row] : 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const int e = t + i * kQrThreads;
+            Ct[e & 31][e >> 5] = cpre[i];
         }
+        if (rt + kHB < r1) fetch(rt + kHB);
         __syncthreads();
 #pragma unroll 4
         for (int r = 0; r < kHB; ++r) {
@@ -171,46 +202,60 @@ __global__ void __launch_bounds__(kQrThreads) qr_w_part_kernel(const double* A, 
     for (int h = 0; h < 2; ++h) {
         const int aa = a0 + 16 * h;
         if (aa >= nb) continue;
-        double* out = Wp + ((size_t)blockIdx.y * kHB + aa) * (size_t)nc;
+        double* out = Wp + ((size_t)rc * kHB + aa) * (size_t)nc;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int64_t col = c0 + cg + u;
             if (col < nc) out[col] = h ? acc1[u] : acc0[u];
         }
     }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kQrThreads) qr_w_part_kernel(const double* A, int64_t ld,
+                                                               int64_t k, int64_t n, int64_t j0,
+                                                               int nb, int64_t chunk_rows,
+                                                               double* Wp) {
+    extern __shared__ __align__(16) double qsm[];
+    qr_w_part_tile(A, ld, k, n, j0, nb, chunk_rows, Wp, blockIdx.x, blockIdx.y, qsm);
 }
 
 // C -= V (T^T W) on one tile of 256 rows x 64 trailing columns, W the
 // fixed-order sum of the chunk partials; a thread: rows r0 and r0 + 16 of
 // each 32-row step x four consecutive columns.  Tiles holding the next
-// panel's columns (blockIdx.x == 0) then write that panel's Gram partial
+// panel's columns (column tile 0) then write that panel's Gram partial
 // over their rows below the current panel (rows j0 + nb on).
-__global__ void __launch_bounds__(kQrThreads) qr_apply_kernel(double* A, int64_t ld, int64_t k,
-                                                              int64_t n, int64_t j0, int nb,
-                                                              int nchunks, const double* Wp,
-                                                              const double* T, int nb_next,
-                                                              double* Gp_next) {
+__device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64_t j0, int nb,
+                              int nchunks, const double* Wp, const double* T, int nb_next,
+                              double* Gp_next, int ct, int rtile, double* sm) {
     // W0 and Tt are dead once Wt = T^T W0 is formed; the row loop reuses
     // their storage for the V and Gram tiles (its first barrier orders it).
-    __shared__ __align__(16) double W0[kHB][kQrWs];
-    __shared__ __align__(16) double Wt[kHB][kQrWs];
-    __shared__ double Tt[kHB][kHB + 1];
-    double (&Vt)[kHB][kHB + 1] = Tt;
+    double (*W0)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm);
+    double (*Wt)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm + kHB * kQrWs);
+    double (*Tt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(sm + 2 * kHB * kQrWs);
+    double (*Vt)[kHB + 1] = Tt;
     double (*Ct)[kQrWs] = W0;
     const int t = threadIdx.x;
     const int64_t nc = n - j0 - nb, krem = k - j0;
-    const int64_t c0 = (int64_t)blockIdx.x * kQrWc;
+    const int64_t c0 = (int64_t)ct * kQrWc;
+    __syncthreads();  // a previous tile of this CTA may still read W0 / Tt
     for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
         const int aa = e / kQrWc, c = e % kQrWc;
         const int64_t col = c0 + c;
+        double part[kQrChunks];
+#pragma unroll
+        for (int q = 0; q < kQrChunks; ++q)
+            part[q] = (q < nchunks && aa < nb && col < nc)
+                          ? __ldcg(Wp + ((size_t)q * kHB + aa) * (size_t)nc + col)
+                          : 0.0;
         double sum = 0.0;
-        if (aa < nb && col < nc)
-            for (int q = 0; q < nchunks; ++q) sum += Wp[((size_t)q * kHB + aa) * (size_t)nc + col];
+#pragma unroll
+        for (int q = 0; q < kQrChunks; ++q) sum += part[q];
         W0[aa][c] = sum;
     }
     for (int e = t; e < kHB * kHB; e += kQrThreads) {
         const int aa = e & 31, b = e >> 5;
-        Tt[aa][b] = (aa < nb && b < nb) ? T[(size_t)b * nb + aa] : 0.0;  // T(aa, b)
+        Tt[aa][b] = (aa < nb && b < nb) ? __ldcg(T + (size_t)b * nb + aa) : 0.0;  // T(aa, b)
     }
     __syncthreads();
     for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
@@ -219,20 +264,46 @@ __global__ void __launch_bounds__(kQrThreads) qr_apply_kernel(double* A, int64_t
         for (int aa = 0; aa <= b; ++aa) sum += Tt[aa][b] * W0[aa][c];
         Wt[b][c] = sum;
     }
-    const bool gram = Gp_next != nullptr && blockIdx.x == 0;
+    const bool gram = Gp_next != nullptr && ct == 0;
     const int rr0 = t & 15, cg = (t >> 4) * 4;
     const int ga = t & 31, gb = (t >> 5) * 4;
     double gacc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int64_t r0 = (int64_t)blockIdx.y * kQrRowTile;
+    const int64_t r0 = (int64_t)rtile * kQrRowTile;
     int64_t r1 = r0 + kQrRowTile;
     if (r1 > krem) r1 = krem;
+    // V of the next 32-row sub-tile and this thread's next 8 entries of C
+    // are loaded while the current sub-tile is updated.
+    constexpr int NV = kHB * kHB / kQrThreads;
+    double vpre[NV], cpre[8];
+    auto fetch = [&](int64_t rt) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int e = t + i * kQrThreads, rr = e & 31, aa = e >> 5;
+            const int64_t row = rt + rr;
+            vpre[i] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t row = rt + rr0 + 16 * h, col = c0 + cg + u;
+                cpre[h * 4 + u] = (row < r1 && col < nc)
+                                      ? __ldcg(A + (size_t)(j0 + nb + col) * ld + j0 + row)
+                                      : 0.0;
+            }
+    };
+    if (r0 < r1) fetch(r0);
     for (int64_t rt = r0; rt < r1; rt += kHB) {
         __syncthreads();
-        for (int e = t; e < kHB * kHB; e += kQrThreads) {
-            const int rr = e & 31, aa = e >> 5;
-            const int64_t row = rt + rr;
-            Vt[rr][aa] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int e = t + i * kQrThreads;
+            Vt[e & 31][e >> 5] = vpre[i];
         }
+        double cur[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) cur[i] = cpre[i];
+        if (rt + kHB < r1) fetch(rt + kHB);
         __syncthreads();
         double s0[4] = {0.0, 0.0, 0.0, 0.0}, s1[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 4
@@ -258,9 +329,8 @@ __global__ void __launch_bounds__(kQrThreads) qr_apply_kernel(double* A, int64_t
                 const int64_t col = c0 + cg + u;
                 double nv = 0.0;
                 if (row < r1 && col < nc) {
-                    double* ap = A + (size_t)(j0 + nb + col) * ld + j0 + row;
-                    nv = *ap - (h ? s1[u] : s0[u]);
-                    *ap = nv;
+                    nv = cur[h * 4 + u] - (h ? s1[u] : s0[u]);
+                    A[(size_t)(j0 + nb + col) * ld + j0 + row] = nv;
                 }
                 if (gram && cg + u < kHB) Ct[rr][cg + u] = (row >= nb && cg + u < nb_next) ? nv : 0.0;
             }
@@ -277,7 +347,133 @@ __global__ void __launch_bounds__(kQrThreads) qr_apply_kernel(double* A, int64_t
     if (gram) {
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            Gp_next[(size_t)blockIdx.y * kHB * kHB + ga * kHB + gb + u] = gacc[u];
+            Gp_next[(size_t)rtile * kHB * kHB + ga * kHB + gb + u] = gacc[u];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kQrThreads) qr_apply_kernel(double* A, int64_t ld, int64_t k,
+                                                              int64_t n, int64_t j0, int nb,
+                                                              int nchunks, const double* Wp,
+                                                              const double* T, int nb_next,
+                                                              double* Gp_next) {
+    extern __shared__ __align__(16) double qsm[];
+    qr_apply_tile(A, ld, k, n, j0, nb, nchunks, Wp, T, nb_next, Gp_next, blockIdx.x, blockIdx.y, qsm);
+}
+
+// ------------------------------------------------------ one launch per QR
+//
+// Every read of data another CTA may have written earlier in the same
+// launch (A, Q1, the Gram and W partials, T, R1) goes through __ldcg (L2,
+// not the SM's non-coherent L1), in the phase functions above and in
+// qr_panel.cuh.
+//
+// The same phases as the per-phase kernels above, run by one cooperative
+// launch (one CTA per SM, all resident) that separates them with a grid
+// barrier instead of kernel boundaries:
+//   panel passes (hr_q1, hr_v) on up to kQrPanelCtas CTAs, then the W
+//   partials and the apply tiles spread over every CTA.
+// The barrier is a counter and a generation word in global memory; waits
+// are bounded (kGridSpinLimit polls with a short sleep), and a CTA whose
+// wait expires sets an error word and leaves, so a broken barrier ends the
+// kernel with an error the host reports instead of hanging the GPU.
+
+constexpr long long kGridSpinLimit = 1ll << 22;
+
+struct GridSync {
+    unsigned int arrive;
+    unsigned int gen;
+    int err;
+    int pad;
+};
+
+__device__ bool grid_sync(GridSync* gs, unsigned int& gen, int* sflag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int g = gen;
+        if (atomicAdd(&gs->arrive, 1u) == gridDim.x - 1) {
+            atomicExch(&gs->arrive, 0u);
+            __threadfence();
+            atomicExch(&gs->gen, g + 1u);
+        } else {
+            long long k = 0;
+            while (*(volatile unsigned int*)&gs->gen == g) {
+                if (++k > kGridSpinLimit) {
+                    atomicExch(&gs->err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        *sflag = *(volatile int*)&gs->err;
+    }
+    __syncthreads();
+    gen += 1u;
+    return *sflag == 0;
+}
+
+struct QrPersistArgs {
+    double* A;
+    int64_t ld, k, n;
+    QrScratch q;
+    GridSync* gs;
+};
+
+__global__ void __launch_bounds__(kQrThreads, 1) qr_persist_kernel(QrPersistArgs a) {
+    extern __shared__ __align__(16) double hsm[];
+    __shared__ int sflag;
+    unsigned int gen = 0;
+    const int cta = blockIdx.x, ncta = gridDim.x;
+    const int64_t k = a.k, n = a.n;
+    const int nb0 = (int)(n < kQrNb ? n : kQrNb);
+    const int tiles0 = (int)qr_row_tiles(k);
+    for (int tl = cta; tl < tiles0; tl += ncta) qr_gram_tile(a.A, a.ld, k, nb0, tl, a.q.Gp, hsm);
+    if (!grid_sync(a.gs, gen, &sflag)) return;
+    int ngp = tiles0;
+    for (int64_t j0 = 0; j0 < n; j0 += kQrNb) {
+        const int nb = (int)(n - j0 < kQrNb ? n - j0 : kQrNb);
+        const int64_t krem = k - j0;
+        int gp = (int)((krem + kQrRowTile - 1) / kQrRowTile);
+        if (gp > kQrPanelCtas) gp = kQrPanelCtas;
+        if (gp > ncta) gp = ncta;
+        if (gp < 1) gp = 1;
+        HrArgs H;
+        H.A = a.A;
+        H.ld = a.ld;
+        H.k = k;
+        H.j0 = j0;
+        H.nb = nb;
+        H.rpc = ((krem + gp - 1) / gp + kHB - 1) / kHB * kHB;
+        H.Gp = a.q.Gp;
+        H.ngp = ngp;
+        H.Qs = a.q.Qs;
+        H.kq = k;
+        H.G2p = a.q.G2p;
+        H.R1 = a.q.R1;
+        H.fail = a.q.flag + 1;
+        H.T = a.q.T;
+        H.tau = a.q.tau;
+        if (cta < gp) hr_q1(H, cta, hsm);
+        if (!grid_sync(a.gs, gen, &sflag)) return;
+        if (cta < gp) hr_v(H, cta, gp, hsm);
+        if (!grid_sync(a.gs, gen, &sflag)) return;
+        const int64_t nc = n - j0 - nb;
+        if (nc <= 0) break;
+        const int64_t chunk_rows = ((krem + kQrChunks - 1) / kQrChunks + kHB - 1) / kHB * kHB;
+        const int nchunks = (int)((krem + chunk_rows - 1) / chunk_rows);
+        const int ctiles = (int)((nc + kQrWc - 1) / kQrWc);
+        for (int tl = cta; tl < ctiles * nchunks; tl += ncta)
+            qr_w_part_tile(a.A, a.ld, k, n, j0, nb, chunk_rows, a.q.Wp, tl % ctiles, tl / ctiles, hsm);
+        if (!grid_sync(a.gs, gen, &sflag)) return;
+        const int nb_next = (int)(nc < kQrNb ? nc : kQrNb);
+        const int rtiles = (int)qr_row_tiles(krem);
+        for (int tl = cta; tl < ctiles * rtiles; tl += ncta)
+            qr_apply_tile(a.A, a.ld, k, n, j0, nb, nchunks, a.q.Wp, a.q.T, nb_next, a.q.Gp,
+                          tl % ctiles, tl / ctiles, hsm);
+        ngp = rtiles;
+        if (!grid_sync(a.gs, gen, &sflag)) return;
     }
 }
 
@@ -432,11 +628,45 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_hr_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)hr_v_smem()));
     TOMOS_CUDA_TRY(cudaMemsetAsync(q.flag, 0, sizeof(int) * 4, st));
+    bool done = false;
     {
-        const int nb0 = (int)(n < kQrNb ? n : kQrNb);
-        qr_gram_kernel<<<(unsigned)qr_row_tiles(k), kQrThreads, 0, st>>>(SA, ld, k, nb0, q.Gp);
-        TOMOS_LAUNCH_CHECK("qr_gram_kernel");
+        // One cooperative launch when every CTA of a full wave can be resident.
+        int dev = 0, coop = 0, per_sm = 0;
+        TOMOS_CUDA_TRY(cudaGetDevice(&dev));
+        TOMOS_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        const size_t psmem = hr_v_smem() > kQrTileSmemDoubles * sizeof(double)
+                                 ? hr_v_smem()
+                                 : kQrTileSmemDoubles * sizeof(double);
+        TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_persist_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem));
+        TOMOS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qr_persist_kernel,
+                                                                     kQrThreads, psmem));
+        if (coop && per_sm >= 1) {
+            QrPersistArgs pa;
+            pa.A = SA;
+            pa.ld = ld;
+            pa.k = k;
+            pa.n = n;
+            pa.q = q;
+            pa.gs = static_cast<GridSync*>(q.gsync);
+            TOMOS_CUDA_TRY(cudaMemsetAsync(q.gsync, 0, sizeof(GridSync), st));
+            void* args[] = {&pa};
+            cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr_persist_kernel,
+                                                        dim3((unsigned)sm_count()), dim3(kQrThreads),
+                                                        args, psmem, st);
+            if (e == cudaSuccess) {
+                done = true;
+            } else {
+                cudaGetLastError();  // fall back to the per-phase kernels
+            }
+        }
     }
+    const size_t tile_smem = kQrTileSmemDoubles * sizeof(double);
+    if (!done) {
+    const int nb0 = (int)(n < kQrNb ? n : kQrNb);
+    qr_gram_kernel<<<(unsigned)qr_row_tiles(k), kQrThreads, kHB * (kHB + 1) * sizeof(double), st>>>(
+        SA, ld, k, nb0, q.Gp);
+    TOMOS_LAUNCH_CHECK("qr_gram_kernel");
     int ngp = (int)qr_row_tiles(k);
     for (int64_t j0 = 0; j0 < n; j0 += kQrNb) {
         const int nb = (int)(n - j0 < kQrNb ? n - j0 : kQrNb);
@@ -469,22 +699,28 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
         const int64_t chunk_rows = ((krem + kQrChunks - 1) / kQrChunks + kHB - 1) / kHB * kHB;
         const int nchunks = (int)((krem + chunk_rows - 1) / chunk_rows);
         const unsigned ctiles = (unsigned)((nc + kQrWc - 1) / kQrWc);
-        qr_w_part_kernel<<<dim3(ctiles, (unsigned)nchunks), kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb,
-                                                                                 chunk_rows, q.Wp);
+        qr_w_part_kernel<<<dim3(ctiles, (unsigned)nchunks), kQrThreads, tile_smem, st>>>(
+            SA, ld, k, n, j0, nb, chunk_rows, q.Wp);
         TOMOS_LAUNCH_CHECK("qr_w_part_kernel");
         const int nb_next = (int)(nc < kQrNb ? nc : kQrNb);
         const unsigned rtiles = (unsigned)qr_row_tiles(krem);
-        qr_apply_kernel<<<dim3(ctiles, rtiles), kQrThreads, 0, st>>>(SA, ld, k, n, j0, nb, nchunks, q.Wp,
-                                                                     q.T, nb_next, q.Gp);
+        qr_apply_kernel<<<dim3(ctiles, rtiles), kQrThreads, tile_smem, st>>>(
+            SA, ld, k, n, j0, nb, nchunks, q.Wp, q.T, nb_next, q.Gp);
         TOMOS_LAUNCH_CHECK("qr_apply_kernel");
         ngp = (int)rtiles;
     }
+    }  // per-phase kernels
     qr_extract_kernel<<<(unsigned)((n * n + 255) / 256 < 4096 ? (n * n + 255) / 256 : 4096), 256, 0,
                         st>>>(SA, ld, n, q.Rt, R, q.flag);
     TOMOS_LAUNCH_CHECK("qr_extract_kernel");
     int flag = 0;
+    GridSync gsh{};
     TOMOS_CUDA_TRY(cudaMemcpyAsync(&flag, q.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (done)
+        TOMOS_CUDA_TRY(cudaMemcpyAsync(&gsh, q.gsync, sizeof(gsh), cudaMemcpyDeviceToHost, st));
     TOMOS_CUDA_TRY(cudaStreamSynchronize(st));
+    if (gsh.err)
+        return fail(TOMOS_ERR_CUDA, "sketch_qr: a bounded grid barrier wait expired");
     if (flag)
         return fail(TOMOS_ERR_NUMERIC,
                     "generate_sketch_qr_precond: trtri failed -- R is singular.");

@@ -183,17 +183,17 @@ struct HrArgs {
     int ngp;
     double* Qs;         // Q1 scratch, column-major k_rem x 32 (ld kq)
     int64_t kq;
-    double* G2p;        // G2 partials (gridDim x 32 x 32)
+    double* G2p;        // G2 partials (one per CTA of the panel passes)
     double* R1;         // 32 x 32 (row-major [i * 32 + j])
     int* fail;          // nonzero: fall back to Householder column steps
     double* T;          // nb x nb, T(a, b) at T[b * nb + a]
     double* tau;        // n
 };
 
-// Panel rows of this CTA, [r0, r1) relative to j0.
-__device__ __forceinline__ void hr_rows(const HrArgs& H, int64_t& r0, int64_t& r1) {
+// Panel rows of CTA `cta` of the panel passes, [r0, r1) relative to j0.
+__device__ __forceinline__ void hr_rows(const HrArgs& H, int cta, int64_t& r0, int64_t& r1) {
     const int64_t krem = H.k - H.j0;
-    r0 = (int64_t)blockIdx.x * H.rpc;
+    r0 = (int64_t)cta * H.rpc;
     r1 = r0 + H.rpc;
     if (r1 > krem) r1 = krem;
     if (r0 > krem) r0 = krem;
@@ -205,18 +205,27 @@ __device__ __forceinline__ void hr_reduce_gram(const double* part, int np, int n
     for (int e = threadIdx.x; e < kHB * kHB; e += blockDim.x) {
         const int i = e >> 5, j = e & 31;
         double s = 0.0;
-        if (i < nb && j < nb)
-            for (int p = 0; p < np; ++p) s += part[(size_t)p * kHB * kHB + e];
-        else
+        if (i < nb && j < nb) {
+            // eight loads in flight, summed in partial order
+            for (int p0 = 0; p0 < np; p0 += 8) {
+                double v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    v[u] = p0 + u < np ? __ldcg(part + (size_t)(p0 + u) * kHB * kHB + e) : 0.0;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) s += v[u];
+            }
+        } else {
             s = (i == j) ? 1.0 : 0.0;
+        }
         G[i][j] = s;
     }
     __syncthreads();
 }
 
 // Pass 1: R1 from the G1 partials, Q1 = P R1^-1 into Qs, G2 partials.
-__global__ void __launch_bounds__(256) qr_hr_q1_kernel(HrArgs H) {
-    extern __shared__ __align__(16) double hsm[];
+// CTA `cta` of the pass (0 writes R1 and the fallback flag).
+__device__ void hr_q1(const HrArgs& H, int cta, double* hsm) {
     HMat& G = *reinterpret_cast<HMat*>(hsm);
     HMat& R = *reinterpret_cast<HMat*>(hsm + 1 * kHB * (kHB + 1));
     HMat& X = *reinterpret_cast<HMat*>(hsm + 2 * kHB * (kHB + 1));
@@ -247,24 +256,37 @@ __global__ void __launch_bounds__(256) qr_hr_q1_kernel(HrArgs H) {
         X[i][j] /= dsc[i];
     }
     __syncthreads();
-    if (blockIdx.x == 0) {
+    if (cta == 0) {
         for (int e = t; e < kHB * kHB; e += blockDim.x) H.R1[e] = R[e >> 5][e & 31];
         if (t == 0) *H.fail = okflag ? 0 : 1;
     }
-    double* g2 = H.G2p + (size_t)blockIdx.x * kHB * kHB;
+    double* g2 = H.G2p + (size_t)cta * kHB * kHB;
     if (!okflag) return;
 
     int64_t r0, r1;
-    hr_rows(H, r0, r1);
+    hr_rows(H, cta, r0, r1);
     const int i = t & 31, c0 = (t >> 5) * 4;  // Q1 tile: row i, columns c0..c0+3
     double acc[4] = {0.0, 0.0, 0.0, 0.0};     // G2 partial: (a = i, b = c0..c0+3)
+    // The next 32-row panel tile is loaded while the current one is used
+    // (blockDim.x == 256: four entries a thread).
+    double pre[4];
+    auto fetch = [&](int64_t rt) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = t + u * 256, r = e & 31, c = e >> 5;
+            const int64_t row = rt + r;
+            pre[u] = (row < r1 && c < nb) ? __ldcg(H.A + (size_t)(H.j0 + c) * H.ld + H.j0 + row) : 0.0;
+        }
+    };
+    if (r0 < r1) fetch(r0);
     for (int64_t rt = r0; rt < r1; rt += kHB) {
         __syncthreads();
-        for (int e = t; e < kHB * kHB; e += blockDim.x) {
-            const int r = e & 31, c = e >> 5;
-            const int64_t row = rt + r;
-            Pt[r][c] = (row < r1 && c < nb) ? H.A[(size_t)(H.j0 + c) * H.ld + H.j0 + row] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = t + u * 256;
+            Pt[e & 31][e >> 5] = pre[u];
         }
+        if (rt + kHB < r1) fetch(rt + kHB);
         __syncthreads();
         double q[4] = {0.0, 0.0, 0.0, 0.0};
         for (int kk = 0; kk < kHB; ++kk) {
@@ -304,14 +326,17 @@ __device__ void hr_fallback_panel(const HrArgs& H, HMat& Gram, HMat& Tm, double*
     for (int j = 0; j < nb; ++j) {
         double* a = col(j);
         double ss = 0.0;
-        for (int64_t r = j + 1 + t; r < krem; r += blockDim.x) ss += a[r] * a[r];
+        for (int64_t r = j + 1 + t; r < krem; r += blockDim.x) {
+            const double v = __ldcg(a + r);
+            ss += v * v;
+        }
         ss = warp_sum(ss);
         if (lane == 0) red[warp] = ss;
         __syncthreads();
         if (t == 0) {
             double xn2 = 0.0;
             for (int w = 0; w < nwarp; ++w) xn2 += red[w];
-            const double alpha = a[j];
+            const double alpha = __ldcg(a + j);
             double tau = 0.0, beta = alpha, scal = 0.0;
             if (xn2 > 0.0) {
                 beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
@@ -324,7 +349,7 @@ __device__ void hr_fallback_panel(const HrArgs& H, HMat& Gram, HMat& Tm, double*
         }
         __syncthreads();
         const double tau = bc[0], beta = bc[1], scal = bc[2];
-        for (int64_t r = j + 1 + t; r < krem; r += blockDim.x) a[r] *= scal;
+        for (int64_t r = j + 1 + t; r < krem; r += blockDim.x) a[r] = __ldcg(a + r) * scal;
         __syncthreads();
         if (t == 0) {
             a[j] = beta;
@@ -334,8 +359,8 @@ __device__ void hr_fallback_panel(const HrArgs& H, HMat& Gram, HMat& Tm, double*
         // w_c = v^T a_c for the later columns, then a_c -= tau w_c v
         for (int c = j + 1 + warp; c < nb; c += nwarp) {
             const double* ac = col(c);
-            double w = lane == 0 ? ac[j] : 0.0;
-            for (int64_t r = j + 1 + lane; r < krem; r += 32) w += a[r] * ac[r];
+            double w = lane == 0 ? __ldcg(ac + j) : 0.0;
+            for (int64_t r = j + 1 + lane; r < krem; r += 32) w += __ldcg(a + r) * __ldcg(ac + r);
             w = warp_sum(w);
             if (lane == 0) wsum[c] = w;
         }
@@ -343,8 +368,8 @@ __device__ void hr_fallback_panel(const HrArgs& H, HMat& Gram, HMat& Tm, double*
         for (int c = j + 1 + warp; c < nb; c += nwarp) {
             double* ac = col(c);
             const double tw = tau * wsum[c];
-            if (lane == 0) ac[j] -= tw;
-            for (int64_t r = j + 1 + lane; r < krem; r += 32) ac[r] -= tw * a[r];
+            if (lane == 0) ac[j] = __ldcg(ac + j) - tw;
+            for (int64_t r = j + 1 + lane; r < krem; r += 32) ac[r] = __ldcg(ac + r) - tw * __ldcg(a + r);
         }
         __syncthreads();
     }
@@ -356,8 +381,8 @@ __device__ void hr_fallback_panel(const HrArgs& H, HMat& Gram, HMat& Tm, double*
             const double* vx = col(x);
             const double* vy = col(y);
             for (int64_t r = y + lane; r < krem; r += 32) {
-                const double ex = r == x ? 1.0 : vx[r];
-                const double ey = r == y ? 1.0 : vy[r];
+                const double ex = r == x ? 1.0 : __ldcg(vx + r);
+                const double ey = r == y ? 1.0 : __ldcg(vy + r);
                 g += ex * ey;
             }
             g = warp_sum(g);
@@ -389,10 +414,10 @@ __device__ void hr_fallback_panel(const HrArgs& H, HMat& Gram, HMat& Tm, double*
     }
 }
 
-// Pass 2: R2, the reconstruction (all CTAs), the top block, T and tau
-// (CTA 0) and V below the top block (each CTA its rows).
-__global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
-    extern __shared__ __align__(16) double hsm[];
+// Pass 2: R2, the reconstruction (every CTA of the pass), the top block,
+// T and tau (CTA 0) and V below the top block (each CTA its rows); `ncta`
+// CTAs ran pass 1 (its G2 partials).
+__device__ void hr_v(const HrArgs& H, int cta, int ncta, double* hsm) {
     constexpr int MS = kHB * (kHB + 1);
     HMat& G = *reinterpret_cast<HMat*>(hsm);
     HMat& R2 = *reinterpret_cast<HMat*>(hsm + 1 * MS);
@@ -407,20 +432,20 @@ __global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
     const int t = threadIdx.x;
     const int nb = H.nb;
 
-    bool ok = *H.fail == 0;
+    bool ok = __ldcg(H.fail) == 0;
     if (ok) {
-        hr_reduce_gram(H.G2p, gridDim.x, nb, G);
+        hr_reduce_gram(H.G2p, ncta, nb, G);
         ok = cta_chol(G, R2, 0.25, &okflag);
         cta_inv_upper(R2, X2, Qt);
     }
     if (!ok) {
-        if (blockIdx.x == 0) hr_fallback_panel(H, G, R2, red, bc);
+        if (cta == 0) hr_fallback_panel(H, G, R2, red, bc);
         return;
     }
     // Q_top = Q1_top R2^-1 (identity padding), then Q_top - S = L U.
     for (int e = t; e < kHB * kHB; e += blockDim.x) {
         const int r = e & 31, c = e >> 5;
-        G[r][c] = (r < nb && c < nb) ? H.Qs[(size_t)c * H.kq + r] : (r == c ? 1.0 : 0.0);
+        G[r][c] = (r < nb && c < nb) ? __ldcg(H.Qs + (size_t)c * H.kq + r) : (r == c ? 1.0 : 0.0);
     }
     __syncthreads();
     cta_mul(G, X2, Qt);
@@ -438,9 +463,10 @@ __global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
     cta_mul(X2, Ui, M);  // V2 = Q1_bot R2^-1 U^-1
     __syncthreads();
 
-    if (blockIdx.x == 0) {
+    if (cta == 0) {
         // Y = L^-1 into G; T = -U S Y^T; R = R2 R1 -> R_h = S R.
         cta_inv_unit_lower(Qt, G, X2);
+        for (int e = t; e < kHB * kHB; e += blockDim.x) X2[e >> 5][e & 31] = __ldcg(H.R1 + e);
         for (int e = t; e < nb * nb; e += blockDim.x) {
             const int i = e % nb, j = e / nb;
             // T(i, j) = -sum_k U(i, k) s_k Y(j, k), U(i, k) = Qt[i][k] for k >= i
@@ -450,12 +476,13 @@ __global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
             H.T[(size_t)j * nb + i] = -s + 0.0;
             if (i == j) H.tau[H.j0 + i] = -s + 0.0;
         }
-        // R = R2 R1 into Ui (R1 row-major in global), then the top block:
+        // R = R2 R1 into Ui (R1 in X2), then the top block:
         // R_h = S R on and above the diagonal, L strictly below.
+        __syncthreads();
         for (int e = t; e < kHB * kHB; e += blockDim.x) {
             const int i = e >> 5, j = e & 31;
             double s = 0.0;
-            for (int k = i; k <= j; ++k) s += R2[i][k] * H.R1[k * kHB + j];
+            for (int k = i; k <= j; ++k) s += R2[i][k] * X2[k][j];
             Ui[i][j] = i <= j ? s : 0.0;
         }
         __syncthreads();
@@ -467,17 +494,28 @@ __global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
     }
     // V2 rows: local rows >= nb of this CTA's block.
     int64_t r0, r1;
-    hr_rows(H, r0, r1);
+    hr_rows(H, cta, r0, r1);
     if (r0 < nb) r0 = nb;
     HMat& Pt = G;
     const int i = t & 31, c0 = (t >> 5) * 4;
+    double pre[4];  // the next Q1 tile (blockDim.x == 256: four entries a thread)
+    auto fetch = [&](int64_t rt) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = t + u * 256, r = e & 31, c = e >> 5;
+            const int64_t row = rt + r;
+            pre[u] = (row < r1 && c < nb) ? __ldcg(H.Qs + (size_t)c * H.kq + row) : 0.0;
+        }
+    };
+    if (r0 < r1) fetch(r0);
     for (int64_t rt = r0; rt < r1; rt += kHB) {
         __syncthreads();
-        for (int e = t; e < kHB * kHB; e += blockDim.x) {
-            const int r = e & 31, c = e >> 5;
-            const int64_t row = rt + r;
-            Pt[r][c] = (row < r1 && c < nb) ? H.Qs[(size_t)c * H.kq + row] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = t + u * 256;
+            Pt[e & 31][e >> 5] = pre[u];
         }
+        if (rt + kHB < r1) fetch(rt + kHB);
         __syncthreads();
         double q[4] = {0.0, 0.0, 0.0, 0.0};
         for (int kk = 0; kk < kHB; ++kk) {
@@ -492,6 +530,16 @@ __global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
                 if (c0 + u < nb) H.A[(size_t)(H.j0 + c0 + u) * H.ld + H.j0 + row] = q[u];
         }
     }
+}
+
+__global__ void __launch_bounds__(256) qr_hr_q1_kernel(HrArgs H) {
+    extern __shared__ __align__(16) double hsm[];
+    hr_q1(H, blockIdx.x, hsm);
+}
+
+__global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
+    extern __shared__ __align__(16) double hsm[];
+    hr_v(H, blockIdx.x, gridDim.x, hsm);
 }
 
 inline size_t hr_q1_smem() { return (4 * kHB * (kHB + 1) + kHB) * sizeof(double); }
