@@ -178,8 +178,10 @@ tomos_status tomos_countsketch_hash(int64_t m, int64_t s, uint64_t bucket_seed,
  * S the hash CountSketch above (replaces apply_count_sketch,
  * src/core/sketch/countsketch.cpp:20-26, whose dense-source CUDA path the
  * reference omits, sketch_registries.cpp:29-41).  Deterministic: each
- * bucket is summed by one owner in increasing row order, FP64
- * accumulation.  Packed A is read at `tier` (HALF reads only wh).
+ * bucket is summed by one owner in increasing row order in FP32 (bit for
+ * bit the reference's countsketch_apply_impl<float>,
+ * countsketch_kernels.cpp:70-83), stored as FP64.  Packed A is read at
+ * `tier` (HALF reads only wh).
  * fro2 (device, may be NULL) receives sum(A_ij^2) of the values read and
  * colsq (device, may be NULL, cols entries) the sum of squares of every
  * column, both in the same pass. */
@@ -189,6 +191,20 @@ tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t
                                      double* SA, int64_t ld_sa, double* fro2,
                                      double* colsq, void* scratch,
                                      size_t scratch_bytes, void* stream);
+/* tomos_countsketch_apply at the HALF tier of a row-major FP32_16 A (rows
+ * 16-byte aligned) that also writes, in the same pass, the fp32_16_half_only
+ * fp16 copy of A's wh plane (fp32_16_pack.hpp:553-571) to `plane` (device,
+ * 16-byte aligned, m x ld_plane halves, ld_plane a multiple of 8 and >=
+ * cols).  Passed to tomos_lsqr_solve_dense as opts.staged_plane, it spares
+ * the solve the staging pass over A its HALF-tier iterations need.  No
+ * reference counterpart (the reference's HALF tier decodes wh in every
+ * GEMV). */
+tomos_status tomos_countsketch_apply_stage(const tomos_dense* A, int64_t s,
+                                           uint64_t bucket_seed, uint64_t sign_seed,
+                                           double* SA, int64_t ld_sa, double* fro2,
+                                           double* colsq, void* plane, int64_t ld_plane,
+                                           void* scratch, size_t scratch_bytes,
+                                           void* stream);
 tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64_t s,
                                          uint64_t bucket_seed, uint64_t sign_seed,
                                          double* SA, int64_t ld_sa, double* fro2,
@@ -251,6 +267,13 @@ typedef struct tomos_lsqr_opts {
                                 TOMOS_LSQR_TIMING buckets, lsqr.cpp:85-166);
                                 iterations then run as plain launches
                                 instead of graph replays                    */
+    const void* staged_plane; /* device, may be NULL: the fixed fp16 copy of
+                                a row-major FP32_16 A's wh plane that
+                                tomos_countsketch_apply_stage wrote (m x
+                                staged_ld halves); HALF-tier iterations read
+                                it instead of staging their own copy. The
+                                caller keeps it equal to A's wh plane.      */
+    int64_t staged_ld;
 } tomos_lsqr_opts;
 
 typedef struct tomos_lsqr_report {

@@ -151,6 +151,34 @@ def test_fused_pass_matches_oracle_lsqr(orc, numeric, n, ld, tier):
     assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-4
 
 
+def test_prestaged_plane_same_solve():
+    """A solve handed the plane the staging sketch wrote runs the same passes
+    as one that stages its own copy: bit-identical x and reports."""
+    A0, b = scaled_problem(20000, 300, 11)
+    A = to_dense(A0, L.ROW_MAJOR, NT.FP32_16, pad=4)  # 16-byte aligned rows
+    SA, _, colsq, plane = tb.apply_count_sketch(A, 1200, tier=tb.Tier.HALF, with_colsq=True,
+                                                stage=True)
+    Rinv = tb.generate_sketch_qr_precond(SA)
+    d, anorm = tb.column_scale(colsq)
+    out = []
+    for staged in (None, plane):
+        ws = tb.create_lsqr_workspace(None, A.size, NT.FP32, NT.FP64)
+        tb.add_precond(Rinv, ws)
+        x = torch.zeros(300, device="cuda")
+        rep = tb.lsqr_solve(None, A, cuda(b), x, ws, 1e-6, 100, 0.0, restarts=6,
+                            stop_rule=tb.StopRule.BACKWARD, inner_rtol=2e-3, anorm_fro=anorm,
+                            col_scale=d, staged_plane=staged)
+        out.append((x.cpu().numpy(), rep))
+    (x0, r0), (x1, r1) = out
+    assert r0["converged"] == 1 and r0["backward_error"] <= 1e-6
+    assert np.array_equal(x0, x1)
+    assert r0["iterations"] == r1["iterations"] and r0["backward_error"] == r1["backward_error"]
+    ws = tb.create_lsqr_workspace(None, A.size, NT.FP32)
+    with pytest.raises(tb.TomosError):
+        tb.lsqr_solve(None, A, cuda(b), torch.zeros(300, device="cuda"), ws, 1e-6, 10, 0.0,
+                      staged_plane=plane[:, 1:])
+
+
 def test_backward_error_entry(orc):
     A0, b = scaled_problem(5000, 60, 8)
     A = to_dense(A0, L.ROW_MAJOR)

@@ -50,6 +50,32 @@ def test_apply_vs_oracle(orc, numeric, tier, layout):
     np.testing.assert_allclose(fro2.item(), (Ad.astype(np.float64) ** 2).sum(), rtol=tol)
 
 
+@pytest.mark.parametrize("n,pad,s", [(301, 3, 113), (1000, 0, 113), (1100, 4, 5)])
+def test_apply_stage(orc, n, pad, s):
+    """The staging sketch: SA bit for bit the HALF-tier sketch, and the plane
+    it writes holds fp32_16_half_only of every wh word (values outside the
+    fp16 range included: the columns span 1e-9 .. 1e9).  s = 5 gives
+    buckets of ~1400 rows (past the in-shared-memory row list and sort)
+    and n = 1100 two column panels."""
+    rng = np.random.default_rng(n)
+    m = 7001
+    A0 = (rng.standard_normal((m, n)) * np.logspace(-9, 9, n)).astype(np.float32)
+    A = to_dense(A0, L.ROW_MAJOR, NT.FP32_16, pad=pad)
+    SA0, f0, c0 = tb.apply_count_sketch(A, s, tier=tb.Tier.HALF, with_colsq=True)
+    SA, f1, c1, plane = tb.apply_count_sketch(A, s, tier=tb.Tier.HALF, with_colsq=True, stage=True)
+    # bitwise (columns past the fp16 range decode to +-Inf, so sums hold NaN)
+    assert torch.equal(SA.storage.view(torch.int64), SA0.storage.view(torch.int64))
+    assert torch.equal(f0.view(torch.int64), f1.view(torch.int64))
+    assert torch.equal(c0.view(torch.int64), c1.view(torch.int64))
+    got = plane[:, :n].view(torch.float16).float().cpu().numpy()
+    want = decoded(orc, A, tb.Tier.HALF).astype(np.float32)
+    assert np.array_equal(got, want)
+    ref = orc.countsketch_apply(want, s, row_major=True, acc="f32")
+    assert np.array_equal(SA.view().cpu().numpy(), ref, equal_nan=True)
+    with pytest.raises(tb.TomosError):
+        tb.apply_count_sketch(to_dense(A0, L.COL_MAJOR, NT.FP32_16), s, tier=tb.Tier.HALF, stage=True)
+
+
 def test_apply_reference_golden(orc):
     g = np.load(os.path.join(GOLD, "countsketch.npz"))
     A = to_dense(g["X"], L.COL_MAJOR)

@@ -341,9 +341,14 @@ def countsketch_hash(m, s, bucket_seed=CS_BUCKET_SEED, sign_seed=CS_SIGN_SEED, s
 
 
 def apply_count_sketch(A, s, tier=Tier.AUTO, bucket_seed=CS_BUCKET_SEED, sign_seed=CS_SIGN_SEED,
-                       with_colsq=False, stream=None):
+                       with_colsq=False, stage=False, stream=None):
     """SA = S A (s x n, column-major FP64 Dense) and ||A||_F^2 of the values
-    read; with_colsq also returns the column sums of squares (same pass)."""
+    read; with_colsq also returns the column sums of squares (same pass).
+    stage (row-major FP32_16 A, HALF tier): the same pass also writes the
+    fixed fp16 copy of A's wh plane, returned last (an m x ld int16 tensor
+    for lsqr_solve's staged_plane)."""
+    if stage:
+        return _count_sketch_stage(A, s, bucket_seed, sign_seed, with_colsq, stream)
     n = A.size[1]
     SA = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (s, n))
     fro2 = torch.zeros(1, dtype=torch.float64, device="cuda")
@@ -358,6 +363,27 @@ def apply_count_sketch(A, s, tier=Tier.AUTO, bucket_seed=CS_BUCKET_SEED, sign_se
     if with_colsq:
         return SA, fro2, colsq[:n]
     return SA, fro2
+
+
+def _count_sketch_stage(A, s, bucket_seed, sign_seed, with_colsq, stream):
+    if isinstance(A, Csr) or A.numeric != NumericType.FP32_16 or A.layout != Layout.ROW_MAJOR:
+        raise TomosError(C.TOMOS_ERR_INVALID, "apply_count_sketch: stage needs a row-major FP32_16 A")
+    m, n = A.size
+    ldp = (n + 7) // 8 * 8
+    plane = torch.empty((max(m, 1), ldp), dtype=torch.int16, device="cuda")
+    SA = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (s, n))
+    fro2 = torch.zeros(1, dtype=torch.float64, device="cuda")
+    colsq = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda") if with_colsq else None
+    nb = C.lib().tomos_countsketch_scratch_bytes(m, n, s)
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
+    d = A.desc()
+    C.check(C.lib().tomos_countsketch_apply_stage(ctypes.byref(d), s, bucket_seed, sign_seed,
+                                                  _ptr(SA.storage), s, _ptr(fro2), _ptr(colsq),
+                                                  _ptr(plane), ldp, _ptr(scratch), nb,
+                                                  _stream(stream)), "apply_count_sketch")
+    if with_colsq:
+        return SA, fro2, colsq[:n], plane
+    return SA, fro2, plane
 
 
 def generate_sketch_qr_precond(sketched, R_out=None, stream=None):
@@ -434,10 +460,12 @@ def add_precond(precond, workspace):
 def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=None,
                residual_history=None, restarts=1, stop_rule=StopRule.RELRES, inner_rtol=0.0,
                anorm_fro=0.0, warm_start=False, tier=None, profile=False, col_scale=None,
-               stream=None):
+               staged_plane=None, stream=None):
     """include/core/solver.hpp:68-78.  A: Dense or Csr on the device; b, x:
     FP32 Dense column vectors or float32 CUDA tensors.  iterations and
     residual_history, when lists, receive the reference's out-parameters.
+    staged_plane: the (m x ld) int16 tensor apply_count_sketch(..., stage=True)
+    filled for this A (HALF-tier iterations then skip their staging pass).
     Returns the solver report as a dict."""
     opts = C.LsqrOpts()
     opts.tol = float(tol)
@@ -457,6 +485,9 @@ def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=N
     opts.anorm_fro = float(anorm_fro)
     opts.profile = 1 if profile else 0
     opts.col_scale = col_scale.data_ptr() if col_scale is not None else None
+    if staged_plane is not None:
+        opts.staged_plane = staged_plane.data_ptr()
+        opts.staged_ld = staged_plane.stride(0)
     cap = max(1, int(max_iters) * int(restarts) + int(restarts))
     hist = (ctypes.c_double * cap)()
     opts.history = hist

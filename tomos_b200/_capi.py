@@ -45,7 +45,8 @@ class LsqrOpts(ctypes.Structure):
                 ("max_relres", c_dbl), ("stop_rule", c_i32), ("iter_tier", c_i32),
                 ("implicit_duplicate", c_i32), ("warm_start", c_i32), ("inner_rtol", c_dbl),
                 ("anorm_fro", c_dbl), ("col_scale", c_vp), ("history", ctypes.POINTER(c_dbl)),
-                ("history_cap", c_i32), ("profile", c_i32)]
+                ("history_cap", c_i32), ("profile", c_i32), ("staged_plane", c_vp),
+                ("staged_ld", c_i64)]
 
 
 class LsqrReport(ctypes.Structure):
@@ -85,6 +86,9 @@ SIGNATURES = {
     "tomos_countsketch_scratch_bytes": (c_sz, [c_i64, c_i64, c_i64]),
     "tomos_countsketch_apply": (c_i32, [ctypes.POINTER(DenseDesc), c_i32, c_i64, c_u64, c_u64,
                                         c_vp, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
+    "tomos_countsketch_apply_stage": (c_i32, [ctypes.POINTER(DenseDesc), c_i64, c_u64, c_u64,
+                                              c_vp, c_i64, c_vp, c_vp, c_vp, c_i64, c_vp, c_sz,
+                                              c_vp]),
     "tomos_countsketch_apply_csr": (c_i32, [ctypes.POINTER(CsrDesc), c_i32, c_i64, c_u64, c_u64,
                                             c_vp, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
     "tomos_sketch_qr_scratch_bytes": (c_sz, [c_i64, c_i64]),

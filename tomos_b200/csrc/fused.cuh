@@ -69,6 +69,37 @@ __device__ __forceinline__ void half2_to_f32(uint32_t w, float& a, float& b) {
     b = t.y;
 }
 
+// half_only_bits without branches (selects only), for control-1 halves.
+__device__ __forceinline__ uint32_t half_only_bits_flagged(uint32_t h) {
+    const uint32_t sign = h & 0x8000u;
+    const uint32_t sig = 0x200u | ((h >> 1) & 0x1FFu);
+    const uint32_t sub = sign | ((sig >> ((h >> 10) & 0xFu)) & 0x3FFu);
+    return (h & 0x4000u) ? (sign | 0x7C00u) : sub;
+}
+
+// fp32_16_half_only on both halves of a word (control-1 halves only),
+// branch-free: a warp whose lanes disagree on which halves are flagged
+// runs it once.
+__device__ __forceinline__ uint32_t fix_half_pair(uint32_t w) {
+    const uint32_t lo = w & 0xFFFFu, hi = w >> 16;
+    const uint32_t flo = (lo & 1u) ? half_only_bits_flagged(lo) : lo;
+    const uint32_t fhi = (hi & 1u) ? half_only_bits_flagged(hi) : hi;
+    return flo | (fhi << 16);
+}
+
+// Fixes only the words of a chunk that hold a control-1 half (rare: the
+// warp runs fix_half_pair for a word only when some lane's word needs it).
+__device__ __forceinline__ void fix_half_chunk(uint4& h) {
+    if (h.x & 0x00010001u) h.x = fix_half_pair(h.x);
+    if (h.y & 0x00010001u) h.y = fix_half_pair(h.y);
+    if (h.z & 0x00010001u) h.z = fix_half_pair(h.z);
+    if (h.w & 0x00010001u) h.w = fix_half_pair(h.w);
+}
+
+__device__ __forceinline__ float2 h2f2(uint32_t w) {
+    return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+
 // FP32_16 wh only: the words are fp16 values unless their control bit is
 // set; after the plain conversion, only elements whose control bit is set
 // (rare) are redone with the exact fp32_16_half_only decode.

@@ -480,12 +480,7 @@ __global__ void __launch_bounds__(128) stage_half_kernel(const uint16_t* __restr
         uint4* dst = reinterpret_cast<uint4*>(h16 + (size_t)r * ldh);
         for (int64_t c = threadIdx.x; c < nch; c += blockDim.x) {
             uint4 w = __ldcs(src + c);
-            if ((w.x | w.y | w.z | w.w) & 0x00010001u) {
-                if (w.x & 0x00010001u) w.x = fix_half_pair(w.x);
-                if (w.y & 0x00010001u) w.y = fix_half_pair(w.y);
-                if (w.z & 0x00010001u) w.z = fix_half_pair(w.z);
-                if (w.w & 0x00010001u) w.w = fix_half_pair(w.w);
-            }
+            fix_half_chunk(w);
             dst[c] = w;
         }
     }
@@ -680,8 +675,18 @@ struct DensePass : PassOps {
         staged.values_lo = nullptr;
         staged.ld = (A->cols + 7) / 8 * 8;
     }
+    // A copy the caller staged already (tomos_countsketch_apply_stage).
+    const void* given = nullptr;
+    int64_t given_ld = 0;
     tomos_status prepare(cudaStream_t st) override {
         if (!stage) return TOMOS_OK;
+        if (given) {
+            staged = *A;
+            staged.values = const_cast<void*>(given);  // read only
+            staged.values_lo = nullptr;
+            staged.ld = given_ld;
+            return TOMOS_OK;
+        }
         const int64_t m = A->rows, n = A->cols, ldh = (n + 7) / 8 * 8;
         const size_t bytes = (size_t)m * ldh * sizeof(uint16_t);
         if (bytes > ws->h16_bytes) {
@@ -743,7 +748,8 @@ struct DensePass : PassOps {
     }
     uint64_t key() override {
         return reinterpret_cast<uint64_t>(A->values) ^ ((uint64_t)A->layout << 60) ^
-               ((uint64_t)A->ld << 20) ^ (stage ? reinterpret_cast<uint64_t>(ws->h16) * 31 : 0);
+               ((uint64_t)A->ld << 20) ^
+               (stage ? reinterpret_cast<uint64_t>(staged.values) * 31 ^ ((uint64_t)staged.ld << 40) : 0);
     }
     int64_t rows() override { return A->rows; }
     int64_t cols() override { return A->cols; }
@@ -1214,6 +1220,17 @@ tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float*
         return TOMOS_OK;
     }
     DensePass ops(ws, A, ie, ze);
+    if (opts->staged_plane) {
+        if (A->numeric != TOMOS_FP32_16 || A->layout != TOMOS_ROW_MAJOR)
+            return fail(TOMOS_ERR_INVALID, "lsqr_solve: staged_plane needs a row-major FP32_16 A");
+        if (reinterpret_cast<uintptr_t>(opts->staged_plane) % 16 != 0 || opts->staged_ld < A->cols ||
+            opts->staged_ld % 8 != 0)
+            return fail(TOMOS_ERR_INVALID,
+                        "lsqr_solve: staged_plane must be 16-byte aligned with staged_ld a multiple "
+                        "of 8 and >= cols");
+        ops.given = opts->staged_plane;
+        ops.given_ld = opts->staged_ld;
+    }
     PassPlan a = ops.plan(true), b2 = ops.plan(false);
     if (!a.fused || !b2.fused) {
         s = ensure_scratch(ws, dense_pass_scratch(A));

@@ -67,20 +67,8 @@ struct RowPassParams {
     int copy_bytes;  // bytes copied per row and plane (16-byte multiple)
 };
 
-// fp32_16_half_only on both halves of a word (control-1 halves only).
-__device__ __forceinline__ uint32_t fix_half_pair(uint32_t w) {
-    uint32_t lo = w & 0xFFFFu, hi = w >> 16;
-    if (lo & 1u) lo = half_only_bits(lo);
-    if (hi & 1u) hi = half_only_bits(hi);
-    return lo | (hi << 16);
-}
-
 __device__ __forceinline__ uint4 lds128(const uint8_t* p) {
     return *reinterpret_cast<const uint4*>(p);
-}
-
-__device__ __forceinline__ float2 h2f2(uint32_t w) {
-    return __half22float2(*reinterpret_cast<const __half2*>(&w));
 }
 
 // Decodes this lane's NCH chunks of one row part from shared memory into
@@ -102,12 +90,7 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
         }
         if (any & 0x00010001u) {
 #pragma unroll
-            for (int k = 0; k < NCH; ++k) {
-                h[k].x = fix_half_pair(h[k].x);
-                h[k].y = fix_half_pair(h[k].y);
-                h[k].z = fix_half_pair(h[k].z);
-                h[k].w = fix_half_pair(h[k].w);
-            }
+            for (int k = 0; k < NCH; ++k) fix_half_chunk(h[k]);
         }
 #pragma unroll
         for (int k = 0; k < NCH; ++k) {
