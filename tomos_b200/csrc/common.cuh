@@ -127,6 +127,21 @@ __host__ __device__ __forceinline__ float decode_fp32_16_exact(uint32_t h, uint3
     return u2f(sign | mag);
 }
 
+// decode_fp32_16_exact without branches, equal to it for every (h, r)
+// (checked over all 2^32 pairs): the exponent is 112 + e5 for control-0
+// words and 112 + e5 + 15 (upward step) or 112 - e5 (downward step) for
+// control-1 words, and the step field 14 stands for +-Inf / +-0.  A warp
+// then never diverges on the rare control-1 elements.
+__host__ __device__ __forceinline__ float decode_fp32_16_exact_nb(uint32_t hh, uint32_t rr) {
+    const uint32_t e5 = (hh >> 10) & 0x1Fu;
+    const uint32_t c = hh & 1u, dir = (hh >> 14) & 1u;
+    const int32_t off = c ? (dir ? (int32_t)e5 + 15 : -(int32_t)e5) : (int32_t)e5;
+    const uint32_t mag = ((uint32_t)(off + 112) << 23) + ((hh & 0x3FEu) << 13) + (rr >> 2) - ((rr & 1u) << 14);
+    const uint32_t special = c & ((e5 & 0xFu) == 14u);
+    const uint32_t res = special ? (dir ? 0x7F800000u : 0u) : mag;
+    return u2f(((hh & 0x8000u) << 16) | res);
+}
+
 // wh -> the fp16 bit pattern fp32_16_half_only produces
 // (fp32_16_pack.hpp:553-571): control-0 words are already fp16; overflow
 // saturates to signed Inf; underflow steps become an fp16 subnormal by

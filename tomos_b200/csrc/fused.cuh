@@ -145,8 +145,9 @@ struct ChunkDecoder<Elem::A16> {
         h = __ldcs(reinterpret_cast<const uint4*>(static_cast<const uint16_t*>(P.hi) + off));
         r = __ldcs(reinterpret_cast<const uint4*>(static_cast<const uint16_t*>(P.lo) + off));
     }
-    // The normal-range formula for every element, then the exact decode
-    // only for elements whose control bit is set (rare).
+    // The branch-free exact decode for every element: control-1 words
+    // are rare per element but common per warp, where a branch would make
+    // the whole warp wait on them.
     static __device__ __forceinline__ void decode(const uint4& h, const uint4& r, float* f) {
         const uint32_t wh[4] = {h.x, h.y, h.z, h.w};
         const uint32_t wr[4] = {r.x, r.y, r.z, r.w};
@@ -154,16 +155,7 @@ struct ChunkDecoder<Elem::A16> {
         for (int k = 0; k < 8; ++k) {
             const uint32_t hh = (wh[k >> 1] >> ((k & 1) * 16)) & 0xFFFFu;
             const uint32_t rr = (wr[k >> 1] >> ((k & 1) * 16)) & 0xFFFFu;
-            const uint32_t mag = ((hh & 0x7FFEu) << 13) + 0x38000000u + (rr >> 2) - ((rr & 1u) << 14);
-            f[k] = __uint_as_float(((hh & 0x8000u) << 16) | mag);
-        }
-        if ((h.x | h.y | h.z | h.w) & 0x00010001u) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t hh = (wh[k >> 1] >> ((k & 1) * 16)) & 0xFFFFu;
-                const uint32_t rr = (wr[k >> 1] >> ((k & 1) * 16)) & 0xFFFFu;
-                if (hh & 1u) f[k] = decode_fp32_16_exact(hh, rr);
-            }
+            f[k] = decode_fp32_16_exact_nb(hh, rr);
         }
     }
 };

@@ -387,7 +387,8 @@ static tomos_status ensure_history(tomos_workspace* ws, int cap) {
 template <Elem E, int NCH, int G, bool ACC64>
 static tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
     constexpr int ESZ = (E == Elem::F32) ? 4 : 2;
-    constexpr int RS = kRowWarps / G;
+    constexpr int CW = RowWarps<E, ACC64>::value;
+    constexpr int RS = CW / G;
     RowPassParams T;
     T.f = P;
     T.err = err;
@@ -397,28 +398,45 @@ static tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cud
     if (ns > kRowMaxStages) ns = kRowMaxStages;
     if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
     T.nstage = ns;
-    const size_t smem = fused_rows_smem<E, NCH>(ns, RS, T.copy_bytes);
+    const size_t smem = fused_rows_smem<E, NCH, ACC64>(ns, RS, T.copy_bytes);
     auto kern = fused_rows_kernel<E, NCH, G, ACC64>;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<grid, kRowThreads, smem, st>>>(T);
+    kern<<<grid, (CW + 1) * 32, smem, st>>>(T);
     TOMOS_LAUNCH_CHECK("fused_rows_kernel");
     return TOMOS_OK;
 }
 
-// Columns one consumer warp covers at its widest: 32 lanes x 16-byte
-// chunks x (4, 16-bit storage / 8, FP32) -- halved for ACC64, whose p is
-// held in FP64 registers.
+static bool elem_two_planes(Elem e) {
+    return e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R;
+}
+
+// 16-byte chunks a lane takes per row part at most (RowNchMax).
 static int fused_nch_max(Elem e, bool acc64) {
-    const int nmax = (e == Elem::F32) ? 8 : 4;
-    return acc64 ? nmax / 2 : nmax;
+    const int base = (e == Elem::F32) ? 8 : 4;
+    return (acc64 && elem_two_planes(e)) ? base / 2 : base;
+}
+
+// Consumer warps of a pass (RowWarps).
+static int fused_warps(Elem e, bool acc64) {
+    return (acc64 && !elem_two_planes(e)) ? 8 : 12;
+}
+
+// Warps per row a pass may split a row over (divisors of its consumer
+// warps).
+static const int* fused_g_list(Elem e, bool acc64, int* count) {
+    static const int g12[] = {2, 3, 4, 6, 12};
+    static const int g8[] = {2, 4, 8};
+    const bool eight = fused_warps(e, acc64) == 8;
+    *count = eight ? 3 : 5;
+    return eight ? g8 : g12;
 }
 
 // (nch, g) pairs with an instantiation: one warp per row with 1..NCHMAX
-// chunks per lane, or G = 2, 3, 4, 6, 12 warps per row at NCHMAX.
+// chunks per lane, or G warps per row (fused_g_list) at NCHMAX.
 template <Elem E, bool ACC64>
 static tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int g, int grid,
                                    cudaStream_t st) {
-    constexpr int NMAX = ((E == Elem::F32) ? 8 : 4) / (ACC64 ? 2 : 1);
+    constexpr int NMAX = RowNchMax<E, ACC64>::value;
     if (g == 1) {
         switch (nch) {
             case 1: return launch_fused_t<E, 1, 1, ACC64>(P, err, grid, st);
@@ -432,13 +450,22 @@ static tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int 
             default: break;
         }
     } else if (nch == NMAX) {
-        switch (g) {
-            case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
-            case 3: return launch_fused_t<E, NMAX, 3, ACC64>(P, err, grid, st);
-            case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
-            case 6: return launch_fused_t<E, NMAX, 6, ACC64>(P, err, grid, st);
-            case 12: return launch_fused_t<E, NMAX, 12, ACC64>(P, err, grid, st);
-            default: break;
+        if constexpr (RowWarps<E, ACC64>::value == 8) {
+            switch (g) {
+                case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
+                case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
+                case 8: return launch_fused_t<E, NMAX, 8, ACC64>(P, err, grid, st);
+                default: break;
+            }
+        } else {
+            switch (g) {
+                case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
+                case 3: return launch_fused_t<E, NMAX, 3, ACC64>(P, err, grid, st);
+                case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
+                case 6: return launch_fused_t<E, NMAX, 6, ACC64>(P, err, grid, st);
+                case 12: return launch_fused_t<E, NMAX, 12, ACC64>(P, err, grid, st);
+                default: break;
+            }
         }
     }
     return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
@@ -487,7 +514,7 @@ __global__ void __launch_bounds__(128) stage_half_kernel(const uint16_t* __restr
 }
 
 // Chooses the fused pass when A is row-major with 16-byte aligned rows
-// and n fits 12 consumer warps (12288 columns, 6144 for ACC64); otherwise
+// and n fits the consumer warps (12288 columns; 8192 or 6144 for ACC64); otherwise
 // the generic two-kernel path.
 PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64) {
     PassPlan pl;
@@ -509,7 +536,10 @@ PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool
         }
     }
     if (nch == 0) {
-        for (int gg : {2, 3, 4, 6, 12}) {
+        int ng = 0;
+        const int* gl = fused_g_list(e, pl.acc64, &ng);
+        for (int q = 0; q < ng; ++q) {
+            const int gg = gl[q];
             if ((int64_t)gg * 32 * nmax * vec >= A->cols) {
                 nch = nmax;
                 g = gg;

@@ -7,8 +7,9 @@
 //     ss  += ut_i^2                         per-CTA partial, FP64
 // so the two products of an LSQR iteration cost one read of A.
 //
-// Roles (one CTA per SM, 13 warps):
-//   producer (warp 12, lane 0)           consumers (warps 0..11)
+// Roles (one CTA per SM, CW + 1 warps; CW = 12, or 8 for ACC64 over one
+// plane):
+//   producer (warp CW, lane 0)           consumers (warps 0..CW-1)
 //   wait empty[s]                        wait full[s]
 //   expect_tx(full[s], bytes)            copy its row part to registers,
 //   cp.async.bulk per plane (one per       decode, arrive empty[s]
@@ -17,12 +18,13 @@
 //                                        dot with p (packed FP32x2 FMAs),
 //                                        shuffle reduce, ut,
 //                                        q += ut * row (packed FMAs)
-// A stage holds RS = 12 / G rows.  G consumer warps share a row when n is
-// wider than one warp's columns (1024, or 512 for ACC64; G divides 12);
-// their partial dots meet in shared memory behind a named barrier per row.  Lane l of part g
-// owns the 16-byte chunks g*32*NCH + k*32 + l (k < NCH) of its row, so p
-// and the q accumulators live in registers and every shared-memory read
-// is a conflict-free 16-byte access.
+// A stage holds RS = CW / G rows.  G consumer warps share a row when n is
+// wider than one warp's columns (1024, 512 for the two-plane ACC64
+// passes; G divides CW); their partial dots meet in shared memory behind
+// a named barrier per row.  Lane l of part g owns the 16-byte chunks
+// g*32*NCH + k*32 + l (k < NCH) of its row, so p and the q accumulators
+// live in registers and every shared-memory read is a conflict-free
+// 16-byte access.
 //
 // FP32_16 wh words with the control bit set (values outside the fp16
 // range) are rare; one OR over a row's words tests for them and only then
@@ -31,9 +33,10 @@
 // ACC64 (the exact tiers, restart residuals, backward errors) forms every
 // product exactly and sums it in FP64, as the reference's accurate tier
 // does: p is held in FP64 registers, so an element costs one conversion
-// and one DFMA.  To stay within the register budget an ACC64 warp covers
-// half as many columns (16 per lane) and rows are split over G = 2..12
-// warps sooner.  HALF-tier and FP32 passes accumulate in FP32.
+// and one DFMA, and the dot runs as four independent FP64 chains.  Those
+// registers are why a one-plane ACC64 CTA has 8 consumer warps (each warp
+// still covers 1024 columns); the two-plane exact decodes keep 12 warps
+// at 512 columns a warp.  HALF-tier and FP32 passes accumulate in FP32.
 //
 // Every mbarrier wait is bounded.  A consumer whose wait expires records
 // the failure in *err and stops waiting (it still runs the remaining
@@ -50,8 +53,28 @@
 
 namespace tomos_b200 {
 
-constexpr int kRowWarps = 12;  // 13 warps with the producer: up to 128 registers
-constexpr int kRowThreads = (kRowWarps + 1) * 32;
+template <Elem E>
+struct RowPlanes;
+
+// Consumer warps of a pass.  13 warps (with the producer) leave 128
+// registers a thread; the FP64-accumulating passes over one plane keep p
+// in FP64 and a whole row part per lane, and run 8 consumers (9 warps: up
+// to 168 registers) so that a warp still covers 1024 columns.  The exact
+// two-plane decodes are ALU-heavy and keep 12 warps (a warp covering 512
+// columns) to hide their latency.
+template <Elem E, bool ACC64>
+struct RowWarps {
+    static constexpr int value = (ACC64 && RowPlanes<E>::value == 1) ? 8 : 12;
+};
+constexpr int kRowWarps = 12;  // the widest configuration (shared arrays)
+
+// 16-byte chunks a lane takes per row part at most (a warp covers 32 x
+// that x VEC columns).
+template <Elem E, bool ACC64>
+struct RowNchMax {
+    static constexpr int base = (E == Elem::F32) ? 8 : 4;
+    static constexpr int value = (ACC64 && RowWarps<E, ACC64>::value == 12) ? base / 2 : base;
+};
 constexpr int kRowMaxStages = 12;
 constexpr size_t kRowSmemBudget = 200 * 1024;
 
@@ -80,7 +103,38 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
                                            float2 (&a)[NCH * ChunkElems<E>::value / 2]) {
     constexpr int VEC = ChunkElems<E>::value;
     constexpr int HV = VEC / 2;
-    if constexpr (E == Elem::H16) {
+    if constexpr (E == Elem::A16) {
+        // Chunks in which no lane of the warp holds a control-1 word (most)
+        // take the normal-range formula; the others the branch-free exact
+        // decode -- the choice is uniform over the warp.
+        const unsigned am = __activemask();
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            const bool lv = (live >> k) & 1u;
+            uint4 h = make_uint4(0, 0, 0, 0), r = make_uint4(0, 0, 0, 0);
+            if (lv) {
+                h = lds128(hrow + coff[k]);
+                r = lds128(lrow + coff[k]);
+            }
+            float f[8];
+            if (__any_sync(am, ((h.x | h.y | h.z | h.w) & 0x00010001u) != 0u)) {
+                ChunkDecoder<E>::decode(h, r, f);
+            } else {
+                const uint32_t wh[4] = {h.x, h.y, h.z, h.w};
+                const uint32_t wr[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const uint32_t hh = (wh[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+                    const uint32_t rr = (wr[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+                    const uint32_t mag = ((hh & 0x7FFEu) << 13) + 0x38000000u + (rr >> 2) - ((rr & 1u) << 14);
+                    f[q] = __uint_as_float(((hh & 0x8000u) << 16) | mag);
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < HV; ++e)
+                a[k * HV + e] = lv ? make_float2(f[2 * e], f[2 * e + 1]) : make_float2(0.0f, 0.0f);
+        }
+    } else if constexpr (E == Elem::H16) {
         uint4 h[NCH];
         uint32_t any = 0;
 #pragma unroll
@@ -129,13 +183,16 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
 }
 
 template <Elem E, int NCH, int G, bool ACC64>
-__global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParams T) {
+__global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused_rows_kernel(RowPassParams T) {
+    constexpr int CW = RowWarps<E, ACC64>::value;  // consumer warps
+    constexpr int NTHREADS = (CW + 1) * 32;
+    static_assert(CW % G == 0, "G divides the consumer warps");
     const FusedParams& P = T.f;
     if (P.skip && *P.skip) return;
     constexpr int VEC = ChunkElems<E>::value;
     constexpr int PER = NCH * VEC;      // columns per lane
     constexpr int WCOLS = 32 * PER;     // columns per consumer warp
-    constexpr int RS = kRowWarps / G;   // rows per stage
+    constexpr int RS = CW / G;          // rows per stage
     constexpr int PLANES = RowPlanes<E>::value;
     constexpr int ESZ = (E == Elem::F32) ? 4 : 2;
     static_assert(PER % 4 == 0, "pairs of pairs");
@@ -164,7 +221,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParam
     if (threadIdx.x == 0) {
         for (int s = 0; s < nstage; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kRowWarps);
+            mbar_init(&empty[s], CW);
         }
         abort_flag = 0;
         fence_barrier_init();
@@ -178,7 +235,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParam
     const int rg = warp / G;    // row of the stage
     const int part = warp % G;  // column part of the row
 
-    if (warp == kRowWarps) {
+    if (warp == CW) {
         // ---------------------------------------------------------- producer
         if (lane == 0) {
             const bool contiguous = (int64_t)P.ld * ESZ == cb;
@@ -306,13 +363,15 @@ __global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParam
 
             double dsum;
             if constexpr (ACC64) {
-                double d0 = 0.0, d1 = 0.0;
+                double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
 #pragma unroll
-                for (int j = 0; j < PER / 2; ++j) {
+                for (int j = 0; j < PER / 2; j += 2) {
                     d0 = fma((double)a[j].x, pv[2 * j], d0);
                     d1 = fma((double)a[j].y, pv[2 * j + 1], d1);
+                    d2 = fma((double)a[j + 1].x, pv[2 * j + 2], d2);
+                    d3 = fma((double)a[j + 1].y, pv[2 * j + 3], d3);
                 }
-                double dd = d0 + d1;
+                double dd = (d0 + d1) + (d2 + d3);
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(0xffffffffu, dd, o);
                 dsum = dd;
@@ -352,7 +411,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParam
     // memory can hold the cross-warp reduction.
     __syncthreads();
     float* red = reinterpret_cast<float*>(smem);
-    if (warp < kRowWarps) {
+    if (warp < CW) {
 #pragma unroll
         for (int k = 0; k < NCH; ++k) {
             float4* dst = reinterpret_cast<float4*>(&red[(size_t)warp * WCOLS + (k * 32 + lane) * VEC]);
@@ -366,7 +425,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParam
     }
     __syncthreads();
     float* qout = P.qpart + (size_t)blockIdx.x * P.qstride;
-    for (int64_t j = threadIdx.x; j < P.n; j += kRowThreads) {
+    for (int64_t j = threadIdx.x; j < P.n; j += NTHREADS) {
         const int g = (int)(j / WCOLS);
         const int loc = (int)(j % WCOLS);
         float sum = 0.0f;
@@ -377,18 +436,18 @@ __global__ void __launch_bounds__(kRowThreads, 1) fused_rows_kernel(RowPassParam
     if (threadIdx.x == 0) {
         double sum = 0.0;
 #pragma unroll
-        for (int w = 0; w < kRowWarps; ++w) sum += ssw[w];
+        for (int w = 0; w < CW; ++w) sum += ssw[w];
         P.sspart[blockIdx.x] = sum;
     }
 }
 
 // Dynamic shared memory of one launch: the stage ring, at least the
 // cross-warp reduction buffer.
-template <Elem E, int NCH>
+template <Elem E, int NCH, bool ACC64>
 inline size_t fused_rows_smem(int nstage, int rows_per_stage, int copy_bytes) {
     constexpr int VEC = ChunkElems<E>::value;
     const size_t ring = (size_t)nstage * rows_per_stage * copy_bytes * RowPlanes<E>::value;
-    const size_t red = (size_t)kRowWarps * NCH * 32 * VEC * sizeof(float);
+    const size_t red = (size_t)RowWarps<E, ACC64>::value * NCH * 32 * VEC * sizeof(float);
     return ring > red ? ring : red;
 }
 
