@@ -33,6 +33,7 @@
 #include "gemv.cuh"
 #include "lsqr.cuh"
 #include "rowpass.cuh"
+#include "rowpass_mma.cuh"
 
 namespace tomos_b200 {
 
@@ -406,6 +407,41 @@ static tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cud
     return TOMOS_OK;
 }
 
+// The staged-fp16 pass on the tensor cores (rowpass_mma.cuh).
+template <int TPW>
+static tomos_status launch_fused_mma_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
+    MmaPassParams T;
+    T.f = P;
+    T.err = err;
+    T.cb = (int)((((int64_t)P.n * 2) + 15) / 16 * 16);
+    // an odd number of 16-byte units between rows keeps ldmatrix free of
+    // bank conflicts
+    T.pitch = ((T.cb / 16) % 2 == 1) ? T.cb : T.cb + 16;
+    const size_t stage = (size_t)kMmaRows * T.pitch;
+    int ns = (int)((kRowSmemBudget - 64) / stage);
+    if (ns > kMmaMaxStages) ns = kMmaMaxStages;
+    if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
+    T.nstage = ns;
+    const size_t smem = fused_rows_mma_smem(ns, T.pitch);
+    auto kern = fused_rows_mma_kernel<TPW>;
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, kMmaThreads, smem, st>>>(T);
+    TOMOS_LAUNCH_CHECK("fused_rows_mma_kernel");
+    return TOMOS_OK;
+}
+
+static tomos_status launch_fused_mma(const FusedParams& P, int* err, int tpw, int grid, cudaStream_t st) {
+    switch (tpw) {
+        case 1: return launch_fused_mma_t<1>(P, err, grid, st);
+        case 2: return launch_fused_mma_t<2>(P, err, grid, st);
+        case 3: return launch_fused_mma_t<3>(P, err, grid, st);
+        case 4: return launch_fused_mma_t<4>(P, err, grid, st);
+        case 5: return launch_fused_mma_t<5>(P, err, grid, st);
+        case 6: return launch_fused_mma_t<6>(P, err, grid, st);
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no tensor-core instantiation");
+    }
+}
+
 static bool elem_two_planes(Elem e) {
     return e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R;
 }
@@ -551,6 +587,11 @@ PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool
         pl.fused = true;
         pl.nch = nch;
         pl.g = g;
+        // the staged fp16 plane of an iteration: both products on the
+        // tensor cores when n fits 12 warps x kMmaMaxTpw k-tiles
+        const int64_t ktiles = (A->cols + 15) / 16;
+        if (e == Elem::F16 && !pl.acc64 && ktiles <= (int64_t)kMmaWarps * kMmaMaxTpw)
+            pl.tpw = (int)((ktiles + kMmaWarps - 1) / kMmaWarps);
         int64_t grid = sm_count();
         const int64_t min_rows_cta = 64;
         const int64_t gr = (A->rows + min_rows_cta - 1) / min_rows_cta;
@@ -596,7 +637,8 @@ tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A,
         P.sspart = ws->sspart;
         P.qstride = pl.qstride;
         P.skip = skip;
-        tomos_status ls = launch_fused(pl.e, pl.acc64, P, &ws->st->pipe_err, pl.nch, pl.g, pl.grid, st);
+        tomos_status ls = pl.tpw > 0 ? launch_fused_mma(P, &ws->st->pipe_err, pl.tpw, pl.grid, st)
+                                     : launch_fused(pl.e, pl.acc64, P, &ws->st->pipe_err, pl.nch, pl.g, pl.grid, st);
         if (ls) return ls;
         ws->launches += 1;
         return TOMOS_OK;
@@ -891,6 +933,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
                                  (uint64_t)pl_iter.nch,
                                  (uint64_t)pl_iter.g,
                                  (uint64_t)pl_iter.grid,
+                                 (uint64_t)pl_iter.tpw,
                                  reinterpret_cast<uint64_t>(x),
                                  (uint64_t)ws->has_precond,
                                  (uint64_t)n,

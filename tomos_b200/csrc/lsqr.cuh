@@ -46,6 +46,7 @@ struct PassPlan {
     int gq = 1;      // rows of A^T partials
     int gs = 1;      // ||ut||^2 partials
     int64_t qstride = 0;
+    int tpw = 0;     // > 0: the tensor-core pass, k-tiles per consumer warp
 };
 
 // One pass over A producing ut = cp*A p + cu*u_in in the workspace's u,
