@@ -24,6 +24,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "mbarrier.cuh"  // smem_addr
 #include "qr_panel.cuh"
 
 namespace tomos_b200 {
@@ -33,7 +34,7 @@ constexpr int kQrNb = 32;        // panel width
 constexpr int kQrWc = 64;        // trailing columns per update tile
 constexpr int kQrChunks = 8;     // row chunks of the W partials
 constexpr int kQrRowTile = 256;  // rows per apply tile (and per Gram partial)
-constexpr int kQrPanelCtas = 16; // CTAs of the panel passes
+constexpr int kQrPanelCtas = 64; // CTAs of the panel passes (~64 rows each)
 
 struct QrScratch {
     double* tau;    // n
@@ -92,10 +93,20 @@ __device__ __forceinline__ double vref(const double* A, int64_t ld, int64_t j0, 
     return i == a ? 1.0 : 0.0;
 }
 
+// D = A B + C for one m8n8k4 FP64 tile on the tensor cores.  Lane l holds
+// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 // Gram partials of the first panel: tile `tile` sums rows [256 t, 256 t + 256).
 // Shared tiles of the phase functions below, carved from `sm` (dynamic
 // shared memory of the calling kernel, 16-byte aligned).
-constexpr int kQrTileSmemDoubles = 2 * kHB * (kQrWc + 2) + kHB * (kHB + 1);
+// (the trailing update's W, T^T W and T tiles plus its copy stages)
+constexpr int kQrTileSmemDoubles =
+    2 * kHB * (kQrWc + 2) + kHB * (kHB + 1) + 3 * (kHB * (kHB + 1) + kHB * (kQrWc + 2));
 
 __device__ void qr_gram_tile(const double* A, int64_t ld, int64_t k, int nb, int tile, double* Gp,
                              double* sm) {
@@ -131,82 +142,118 @@ __global__ void __launch_bounds__(kQrThreads) qr_gram_kernel(const double* A, in
     qr_gram_tile(A, ld, k, nb, blockIdx.x, Gp, qsm);
 }
 
-// Shared tiles of the trailing update keep an even row stride so that
-// four consecutive doubles load as two 16-byte accesses.
+// Shared tiles of the trailing update keep an even row stride.
 constexpr int kQrWs = kQrWc + 2;
+// Sub-tiles (32 rows of V and of C) in flight in the trailing update.
+constexpr int kQrStages = 3;
+constexpr int kQrStageDoubles = kHB * (kHB + 1) + kHB * kQrWs;
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The V and C sub-tiles of rows [rt, rt + 32) (relative to j0) into one
+// stage: V(i, a) = A[j0 + a][j0 + i] as stored (the unit diagonal and the
+// zeros above it are set by qr_fix_v once the copies landed), C(i, c) the
+// trailing columns c0 + c.  Rows past r1, reflectors past nb and columns
+// past nc read as zeros.  One asynchronous copy group per call.
+__device__ __forceinline__ void qr_issue_vc(const double* A, int64_t ld, int64_t j0, int nb, int64_t nc,
+                                            int64_t c0, int64_t rt, int64_t r1, double* stage) {
+    double (*Vs)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
+    double (*Cs)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * (kHB + 1));
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < kHB * kHB / kQrThreads; ++i) {
+        const int e = t + i * kQrThreads, r = e & 31, aa = e >> 5;
+        const int64_t row = rt + r;
+        const bool ok = row < r1 && aa < nb;
+        cp_async8(&Vs[r][aa], ok ? A + (size_t)(j0 + aa) * ld + j0 + row : A, ok);
+    }
+#pragma unroll
+    for (int i = 0; i < kHB * kQrWc / kQrThreads; ++i) {
+        const int e = t + i * kQrThreads, r = e & 31, c = e >> 5;
+        const int64_t row = rt + r, col = c0 + c;
+        const bool ok = row < r1 && col < nc;
+        cp_async8(&Cs[r][c], ok ? A + (size_t)(j0 + nb + col) * ld + j0 + row : A, ok);
+    }
+    cp_async_commit();
+}
+
+// The panel's first 32 rows of V: unit diagonal, zeros above it.
+__device__ __forceinline__ void qr_fix_v(double* stage, int64_t rt) {
+    if (rt != 0) return;
+    double (*Vs)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
+    for (int e = threadIdx.x; e < kHB * kHB; e += kQrThreads) {
+        const int r = e & 31, aa = e >> 5;
+        if (r <= aa) Vs[r][aa] = r == aa ? 1.0 : 0.0;
+    }
+}
 
 // W partials: Wp[chunk][a][c] = sum over the chunk's rows of V(i, a) C(i, c),
-// C the trailing columns j0 + nb + c.  A CTA: one row chunk x 64 columns;
-// a thread: reflectors a0 and a0 + 16 x four consecutive columns.
+// C the trailing columns j0 + nb + c.  A CTA: one row chunk x 64 columns,
+// 32-row sub-tiles streamed through kQrStages shared-memory stages by
+// asynchronous copies; warp w: all 32 reflectors x columns 8w..8w+7 as four
+// m8n8 FP64 tensor-core tiles, 4 rows of a sub-tile per step.
 __device__ void qr_w_part_tile(const double* A, int64_t ld, int64_t k, int64_t n, int64_t j0, int nb,
                                int64_t chunk_rows, double* Wp, int ct, int rc, double* sm) {
-    double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm);
-    double (*Vt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(sm + kHB * kQrWs);
     const int t = threadIdx.x;
-    const int a0 = t & 15, cg = (t >> 4) * 4;
+    const int lane = t & 31, warp = t >> 5, g = lane >> 2, q = lane & 3;
+    const int cw = warp * 8;
     const int64_t nc = n - j0 - nb, krem = k - j0;
     const int64_t c0 = (int64_t)ct * kQrWc;
     const int64_t r0 = (int64_t)rc * chunk_rows;
     int64_t r1 = r0 + chunk_rows;
     if (r1 > krem) r1 = krem;
-    double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
-    // The next 32-row sub-tile is loaded into registers while the current
-    // one is multiplied (its L2 latency hidden behind the FMAs).
-    constexpr int NV = kHB * kHB / kQrThreads, NC = kHB * kQrWc / kQrThreads;
-    double vpre[NV], cpre[NC];
-    auto fetch = [&](int64_t rt) {
+    const int nsub = r1 > r0 ? (int)((r1 - r0 + kHB - 1) / kHB) : 0;
+    double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    __syncthreads();  // a previous tile of this CTA may still read the stages
 #pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            const int e = t + i * kQrThreads, r = e & 31, aa = e >> 5;
-            const int64_t row = rt + r;
-            vpre[i] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-            const int e = t + i * kQrThreads, r = e & 31, c = e >> 5;
-            const int64_t row = rt + r, col = c0 + c;
-            cpre[i] = (row < r1 && col < nc) ? __ldcg(A + (size_t)(j0 + nb + col) * ld + j0 + row) : 0.0;
-        }
-    };
-    if (r0 < r1) fetch(r0);
-    for (int64_t rt = r0; rt < r1; rt += kHB) {
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            const int e = t + i * kQrThreads;
-            Vt[e & 31][e >> 5] = vpre[i];
-        }
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-            const int e = t + i * kQrThreads;
-            Ct[e & 31][e >> 5] = cpre[i];
-        }
-        if (rt + kHB < r1) fetch(rt + kHB);
-        __syncthreads();
-#pragma unroll 4
-        for (int r = 0; r < kHB; ++r) {
-            const double v0 = Vt[r][a0], v1 = Vt[r][a0 + 16];
-            const double2 cA = *reinterpret_cast<const double2*>(&Ct[r][cg]);
-            const double2 cB = *reinterpret_cast<const double2*>(&Ct[r][cg + 2]);
-            acc0[0] += v0 * cA.x;
-            acc0[1] += v0 * cA.y;
-            acc0[2] += v0 * cB.x;
-            acc0[3] += v0 * cB.y;
-            acc1[0] += v1 * cA.x;
-            acc1[1] += v1 * cA.y;
-            acc1[2] += v1 * cB.x;
-            acc1[3] += v1 * cB.y;
-        }
+    for (int i = 0; i < kQrStages - 1; ++i) {
+        if (i < nsub) qr_issue_vc(A, ld, j0, nb, nc, c0, r0 + (int64_t)i * kHB, r1, sm + i * kQrStageDoubles);
+        else cp_async_commit();
     }
+    for (int i = 0; i < nsub; ++i) {
+        const int ni = i + kQrStages - 1;
+        if (ni < nsub)
+            qr_issue_vc(A, ld, j0, nb, nc, c0, r0 + (int64_t)ni * kHB, r1, sm + (ni % kQrStages) * kQrStageDoubles);
+        else
+            cp_async_commit();
+        cp_async_wait<kQrStages - 1>();  // this thread's copies of sub-tile i
+        __syncthreads();                 // everyone's
+        double* stage = sm + (i % kQrStages) * kQrStageDoubles;
+        const int64_t rt = r0 + (int64_t)i * kHB;
+        if (rt == 0) {
+            qr_fix_v(stage, rt);
+            __syncthreads();
+        }
+        double (*Vt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
+        double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * (kHB + 1));
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int aa = a0 + 16 * h;
+        for (int ks = 0; ks < kHB / 4; ++ks) {
+            const double b = Ct[4 * ks + q][cw + g];  // B[k][c] = C(row, col)
+#pragma unroll
+            for (int blk = 0; blk < 4; ++blk)
+                dmma884(acc[blk][0], acc[blk][1], Vt[4 * ks + q][8 * blk + g], b);  // A[a][k] = V(row, a)
+        }
+        __syncthreads();  // the stage is refilled two sub-tiles on
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int blk = 0; blk < 4; ++blk) {
+        const int aa = 8 * blk + g;
         if (aa >= nb) continue;
         double* out = Wp + ((size_t)rc * kHB + aa) * (size_t)nc;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int64_t col = c0 + cg + u;
-            if (col < nc) out[col] = h ? acc1[u] : acc0[u];
+        for (int u = 0; u < 2; ++u) {
+            const int64_t col = c0 + cw + 2 * q + u;
+            if (col < nc) out[col] = acc[blk][u];
         }
     }
     __syncthreads();
@@ -221,36 +268,49 @@ __global__ void __launch_bounds__(kQrThreads) qr_w_part_kernel(const double* A, 
 }
 
 // C -= V (T^T W) on one tile of 256 rows x 64 trailing columns, W the
-// fixed-order sum of the chunk partials; a thread: rows r0 and r0 + 16 of
-// each 32-row step x four consecutive columns.  Tiles holding the next
-// panel's columns (column tile 0) then write that panel's Gram partial
-// over their rows below the current panel (rows j0 + nb on).
+// fixed-order sum of the chunk partials.  The 32-row sub-tiles of V and C
+// stream through kQrStages shared-memory stages by asynchronous copies;
+// warp w: the 32 rows of a sub-tile x columns 8w..8w+7 as four m8n8 FP64
+// tensor-core tiles (C the accumulator, A = -V, B = T^T W).  Tiles holding
+// the next panel's columns (column tile 0) then write that panel's Gram
+// partial over their rows below the current panel (rows j0 + nb on),
+// again on the tensor cores.
 __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64_t j0, int nb,
                               int nchunks, const double* Wp, const double* T, int nb_next,
                               double* Gp_next, int ct, int rtile, double* sm) {
-    // W0 and Tt are dead once Wt = T^T W0 is formed; the row loop reuses
-    // their storage for the V and Gram tiles (its first barrier orders it).
     double (*W0)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm);
     double (*Wt)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm + kHB * kQrWs);
     double (*Tt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(sm + 2 * kHB * kQrWs);
-    double (*Vt)[kHB + 1] = Tt;
-    double (*Ct)[kQrWs] = W0;
+    double (*Gt)[kHB + 1] = Tt;  // the Gram tile reuses T's storage
+    double* stages = sm + 2 * kHB * kQrWs + kHB * (kHB + 1);
     const int t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5, g = lane >> 2, q = lane & 3;
+    const int cw = warp * 8;
     const int64_t nc = n - j0 - nb, krem = k - j0;
     const int64_t c0 = (int64_t)ct * kQrWc;
-    __syncthreads();  // a previous tile of this CTA may still read W0 / Tt
+    const int64_t r0 = (int64_t)rtile * kQrRowTile;
+    int64_t r1 = r0 + kQrRowTile;
+    if (r1 > krem) r1 = krem;
+    const int nsub = r1 > r0 ? (int)((r1 - r0 + kHB - 1) / kHB) : 0;
+    __syncthreads();  // a previous tile of this CTA may still read the buffers
+    // the first sub-tiles' copies fly while W and T^T W are formed
+#pragma unroll
+    for (int i = 0; i < kQrStages - 1; ++i) {
+        if (i < nsub) qr_issue_vc(A, ld, j0, nb, nc, c0, r0 + (int64_t)i * kHB, r1, stages + i * kQrStageDoubles);
+        else cp_async_commit();
+    }
     for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
         const int aa = e / kQrWc, c = e % kQrWc;
         const int64_t col = c0 + c;
         double part[kQrChunks];
 #pragma unroll
-        for (int q = 0; q < kQrChunks; ++q)
-            part[q] = (q < nchunks && aa < nb && col < nc)
-                          ? __ldcg(Wp + ((size_t)q * kHB + aa) * (size_t)nc + col)
-                          : 0.0;
+        for (int qq = 0; qq < kQrChunks; ++qq)
+            part[qq] = (qq < nchunks && aa < nb && col < nc)
+                           ? __ldcg(Wp + ((size_t)qq * kHB + aa) * (size_t)nc + col)
+                           : 0.0;
         double sum = 0.0;
 #pragma unroll
-        for (int q = 0; q < kQrChunks; ++q) sum += part[q];
+        for (int qq = 0; qq < kQrChunks; ++qq) sum += part[qq];
         W0[aa][c] = sum;
     }
     for (int e = t; e < kHB * kHB; e += kQrThreads) {
@@ -265,89 +325,72 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
         Wt[b][c] = sum;
     }
     const bool gram = Gp_next != nullptr && ct == 0;
-    const int rr0 = t & 15, cg = (t >> 4) * 4;
-    const int ga = t & 31, gb = (t >> 5) * 4;
-    double gacc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int64_t r0 = (int64_t)rtile * kQrRowTile;
-    int64_t r1 = r0 + kQrRowTile;
-    if (r1 > krem) r1 = krem;
-    // V of the next 32-row sub-tile and this thread's next 8 entries of C
-    // are loaded while the current sub-tile is updated.
-    constexpr int NV = kHB * kHB / kQrThreads;
-    double vpre[NV], cpre[8];
-    auto fetch = [&](int64_t rt) {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            const int e = t + i * kQrThreads, rr = e & 31, aa = e >> 5;
-            const int64_t row = rt + rr;
-            vpre[i] = (row < r1 && aa < nb) ? vref(A, ld, j0, row, aa) : 0.0;
+    // Gram tiles of warp w: rows 8 (w / 2) .., columns 8 (2 (w % 2) + {0, 1}) ..
+    const int gab = warp >> 1, gbb = 2 * (warp & 1);
+    double gacc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int i = 0; i < nsub; ++i) {
+        const int ni = i + kQrStages - 1;
+        if (ni < nsub)
+            qr_issue_vc(A, ld, j0, nb, nc, c0, r0 + (int64_t)ni * kHB, r1,
+                        stages + (ni % kQrStages) * kQrStageDoubles);
+        else
+            cp_async_commit();
+        cp_async_wait<kQrStages - 1>();
+        __syncthreads();  // sub-tile i of every thread; Wt (first pass); Gt free
+        double* stage = stages + (i % kQrStages) * kQrStageDoubles;
+        const int64_t rt = r0 + (int64_t)i * kHB;
+        if (rt == 0) {
+            qr_fix_v(stage, rt);
+            __syncthreads();
         }
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int64_t row = rt + rr0 + 16 * h, col = c0 + cg + u;
-                cpre[h * 4 + u] = (row < r1 && col < nc)
-                                      ? __ldcg(A + (size_t)(j0 + nb + col) * ld + j0 + row)
-                                      : 0.0;
-            }
-    };
-    if (r0 < r1) fetch(r0);
-    for (int64_t rt = r0; rt < r1; rt += kHB) {
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            const int e = t + i * kQrThreads;
-            Vt[e & 31][e >> 5] = vpre[i];
-        }
+        double (*Vt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
+        double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * (kHB + 1));
         double cur[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) cur[i] = cpre[i];
-        if (rt + kHB < r1) fetch(rt + kHB);
-        __syncthreads();
-        double s0[4] = {0.0, 0.0, 0.0, 0.0}, s1[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 4
-        for (int aa = 0; aa < kHB; ++aa) {
-            const double v0 = Vt[rr0][aa], v1 = Vt[rr0 + 16][aa];
-            const double2 wA = *reinterpret_cast<const double2*>(&Wt[aa][cg]);
-            const double2 wB = *reinterpret_cast<const double2*>(&Wt[aa][cg + 2]);
-            s0[0] += v0 * wA.x;
-            s0[1] += v0 * wA.y;
-            s0[2] += v0 * wB.x;
-            s0[3] += v0 * wB.y;
-            s1[0] += v1 * wA.x;
-            s1[1] += v1 * wA.y;
-            s1[2] += v1 * wB.x;
-            s1[3] += v1 * wB.y;
+        for (int blk = 0; blk < 4; ++blk) {
+            cur[2 * blk] = Ct[8 * blk + g][cw + 2 * q];
+            cur[2 * blk + 1] = Ct[8 * blk + g][cw + 2 * q + 1];
         }
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int rr = rr0 + 16 * h;
+        for (int ks = 0; ks < kHB / 4; ++ks) {
+            const double b = Wt[4 * ks + q][cw + g];  // B[a][c] = (T^T W)(a, col)
+#pragma unroll
+            for (int blk = 0; blk < 4; ++blk)
+                dmma884(cur[2 * blk], cur[2 * blk + 1], -Vt[8 * blk + g][4 * ks + q], b);  // A = -V
+        }
+#pragma unroll
+        for (int blk = 0; blk < 4; ++blk) {
+            const int rr = 8 * blk + g;
             const int64_t row = rt + rr;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int64_t col = c0 + cg + u;
-                double nv = 0.0;
-                if (row < r1 && col < nc) {
-                    nv = cur[h * 4 + u] - (h ? s1[u] : s0[u]);
-                    A[(size_t)(j0 + nb + col) * ld + j0 + row] = nv;
-                }
-                if (gram && cg + u < kHB) Ct[rr][cg + u] = (row >= nb && cg + u < nb_next) ? nv : 0.0;
+            for (int u = 0; u < 2; ++u) {
+                const int cl = cw + 2 * q + u;
+                const int64_t col = c0 + cl;
+                const bool in = row < r1 && col < nc;
+                if (in) A[(size_t)(j0 + nb + col) * ld + j0 + row] = cur[2 * blk + u];
+                if (gram && cl < kHB) Gt[rr][cl] = (in && row >= nb && cl < nb_next) ? cur[2 * blk + u] : 0.0;
             }
         }
         if (gram) {
             __syncthreads();
-            for (int q = 0; q < kHB; ++q) {
-                const double x = Ct[q][ga];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) gacc[u] += x * Ct[q][gb + u];
+            for (int ks = 0; ks < kHB / 4; ++ks) {
+                const double a = Gt[4 * ks + q][8 * gab + g];  // A[a][r] = C(r, a)
+#pragma unroll
+                for (int bb = 0; bb < 2; ++bb)
+                    dmma884(gacc[bb][0], gacc[bb][1], a, Gt[4 * ks + q][8 * (gbb + bb) + g]);
             }
         }
+        __syncthreads();  // the stage is refilled two sub-tiles on; Gt rewritten
     }
+    cp_async_wait<0>();
     if (gram) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-            Gp_next[(size_t)rtile * kHB * kHB + ga * kHB + gb + u] = gacc[u];
+        for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                Gp_next[(size_t)rtile * kHB * kHB + (8 * gab + g) * kHB + 8 * (gbb + bb) + 2 * q + u] =
+                    gacc[bb][u];
     }
     __syncthreads();
 }
@@ -435,7 +478,7 @@ __global__ void __launch_bounds__(kQrThreads, 1) qr_persist_kernel(QrPersistArgs
     for (int64_t j0 = 0; j0 < n; j0 += kQrNb) {
         const int nb = (int)(n - j0 < kQrNb ? n - j0 : kQrNb);
         const int64_t krem = k - j0;
-        int gp = (int)((krem + kQrRowTile - 1) / kQrRowTile);
+        int gp = (int)((krem + 63) / 64);
         if (gp > kQrPanelCtas) gp = kQrPanelCtas;
         if (gp > ncta) gp = ncta;
         if (gp < 1) gp = 1;
@@ -663,6 +706,10 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     }
     const size_t tile_smem = kQrTileSmemDoubles * sizeof(double);
     if (!done) {
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_w_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tile_smem));
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tile_smem));
     const int nb0 = (int)(n < kQrNb ? n : kQrNb);
     qr_gram_kernel<<<(unsigned)qr_row_tiles(k), kQrThreads, kHB * (kHB + 1) * sizeof(double), st>>>(
         SA, ld, k, nb0, q.Gp);
@@ -671,7 +718,7 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     for (int64_t j0 = 0; j0 < n; j0 += kQrNb) {
         const int nb = (int)(n - j0 < kQrNb ? n - j0 : kQrNb);
         const int64_t krem = k - j0;
-        int gp = (int)((krem + kQrRowTile - 1) / kQrRowTile);
+        int gp = (int)((krem + 63) / 64);
         if (gp > kQrPanelCtas) gp = kQrPanelCtas;
         if (gp < 1) gp = 1;
         HrArgs H;
