@@ -259,8 +259,9 @@ def run_ours(args):
     # roofline of the dominant kernel (the fused pass over the wh plane):
     # one profiled solve times every pass with CUDA events on its stream.
     gpu_solve.profile = True
-    _, prof_p = gpu_solve(tb, torch, Ap, b, s)
-    _, prof_f = gpu_solve(tb, torch, Af, b, s)
+    for _ in range(2):  # the second of each is kept
+        _, prof_p = gpu_solve(tb, torch, Ap, b, s)
+        _, prof_f = gpu_solve(tb, torch, Af, b, s)
     gpu_solve.profile = False
     peak, peak_kind = measured_peak()
     pass_ms = prof_p["iter_pass_ms"] / max(1, prof_p["iter_pass_count"])

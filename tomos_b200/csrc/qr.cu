@@ -573,41 +573,44 @@ __global__ void __launch_bounds__(32) qr_trtri_diag_kernel(const double* Rt, int
 // at n), X_IJ = -X_II R_IJ X_JJ, in two batched products
 //   mode 0:  T_p  = R_IJ X_JJ      (R from Rt, row-major)
 //   mode 1:  X_IJ = -X_II T_p
-// X_II and X_JJ come from the previous level.  64 x 64 output tiles,
-// k-steps of 16 through shared memory, 4 x 4 outputs per thread.
+// X_II and X_JJ come from the previous level.  32 x 32 output tiles (many
+// CTAs even at the widest level), k-steps of 32 through shared memory,
+// each warp two m8n8 FP64 tensor-core tiles.
 __global__ void __launch_bounds__(256) trtri_level_kernel(const double* Rt, int64_t n, double* X,
                                                           int64_t ldx, double* Tb, int64_t b,
                                                           int mode) {
-    __shared__ double As[16][64 + 1];
-    __shared__ double Bs[16][64 + 1];
+    __shared__ double As[32][32 + 1];  // [k][row]
+    __shared__ double Bs[32][32 + 1];  // [k][col]
     const int64_t p = blockIdx.z;
     const int64_t I0 = 2 * b * p, J0 = I0 + b;
     const int64_t Jn = n - J0 < b ? n - J0 : b;
     if (Jn <= 0) return;
     const int64_t M = b, N = Jn, K = mode == 0 ? Jn : b;
-    const int64_t row0 = (int64_t)blockIdx.y * 64, col0 = (int64_t)blockIdx.x * 64;
+    const int64_t row0 = (int64_t)blockIdx.y * 32, col0 = (int64_t)blockIdx.x * 32;
     if (row0 >= M || col0 >= N) return;
     double* T = Tb + (size_t)p * b * b;  // b x Jn, column-major, ld b
-    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    double acc[4][4] = {};
-    for (int64_t k0 = 0; k0 < K; k0 += 16) {
+    const int t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5, g = lane >> 2, q = lane & 3;
+    const int mb = warp >> 1, nb0 = 2 * (warp & 1);
+    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int64_t k0 = 0; k0 < K; k0 += 32) {
         __syncthreads();
-        for (int e = t; e < 64 * 16; e += 256) {
+        for (int e = t; e < 32 * 32; e += 256) {
             int i, kk;
             double v = 0.0;
             if (mode == 0) {  // R row-major: consecutive threads along k
-                i = e / 16;
-                kk = e % 16;
+                i = e >> 5;
+                kk = e & 31;
                 if (row0 + i < M && k0 + kk < K) v = Rt[(size_t)(I0 + row0 + i) * n + J0 + k0 + kk];
             } else {          // X column-major: consecutive threads along rows
-                i = e % 64;
-                kk = e / 64;
+                i = e & 31;
+                kk = e >> 5;
                 if (row0 + i < M && k0 + kk < K) v = X[(size_t)(I0 + k0 + kk) * ldx + I0 + row0 + i];
             }
             As[kk][i] = v;
         }
-        for (int e = t; e < 64 * 16; e += 256) {
-            const int kk = e % 16, j = e / 16;
+        for (int e = t; e < 32 * 32; e += 256) {
+            const int kk = e & 31, j = e >> 5;
             double v = 0.0;
             if (k0 + kk < K && col0 + j < N)
                 v = mode == 0 ? X[(size_t)(J0 + col0 + j) * ldx + J0 + k0 + kk]
@@ -616,29 +619,23 @@ __global__ void __launch_bounds__(256) trtri_level_kernel(const double* Rt, int6
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            double a[4], bb[4];
+        for (int ks = 0; ks < 8; ++ks) {
+            const double a = As[4 * ks + q][8 * mb + g];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                a[u] = As[kk][ty * 4 + u];
-                bb[u] = Bs[kk][tx * 4 + u];
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * bb[v];
+            for (int nn = 0; nn < 2; ++nn)
+                dmma884(acc[nn][0], acc[nn][1], a, Bs[4 * ks + q][8 * (nb0 + nn) + g]);
         }
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int nn = 0; nn < 2; ++nn)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int64_t i = row0 + ty * 4 + u, j = col0 + tx * 4 + v;
+        for (int u = 0; u < 2; ++u) {
+            const int64_t i = row0 + 8 * mb + g, j = col0 + 8 * (nb0 + nn) + 2 * q + u;
             if (i >= M || j >= N) continue;
             if (mode == 0)
-                T[(size_t)j * b + i] = acc[u][v];
+                T[(size_t)j * b + i] = acc[nn][u];
             else
-                X[(size_t)(J0 + j) * ldx + I0 + i] = -acc[u][v];
+                X[(size_t)(J0 + j) * ldx + I0 + i] = -acc[nn][u];
         }
 }
 
@@ -779,7 +776,7 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     TOMOS_LAUNCH_CHECK("qr_trtri_diag_kernel");
     for (int64_t b = 32; b < n; b *= 2) {
         const int64_t pairs = (n - b + 2 * b - 1) / (2 * b);
-        const dim3 g((unsigned)((b + 63) / 64), (unsigned)((b + 63) / 64), (unsigned)pairs);
+        const dim3 g((unsigned)((b + 31) / 32), (unsigned)((b + 31) / 32), (unsigned)pairs);
         trtri_level_kernel<<<g, 256, 0, st>>>(q.Rt, n, SA, ld, q.Tb, b, 0);
         TOMOS_LAUNCH_CHECK("trtri_level_kernel");
         trtri_level_kernel<<<g, 256, 0, st>>>(q.Rt, n, SA, ld, q.Tb, b, 1);
