@@ -732,8 +732,9 @@ static tomos_status enqueue_nside(tomos_workspace* ws, const NSide& S, cudaStrea
 }
 
 // HALF-tier iterations over a row-major FP32_16 A read a staged fp16 copy
-// of its wh plane (one conversion per solve, in the workspace); the
-// restart passes read A itself.
+// of its wh plane (one conversion per solve, in the workspace, or the
+// caller's staged_plane) -- on the tensor cores when n fits that pass.
+// The restart passes read A itself.
 struct DensePass : PassOps {
     tomos_workspace* ws;
     const tomos_dense* A;

@@ -41,9 +41,14 @@
 // (named barriers with arrive / sync halves), so the ut of one stage runs
 // beside the products of its neighbours.  The producer warp and the stage
 // ring are as in rowpass.cuh;
-// the ring is zeroed before the first copy, so rows past the CTA's range
-// and the columns past n that a 16-wide tile reads are finite (they meet a
-// zero of p or of ut).  Every mbarrier wait is bounded.
+// the ring is zeroed before the first copy.  The rows past the CTA's range
+// in its last stage hold stale values and are masked in the product-2
+// fragments (an infinity there would meet a zero ut).  The columns past n
+// that the last 16-wide tile of product 1 reads are the next row's first
+// values and meet zeros of p: only an infinite HALF-tier value there (an
+// element beyond the fp16 range, which makes the HALF-tier operator itself
+// non-finite) could turn the product into a NaN, so they are not masked
+// (masking cost 5% of the pass).  Every mbarrier wait is bounded.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -105,6 +110,12 @@ __device__ __forceinline__ void split_half(float x, int s, __half& hi, __half& l
     const float v = ldexpf(x, s);
     hi = __float2half_rn(v);
     lo = __float2half_rn((v - __half2float(hi)) * 2048.0f);
+}
+
+// Zeroes the fp16 halves of a fragment register whose index (column of
+// product 1, row of product 2) is not below `lim`.
+__device__ __forceinline__ uint32_t mask_pair(uint32_t v, int i0, int lim) {
+    return v & ((i0 < lim ? 0x0000FFFFu : 0u) | (i0 + 1 < lim ? 0xFFFF0000u : 0u));
 }
 
 template <int TPW>
@@ -300,7 +311,12 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
         uint32_t ph = 0;
         // product 2 of the stage before (its B2 from the ut warp), then
         // release that stage
-        auto product2 = [&](int tp, int sp_slot) {
+        // valid rows of stage tp (16 but in the CTA's last stage)
+        auto rows_of = [&](int tp) {
+            const int64_t left = r1 - (r0 + (int64_t)tp * kMmaRows);
+            return left < kMmaRows ? (int)left : kMmaRows;
+        };
+        auto product2 = [&](int tp, int sp_slot, int rv) {
             const int b = tp & 1;
             named_bar_sync(3 + b, kBar);
             const int de = e_move[b];
@@ -317,13 +333,29 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                 bb1 = *reinterpret_cast<const uint32_t*>(&ub[b][g][2 * tq + 8]);
             }
             const uint32_t st = ring + (uint32_t)(sp_slot * stage_bytes);
-            if (!failed) {
+            if (!failed && rv == kMmaRows) {
 #pragma unroll
                 for (int tt = 0; tt < TPW; ++tt) {
                     const int mt = warp * TPW + tt;
                     if (mt < ktiles) {
                         uint32_t a[4];
                         ldsm_x4_t(st + off2 + (uint32_t)(mt * 32), a);
+                        mma16816(d2[tt], a, bb0, bb1);
+                    }
+                }
+            } else if (!failed) {
+#pragma unroll
+                for (int tt = 0; tt < TPW; ++tt) {
+                    const int mt = warp * TPW + tt;
+                    if (mt < ktiles) {
+                        uint32_t a[4];
+                        ldsm_x4_t(st + off2 + (uint32_t)(mt * 32), a);
+                        // rows past the CTA's last row hold stale values (an
+                        // infinity among them would meet a zero ut)
+                        a[0] = mask_pair(a[0], 2 * tq, rv);
+                        a[1] = mask_pair(a[1], 2 * tq, rv);
+                        a[2] = mask_pair(a[2], 2 * tq + 8, rv);
+                        a[3] = mask_pair(a[3], 2 * tq + 8, rv);
                         mma16816(d2[tt], a, bb0, bb1);
                     }
                 }
@@ -362,14 +394,14 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                 red[t & 1][warp][g + 8] = make_float2(d1[2] + d1b[2], d1[3] + d1b[3]);
             }
             named_bar_arrive(1 + (t & 1), kBar);
-            if (t > 0) product2(t - 1, prev_slot);
+            if (t > 0) product2(t - 1, prev_slot, rows_of(t - 1));
             prev_slot = s;
             if (++s == nstage) {
                 s = 0;
                 ph ^= 1u;
             }
         }
-        if (ntiles > 0) product2(ntiles - 1, prev_slot);
+        if (ntiles > 0) product2(ntiles - 1, prev_slot, rows_of(ntiles - 1));
         // q partial: column g (+8) of each tile from lanes with tq == 0,
         // scaled by the ut warp's final exponent
         named_bar_sync(5, kBar);
