@@ -337,10 +337,10 @@ def run_ours(args):
                          "pass_ms_half": pass_ms, "pass_ms_fp32": pass_ms_f},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
-                         "kernel": "fused_rows_kernel<F16> (staged fp16 plane; one LSQR "
+                         "kernel": "fused_rows_mma_kernel (staged fp16 plane, tensor cores; one LSQR "
                                    "iteration's A p and A^T u)",
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "traffic": ncu_traffic("fused_pass_h16_1e6x1000")},
+                         "traffic": ncu_traffic("fused_pass_mma_f16_1e6x1000")},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
