@@ -90,3 +90,76 @@ def test_csr_lsqr_preconditioned(orc, numeric):
     eta = orc.backward_error_scaled(D, b, xx)
     assert rep["converged"] == 1 and eta <= 1.05e-6, (eta, rep)
     assert orc.backward_error(D, b, xx) <= eta * 1.01
+
+
+def ragged_csr(m, n, seed):
+    """Row lengths 0..96, 5% empty rows, eight rows of 300 entries (longer
+    than any lane group's first loads), the last 7 columns empty."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(0, 97, m)
+    lens[rng.random(m) < 0.05] = 0
+    lens[rng.choice(m, 8, replace=False)] = 300
+    rp = np.zeros(m + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(n - 7, k, replace=False)) for k in lens]).astype(np.int32)
+    v = (rng.standard_normal(rp[-1]) * 10.0 ** rng.uniform(-1, 1, rp[-1])).astype(np.float32)
+    return rp.astype(np.int32), ci, v
+
+
+def decoded_dense(orc, rp, ci, v, m, n, numeric, tier):
+    """The values a tier reads, scattered into a dense FP64 matrix."""
+    if numeric == NT.FP32:
+        vv = v.astype(np.float64)
+    else:
+        wh, wr = orc.fp32_16_split(v) if numeric == NT.FP32_16 else orc.fp32_bf16_split(v)
+        kind = "fp32_16" if numeric == NT.FP32_16 else "fp32_bf16"
+        vv = orc.decode(kind, wh, wr, "half" if tier == tb.Tier.HALF else "accurate").astype(np.float64)
+    D = np.zeros((m, n))
+    rows = np.repeat(np.arange(m), np.diff(rp))
+    D[rows, ci] = vv
+    return D
+
+
+@pytest.mark.parametrize("numeric,tier", [(NT.FP32, tb.Tier.AUTO), (NT.FP32_16, tb.Tier.HALF),
+                                          (NT.FP32_16, tb.Tier.ACCURATE)])
+def test_csr_ragged_products(orc, numeric, tier):
+    """Both products on ragged rows (empty, short and long) and empty columns."""
+    m, n = 5000, 700
+    rp, ci, v = ragged_csr(m, n, 3)
+    A = make(rp, ci, v, m, n, numeric)
+    Dd = decoded_dense(orc, rp, ci, v, m, n, numeric, tier)
+    rng = np.random.default_rng(4)
+    for trans, M in ((tb.NO_TRANSPOSE, Dd), (tb.TRANSPOSE, Dd.T)):
+        x = rng.standard_normal(M.shape[1]).astype(np.float32)
+        y0 = rng.standard_normal(M.shape[0]).astype(np.float32)
+        y = cuda(y0)
+        tb.mv_apply(tb.Device.CUDA, trans, 1.5, A, cuda(x), 0.5, y, tier=tier)
+        ref = 1.5 * (M @ x) + 0.5 * y0
+        scale = 1.5 * (np.abs(M) @ np.abs(x)) + 0.5 * np.abs(y0)
+        assert np.all(np.abs(y.cpu().numpy() - ref) <= 2e-5 * scale + 1e-30)
+
+
+@pytest.mark.parametrize("numeric,tier", [(NT.FP32, tb.Tier.AUTO), (NT.FP32_16, tb.Tier.HALF),
+                                          (NT.FP32_16, tb.Tier.ACCURATE)])
+def test_csr_ragged_lsqr_iterations(orc, numeric, tier):
+    """Six LSQR iterations over ragged CSR storage against the oracle's LSQR
+    on the values the tier reads (FP32 arithmetic in both, different
+    summation order); a second solve gives a bit-identical x."""
+    m, n = 5000, 700
+    rp, ci, v = ragged_csr(m, n, 5)
+    A = make(rp, ci, v, m, n, numeric)
+    Dd = decoded_dense(orc, rp, ci, v, m, n, numeric, tier)
+    b = np.random.default_rng(6).standard_normal(m).astype(np.float32)
+    x_ref, it_ref, h_ref = orc.lsqr_f32(Dd.astype(np.float32), b, None, 0.0, 6, 0.0, 1)
+    xs = []
+    for _ in range(2):
+        ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32)
+        x = torch.zeros(n, device="cuda")
+        rep = tb.lsqr_solve(None, A, cuda(b), x, ws, 0.0, 6, 0.0, tier=tier)
+        xs.append(x)
+    assert rep["iterations"] == it_ref == 6
+    np.testing.assert_allclose(rep["history"][:6], h_ref[:6], rtol=1e-4)
+    xx = xs[0].cpu().numpy()
+    assert np.linalg.norm(xx - x_ref) / np.linalg.norm(x_ref) < 1e-4
+    assert np.all(xx[n - 7:] == 0.0)
+    assert torch.equal(xs[0], xs[1])

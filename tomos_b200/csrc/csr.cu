@@ -17,6 +17,7 @@
 // and value arrays per iteration.
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "common.cuh"
 #include "gemv.cuh"
@@ -197,22 +198,492 @@ static int csr_grid(int64_t m) {
 
 static int64_t csr_qstride(int64_t n) { return ((n + 31) / 32) * 32 < 32 ? 32 : ((n + 31) / 32) * 32; }
 
-// Fused LSQR pass over CSR storage.
+// ------------------------------------------------------------------
+// The CSR LSQR pass as two gathers over a per-solve column-major copy.
+//
+// The fused row pass above keeps A^T ut deterministic with a private
+// accumulator per warp (n floats of shared memory each), which caps a
+// CTA at a few warps; a 20-nonzero row moves 120 bytes through a chain of
+// dependent loads, so only a few KB are in flight per SM where the memory
+// system needs tens.  The solver therefore runs each pass as two gathers:
+//   csr_rows_kernel: ut_i = cp (A p)_i + cu u_i with G lanes per row and
+//     two rows per lane group in flight, ||ut||^2 per CTA;
+//   csc_cols_kernel: q_j = sum_i A[i, j] ut_i over a column-major (CSC)
+//     copy of A, a warp per column, eight loads in flight per lane, ut
+//     gathered from L2.
+// Both sum in a fixed order.  The copy (row indices and both value planes,
+// permuted) is built once per solve by a stable counting sort: entries per
+// (row block, column), a scan over blocks and columns, then each row block
+// scatters its rows in order.  Entries whose column lies outside [0, n)
+// are skipped by every kernel here.
+
+constexpr int kCscBlocksPerSm = 8;
+constexpr int kRowsThreads = 256;
+
+__device__ __forceinline__ void csc_block_rows(int64_t m, int nb, int b, int64_t* r0, int64_t* r1) {
+    const int64_t per = (m + nb - 1) / nb;
+    *r0 = (int64_t)b * per;
+    if (*r0 > m) *r0 = m;
+    *r1 = *r0 + per < m ? *r0 + per : m;
+}
+
+// cnt[b * n + j] = entries of column j in row block b.
+__global__ void __launch_bounds__(256) csc_count_kernel(const int32_t* __restrict__ row_ptrs,
+                                                        const int32_t* __restrict__ col_idxs, int64_t m,
+                                                        int32_t n, int32_t* __restrict__ cnt) {
+    extern __shared__ int32_t ccount[];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) ccount[j] = 0;
+    __syncthreads();
+    int64_t r0, r1;
+    csc_block_rows(m, gridDim.x, blockIdx.x, &r0, &r1);
+    if (r0 < r1) {
+        const int32_t k1 = row_ptrs[r1];
+        for (int32_t k = row_ptrs[r0] + (int32_t)threadIdx.x; k < k1; k += blockDim.x) {
+            const int32_t c = __ldg(col_idxs + k);
+            if ((uint32_t)c < (uint32_t)n) atomicAdd(&ccount[c], 1);
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) cnt[(size_t)blockIdx.x * n + j] = ccount[j];
+}
+
+// cnt[b][j] := entries of column j in the blocks before b; tot[j] := all.
+// A CTA owns 32 columns; its 8 warps split the blocks into 8 runs.
+__global__ void __launch_bounds__(256) csc_block_scan_kernel(int32_t* __restrict__ cnt, int nb, int32_t n,
+                                                             int32_t* __restrict__ tot) {
+    __shared__ int32_t part[8][33];
+    const int jl = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int64_t j = (int64_t)blockIdx.x * 32 + jl;
+    const int per = (nb + 7) / 8;
+    const int b0 = g * per < nb ? g * per : nb;
+    const int b1 = b0 + per < nb ? b0 + per : nb;
+    int32_t s = 0;
+    if (j < n)
+        for (int b = b0; b < b1; ++b) s += cnt[(size_t)b * n + j];
+    part[g][jl] = s;
+    __syncthreads();
+    int32_t run = 0;
+    for (int h = 0; h < g; ++h) run += part[h][jl];
+    if (j < n) {
+        for (int b = b0; b < b1; ++b) {
+            const int32_t c = cnt[(size_t)b * n + j];
+            cnt[(size_t)b * n + j] = run;
+            run += c;
+        }
+        if (g == 7) tot[j] = run;
+    }
+}
+
+// col_ptr[0..n] = exclusive scan of tot (one CTA of 1024 threads).
+__global__ void __launch_bounds__(1024) csc_col_ptr_kernel(const int32_t* __restrict__ tot, int32_t n,
+                                                           int32_t* __restrict__ col_ptr) {
+    __shared__ int32_t wsum[32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int per = (n + 1023) / 1024;
+    const int j0 = t * per < n ? t * per : n;
+    const int j1 = j0 + per < n ? j0 + per : n;
+    int32_t s = 0;
+    for (int j = j0; j < j1; ++j) s += tot[j];
+    int32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const int32_t v = wsum[lane];
+        int32_t iv = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, iv, o);
+            if (lane >= o) iv += y;
+        }
+        wsum[lane] = iv - v;
+    }
+    __syncthreads();
+    int32_t run = wsum[w] + incl - s;
+    for (int j = j0; j < j1; ++j) {
+        col_ptr[j] = run;
+        run += tot[j];
+    }
+    if (t == 1023) col_ptr[n] = run;
+}
+
+// The CSC copy: one warp per row block walks its rows in order, so each
+// column keeps its entries in increasing row order.  Sixteen rows' first
+// 32 entries are loaded before any is placed.  VB: bytes of a value in the
+// first plane (4: FP32, 2: a packed wh plane); lo: the second 16-bit plane
+// or NULL.
+template <int VB>
+__global__ void __launch_bounds__(32) csc_scatter_kernel(const int32_t* __restrict__ row_ptrs,
+                                                         const int32_t* __restrict__ col_idxs,
+                                                         const void* __restrict__ hi,
+                                                         const uint16_t* __restrict__ lo, int64_t m,
+                                                         int32_t n, const int32_t* __restrict__ cnt,
+                                                         const int32_t* __restrict__ col_ptr,
+                                                         int32_t* __restrict__ rows_out,
+                                                         void* __restrict__ hi_out,
+                                                         uint16_t* __restrict__ lo_out) {
+    using V = typename std::conditional<VB == 4, uint32_t, uint16_t>::type;
+    extern __shared__ int32_t cur[];
+    const int lane = threadIdx.x;
+    for (int j = lane; j < n; j += 32) cur[j] = col_ptr[j] + cnt[(size_t)blockIdx.x * n + j];
+    __syncwarp();
+    const V* h = static_cast<const V*>(hi);
+    V* ho = static_cast<V*>(hi_out);
+    int64_t r0, r1;
+    csc_block_rows(m, gridDim.x, blockIdx.x, &r0, &r1);
+    constexpr int R = 16;
+    for (int64_t i0 = r0; i0 < r1; i0 += R) {
+        const int nr = r1 - i0 < R ? (int)(r1 - i0) : R;
+        const int32_t rp = lane <= nr ? __ldg(row_ptrs + i0 + lane) : 0;
+        int32_t c[R];
+        V hv[R];
+        uint16_t lv[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+            const int32_t k0 = __shfl_sync(0xffffffffu, rp, t), k1 = __shfl_sync(0xffffffffu, rp, t + 1);
+            const int32_t k = k0 + lane;
+            const bool ok = t < nr && k < k1;
+            c[t] = ok ? __ldg(col_idxs + k) : -1;
+            hv[t] = ok ? h[k] : (V)0;
+            lv[t] = (ok && lo) ? lo[k] : (uint16_t)0;
+        }
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+            const int32_t k0 = __shfl_sync(0xffffffffu, rp, t), k1 = __shfl_sync(0xffffffffu, rp, t + 1);
+            if ((uint32_t)c[t] < (uint32_t)n) {
+                const int32_t pos = atomicAdd(&cur[c[t]], 1);
+                rows_out[pos] = (int32_t)(i0 + t);
+                ho[pos] = hv[t];
+                if (lo) lo_out[pos] = lv[t];
+            }
+            if (t < nr && k1 - k0 > 32) {  // the rest of a long row
+                for (int32_t k = k0 + 32 + lane; k < k1; k += 32) {
+                    const int32_t cc = __ldg(col_idxs + k);
+                    if ((uint32_t)cc < (uint32_t)n) {
+                        const int32_t pos = atomicAdd(&cur[cc], 1);
+                        rows_out[pos] = (int32_t)(i0 + t);
+                        ho[pos] = h[k];
+                        if (lo) lo_out[pos] = lo[k];
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ut_i = cp (A p)_i + cu u_i for every row (u_out, when write_u) and
+// ||ut||^2 per CTA (sspart, when set).  2^lg lanes per row; a warp holds
+// two rounds of 32 >> lg rows.  Each lane sums its entries in order, then
+// the group sums by a fixed butterfly.
+template <Elem E, bool ACC64>
+__global__ void __launch_bounds__(kRowsThreads, 4) csr_rows_kernel(CsrPassParams P, int lg) {
+    if (P.skip && *P.skip) return;
+    using Dot = typename std::conditional<ACC64, double, float>::type;
+    __shared__ double ssw[kRowsThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int G = 1 << lg, sub = lane & (G - 1), grp = lane >> lg, rpw = 32 >> lg;
+    double cp = P.cp_h, cu = P.cu_h;
+    if (P.coef) {
+        cp = P.coef[0];
+        cu = P.coef[1];
+    }
+    const bool dot = cp != 0.0;
+    const uint32_t n = (uint32_t)P.n;
+    const int64_t step = (int64_t)gridDim.x * nw * 2 * rpw;
+    double ss = 0.0;
+    for (int64_t base = ((int64_t)blockIdx.x * nw + w) * 2 * rpw; base < P.m; base += step) {
+        const int64_t ia = base + grp, ib = base + rpw + grp;
+        int32_t ka0 = 0, ka1 = 0, kb0 = 0, kb1 = 0;
+        if (dot && ia < P.m) {
+            ka0 = __ldg(P.row_ptrs + ia);
+            ka1 = __ldg(P.row_ptrs + ia + 1);
+        }
+        if (dot && ib < P.m) {
+            kb0 = __ldg(P.row_ptrs + ib);
+            kb1 = __ldg(P.row_ptrs + ib + 1);
+        }
+        Dot da = 0, db = 0;
+        {
+            int32_t ca[4], cb[4];
+            float va[4], vb[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int32_t k = ka0 + sub + t * G;
+                ca[t] = k < ka1 ? __ldg(P.col_idxs + k) : -1;
+                va[t] = k < ka1 ? load_elem<E>(P.hi, P.lo, k) : 0.0f;
+                const int32_t kk = kb0 + sub + t * G;
+                cb[t] = kk < kb1 ? __ldg(P.col_idxs + kk) : -1;
+                vb[t] = kk < kb1 ? load_elem<E>(P.hi, P.lo, kk) : 0.0f;
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const float pa = (uint32_t)ca[t] < n ? __ldg(P.p + ca[t]) : 0.0f;
+                const float pb = (uint32_t)cb[t] < n ? __ldg(P.p + cb[t]) : 0.0f;
+                da += (Dot)va[t] * (Dot)pa;
+                db += (Dot)vb[t] * (Dot)pb;
+            }
+        }
+        for (int32_t k = ka0 + sub + 4 * G; k < ka1; k += G) {
+            const int32_t c = __ldg(P.col_idxs + k);
+            if ((uint32_t)c < n) da += (Dot)load_elem<E>(P.hi, P.lo, k) * (Dot)__ldg(P.p + c);
+        }
+        for (int32_t k = kb0 + sub + 4 * G; k < kb1; k += G) {
+            const int32_t c = __ldg(P.col_idxs + k);
+            if ((uint32_t)c < n) db += (Dot)load_elem<E>(P.hi, P.lo, k) * (Dot)__ldg(P.p + c);
+        }
+        for (int o = G >> 1; o > 0; o >>= 1) {
+            da += __shfl_xor_sync(0xffffffffu, da, o);
+            db += __shfl_xor_sync(0xffffffffu, db, o);
+        }
+        if (sub == 0) {
+            if (ia < P.m) {
+                const float uf = (float)(cp * (double)da + cu * (double)__ldg(P.u_in + ia));
+                if (P.write_u) P.u_out[ia] = uf;
+                ss += (double)uf * (double)uf;
+            }
+            if (ib < P.m) {
+                const float uf = (float)(cp * (double)db + cu * (double)__ldg(P.u_in + ib));
+                if (P.write_u) P.u_out[ib] = uf;
+                ss += (double)uf * (double)uf;
+            }
+        }
+    }
+    if (!P.sspart) return;
+    ss = warp_sum(ss);
+    if (lane == 0) ssw[w] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < nw; ++k) s += ssw[k];
+        P.sspart[blockIdx.x] = s;
+    }
+}
+
+// q_j = sum_i A[i, j] u_i over the CSC copy: a warp per column, each lane
+// summing its entries in order, then a fixed butterfly.
+template <Elem E, bool ACC64>
+__global__ void __launch_bounds__(256) csc_cols_kernel(const int32_t* __restrict__ col_ptr,
+                                                       const int32_t* __restrict__ rows, const void* hi,
+                                                       const void* lo, int64_t n,
+                                                       const float* __restrict__ u, const int* skip,
+                                                       float* __restrict__ q) {
+    if (skip && *skip) return;
+    using Dot = typename std::conditional<ACC64, double, float>::type;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int64_t W = (int64_t)gridDim.x * nw;
+    for (int64_t j = (int64_t)blockIdx.x * nw + (threadIdx.x >> 5); j < n; j += W) {
+        const int32_t k0 = __ldg(col_ptr + j), k1 = __ldg(col_ptr + j + 1);
+        Dot d = 0;
+        int32_t k = k0 + lane;
+        for (; k + 7 * 32 < k1; k += 8 * 32) {
+            int32_t r[8];
+            float v[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                r[t] = __ldg(rows + k + 32 * t);
+                v[t] = load_elem<E>(hi, lo, k + 32 * t);
+            }
+#pragma unroll
+            for (int t = 0; t < 8; ++t) d += (Dot)v[t] * (Dot)__ldg(u + r[t]);
+        }
+        for (; k < k1; k += 32) d += (Dot)load_elem<E>(hi, lo, k) * (Dot)__ldg(u + __ldg(rows + k));
+        d = warp_sum(d);
+        if (lane == 0) q[j] = (float)d;
+    }
+}
+
+// Lanes per row for the row gather: 4 loads per lane cover a row of
+// average length.
+static int csr_rows_lg(const tomos_csr* A) {
+    const double avg = A->rows > 0 ? (double)A->nnz / (double)A->rows : 0.0;
+    if (avg <= 16.0) return 2;
+    if (avg <= 32.0) return 3;
+    if (avg <= 64.0) return 4;
+    return 5;
+}
+
+static int csr_rows_grid(int64_t m, int lg, int cap) {
+    const int64_t rows_cta = (int64_t)(kRowsThreads / 32) * 2 * (32 >> lg);
+    int64_t g = (m + rows_cta - 1) / rows_cta;
+    if (g > cap) g = cap;
+    return (int)(g < 1 ? 1 : g);
+}
+
+template <Elem E, bool ACC64>
+static tomos_status launch_rows_t(const CsrPassParams& P, int lg, int grid, cudaStream_t st) {
+    csr_rows_kernel<E, ACC64><<<grid, kRowsThreads, 0, st>>>(P, lg);
+    TOMOS_LAUNCH_CHECK("csr_rows_kernel");
+    return TOMOS_OK;
+}
+
+static tomos_status launch_rows(Elem e, bool acc64, const CsrPassParams& P, int lg, int grid,
+                                cudaStream_t st) {
+    switch (e) {
+        case Elem::F32: return acc64 ? launch_rows_t<Elem::F32, true>(P, lg, grid, st)
+                                     : launch_rows_t<Elem::F32, false>(P, lg, grid, st);
+        case Elem::H16: return acc64 ? launch_rows_t<Elem::H16, true>(P, lg, grid, st)
+                                     : launch_rows_t<Elem::H16, false>(P, lg, grid, st);
+        case Elem::B16: return acc64 ? launch_rows_t<Elem::B16, true>(P, lg, grid, st)
+                                     : launch_rows_t<Elem::B16, false>(P, lg, grid, st);
+        case Elem::A16: return launch_rows_t<Elem::A16, true>(P, lg, grid, st);
+        case Elem::AB16: return launch_rows_t<Elem::AB16, true>(P, lg, grid, st);
+        case Elem::AB16R: return launch_rows_t<Elem::AB16R, true>(P, lg, grid, st);
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "csr: element type");
+    }
+}
+
+// The CSC copy of a CSR matrix inside one device buffer.
+struct CscCopy {
+    int32_t* col_ptr = nullptr;  // n + 1
+    int32_t* tot = nullptr;      // n
+    int32_t* cnt = nullptr;      // nb x n
+    int32_t* rows = nullptr;     // nnz
+    void* hi = nullptr;          // nnz x vb
+    uint16_t* lo = nullptr;      // nnz (packed storage with an exact tier), else NULL
+    int nb = 0;
+    size_t bytes = 0;
+};
+
+static size_t csc_align(size_t b) { return (b + 255) / 256 * 256; }
+
+static CscCopy csc_layout(void* base, const tomos_csr* A, bool with_lo) {
+    CscCopy c;
+    const int64_t n = A->cols, nnz = A->nnz;
+    int64_t nb = (int64_t)sm_count() * kCscBlocksPerSm;
+    if (nb > A->rows) nb = A->rows;
+    const int64_t cap = ((int64_t)64 << 20) / (n > 0 ? n : 1);
+    if (nb > cap) nb = cap;
+    if (nb < 1) nb = 1;
+    c.nb = (int)nb;
+    const int vb = A->numeric == TOMOS_FP32 ? 4 : 2;
+    char* p = static_cast<char*>(base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char* q = p ? p + off : nullptr;
+        off += csc_align(bytes);
+        return q;
+    };
+    c.col_ptr = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (n + 1)));
+    c.tot = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (n > 0 ? n : 1)));
+    c.cnt = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * nb * n));
+    c.rows = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * nnz));
+    c.hi = take((size_t)vb * nnz);
+    c.lo = with_lo ? reinterpret_cast<uint16_t*>(take(sizeof(uint16_t) * nnz)) : nullptr;
+    c.bytes = off;
+    return c;
+}
+
+// Builds the CSC copy (4 launches).
+static tomos_status csc_build(const tomos_csr* A, const CscCopy& c, const void* lo_in, cudaStream_t st) {
+    const int64_t m = A->rows;
+    const int32_t n = (int32_t)A->cols;
+    const int32_t* rp = static_cast<const int32_t*>(A->row_ptrs);
+    const int32_t* ci = static_cast<const int32_t*>(A->col_idxs);
+    const size_t smem = sizeof(int32_t) * (size_t)n;
+    if (smem > 48 * 1024) {
+        TOMOS_CUDA_TRY(cudaFuncSetAttribute(csc_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        TOMOS_CUDA_TRY(cudaFuncSetAttribute(csc_scatter_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        TOMOS_CUDA_TRY(cudaFuncSetAttribute(csc_scatter_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    csc_count_kernel<<<c.nb, 256, smem, st>>>(rp, ci, m, n, c.cnt);
+    TOMOS_LAUNCH_CHECK("csc_count_kernel");
+    csc_block_scan_kernel<<<(unsigned)((n + 31) / 32), 256, 0, st>>>(c.cnt, c.nb, n, c.tot);
+    TOMOS_LAUNCH_CHECK("csc_block_scan_kernel");
+    csc_col_ptr_kernel<<<1, 1024, 0, st>>>(c.tot, n, c.col_ptr);
+    TOMOS_LAUNCH_CHECK("csc_col_ptr_kernel");
+    const uint16_t* lo = c.lo ? static_cast<const uint16_t*>(lo_in) : nullptr;
+    if (A->numeric == TOMOS_FP32)
+        csc_scatter_kernel<4><<<c.nb, 32, smem, st>>>(rp, ci, A->values, nullptr, m, n, c.cnt, c.col_ptr,
+                                                       c.rows, c.hi, nullptr);
+    else
+        csc_scatter_kernel<2><<<c.nb, 32, smem, st>>>(rp, ci, A->values, lo, m, n, c.cnt, c.col_ptr,
+                                                       c.rows, c.hi, c.lo);
+    TOMOS_LAUNCH_CHECK("csc_scatter_kernel");
+    return TOMOS_OK;
+}
+
+template <Elem E, bool ACC64>
+static tomos_status launch_cols_t(const CscCopy& c, int64_t n, const float* u, const int* skip, float* q,
+                                  cudaStream_t st) {
+    int64_t grid = (n + 7) / 8;
+    const int64_t cap = (int64_t)sm_count() * 8;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    csc_cols_kernel<E, ACC64><<<(unsigned)grid, 256, 0, st>>>(c.col_ptr, c.rows, c.hi, c.lo, n, u, skip, q);
+    TOMOS_LAUNCH_CHECK("csc_cols_kernel");
+    return TOMOS_OK;
+}
+
+static tomos_status launch_cols(Elem e, bool acc64, const CscCopy& c, int64_t n, const float* u,
+                                const int* skip, float* q, cudaStream_t st) {
+    switch (e) {
+        case Elem::F32: return acc64 ? launch_cols_t<Elem::F32, true>(c, n, u, skip, q, st)
+                                     : launch_cols_t<Elem::F32, false>(c, n, u, skip, q, st);
+        case Elem::H16: return acc64 ? launch_cols_t<Elem::H16, true>(c, n, u, skip, q, st)
+                                     : launch_cols_t<Elem::H16, false>(c, n, u, skip, q, st);
+        case Elem::B16: return acc64 ? launch_cols_t<Elem::B16, true>(c, n, u, skip, q, st)
+                                     : launch_cols_t<Elem::B16, false>(c, n, u, skip, q, st);
+        case Elem::A16: return launch_cols_t<Elem::A16, true>(c, n, u, skip, q, st);
+        case Elem::AB16: return launch_cols_t<Elem::AB16, true>(c, n, u, skip, q, st);
+        case Elem::AB16R: return launch_cols_t<Elem::AB16R, true>(c, n, u, skip, q, st);
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "csr: element type");
+    }
+}
+
+// The CSR LSQR pass: the two gathers over the CSC copy, or the fused row
+// pass when the copy does not fit in device memory.
 struct CsrPass : PassOps {
     tomos_workspace* ws;
     const tomos_csr* A;
     Elem iter_e, init_e;
+    bool csc = false;
+    CscCopy cc;
+    int lg = 3;
     CsrPass(tomos_workspace* w, const tomos_csr* a, Elem ie, Elem ze) : ws(w), A(a), iter_e(ie), init_e(ze) {}
+    tomos_status prepare(cudaStream_t st) override {
+        const bool with_lo = A->numeric != TOMOS_FP32 && (elem_is_exact(iter_e) || elem_is_exact(init_e));
+        const CscCopy need = csc_layout(nullptr, A, with_lo);
+        if (need.bytes > ws->csc_bytes) {
+            if (ws->csc) cudaFree(ws->csc);
+            ws->csc = nullptr;
+            ws->csc_bytes = 0;
+            if (cudaMalloc(&ws->csc, need.bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return TOMOS_OK;  // not enough memory: the fused row pass
+            }
+            ws->csc_bytes = need.bytes;
+        }
+        cc = csc_layout(ws->csc, A, with_lo);
+        lg = csr_rows_lg(A);
+        tomos_status s = csc_build(A, cc, with_lo ? csr_lo(A) : nullptr, st);
+        if (s) return s;
+        ws->launches += 4;
+        csc = true;
+        return TOMOS_OK;
+    }
     PassPlan plan(bool init) override {
         PassPlan pl;
         pl.fused = true;
         pl.e = init ? init_e : iter_e;
         pl.acc64 = init || elem_is_exact(pl.e);
+        pl.qstride = ws->qstride;
+        if (csc) {
+            pl.grid = csr_rows_grid(A->rows, lg, ws->gmax);
+            pl.gq = 1;  // csc_cols_kernel writes A^T ut whole
+            pl.gs = pl.grid;
+            pl.nch = lg;
+            pl.g = 2;
+            return pl;
+        }
         pl.grid = csr_grid(A->rows);
         if (pl.grid > ws->gmax) pl.grid = ws->gmax;
         pl.gq = pl.grid;
         pl.gs = pl.grid;
-        pl.qstride = ws->qstride;
         pl.nch = csr_warps_for(A->cols);
         return pl;
     }
@@ -236,12 +707,19 @@ struct CsrPass : PassOps {
         P.sspart = ws->sspart;
         P.skip = skip;
         P.write_u = 1;
+        if (csc) {
+            tomos_status s = launch_rows(pl.e, pl.acc64, P, pl.nch, pl.grid, st);
+            if (s) return s;
+            ws->launches += 2;
+            return launch_cols(pl.e, pl.acc64, cc, A->cols, ws->u, skip, ws->qpart, st);
+        }
         ws->launches += 1;
         return launch_csr(pl.e, pl.acc64, P, pl.grid, pl.nch, st);
     }
     tomos_status fro2(double* out, const double* d, cudaStream_t st) override;
     uint64_t key() override {
-        return reinterpret_cast<uint64_t>(A->values) ^ (reinterpret_cast<uint64_t>(A->col_idxs) << 1);
+        return reinterpret_cast<uint64_t>(A->values) ^ (reinterpret_cast<uint64_t>(A->col_idxs) << 1) ^
+               (reinterpret_cast<uint64_t>(cc.rows) << 3) ^ (uint64_t)csc;
     }
     int64_t rows() override { return A->rows; }
     int64_t cols() override { return A->cols; }
@@ -434,7 +912,8 @@ tomos_status tomos_csr_gemv(int32_t trans, double alpha, const tomos_csr* A, int
             TOMOS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(float) * A->rows, st));
         }
         if (A->rows == 0) return TOMOS_OK;
-        return launch_csr(e, elem_is_exact(e), P, grid, 8, st);
+        const int lg = csr_rows_lg(A);
+        return launch_rows(e, elem_is_exact(e), P, lg, csr_rows_grid(A->rows, lg, sm_count() * 4), st);
     }
     const size_t need = (size_t)grid * P.qstride * sizeof(float);
     if (!scratch || scratch_bytes < need)

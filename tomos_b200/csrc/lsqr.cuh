@@ -149,6 +149,10 @@ struct tomos_workspace {
     // adjoint solve (adjoint.cu): FP64 n-vectors and its device state,
     // allocated by the first adjoint call.
     void* adj = nullptr;
+    // column-major copy of a CSR matrix for the CSR pass (csr.cu), rebuilt
+    // by every CSR solve and grown as needed.
+    void* csc = nullptr;
+    size_t csc_bytes = 0;
 
     bool has_precond = false;
     tomos_dense precond{};
