@@ -114,8 +114,11 @@ def test_qr_known_4x2():
     np.testing.assert_allclose(Rinv.T @ A.T @ A @ Rinv, np.eye(2), atol=1e-10)
 
 
-@pytest.mark.parametrize("k,n", [(64, 64), (97, 33), (700, 100), (4000, 1000)])
+@pytest.mark.parametrize("k,n", [(64, 64), (97, 33), (700, 100), (4000, 1000), (4001, 1777), (3000, 1537)])
 def test_qr_property_and_vs_lapack(k, n):
+    """From 1536 columns the QR is blocked (256-column blocks, the rest of
+    the matrix updated by FP64 tensor-core products); 1537 leaves a last
+    block of one column, 1777 a ragged one."""
     rng = np.random.default_rng(k + n)
     SA = rng.standard_normal((k, n)) * np.logspace(0, 4, n)
     Rinv, R = qr_on_gpu(SA)

@@ -21,10 +21,12 @@
 // R^{-1} is then formed recursively: 32 x 32 diagonal blocks by back
 // substitution, then levels of X_IJ = -X_II R_IJ X_JJ with doubling block
 // size, each two batched FP64 products.
+#include <cstdlib>
 #include <string>
 
 #include "common.cuh"
 #include "mbarrier.cuh"  // smem_addr
+#include "qr_gemm.cuh"
 #include "qr_panel.cuh"
 
 namespace tomos_b200 {
@@ -33,8 +35,9 @@ constexpr int kQrThreads = 256;
 constexpr int kQrNb = 32;        // panel width
 constexpr int kQrWc = 64;        // trailing columns per update tile
 constexpr int kQrChunks = 8;     // row chunks of the W partials
+constexpr int kQrMaxChunks = 32; // ... when few column tiles leave SMs idle (one-launch QR)
 constexpr int kQrRowTile = 256;  // rows per apply tile (and per Gram partial)
-constexpr int kQrPanelCtas = 64; // CTAs of the panel passes (~64 rows each)
+constexpr int kQrPanelCtas = 128; // CTAs of the panel passes (~64 rows each)
 
 struct QrScratch {
     double* tau;    // n
@@ -43,13 +46,37 @@ struct QrScratch {
     double* Gp;     // Gram partials of the next panel (k / 256 tiles)
     double* G2p;    // Gram partials of Q1 (kQrPanelCtas)
     double* Qs;     // Q1 of the current panel, k x 32 column-major
-    double* Wp;     // kQrChunks x 32 x n  (W partials)
+    double* Wp;     // kQrMaxChunks x 32 x n  (W partials)
+    double* Wr;     // 32 x n, their sum when there are more than kQrChunks
     double* Rt;     // n x n  (R transposed: row i of R contiguous)
     double* Tb;     // products of one level of the recursive inversion
     int* flag;      // [0] singular R, [1] panel fallback
     void* gsync;    // grid barrier of the one-launch QR
+    // blocked QR (n from kQrBlockedMinN): per block of kQrBlock columns
+    double* Tp;     // the panels' T factors, kQrBlock / 32 x 32 x 32
+    double* Vb;     // reflectors, k x kQrBlock
+    double* Z;      // V T, k x kQrBlock
+    double* Y;      // V^T V, kQrBlock x kQrBlock
+    double* Tb2;    // the block's T, kQrBlock x kQrBlock
+    double* Wb;     // Z^T C, kQrBlock x n
+    double* Pk;     // split-K partials, kGmaxSplits x kQrBlock x max(n, kQrBlock)
     size_t bytes;
 };
+
+// Columns from which the blocked QR is used (TOMOS_QR_BLOCKED=0 turns it
+// off, =1 uses it whenever there is more than one block).
+constexpr int64_t kQrBlockedMinN = 1536;
+
+static bool qr_blocked(int64_t n) {
+    static int mode = -1;
+    if (mode < 0) {
+        const char* e = std::getenv("TOMOS_QR_BLOCKED");
+        mode = e ? std::atoi(e) : 2;
+    }
+    if (mode == 0) return false;
+    if (mode == 1) return n > kQrBlock;
+    return n >= kQrBlockedMinN;
+}
 
 static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -72,7 +99,8 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
     q.Gp = reinterpret_cast<double*>(take(sizeof(double) * tiles * kHB * kHB));
     q.G2p = reinterpret_cast<double*>(take(sizeof(double) * kQrPanelCtas * kHB * kHB));
     q.Qs = reinterpret_cast<double*>(take(sizeof(double) * kk * kHB));
-    q.Wp = reinterpret_cast<double*>(take(sizeof(double) * kQrChunks * kHB * nn));
+    q.Wp = reinterpret_cast<double*>(take(sizeof(double) * kQrMaxChunks * kHB * nn));
+    q.Wr = reinterpret_cast<double*>(take(sizeof(double) * kHB * nn));
     q.Rt = reinterpret_cast<double*>(take(sizeof(double) * nn * nn));
     size_t tb = 1;  // the largest level of the recursive inversion
     for (int64_t b = 32; b < n; b *= 2) {
@@ -82,6 +110,17 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
     q.Tb = reinterpret_cast<double*>(take(sizeof(double) * tb));
     q.flag = reinterpret_cast<int*>(take(sizeof(int) * 4));
     q.gsync = take(64);
+    q.Tp = q.Vb = q.Z = q.Y = q.Tb2 = q.Wb = q.Pk = nullptr;
+    if (qr_blocked(n)) {
+        const size_t bb = kQrBlock, nw = nn > bb ? nn : bb;
+        q.Tp = reinterpret_cast<double*>(take(sizeof(double) * (bb / kHB) * kHB * kHB));
+        q.Vb = reinterpret_cast<double*>(take(sizeof(double) * kk * bb));
+        q.Z = reinterpret_cast<double*>(take(sizeof(double) * kk * bb));
+        q.Y = reinterpret_cast<double*>(take(sizeof(double) * bb * bb));
+        q.Tb2 = reinterpret_cast<double*>(take(sizeof(double) * bb * bb));
+        q.Wb = reinterpret_cast<double*>(take(sizeof(double) * bb * nn));
+        q.Pk = reinterpret_cast<double*>(take(sizeof(double) * kGmaxSplits * bb * nw));
+    }
     q.bytes = off;
     return q;
 }
@@ -457,9 +496,14 @@ __device__ bool grid_sync(GridSync* gs, unsigned int& gen, int* sflag) {
     return *sflag == 0;
 }
 
+// One launch factors columns [jb, je): panels of 32, the trailing update
+// restricted to the range.  Panel p's T goes to Tp + p * t_stride.
 struct QrPersistArgs {
     double* A;
     int64_t ld, k, n;
+    int64_t jb, je;
+    double* Tp;
+    int64_t t_stride;
     QrScratch q;
     GridSync* gs;
 };
@@ -469,14 +513,16 @@ __global__ void __launch_bounds__(kQrThreads, 1) qr_persist_kernel(QrPersistArgs
     __shared__ int sflag;
     unsigned int gen = 0;
     const int cta = blockIdx.x, ncta = gridDim.x;
-    const int64_t k = a.k, n = a.n;
-    const int nb0 = (int)(n < kQrNb ? n : kQrNb);
-    const int tiles0 = (int)qr_row_tiles(k);
-    for (int tl = cta; tl < tiles0; tl += ncta) qr_gram_tile(a.A, a.ld, k, nb0, tl, a.q.Gp, hsm);
+    const int64_t k = a.k, n = a.je;
+    const int nb0 = (int)(n - a.jb < kQrNb ? n - a.jb : kQrNb);
+    const int tiles0 = (int)qr_row_tiles(k - a.jb);
+    for (int tl = cta; tl < tiles0; tl += ncta)
+        qr_gram_tile(a.A + (size_t)a.jb * a.ld + a.jb, a.ld, k - a.jb, nb0, tl, a.q.Gp, hsm);
     if (!grid_sync(a.gs, gen, &sflag)) return;
     int ngp = tiles0;
-    for (int64_t j0 = 0; j0 < n; j0 += kQrNb) {
+    for (int64_t j0 = a.jb; j0 < n; j0 += kQrNb) {
         const int nb = (int)(n - j0 < kQrNb ? n - j0 : kQrNb);
+        double* Tpan = a.Tp + (size_t)((j0 - a.jb) / kQrNb) * a.t_stride;
         const int64_t krem = k - j0;
         int gp = (int)((krem + 63) / 64);
         if (gp > kQrPanelCtas) gp = kQrPanelCtas;
@@ -496,24 +542,42 @@ __global__ void __launch_bounds__(kQrThreads, 1) qr_persist_kernel(QrPersistArgs
         H.G2p = a.q.G2p;
         H.R1 = a.q.R1;
         H.fail = a.q.flag + 1;
-        H.T = a.q.T;
+        H.T = Tpan;
         H.tau = a.q.tau;
         if (cta < gp) hr_q1(H, cta, hsm);
         if (!grid_sync(a.gs, gen, &sflag)) return;
-        if (cta < gp) hr_v(H, cta, gp, hsm);
+        const int top = gp < ncta ? gp : 0;  // the top block beside the rows
+        if (cta < gp || cta == top) hr_v(H, cta, gp, top, hsm);
         if (!grid_sync(a.gs, gen, &sflag)) return;
         const int64_t nc = n - j0 - nb;
         if (nc <= 0) break;
-        const int64_t chunk_rows = ((krem + kQrChunks - 1) / kQrChunks + kHB - 1) / kHB * kHB;
-        const int nchunks = (int)((krem + chunk_rows - 1) / chunk_rows);
         const int ctiles = (int)((nc + kQrWc - 1) / kQrWc);
+        // row chunks: enough W-partial tiles for every CTA, up to kQrMaxChunks
+        int want = ncta / ctiles;
+        if (want < kQrChunks) want = kQrChunks;
+        if (want > kQrMaxChunks) want = kQrMaxChunks;
+        const int64_t chunk_rows = ((krem + want - 1) / want + kHB - 1) / kHB * kHB;
+        const int nchunks = (int)((krem + chunk_rows - 1) / chunk_rows);
         for (int tl = cta; tl < ctiles * nchunks; tl += ncta)
             qr_w_part_tile(a.A, a.ld, k, n, j0, nb, chunk_rows, a.q.Wp, tl % ctiles, tl / ctiles, hsm);
         if (!grid_sync(a.gs, gen, &sflag)) return;
+        const double* Wuse = a.q.Wp;
+        int nuse = nchunks;
+        if (nchunks > kQrChunks) {  // sum the partials once, in order
+            for (int64_t e = (int64_t)cta * kQrThreads + threadIdx.x; e < (int64_t)kHB * nc;
+                 e += (int64_t)ncta * kQrThreads) {
+                double sum = 0.0;
+                for (int c = 0; c < nchunks; ++c) sum += __ldcg(a.q.Wp + (size_t)c * kHB * nc + e);
+                a.q.Wr[e] = sum;
+            }
+            if (!grid_sync(a.gs, gen, &sflag)) return;
+            Wuse = a.q.Wr;
+            nuse = 1;
+        }
         const int nb_next = (int)(nc < kQrNb ? nc : kQrNb);
         const int rtiles = (int)qr_row_tiles(krem);
         for (int tl = cta; tl < ctiles * rtiles; tl += ncta)
-            qr_apply_tile(a.A, a.ld, k, n, j0, nb, nchunks, a.q.Wp, a.q.T, nb_next, a.q.Gp,
+            qr_apply_tile(a.A, a.ld, k, n, j0, nb, nuse, Wuse, Tpan, nb_next, a.q.Gp,
                           tl % ctiles, tl / ctiles, hsm);
         ngp = rtiles;
         if (!grid_sync(a.gs, gen, &sflag)) return;
@@ -639,6 +703,86 @@ __global__ void __launch_bounds__(256) trtri_level_kernel(const double* Rt, int6
         }
 }
 
+// op(A) B products of the blocked QR (qr_gemm.cuh); K is split over CTAs
+// (partials summed in order) when the tiles alone would leave SMs idle.
+template <bool KMAJOR>
+static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64_t ldb, double* D,
+                            int64_t ldd, int64_t M, int64_t N, int64_t K, double alpha, double beta,
+                            double* P, cudaStream_t st) {
+    if (M <= 0 || N <= 0) return TOMOS_OK;
+    const int64_t tm = (M + kGbm - 1) / kGbm, tn = (N + kGbn - 1) / kGbn;
+    int64_t splits = 1;
+    if (P) {
+        const int64_t target = 2 * (int64_t)sm_count();
+        splits = (target + tm * tn - 1) / (tm * tn);
+        const int64_t kmax = (K + 8 * kGbk - 1) / (8 * kGbk);
+        if (splits > kmax) splits = kmax;
+        if (splits > kGmaxSplits) splits = kGmaxSplits;
+        if (splits < 1) splits = 1;
+    }
+    int64_t kc = (K + splits - 1) / splits;
+    kc = (kc + kGbk - 1) / kGbk * kGbk;
+    if (kc < kGbk) kc = kGbk;
+    splits = (K + kc - 1) / kc;
+    if (splits < 1) splits = 1;
+    GemmArgs g;
+    g.A = A;
+    g.lda = lda;
+    g.B = B;
+    g.ldb = ldb;
+    g.D = D;
+    g.ldd = ldd;
+    g.P = P;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.kc = kc;
+    g.alpha = alpha;
+    g.beta = beta;
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_gemm_kernel<KMAJOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kGemmSmem));
+    qr_gemm_kernel<KMAJOR><<<dim3((unsigned)tm, (unsigned)tn, (unsigned)splits), 256, kGemmSmem, st>>>(g);
+    TOMOS_LAUNCH_CHECK("qr_gemm_kernel");
+    if (splits > 1) {
+        int64_t rb = (M * N + 255) / 256;
+        if (rb > 4096) rb = 4096;
+        qr_gemm_reduce_kernel<<<(unsigned)rb, 256, 0, st>>>(P, (int)splits, M, N, alpha, beta, D, ldd);
+        TOMOS_LAUNCH_CHECK("qr_gemm_reduce_kernel");
+    }
+    return TOMOS_OK;
+}
+
+// Columns [je, n) <- (I - V T^T V^T) [je, n) for the block [jb, je) just
+// factored: V^T V, the block's T (recursive inversion levels), Z = V T,
+// W = Z^T C, C -= V W.
+static tomos_status qr_block_update(double* SA, int64_t ld, int64_t k, int64_t n, int64_t jb, int64_t je,
+                                    const QrScratch& q, cudaStream_t st) {
+    const int64_t krem = k - jb, nc = n - je;
+    const int w = (int)(je - jb);
+    int64_t cb = (krem * w + 255) / 256;
+    if (cb > 4096) cb = 4096;
+    qr_copy_v_kernel<<<(unsigned)cb, 256, 0, st>>>(SA, ld, jb, krem, w, q.Vb, k);
+    TOMOS_LAUNCH_CHECK("qr_copy_v_kernel");
+    tomos_status s = qr_gemm<true>(q.Vb, k, q.Vb, k, q.Y, w, w, w, krem, 1.0, 0.0, q.Pk, st);
+    if (s) return s;
+    qr_block_t_init_kernel<<<(unsigned)((w * w + 255) / 256), 256, 0, st>>>(q.Tp, w, q.Tb2);
+    TOMOS_LAUNCH_CHECK("qr_block_t_init_kernel");
+    for (int64_t b = 32; b < w; b *= 2) {  // V^T V is symmetric: its storage is also row-major
+        const int64_t pairs = (w - b + 2 * b - 1) / (2 * b);
+        const dim3 g((unsigned)((b + 31) / 32), (unsigned)((b + 31) / 32), (unsigned)pairs);
+        trtri_level_kernel<<<g, 256, 0, st>>>(q.Y, w, q.Tb2, w, q.Tb, b, 0);
+        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
+        trtri_level_kernel<<<g, 256, 0, st>>>(q.Y, w, q.Tb2, w, q.Tb, b, 1);
+        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
+    }
+    s = qr_gemm<false>(q.Vb, k, q.Tb2, w, q.Z, k, krem, w, w, 1.0, 0.0, nullptr, st);
+    if (s) return s;
+    double* C = SA + (size_t)je * ld + jb;
+    s = qr_gemm<true>(q.Z, k, C, ld, q.Wb, w, w, nc, krem, 1.0, 0.0, q.Pk, st);
+    if (s) return s;
+    return qr_gemm<false>(q.Vb, k, q.Wb, w, C, ld, krem, nc, w, -1.0, 1.0, nullptr, st);
+}
+
 }  // namespace tomos_b200
 
 using namespace tomos_b200;
@@ -689,15 +833,31 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
             pa.n = n;
             pa.q = q;
             pa.gs = static_cast<GridSync*>(q.gsync);
-            TOMOS_CUDA_TRY(cudaMemsetAsync(q.gsync, 0, sizeof(GridSync), st));
-            void* args[] = {&pa};
-            cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr_persist_kernel,
-                                                        dim3((unsigned)sm_count()), dim3(kQrThreads),
-                                                        args, psmem, st);
-            if (e == cudaSuccess) {
-                done = true;
-            } else {
-                cudaGetLastError();  // fall back to the per-phase kernels
+            const bool blocked = q.Vb != nullptr;
+            const int64_t bw = blocked ? kQrBlock : n;
+            for (int64_t jb = 0; jb < n; jb += bw) {
+                const int64_t je = jb + bw < n ? jb + bw : n;
+                pa.jb = jb;
+                pa.je = je;
+                pa.Tp = blocked ? q.Tp : q.T;
+                pa.t_stride = blocked ? kHB * kHB : 0;
+                // counter and generation start at 0; the error word is
+                // cleared once, so an expired wait in any launch is reported
+                TOMOS_CUDA_TRY(cudaMemsetAsync(q.gsync, 0, jb == 0 ? sizeof(GridSync) : 2 * sizeof(unsigned int), st));
+                void* args[] = {&pa};
+                cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr_persist_kernel,
+                                                            dim3((unsigned)sm_count()), dim3(kQrThreads),
+                                                            args, psmem, st);
+                if (e != cudaSuccess) {
+                    cudaGetLastError();
+                    if (jb == 0) break;  // fall back to the per-phase kernels
+                    return cuda_fail(e, "sketch_qr: cooperative launch");
+                }
+                if (je == n) done = true;
+                if (je < n) {
+                    tomos_status bs = qr_block_update(SA, ld, k, n, jb, je, q, st);
+                    if (bs) return bs;
+                }
             }
         }
     }

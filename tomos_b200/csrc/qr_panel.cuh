@@ -44,25 +44,34 @@ typedef double HMat[kHB][kHB + 1];
 // small block products (X_IJ = -X_II R_IJ X_JJ).
 
 // G (symmetric, upper half read) = R^T R with R upper; G is overwritten.
-// Returns false if a pivot is not above `floor` (or not finite).
+// Returns false if a pivot is not above `floor` (or not finite).  Warp 0
+// runs the 32 right-looking steps (lane l owns column l; row j of R reaches
+// the other lanes by shuffles), the other warps wait at the end.
 __device__ __forceinline__ bool cta_chol(HMat& G, HMat& R, double floor, int* okf) {
     const int t = threadIdx.x;
-    if (t == 0) *okf = 1;
     for (int e = t; e < kHB * kHB; e += blockDim.x) R[e >> 5][e & 31] = 0.0;
-    for (int j = 0; j < kHB; ++j) {
-        __syncthreads();
-        if (t == 0) {
+    __syncthreads();
+    if (t < 32) {
+        const int l = t;
+        int ok = 1;
+        for (int j = 0; j < kHB; ++j) {
             const double d = G[j][j];
-            if (!(d > floor) || !isfinite(d)) *okf = 0;
-            R[j][j] = sqrt(d > floor && isfinite(d) ? d : 1.0);
+            const bool good = d > floor && isfinite(d);
+            if (!good) ok = 0;
+            const double rjj = sqrt(good ? d : 1.0);
+            if (l == j) R[j][j] = rjj;
+            double rjl = 0.0;
+            if (l > j) {
+                rjl = G[j][l] / rjj;
+                R[j][l] = rjl;
+            }
+            for (int i = j + 1; i < kHB; ++i) {
+                const double rji = __shfl_sync(0xffffffffu, rjl, i);
+                if (l >= i) G[i][l] -= rji * rjl;
+            }
+            __syncwarp();
         }
-        __syncthreads();
-        if (t > j && t < kHB) R[j][t] = G[j][t] / R[j][j];
-        __syncthreads();
-        for (int e = t; e < kHB * kHB; e += blockDim.x) {
-            const int i = e >> 5, l = e & 31;
-            if (i > j && l >= i) G[i][l] -= R[j][i] * R[j][l];
-        }
+        if (l == 0) *okf = ok;
     }
     __syncthreads();
     return *okf != 0;
@@ -134,27 +143,32 @@ __device__ __forceinline__ void cta_inv_unit_lower(const HMat& Q, HMat& Y, HMat&
 // +1, as dlarfg's copysign); L strictly below the diagonal, U on and
 // above it.  Step `keep` (if >= 0) is a reflector with nothing below its
 // diagonal, which dlarfg leaves as the identity (tau = 0, R_jj = alpha):
-// there s = +sign(pivot).
+// there s = +sign(pivot).  Warp 0 runs the 32 steps (lane l owns column
+// l; the multipliers of column i reach the other lanes by shuffles).
 __device__ __forceinline__ void cta_lu_signed(HMat& Q, double* sgn, int keep) {
-    const int t = threadIdx.x;
-    for (int i = 0; i < kHB; ++i) {
-        __syncthreads();
-        if (t == 0) {
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int l = threadIdx.x;
+        for (int i = 0; i < kHB; ++i) {
             const double q = Q[i][i];
             double si = q >= 0.0 ? -1.0 : 1.0;
             if (i == keep) si = -si;
-            Q[i][i] = q - si;
-            sgn[i] = si;
-        }
-        __syncthreads();
-        if (t > i && t < kHB) {
-            const double u = Q[i][i];
-            Q[t][i] = u != 0.0 ? Q[t][i] / u : 0.0;
-        }
-        __syncthreads();
-        for (int e = t; e < kHB * kHB; e += blockDim.x) {
-            const int r = e >> 5, c = e & 31;
-            if (r > i && c > i) Q[r][c] -= Q[r][i] * Q[i][c];
+            const double u = q - si;
+            if (l == i) {
+                Q[i][i] = u;
+                sgn[i] = si;
+            }
+            double lm = 0.0;
+            if (l > i) {
+                lm = u != 0.0 ? Q[l][i] / u : 0.0;
+                Q[l][i] = lm;
+            }
+            const double uil = Q[i][l];
+            for (int r = i + 1; r < kHB; ++r) {
+                const double lri = __shfl_sync(0xffffffffu, lm, r);
+                if (l > i) Q[r][l] -= lri * uil;
+            }
+            __syncwarp();
         }
     }
     __syncthreads();
@@ -200,25 +214,33 @@ __device__ __forceinline__ void hr_rows(const HrArgs& H, int cta, int64_t& r0, i
 }
 
 // Sums `np` 32 x 32 partials in order into G and pads it with the
-// identity outside the leading nb x nb block.
+// identity outside the leading nb x nb block.  blockDim.x == 256: four
+// entries a thread, 64 loads in flight.
 __device__ __forceinline__ void hr_reduce_gram(const double* part, int np, int nb, HMat& G) {
-    for (int e = threadIdx.x; e < kHB * kHB; e += blockDim.x) {
-        const int i = e >> 5, j = e & 31;
-        double s = 0.0;
-        if (i < nb && j < nb) {
-            // eight loads in flight, summed in partial order
-            for (int p0 = 0; p0 < np; p0 += 8) {
-                double v[8];
+    const int t = threadIdx.x;
+    bool in[4];
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    v[u] = p0 + u < np ? __ldcg(part + (size_t)(p0 + u) * kHB * kHB + e) : 0.0;
+    for (int c = 0; c < 4; ++c) {
+        const int e = t + 256 * c;
+        in[c] = (e >> 5) < nb && (e & 31) < nb;
+    }
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int p0 = 0; p0 < np; p0 += 16) {
+        double v[16][4];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) s += v[u];
-            }
-        } else {
-            s = (i == j) ? 1.0 : 0.0;
-        }
-        G[i][j] = s;
+        for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                v[u][c] = (p0 + u < np && in[c]) ? __ldcg(part + (size_t)(p0 + u) * kHB * kHB + t + 256 * c) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) s[c] += v[u][c];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int e = t + 256 * c, i = e >> 5, j = e & 31;
+        G[i][j] = in[c] ? s[c] : (i == j ? 1.0 : 0.0);
     }
     __syncthreads();
 }
@@ -415,9 +437,10 @@ __device__ void hr_fallback_panel(const HrArgs& H, HMat& Gram, HMat& Tm, double*
 }
 
 // Pass 2: R2, the reconstruction (every CTA of the pass), the top block,
-// T and tau (CTA 0) and V below the top block (each CTA its rows); `ncta`
-// CTAs ran pass 1 (its G2 partials).
-__device__ void hr_v(const HrArgs& H, int cta, int ncta, double* hsm) {
+// T and tau (CTA `top`) and V below the top block (each CTA its rows);
+// `ncta` CTAs ran pass 1 (its G2 partials).  A `top` CTA past them has no
+// rows and does only the top block, beside the others' rows.
+__device__ void hr_v(const HrArgs& H, int cta, int ncta, int top, double* hsm) {
     constexpr int MS = kHB * (kHB + 1);
     HMat& G = *reinterpret_cast<HMat*>(hsm);
     HMat& R2 = *reinterpret_cast<HMat*>(hsm + 1 * MS);
@@ -453,17 +476,20 @@ __device__ void hr_v(const HrArgs& H, int cta, int ncta, double* hsm) {
     // The last column of a square matrix has no rows below its diagonal.
     const int keep = (H.k - H.j0 == nb) ? nb - 1 : -1;
     cta_lu_signed(Qt, sgn, keep);
-    // U^-1: U is the upper part of Qt (diagonal included)
-    for (int e = t; e < kHB * kHB; e += blockDim.x) {
-        const int i = e >> 5, j = e & 31;
-        G[i][j] = i <= j ? Qt[i][j] : 0.0;
+    const bool rows = cta < ncta;
+    if (rows) {
+        // U^-1: U is the upper part of Qt (diagonal included)
+        for (int e = t; e < kHB * kHB; e += blockDim.x) {
+            const int i = e >> 5, j = e & 31;
+            G[i][j] = i <= j ? Qt[i][j] : 0.0;
+        }
+        __syncthreads();
+        cta_inv_upper(G, Ui, M);
+        cta_mul(X2, Ui, M);  // V2 = Q1_bot R2^-1 U^-1
+        __syncthreads();
     }
-    __syncthreads();
-    cta_inv_upper(G, Ui, M);
-    cta_mul(X2, Ui, M);  // V2 = Q1_bot R2^-1 U^-1
-    __syncthreads();
 
-    if (cta == 0) {
+    if (cta == top) {
         // Y = L^-1 into G; T = -U S Y^T; R = R2 R1 -> R_h = S R.
         cta_inv_unit_lower(Qt, G, X2);
         for (int e = t; e < kHB * kHB; e += blockDim.x) X2[e >> 5][e & 31] = __ldcg(H.R1 + e);
@@ -492,6 +518,7 @@ __device__ void hr_v(const HrArgs& H, int cta, int ncta, double* hsm) {
             H.A[(size_t)(H.j0 + j) * H.ld + H.j0 + i] = v;
         }
     }
+    if (!rows) return;
     // V2 rows: local rows >= nb of this CTA's block.
     int64_t r0, r1;
     hr_rows(H, cta, r0, r1);
@@ -539,7 +566,7 @@ __global__ void __launch_bounds__(256) qr_hr_q1_kernel(HrArgs H) {
 
 __global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
     extern __shared__ __align__(16) double hsm[];
-    hr_v(H, blockIdx.x, gridDim.x, hsm);
+    hr_v(H, blockIdx.x, gridDim.x, 0, hsm);
 }
 
 inline size_t hr_q1_smem() { return (4 * kHB * (kHB + 1) + kHB) * sizeof(double); }
