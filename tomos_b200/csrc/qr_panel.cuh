@@ -43,33 +43,32 @@ typedef double HMat[kHB][kHB + 1];
 // inverses double the solved block size 1 -> 2 -> ... -> 32, each level two
 // small block products (X_IJ = -X_II R_IJ X_JJ).
 
-// G (symmetric, upper half read) = R^T R with R upper; G is overwritten.
-// Returns false if a pivot is not above `floor` (or not finite).  Warp 0
-// runs the 32 right-looking steps (lane l owns column l; row j of R reaches
-// the other lanes by shuffles), the other warps wait at the end.
-__device__ __forceinline__ bool cta_chol(HMat& G, HMat& R, double floor, int* okf) {
+// G (symmetric, upper half read) = R^T R with R upper; G is left as it
+// was.  Returns false if a pivot is not above `floor` (or not finite).
+// Warp 0 runs the 32 right-looking steps on registers: lane l holds column
+// l of G, row j of R reaches the other lanes by shuffles (the other warps
+// wait at the end).
+__device__ __forceinline__ bool cta_chol(const HMat& G, HMat& R, double floor, int* okf) {
     const int t = threadIdx.x;
-    for (int e = t; e < kHB * kHB; e += blockDim.x) R[e >> 5][e & 31] = 0.0;
     __syncthreads();
     if (t < 32) {
         const int l = t;
+        double g[kHB];
+#pragma unroll
+        for (int i = 0; i < kHB; ++i) g[i] = G[i][l];
         int ok = 1;
+#pragma unroll
         for (int j = 0; j < kHB; ++j) {
-            const double d = G[j][j];
+            const double d = __shfl_sync(0xffffffffu, g[j], j);
             const bool good = d > floor && isfinite(d);
             if (!good) ok = 0;
             const double rjj = sqrt(good ? d : 1.0);
-            if (l == j) R[j][j] = rjj;
-            double rjl = 0.0;
-            if (l > j) {
-                rjl = G[j][l] / rjj;
-                R[j][l] = rjl;
-            }
-            for (int i = j + 1; i < kHB; ++i) {
-                const double rji = __shfl_sync(0xffffffffu, rjl, i);
-                if (l >= i) G[i][l] -= rji * rjl;
-            }
-            __syncwarp();
+            const double rjl = l > j ? g[j] / rjj : (l == j ? rjj : 0.0);
+            R[j][l] = rjl;
+            // G(i, l) -= R(j, i) R(j, l) for j < i <= l (entries below the
+            // diagonal of G are never read)
+#pragma unroll
+            for (int i = j + 1; i < kHB; ++i) g[i] -= __shfl_sync(0xffffffffu, rjl, i) * rjl;
         }
         if (l == 0) *okf = ok;
     }
@@ -143,33 +142,34 @@ __device__ __forceinline__ void cta_inv_unit_lower(const HMat& Q, HMat& Y, HMat&
 // +1, as dlarfg's copysign); L strictly below the diagonal, U on and
 // above it.  Step `keep` (if >= 0) is a reflector with nothing below its
 // diagonal, which dlarfg leaves as the identity (tau = 0, R_jj = alpha):
-// there s = +sign(pivot).  Warp 0 runs the 32 steps (lane l owns column
-// l; the multipliers of column i reach the other lanes by shuffles).
+// there s = +sign(pivot).  Warp 0 runs the 32 steps on registers: lane l
+// holds row l, row i of U reaches the other lanes by shuffles.
 __device__ __forceinline__ void cta_lu_signed(HMat& Q, double* sgn, int keep) {
     __syncthreads();
     if (threadIdx.x < 32) {
         const int l = threadIdx.x;
+        double q[kHB];
+#pragma unroll
+        for (int c = 0; c < kHB; ++c) q[c] = Q[l][c];
+#pragma unroll
         for (int i = 0; i < kHB; ++i) {
-            const double q = Q[i][i];
-            double si = q >= 0.0 ? -1.0 : 1.0;
+            const double qii = __shfl_sync(0xffffffffu, q[i], i);
+            double si = qii >= 0.0 ? -1.0 : 1.0;
             if (i == keep) si = -si;
-            const double u = q - si;
-            if (l == i) {
-                Q[i][i] = u;
-                sgn[i] = si;
+            const double u = qii - si;
+            if (l == 0) sgn[i] = si;
+            if (l == i) q[i] = u;
+            const bool below = l > i;
+            const double lm = below ? (u != 0.0 ? q[i] / u : 0.0) : 0.0;
+            if (below) q[i] = lm;
+#pragma unroll
+            for (int c = i + 1; c < kHB; ++c) {
+                const double uic = __shfl_sync(0xffffffffu, q[c], i);
+                if (below) q[c] -= lm * uic;
             }
-            double lm = 0.0;
-            if (l > i) {
-                lm = u != 0.0 ? Q[l][i] / u : 0.0;
-                Q[l][i] = lm;
-            }
-            const double uil = Q[i][l];
-            for (int r = i + 1; r < kHB; ++r) {
-                const double lri = __shfl_sync(0xffffffffu, lm, r);
-                if (l > i) Q[r][l] -= lri * uil;
-            }
-            __syncwarp();
         }
+#pragma unroll
+        for (int c = 0; c < kHB; ++c) Q[l][c] = q[c];
     }
     __syncthreads();
 }
