@@ -703,22 +703,30 @@ __global__ void __launch_bounds__(256) trtri_level_kernel(const double* Rt, int6
         }
 }
 
-// op(A) B products of the blocked QR (qr_gemm.cuh); K is split over CTAs
-// (partials summed in order) when the tiles alone would leave SMs idle.
+// op(A) B products of the blocked QR (qr_gemm.cuh).  With a partial
+// buffer P, K is split over CTAs (partials summed in order) by the count
+// that wastes the least of the last wave of resident CTAs (two per SM),
+// each split keeping at least 16 k-stages.  sub: D -= op(A) B.
 template <bool KMAJOR>
 static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64_t ldb, double* D,
                             int64_t ldd, int64_t M, int64_t N, int64_t K, double alpha, double beta,
-                            double* P, cudaStream_t st) {
+                            double* P, cudaStream_t st, int sub = 0) {
     if (M <= 0 || N <= 0) return TOMOS_OK;
     const int64_t tm = (M + kGbm - 1) / kGbm, tn = (N + kGbn - 1) / kGbn;
     int64_t splits = 1;
     if (P) {
-        const int64_t target = 2 * (int64_t)sm_count();
-        splits = (target + tm * tn - 1) / (tm * tn);
-        const int64_t kmax = (K + 8 * kGbk - 1) / (8 * kGbk);
-        if (splits > kmax) splits = kmax;
-        if (splits > kGmaxSplits) splits = kGmaxSplits;
-        if (splits < 1) splits = 1;
+        const int64_t slots = 2 * (int64_t)sm_count(), tiles = tm * tn;
+        int64_t kmax = K / (16 * kGbk);
+        if (kmax > kGmaxSplits) kmax = kGmaxSplits;
+        double best = -1.0;
+        for (int64_t s = 1; s <= kmax; ++s) {
+            const int64_t ctas = tiles * s, waves = (ctas + slots - 1) / slots;
+            const double eff = (double)ctas / (double)(waves * slots);
+            if (eff > best + 0.02) {  // more splits only for a clear gain
+                best = eff;
+                splits = s;
+            }
+        }
     }
     int64_t kc = (K + splits - 1) / splits;
     kc = (kc + kGbk - 1) / kGbk * kGbk;
@@ -739,6 +747,7 @@ static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64
     g.kc = kc;
     g.alpha = alpha;
     g.beta = beta;
+    g.sub = sub;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_gemm_kernel<KMAJOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kGemmSmem));
     qr_gemm_kernel<KMAJOR><<<dim3((unsigned)tm, (unsigned)tn, (unsigned)splits), 256, kGemmSmem, st>>>(g);
@@ -780,7 +789,7 @@ static tomos_status qr_block_update(double* SA, int64_t ld, int64_t k, int64_t n
     double* C = SA + (size_t)je * ld + jb;
     s = qr_gemm<true>(q.Z, k, C, ld, q.Wb, w, w, nc, krem, 1.0, 0.0, q.Pk, st);
     if (s) return s;
-    return qr_gemm<false>(q.Vb, k, q.Wb, w, C, ld, krem, nc, w, -1.0, 1.0, nullptr, st);
+    return qr_gemm<false>(q.Vb, k, q.Wb, w, C, ld, krem, nc, w, -1.0, 1.0, nullptr, st, 1);
 }
 
 }  // namespace tomos_b200

@@ -1,5 +1,5 @@
 // qr_gemm.cuh -- FP64 products of the blocked QR on the tensor cores
-// (mma.sync m8n8k4 f64), and the pieces that turn a block of panels into
+// (mma.sync m16n8k8 f64), and the pieces that turn a block of panels into
 // one compact-WY transform.
 //
 // A block of kQrBlock columns is factored panel by panel (32 columns, the
@@ -25,7 +25,7 @@ constexpr int kGbn = 64;          // GEMM CTA tile columns
 constexpr int kGbk = 16;          // k per stage
 constexpr int kGpad = 4;          // row padding (doubles) of the stage tiles
 constexpr int kGstages = 3;
-constexpr int kGmaxSplits = 8;
+constexpr int kGmaxSplits = 16;
 constexpr int kGa = kGbm * (kGbk + kGpad) > kGbk * (kGbm + kGpad) ? kGbm * (kGbk + kGpad)
                                                                  : kGbk * (kGbm + kGpad);
 constexpr int kGb = kGbn * (kGbk + kGpad);
@@ -42,19 +42,27 @@ template <int N>
 __device__ __forceinline__ void g_cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
-__device__ __forceinline__ void g_dmma884(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
+// D += A B for one m16n8k8 FP64 tile: with g = lane / 4, q = lane % 4,
+// a = A[g][q], A[g + 8][q], A[g][q + 4], A[g + 8][q + 4]; b = B[q][g],
+// B[q + 4][g]; d = D[g][2q], D[g][2q + 1], D[g + 8][2q], D[g + 8][2q + 1].
+__device__ __forceinline__ void g_dmma1688(double* d, const double* a, const double* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // D (M x N, column-major, ld ldd) = alpha * op(A) B + beta * D, B
 // column-major K x N.  KMAJOR: op(A) = A^T with A column-major K x M;
 // otherwise A is column-major M x K.  CTA tile 128 x 64, k-steps of 16
 // through kGstages shared-memory stages filled by 8-byte asynchronous
-// copies (zero-filled past the edges); 8 warps, each 32 x 32 = sixteen
-// m8n8 tiles.  Split-K: CTA z sums k in [z kc, (z + 1) kc); with gridDim.z
-// > 1 it writes its partial to P + z M N (ld M) for qr_gemm_reduce_kernel.
+// copies (zero-filled past the edges); 8 warps, each 32 x 32 = two by
+// four m16n8k8 tiles.  Split-K: CTA z sums k in [z kc, (z + 1) kc); with
+// gridDim.z > 1 it writes its partial to P + z M N (ld M) for
+// qr_gemm_reduce_kernel.  sub: D -= op(A) B instead (alpha and beta
+// unused): the accumulators start from the D tile, loaded while the first
+// stages are in flight, and A enters negated.
 struct GemmArgs {
     const double* A;
     int64_t lda;
@@ -65,6 +73,7 @@ struct GemmArgs {
     double* P;
     int64_t M, N, K, kc;
     double alpha, beta;
+    int sub;
 };
 
 template <bool KMAJOR>
@@ -106,16 +115,23 @@ __global__ void __launch_bounds__(256, 2) qr_gemm_kernel(GemmArgs g) {
         }
         g_cp_async_commit();
     };
-    double acc[4][4][2];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    double acc[2][4][4];
 #pragma unroll
     for (int s = 0; s < kGstages - 1; ++s) {
         if (s < nk) issue(s, kb + (int64_t)s * kGbk);
         else g_cp_async_commit();
     }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t row = m0 + wm + a * 16 + gq + 8 * (u >> 1);
+                const int64_t col = n0 + wn + b * 8 + 2 * qq + (u & 1);
+                acc[a][b][u] = (g.sub && row < g.M && col < g.N) ? g.D[row + col * g.ldd] : 0.0;
+            }
+    const double asg = g.sub ? -1.0 : 1.0;
     for (int i = 0; i < nk; ++i) {
         const int ni = i + kGstages - 1;
         if (ni < nk) issue(ni % kGstages, kb + (int64_t)ni * kGbk);
@@ -125,35 +141,42 @@ __global__ void __launch_bounds__(256, 2) qr_gemm_kernel(GemmArgs g) {
         const double* As = gsm + (i % kGstages) * kGstage;
         const double* Bs = As + kGa;
 #pragma unroll
-        for (int ks = 0; ks < kGbk / 4; ++ks) {
-            const int kk = ks * 4 + qq;
-            double a[4], b[4];
+        for (int ks = 0; ks < kGbk / 8; ++ks) {
+            double a[2][4], b[4][2];
 #pragma unroll
-            for (int im = 0; im < 4; ++im) {
-                const int row = wm + im * 8 + gq;
-                a[im] = KMAJOR ? As[row * (kGbk + kGpad) + kk] : As[kk * (kGbm + kGpad) + row];
-            }
+            for (int im = 0; im < 2; ++im)
 #pragma unroll
-            for (int in = 0; in < 4; ++in) b[in] = Bs[(wn + in * 8 + gq) * (kGbk + kGpad) + kk];
+                for (int u = 0; u < 4; ++u) {
+                    const int row = wm + im * 16 + gq + 8 * (u & 1), kk = ks * 8 + qq + 4 * (u >> 1);
+                    a[im][u] = asg * (KMAJOR ? As[row * (kGbk + kGpad) + kk] : As[kk * (kGbm + kGpad) + row]);
+                }
 #pragma unroll
-            for (int im = 0; im < 4; ++im)
+            for (int in = 0; in < 4; ++in)
 #pragma unroll
-                for (int in = 0; in < 4; ++in) g_dmma884(acc[im][in][0], acc[im][in][1], a[im], b[in]);
+                for (int u = 0; u < 2; ++u)
+                    b[in][u] = Bs[(wn + in * 8 + gq) * (kGbk + kGpad) + ks * 8 + qq + 4 * u];
+#pragma unroll
+            for (int im = 0; im < 2; ++im)
+#pragma unroll
+                for (int in = 0; in < 4; ++in) g_dmma1688(acc[im][in], a[im], b[in]);
         }
         __syncthreads();  // the stage is refilled kGstages - 1 steps on
     }
     g_cp_async_wait<0>();
     const bool split = gridDim.z > 1;
 #pragma unroll
-    for (int im = 0; im < 4; ++im)
+    for (int im = 0; im < 2; ++im)
 #pragma unroll
         for (int in = 0; in < 4; ++in)
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const int64_t row = m0 + wm + im * 8 + gq, col = n0 + wn + in * 8 + 2 * qq + u;
+            for (int u = 0; u < 4; ++u) {
+                const int64_t row = m0 + wm + im * 16 + gq + 8 * (u >> 1);
+                const int64_t col = n0 + wn + in * 8 + 2 * qq + (u & 1);
                 if (row >= g.M || col >= g.N) continue;
                 if (split) {
                     g.P[(size_t)blockIdx.z * g.M * g.N + row + col * g.M] = acc[im][in][u];
+                } else if (g.sub) {
+                    g.D[row + col * g.ldd] = acc[im][in][u];
                 } else {
                     double v = g.alpha * acc[im][in][u];
                     if (g.beta != 0.0) v += g.beta * g.D[row + col * g.ldd];
