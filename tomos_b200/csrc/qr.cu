@@ -37,6 +37,7 @@ constexpr int kQrWc = 64;        // trailing columns per update tile
 constexpr int kQrChunks = 8;     // row chunks of the W partials
 constexpr int kQrMaxChunks = 32; // ... when few column tiles leave SMs idle (one-launch QR)
 constexpr int kQrRowTile = 256;  // rows per apply tile (and per Gram partial)
+constexpr int kQrMinRowTile = 64; // ... halved down to this when tiles would leave CTAs idle
 constexpr int kQrPanelCtas = 128; // CTAs of the panel passes (~64 rows each)
 
 struct QrScratch {
@@ -92,7 +93,7 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
         return r;
     };
     const size_t nn = n > 0 ? (size_t)n : 1, kk = k > 0 ? (size_t)k : 1;
-    const size_t tiles = (size_t)qr_row_tiles(k > 0 ? k : 1);
+    const size_t tiles = (size_t)((k > 0 ? k : 1) + kQrMinRowTile - 1) / kQrMinRowTile;
     q.tau = reinterpret_cast<double*>(take(sizeof(double) * nn));
     q.T = reinterpret_cast<double*>(take(sizeof(double) * kHB * kHB));
     q.R1 = reinterpret_cast<double*>(take(sizeof(double) * kHB * kHB));
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(kQrThreads) qr_w_part_kernel(const double* A, 
 // again on the tensor cores.
 __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64_t j0, int nb,
                               int nchunks, const double* Wp, const double* T, int nb_next,
-                              double* Gp_next, int ct, int rtile, double* sm) {
+                              double* Gp_next, int ct, int rtile, int row_tile, double* sm) {
     double (*W0)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm);
     double (*Wt)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm + kHB * kQrWs);
     double (*Tt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(sm + 2 * kHB * kQrWs);
@@ -327,8 +328,8 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
     const int cw = warp * 8;
     const int64_t nc = n - j0 - nb, krem = k - j0;
     const int64_t c0 = (int64_t)ct * kQrWc;
-    const int64_t r0 = (int64_t)rtile * kQrRowTile;
-    int64_t r1 = r0 + kQrRowTile;
+    const int64_t r0 = (int64_t)rtile * row_tile;
+    int64_t r1 = r0 + row_tile;
     if (r1 > krem) r1 = krem;
     const int nsub = r1 > r0 ? (int)((r1 - r0 + kHB - 1) / kHB) : 0;
     __syncthreads();  // a previous tile of this CTA may still read the buffers
@@ -440,7 +441,8 @@ __global__ void __launch_bounds__(kQrThreads) qr_apply_kernel(double* A, int64_t
                                                               const double* T, int nb_next,
                                                               double* Gp_next) {
     extern __shared__ __align__(16) double qsm[];
-    qr_apply_tile(A, ld, k, n, j0, nb, nchunks, Wp, T, nb_next, Gp_next, blockIdx.x, blockIdx.y, qsm);
+    qr_apply_tile(A, ld, k, n, j0, nb, nchunks, Wp, T, nb_next, Gp_next, blockIdx.x, blockIdx.y,
+                  kQrRowTile, qsm);
 }
 
 // ------------------------------------------------------ one launch per QR
@@ -575,10 +577,14 @@ __global__ void __launch_bounds__(kQrThreads, 1) qr_persist_kernel(QrPersistArgs
             nuse = 1;
         }
         const int nb_next = (int)(nc < kQrNb ? nc : kQrNb);
-        const int rtiles = (int)qr_row_tiles(krem);
+        // apply tiles: rows halved from 256 (down to 64) while CTAs would idle
+        int row_tile = kQrRowTile;
+        while (row_tile > kQrMinRowTile && (int64_t)ctiles * ((krem + row_tile - 1) / row_tile) < ncta)
+            row_tile /= 2;
+        const int rtiles = (int)((krem + row_tile - 1) / row_tile);
         for (int tl = cta; tl < ctiles * rtiles; tl += ncta)
             qr_apply_tile(a.A, a.ld, k, n, j0, nb, nuse, Wuse, Tpan, nb_next, a.q.Gp,
-                          tl % ctiles, tl / ctiles, hsm);
+                          tl % ctiles, tl / ctiles, row_tile, hsm);
         ngp = rtiles;
         if (!grid_sync(a.gs, gen, &sflag)) return;
     }
