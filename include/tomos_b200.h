@@ -368,6 +368,44 @@ tomos_status tomos_lsqr_adjoint_grad_dense(const tomos_dense* A, int64_t K, cons
                                            int64_t ldgb, float* gradA, int64_t ldga,
                                            void* stream);
 
+/* ------------------------------------------------------------ MatrixMarket */
+
+/* Host-side MatrixMarket files: the reference reads its test systems with
+ * the NIST mmio routines (src/io/mmio.c) through read_mtx_host
+ * (benchmarks/solvers/cuda/lsqr_precision_runner.cu:101-125), an `array`
+ * file's values into an m x n column-major FP64 buffer.  These read the
+ * same files the same way (strtod per value) and also take `coordinate`
+ * files, the integer and pattern fields and symmetric / skew-symmetric
+ * storage (mirrored); complex and hermitian files are rejected. */
+enum tomos_mtx_format { TOMOS_MTX_ARRAY = 0, TOMOS_MTX_COORDINATE = 1 };
+enum tomos_mtx_field { TOMOS_MTX_REAL = 0, TOMOS_MTX_INTEGER = 1, TOMOS_MTX_PATTERN = 2 };
+enum tomos_mtx_symmetry { TOMOS_MTX_GENERAL = 0, TOMOS_MTX_SYMMETRIC = 1, TOMOS_MTX_SKEW = 2 };
+typedef struct tomos_mtx_info {
+    int64_t rows;
+    int64_t cols;
+    int64_t entries;   /* stored entries (coordinate: the nnz line; array:
+                          rows*cols or the stored triangle)              */
+    int32_t format;    /* enum tomos_mtx_format                         */
+    int32_t field;     /* enum tomos_mtx_field                          */
+    int32_t symmetry;  /* enum tomos_mtx_symmetry                       */
+    int32_t reserved;
+} tomos_mtx_info;
+/* mm_read_banner + mm_read_mtx_array_size / mm_read_mtx_crd_size. */
+tomos_status tomos_mtx_read_info(const char* path, tomos_mtx_info* info);
+/* The whole matrix into host memory `out` (FP64, layout COL_MAJOR as
+ * read_mtx_host, or ROW_MAJOR; leading dimension ld); coordinate entries
+ * that repeat a position add. */
+tomos_status tomos_mtx_read_dense(const char* path, int32_t layout, double* out, int64_t ld);
+/* The entries as 0-based triplets in file order, each mirrored entry of a
+ * symmetric file right after its stored one.  *count receives the number
+ * of triplets; more than cap is an error (call with cap = 0 to size). */
+tomos_status tomos_mtx_read_coo(const char* path, int64_t cap, int64_t* rows, int64_t* cols,
+                                double* vals, int64_t* count);
+/* An `array real general` file, column by column, 17 significant digits
+ * (the format generate_tall_thin_mtx.m writes). */
+tomos_status tomos_mtx_write_dense(const char* path, int32_t layout, int64_t rows, int64_t cols,
+                                   const double* a, int64_t ld);
+
 #ifdef __cplusplus
 }
 #endif

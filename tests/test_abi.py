@@ -35,7 +35,8 @@ def test_every_declared_symbol_is_exported():
 
 @pytest.mark.parametrize("struct,name", [(C.DenseDesc, "tomos_dense"), (C.CsrDesc, "tomos_csr"),
                                          (C.LsqrOpts, "tomos_lsqr_opts"),
-                                         (C.LsqrReport, "tomos_lsqr_report")])
+                                         (C.LsqrReport, "tomos_lsqr_report"),
+                                         (C.MtxInfo, "tomos_mtx_info")])
 def test_struct_layout_matches_header(struct, name):
     fields = [f for f, _ in struct._fields_]
     body = "".join(

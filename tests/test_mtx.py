@@ -1,0 +1,158 @@
+"""MatrixMarket files (tomos_mtx_*): the reference's read_mtx_host
+(benchmarks/solvers/cuda/lsqr_precision_runner.cu:101-125, over
+src/io/mmio.c) reads `array real general` files, one value per line
+column by column, as scripts/generate_tall_thin_mtx.m writes them
+(fprintf '%1.16e').  Checked bit for bit against Python's correctly rounded
+parsing and against scipy.io.mmread; the other formats against scipy."""
+import os
+
+import numpy as np
+import pytest
+import scipy.io
+import scipy.sparse
+
+import tomos_b200 as tb
+from tomos_b200 import _capi as C
+
+
+def write_text(path, text):
+    with open(path, "w") as f:
+        f.write(text)
+    return str(path)
+
+
+def matlab_style(path, A):
+    """The generator's format: banner, 'M N', '%1.16e' values column-major."""
+    m, n = A.shape
+    lines = ["%%MatrixMarket matrix array real general", f"{m} {n}"]
+    lines += ["%1.16e" % v for v in np.asarray(A, np.float64).ravel(order="F")]
+    return write_text(path, "\n".join(lines) + "\n")
+
+
+def test_generator_format_bit_exact(tmp_path):
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((37, 11)) * 10.0 ** rng.uniform(-8, 8, (37, 11))
+    A[0, 0], A[1, 0], A[2, 0] = -0.0, 1.0 / 3.0, 5e-324
+    p = matlab_style(tmp_path / "a.mtx", A)
+    got = tb.read_mtx(p)
+    want = np.array([float("%1.16e" % v) for v in A.ravel(order="F")]).reshape(A.shape, order="F")
+    assert got.flags["F_CONTIGUOUS"] and got.shape == A.shape
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+    assert np.array_equal(got, scipy.io.mmread(p))
+    info = tb.mtx_info(p)
+    assert info == {"rows": 37, "cols": 11, "entries": 37 * 11, "format": 0, "field": 0, "symmetry": 0}
+    rm = tb.read_mtx(p, tb.Layout.ROW_MAJOR)
+    assert rm.flags["C_CONTIGUOUS"] and np.array_equal(rm, got)
+
+
+def test_write_read_round_trip(tmp_path):
+    rng = np.random.default_rng(1)
+    A = rng.standard_normal((20, 7)) * 10.0 ** rng.uniform(-300, 300, (20, 7))
+    p = str(tmp_path / "w.mtx")
+    tb.write_mtx(p, A)
+    assert np.array_equal(tb.read_mtx(p).view(np.uint64), A.view(np.uint64))
+    assert np.array_equal(scipy.io.mmread(p), A)
+
+
+def test_coordinate_comments_and_repeats(tmp_path):
+    p = write_text(tmp_path / "c.mtx", """%%MatrixMarket matrix coordinate real general
+% a comment
+%another
+
+4 3 6
+1 1 1.5
+4 3 -2.25e-3
+2 2 7
+1 1 0.5
+3 1 1e10
+4 2 -0
+""")
+    want = scipy.io.mmread(p).toarray()
+    assert np.array_equal(tb.read_mtx(p), want)
+    r, c, v = tb.read_mtx_coo(p)
+    assert list(r) == [0, 3, 1, 0, 2, 3] and list(c) == [0, 2, 1, 0, 0, 1]
+    rp, ci, vals, size = tb.read_mtx_csr(p)
+    S = scipy.sparse.csr_matrix(scipy.io.mmread(p))
+    S.sum_duplicates()
+    S.sort_indices()
+    assert size == (4, 3)
+    assert np.array_equal(rp, S.indptr) and np.array_equal(ci, S.indices)
+    assert np.array_equal(vals, S.data)
+
+
+@pytest.mark.parametrize("text", [
+    "%%MatrixMarket matrix coordinate real symmetric\n3 3 4\n1 1 2\n2 1 -1\n3 2 4.5\n3 3 1\n",
+    "%%MatrixMarket matrix coordinate real skew-symmetric\n3 3 2\n2 1 -1\n3 2 4.5\n",
+    "%%MatrixMarket matrix coordinate integer general\n2 3 3\n1 3 7\n2 1 -4\n2 2 12\n",
+    "%%MatrixMarket matrix coordinate pattern general\n3 2 3\n1 1\n3 2\n2 2\n",
+    "%%MatrixMarket matrix array real symmetric\n3 3\n1\n2\n3\n4\n5\n6\n",
+    "%%MatrixMarket matrix array real skew-symmetric\n3 3\n-1\n2.5\n3\n",
+    "%%MatrixMarket matrix array integer general\n2 2\n1\n-2\n3\n4\n",
+    "%%MATRIXMARKET MATRIX Array REAL General\n1 2\n3\n4\n",
+])
+def test_formats_match_scipy(tmp_path, text):
+    text = text.replace("%%MATRIXMARKET", "%%MatrixMarket")
+    p = write_text(tmp_path / "f.mtx", text)
+    want = scipy.io.mmread(p, spmatrix=False)
+    want = want.toarray() if scipy.sparse.issparse(want) else np.asarray(want)
+    assert np.array_equal(tb.read_mtx(p), want.astype(np.float64))
+
+
+@pytest.mark.parametrize("text,code,msg", [
+    ("not a banner\n2 2\n1\n2\n3\n4\n", C.TOMOS_ERR_INVALID, "not a valid MatrixMarket file"),
+    ("%%MatrixMarket matrix array real general\n% only a comment\n", C.TOMOS_ERR_INVALID,
+     "could not read array size"),
+    ("%%MatrixMarket matrix array real general\n2 2\n1\n2\n3\n", C.TOMOS_ERR_INVALID,
+     "truncated/malformed data"),
+    ("%%MatrixMarket matrix array real general\n2 1\n1\nabc\n", C.TOMOS_ERR_INVALID,
+     "truncated/malformed data"),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1.0\n", C.TOMOS_ERR_INVALID,
+     "outside the matrix"),
+    ("%%MatrixMarket matrix coordinate complex general\n1 1 1\n1 1 1 0\n", C.TOMOS_ERR_UNSUPPORTED,
+     "not supported"),
+    ("%%MatrixMarket matrix array real hermitian\n1 1\n1\n", C.TOMOS_ERR_UNSUPPORTED, "not supported"),
+])
+def test_errors(tmp_path, text, code, msg):
+    p = write_text(tmp_path / "e.mtx", text)
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx(p)
+    assert e.value.code == code and msg in str(e.value)
+
+
+def test_missing_file_and_capacity(tmp_path):
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx(str(tmp_path / "nope.mtx"))
+    assert "could not open" in str(e.value)
+    p = write_text(tmp_path / "c.mtx", "%%MatrixMarket matrix coordinate real general\n2 2 2\n1 1 1\n2 2 2\n")
+    import ctypes
+    cnt = ctypes.c_int64(0)
+    rc = C.lib().tomos_mtx_read_coo(os.fsencode(p), 0, None, None, None, ctypes.byref(cnt))
+    assert rc == C.TOMOS_ERR_INVALID and cnt.value == 2  # cap 0 sizes the call
+
+
+@pytest.mark.gpu
+def test_solve_from_mtx_files(tmp_path, orc):
+    """An LSQR solve of a system read from .mtx files (dense and CSR)
+    matches the oracle's FP64 least-squares solution."""
+    import torch
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((3000, 60))
+    A[rng.random(A.shape) < 0.7] = 0.0
+    b = A @ rng.standard_normal(60) + 1e-8 * rng.standard_normal(3000)
+    pa = matlab_style(tmp_path / "A.mtx", A)
+    pb = matlab_style(tmp_path / "b.mtx", b[:, None])
+    Ah = tb.read_mtx(pa)
+    bh = tb.read_mtx(pb)[:, 0].astype(np.float32)
+    xo = orc.lstsq_f64(Ah.astype(np.float32).astype(np.float64), bh.astype(np.float64))
+    S = scipy.sparse.coo_matrix(Ah)
+    pc = str(tmp_path / "S.mtx")
+    scipy.io.mmwrite(pc, S, precision=17)
+    for M in (tb.dense_from_mtx(pa, tb.NumericType.FP32, tb.Layout.COL_MAJOR),
+              tb.dense_from_mtx(pa, tb.NumericType.FP32, tb.Layout.ROW_MAJOR),
+              tb.csr_from_mtx(pc, tb.NumericType.FP32)):
+        ws = tb.create_lsqr_workspace(None, (3000, 60), tb.NumericType.FP32)
+        x = torch.zeros(60, device="cuda")
+        rep = tb.lsqr_solve(None, M, torch.from_numpy(bh).cuda(), x, ws, 1e-6, 400, 1e-6)
+        assert rep["converged"] == 1
+        xx = x.cpu().numpy().astype(np.float64)
+        assert np.linalg.norm(xx - xo) / np.linalg.norm(xo) < 1e-4

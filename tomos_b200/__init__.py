@@ -10,6 +10,7 @@ libtomos_b200.so.  There is no CPU path: a CPU Context raises.
 """
 import ctypes
 import enum
+import os
 
 import torch
 
@@ -21,7 +22,8 @@ __all__ = [
     "Csr", "Workspace", "create_lsqr_workspace", "add_precond", "lsqr_solve", "mv_apply",
     "split_fp32_16", "combine_fp32_16", "split_fp32_bf16", "combine_fp32_bf16",
     "countsketch_hash", "apply_count_sketch", "generate_sketch_qr_precond", "backward_error",
-    "column_scale",
+    "column_scale", "mtx_info", "read_mtx", "read_mtx_coo", "read_mtx_csr", "write_mtx",
+    "dense_from_mtx", "csr_from_mtx",
     "TomosError", "CS_BUCKET_SEED", "CS_SIGN_SEED", "NO_TRANSPOSE", "TRANSPOSE",
 ]
 
@@ -222,6 +224,114 @@ class Csr:
         d.col_idxs = self.col_idxs.data_ptr()
         d.rounded = 1 if self.rounded else 0
         return d
+
+
+# ------------------------------------------------------------ MatrixMarket
+
+def _path(path):
+    return os.fsencode(path)
+
+
+def mtx_info(path):
+    """Banner and sizes of a MatrixMarket file (mm_read_banner +
+    mm_read_mtx_*_size, src/io/mmio.c): dict with rows, cols, entries,
+    format (0 array, 1 coordinate), field (0 real, 1 integer, 2 pattern),
+    symmetry (0 general, 1 symmetric, 2 skew-symmetric)."""
+    info = C.MtxInfo()
+    C.check(C.lib().tomos_mtx_read_info(_path(path), ctypes.byref(info)), "mtx_info")
+    return info.as_dict()
+
+
+def read_mtx(path, layout=None):
+    """The whole matrix as a host FP64 numpy array (column-major, as the
+    reference's read_mtx_host, lsqr_precision_runner.cu:101-125; Layout.
+    ROW_MAJOR gives a C-ordered array)."""
+    import numpy as np
+    info = mtx_info(path)
+    m, n = info["rows"], info["cols"]
+    layout = Layout.COL_MAJOR if layout is None else Layout(layout)
+    out = np.zeros((m, n), dtype=np.float64, order="F" if layout == Layout.COL_MAJOR else "C")
+    ld = max(1, m if layout == Layout.COL_MAJOR else n)
+    C.check(C.lib().tomos_mtx_read_dense(_path(path), int(layout), out.ctypes.data, ld), "read_mtx")
+    return out
+
+
+def read_mtx_coo(path):
+    """(rows, cols, values) 0-based numpy triplets in file order, symmetric
+    parts mirrored."""
+    import numpy as np
+    cnt = ctypes.c_int64(0)
+    info = mtx_info(path)
+    cap = info["entries"] * (2 if info["symmetry"] else 1)
+    r = np.empty(max(cap, 1), np.int64)
+    c = np.empty(max(cap, 1), np.int64)
+    v = np.empty(max(cap, 1), np.float64)
+    C.check(C.lib().tomos_mtx_read_coo(_path(path), cap, r.ctypes.data, c.ctypes.data, v.ctypes.data,
+                                       ctypes.byref(cnt)), "read_mtx_coo")
+    k = cnt.value
+    return r[:k], c[:k], v[:k]
+
+
+def read_mtx_csr(path):
+    """(row_ptrs int32, col_idxs int32, values FP64, (m, n)) on the host:
+    rows in order, columns increasing within a row, repeated positions
+    summed."""
+    import numpy as np
+    info = mtx_info(path)
+    m, n = info["rows"], info["cols"]
+    r, c, v = read_mtx_coo(path)
+    key = r * max(n, 1) + c
+    order = np.argsort(key, kind="stable")
+    key, v = key[order], v[order]
+    first = np.ones(key.size, bool)
+    first[1:] = key[1:] != key[:-1]
+    starts = np.flatnonzero(first)
+    vals = np.add.reduceat(v, starts) if key.size else v
+    ukey = key[starts]
+    rows, cols = ukey // max(n, 1), ukey % max(n, 1)
+    rp = np.zeros(m + 1, np.int64)
+    np.add.at(rp, rows + 1, 1)
+    rp = np.cumsum(rp)
+    return rp.astype(np.int32), cols.astype(np.int32), vals, (m, n)
+
+
+def write_mtx(path, a, layout=None):
+    """Writes a 2-D array as `array real general` (17 significant digits,
+    column by column)."""
+    import numpy as np
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim != 2:
+        raise TomosError(C.TOMOS_ERR_INVALID, "write_mtx: a 2-D array")
+    af = np.asfortranarray(a)
+    C.check(C.lib().tomos_mtx_write_dense(_path(path), int(Layout.COL_MAJOR), a.shape[0], a.shape[1],
+                                          af.ctypes.data, max(1, a.shape[0])), "write_mtx")
+
+
+def dense_from_mtx(path, store_type=NumericType.FP32, layout=Layout.COL_MAJOR):
+    """A device Dense (FP32 or FP64, packed types through pack()) from a
+    MatrixMarket file, values rounded from FP64 as the reference's
+    fill_dense_from_host does."""
+    st = NumericType(store_type)
+    base = NumericType.FP64 if st == NumericType.FP64 else NumericType.FP32
+    host = read_mtx(path, layout)
+    dt = torch.float64 if base == NumericType.FP64 else torch.float32
+    t = torch.from_numpy(host).to(dt)
+    if Layout(layout) == Layout.COL_MAJOR:
+        t = t.t().contiguous().t()
+    D = Dense.from_tensor(t.cuda(), layout, base)
+    return D if st == base else pack(D, st)
+
+
+def csr_from_mtx(path, store_type=NumericType.FP32):
+    """A device Csr (int32 indices; FP32 values, or packed FP32_16 /
+    FP32_BF16) from a MatrixMarket file."""
+    import numpy as np
+    rp, ci, v, size = read_mtx_csr(path)
+    st = NumericType(store_type)
+    vals = torch.from_numpy(v.astype(np.float32)).cuda()
+    if st != NumericType.FP32:
+        vals = pack(Dense.from_tensor(vals[None, :], Layout.ROW_MAJOR), st).storage
+    return Csr(st, size, torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), vals)
 
 
 # ------------------------------------------------------------------ packing

@@ -62,8 +62,20 @@ class LsqrReport(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class MtxInfo(ctypes.Structure):
+    _fields_ = [("rows", c_i64), ("cols", c_i64), ("entries", c_i64), ("format", c_i32),
+                ("field", c_i32), ("symmetry", c_i32), ("reserved", c_i32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 # Every symbol the header declares, with (restype, argtypes).
 SIGNATURES = {
+    "tomos_mtx_read_info": (c_i32, [ctypes.c_char_p, ctypes.POINTER(MtxInfo)]),
+    "tomos_mtx_read_dense": (c_i32, [ctypes.c_char_p, c_i32, c_vp, c_i64]),
+    "tomos_mtx_read_coo": (c_i32, [ctypes.c_char_p, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_i64)]),
+    "tomos_mtx_write_dense": (c_i32, [ctypes.c_char_p, c_i32, c_i64, c_i64, c_vp, c_i64]),
     "tomos_last_error": (ctypes.c_char_p, []),
     "tomos_version": (ctypes.c_char_p, []),
     "tomos_sync": (c_i32, [c_vp]),

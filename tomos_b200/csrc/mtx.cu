@@ -1,0 +1,247 @@
+// mtx.cu -- MatrixMarket files on the host (tomos_mtx_*).
+//
+// The reference reads its matrices (the tall-thin test systems its MATLAB
+// generator writes, scripts/generate_tall_thin_mtx.m) with the NIST mmio
+// routines (src/io/mmio.c: mm_read_banner, mm_read_mtx_array_size,
+// mm_read_mtx_crd_size) through read_mtx_host
+// (benchmarks/solvers/cuda/lsqr_precision_runner.cu:101-125): an `array`
+// file's values fill an m x n column-major FP64 buffer, one fscanf("%lf")
+// per value.  Here the same files are read with the same number parsing
+// (strtod), plus what the runner leaves out: `coordinate` files (1-based
+// triplets), the `integer` and `pattern` fields, and symmetric /
+// skew-symmetric storage (the stored lower triangle mirrored).  Complex and
+// hermitian files are rejected, as the LSQR path has no complex type.
+// Errors use the runner's wording ("could not open", "not a valid
+// MatrixMarket file", "could not read array size", "truncated/malformed
+// data").
+#include <cctype>
+#include <cerrno>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "tomos_b200.h"
+
+namespace {
+
+struct MtxFile {
+    FILE* f = nullptr;
+    tomos_mtx_info info{};
+    ~MtxFile() {
+        if (f) std::fclose(f);
+    }
+};
+
+std::string lower(const char* s) {
+    std::string r(s);
+    for (char& c : r) c = (char)std::tolower((unsigned char)c);
+    return r;
+}
+
+// Reads one line (without the newline) into buf; false at end of file.
+bool read_line(FILE* f, std::string& buf) {
+    buf.clear();
+    int c;
+    bool any = false;
+    while ((c = std::fgetc(f)) != EOF) {
+        any = true;
+        if (c == '\n') break;
+        buf.push_back((char)c);
+    }
+    if (!buf.empty() && buf.back() == '\r') buf.pop_back();
+    return any;
+}
+
+bool blank(const std::string& s) {
+    for (char c : s)
+        if (!std::isspace((unsigned char)c)) return false;
+    return true;
+}
+
+// Opens the file, parses the banner and the size line; `f` is then at the
+// first value.
+tomos_status mtx_open(const char* path, MtxFile& m) {
+    using tomos_b200::fail;
+    const std::string p = path ? path : "";
+    m.f = path ? std::fopen(path, "r") : nullptr;
+    if (!m.f) return fail(TOMOS_ERR_INVALID, "could not open '" + p + "'");
+    std::string line;
+    char banner[64] = {0}, object[64] = {0}, format[64] = {0}, field[64] = {0}, sym[64] = {0};
+    if (!read_line(m.f, line) ||
+        std::sscanf(line.c_str(), "%63s %63s %63s %63s %63s", banner, object, format, field, sym) != 5 ||
+        std::strcmp(banner, "%%MatrixMarket") != 0 || lower(object) != "matrix")
+        return fail(TOMOS_ERR_INVALID, "'" + p + "': not a valid MatrixMarket file");
+    const std::string fmt = lower(format), fld = lower(field), sy = lower(sym);
+    tomos_mtx_info& in = m.info;
+    if (fmt == "array") in.format = TOMOS_MTX_ARRAY;
+    else if (fmt == "coordinate") in.format = TOMOS_MTX_COORDINATE;
+    else return fail(TOMOS_ERR_INVALID, "'" + p + "': not a valid MatrixMarket file");
+    if (fld == "real" || fld == "double") in.field = TOMOS_MTX_REAL;
+    else if (fld == "integer") in.field = TOMOS_MTX_INTEGER;
+    else if (fld == "pattern" && in.format == TOMOS_MTX_COORDINATE) in.field = TOMOS_MTX_PATTERN;
+    else return fail(TOMOS_ERR_UNSUPPORTED, "'" + p + "': field '" + fld + "' is not supported (real, integer, pattern)");
+    if (sy == "general") in.symmetry = TOMOS_MTX_GENERAL;
+    else if (sy == "symmetric") in.symmetry = TOMOS_MTX_SYMMETRIC;
+    else if (sy == "skew-symmetric") in.symmetry = TOMOS_MTX_SKEW;
+    else return fail(TOMOS_ERR_UNSUPPORTED, "'" + p + "': symmetry '" + sy + "' is not supported");
+    // comments, then the size line
+    do {
+        if (!read_line(m.f, line)) return fail(TOMOS_ERR_INVALID, "'" + p + "': could not read array size");
+    } while (line.empty() || line[0] == '%' || blank(line));
+    long long r = -1, c = -1, z = -1;
+    const int got = std::sscanf(line.c_str(), "%lld %lld %lld", &r, &c, &z);
+    if ((in.format == TOMOS_MTX_ARRAY && got < 2) || (in.format == TOMOS_MTX_COORDINATE && got < 3) || r < 0 ||
+        c < 0 || (in.format == TOMOS_MTX_COORDINATE && z < 0))
+        return fail(TOMOS_ERR_INVALID, "'" + p + "': could not read array size");
+    if (in.symmetry != TOMOS_MTX_GENERAL && r != c)
+        return fail(TOMOS_ERR_INVALID, "'" + p + "': a symmetric matrix must be square");
+    in.rows = r;
+    in.cols = c;
+    if (in.format == TOMOS_MTX_COORDINATE) {
+        in.entries = z;
+    } else if (in.symmetry == TOMOS_MTX_SYMMETRIC) {
+        in.entries = r * (r + 1) / 2;
+    } else if (in.symmetry == TOMOS_MTX_SKEW) {
+        in.entries = r * (r - 1) / 2;
+    } else {
+        in.entries = r * c;
+    }
+    return TOMOS_OK;
+}
+
+bool read_value(FILE* f, double* v) {
+    char tok[128];
+    if (std::fscanf(f, "%127s", tok) != 1) return false;
+    errno = 0;
+    char* end = nullptr;
+    *v = std::strtod(tok, &end);
+    return end && *end == '\0' && end != tok;
+}
+
+bool read_index(FILE* f, long long* v) { return std::fscanf(f, "%lld", v) == 1; }
+
+// Visits every stored entry as (row, col, value), 0-based; symmetric parts
+// are emitted once here (the callers mirror them).
+template <class Fn>
+tomos_status mtx_entries(MtxFile& m, const char* path, Fn&& fn) {
+    using tomos_b200::fail;
+    const tomos_mtx_info& in = m.info;
+    const std::string bad = std::string("'") + path + "': truncated/malformed data";
+    if (in.format == TOMOS_MTX_ARRAY) {
+        for (int64_t j = 0; j < in.cols; ++j) {
+            const int64_t i0 = in.symmetry == TOMOS_MTX_GENERAL ? 0 : (in.symmetry == TOMOS_MTX_SYMMETRIC ? j : j + 1);
+            for (int64_t i = i0; i < in.rows; ++i) {
+                double v;
+                if (!read_value(m.f, &v)) return fail(TOMOS_ERR_INVALID, bad);
+                fn(i, j, v);
+            }
+        }
+        return TOMOS_OK;
+    }
+    for (int64_t e = 0; e < in.entries; ++e) {
+        long long i, j;
+        double v = 1.0;
+        if (!read_index(m.f, &i) || !read_index(m.f, &j)) return fail(TOMOS_ERR_INVALID, bad);
+        if (in.field != TOMOS_MTX_PATTERN && !read_value(m.f, &v)) return fail(TOMOS_ERR_INVALID, bad);
+        if (i < 1 || j < 1 || i > in.rows || j > in.cols)
+            return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': entry " + std::to_string(e + 1) +
+                                               " lies outside the matrix");
+        fn((int64_t)(i - 1), (int64_t)(j - 1), v);
+    }
+    return TOMOS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tomos_status tomos_mtx_read_info(const char* path, tomos_mtx_info* info) {
+    if (!info) return tomos_b200::fail(TOMOS_ERR_INVALID, "tomos_mtx_read_info: null info");
+    MtxFile m;
+    tomos_status s = mtx_open(path, m);
+    if (s) return s;
+    *info = m.info;
+    return TOMOS_OK;
+}
+
+tomos_status tomos_mtx_read_dense(const char* path, int32_t layout, double* out, int64_t ld) {
+    using tomos_b200::fail;
+    MtxFile m;
+    tomos_status s = mtx_open(path, m);
+    if (s) return s;
+    const tomos_mtx_info& in = m.info;
+    const int64_t need = layout == TOMOS_COL_MAJOR ? in.rows : in.cols;
+    if (!out || ld < need || ld < 1)
+        return fail(TOMOS_ERR_INVALID, "tomos_mtx_read_dense: null output or ld too small");
+    auto at = [&](int64_t i, int64_t j) -> double& {
+        return layout == TOMOS_COL_MAJOR ? out[(size_t)j * ld + i] : out[(size_t)i * ld + j];
+    };
+    for (int64_t j = 0; j < in.cols; ++j)
+        for (int64_t i = 0; i < in.rows; ++i) at(i, j) = 0.0;
+    const int32_t sym = in.symmetry;
+    return mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
+        if (in.format == TOMOS_MTX_COORDINATE) at(i, j) += v;  // repeated entries add
+        else at(i, j) = v;
+        if (sym != TOMOS_MTX_GENERAL && i != j) {
+            const double w = sym == TOMOS_MTX_SKEW ? -v : v;
+            if (in.format == TOMOS_MTX_COORDINATE) at(j, i) += w;
+            else at(j, i) = w;
+        }
+    });
+}
+
+tomos_status tomos_mtx_read_coo(const char* path, int64_t cap, int64_t* rows, int64_t* cols, double* vals,
+                                int64_t* count) {
+    using tomos_b200::fail;
+    MtxFile m;
+    tomos_status s = mtx_open(path, m);
+    if (s) return s;
+    if (!count) return fail(TOMOS_ERR_INVALID, "tomos_mtx_read_coo: null count");
+    int64_t k = 0;
+    bool over = false;
+    auto put = [&](int64_t i, int64_t j, double v) {
+        if (k < cap && rows && cols && vals) {
+            rows[k] = i;
+            cols[k] = j;
+            vals[k] = v;
+        } else {
+            over = true;
+        }
+        ++k;
+    };
+    const int32_t sym = m.info.symmetry;
+    s = mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
+        put(i, j, v);
+        if (sym != TOMOS_MTX_GENERAL && i != j) put(j, i, sym == TOMOS_MTX_SKEW ? -v : v);
+    });
+    if (s) return s;
+    *count = k;
+    if (over)
+        return fail(TOMOS_ERR_INVALID, "tomos_mtx_read_coo: " + std::to_string(k) +
+                                           " entries do not fit the given capacity");
+    return TOMOS_OK;
+}
+
+tomos_status tomos_mtx_write_dense(const char* path, int32_t layout, int64_t rows, int64_t cols,
+                                   const double* a, int64_t ld) {
+    using tomos_b200::fail;
+    const int64_t need = layout == TOMOS_COL_MAJOR ? rows : cols;
+    if (rows < 0 || cols < 0 || (rows * cols > 0 && (!a || ld < need)))
+        return fail(TOMOS_ERR_INVALID, "tomos_mtx_write_dense: bad shape, ld or null matrix");
+    FILE* f = path ? std::fopen(path, "w") : nullptr;
+    if (!f) return fail(TOMOS_ERR_INVALID, std::string("could not open '") + (path ? path : "") + "' for writing");
+    bool ok = std::fprintf(f, "%%%%MatrixMarket matrix array real general\n%lld %lld\n", (long long)rows,
+                           (long long)cols) > 0;
+    for (int64_t j = 0; ok && j < cols; ++j)
+        for (int64_t i = 0; ok && i < rows; ++i) {
+            const double v = layout == TOMOS_COL_MAJOR ? a[(size_t)j * ld + i] : a[(size_t)i * ld + j];
+            ok = std::fprintf(f, "%.17g\n", v) > 0;
+        }
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': write failed");
+    return TOMOS_OK;
+}
+
+}  // extern "C"
