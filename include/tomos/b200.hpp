@@ -61,6 +61,7 @@ inline std::size_t elem_bytes(NumericType t) {
     switch (t) {
         case NumericType::FP64: return 8;
         case NumericType::FP32: return 4;
+        case NumericType::FP16: return 2;  // native __half
         case NumericType::FP32_16:
         case NumericType::FP32_BF16: return 4;  // one uint32 slot: wh + wr planes
         default: throw std::runtime_error("no storage registered for this NumericType");
@@ -266,21 +267,20 @@ inline tomos_lsqr_opts opts_for(const Workspace& ws, NumericType a, double tol, 
 }  // namespace b200_detail
 
 // lsqr_solve (include/core/solver.hpp:68-78).  b and x are FP32 Dense
-// vectors; x is overwritten.  mtx_refine_precision (an explicit FP32
-// duplicate of A) is not registered: packed A uses the implicit duplicate
-// (Workspace::use_implicit_duplicate_) instead.
+// vectors; x is overwritten.  mtx_refine_precision: a copy of A at higher
+// precision (FP32, or packed read exactly), e.g. beside an FP16 A
+// (--explicit-duplicates); the initial and restart passes read it.
 inline void lsqr_solve(Context ctx, Dense& A, Dense& b, Dense& x, Workspace& ws, double tol,
                        int max_iters, double max_relres, int* iterations = nullptr,
                        std::vector<double>* residual_history = nullptr, int restarts = 1,
                        Dense* mtx_refine_precision = nullptr) {
     (void)ctx;
-    if (mtx_refine_precision)
-        throw std::runtime_error("lsqr_solve: explicit refine duplicates are not registered");
     if (b.get_value_type() != NumericType::FP32 || x.get_value_type() != NumericType::FP32)
         throw std::runtime_error("lsqr_solve: only FP32 b / x are registered");
     std::vector<double> buf;
     tomos_lsqr_opts o = b200_detail::opts_for(ws, A.get_value_type(), tol, max_iters, max_relres,
                                               restarts, residual_history, buf);
+    if (mtx_refine_precision) o.refine = &mtx_refine_precision->desc();
     b200_detail::check(tomos_lsqr_solve_dense(&A.desc(), static_cast<const float*>(b.data()),
                                               static_cast<float*>(x.data()), ws.handle(), &o,
                                               &ws.last_report, nullptr),

@@ -119,6 +119,14 @@ tomos_status tomos_pack_fp32_bf16(const float* src, int32_t layout, int64_t rows
                                   int64_t cols, int64_t ld_src, uint16_t* wh,
                                   uint16_t* wr, int64_t ld_dst, int32_t rounded,
                                   void* stream);
+/* FP32 -> native IEEE fp16 (round to nearest even, overflow to Inf): a
+ * plain __half Dense, as the reference fills one (fill_dense_from_host<__half>
+ * in lsqr_precision_runner.cu; the storage of --explicit-duplicates, whose
+ * products the reference runs in mv_fp16_native, dense_registries.cpp:
+ * 73-92, 329-333).  FP16 storage is read by every dense product, the
+ * CountSketch and LSQR (iterations in FP32 arithmetic). */
+tomos_status tomos_pack_fp16(const float* src, int32_t layout, int64_t rows, int64_t cols,
+                             int64_t ld_src, uint16_t* dst, int64_t ld_dst, void* stream);
 tomos_status tomos_unpack_fp32_bf16(const uint16_t* wh, const uint16_t* wr,
                                     int32_t layout, int64_t rows, int64_t cols,
                                     int64_t ld_src, float* dst, int64_t ld_dst,
@@ -274,6 +282,11 @@ typedef struct tomos_lsqr_opts {
                                 it instead of staging their own copy. The
                                 caller keeps it equal to A's wh plane.      */
     int64_t staged_ld;
+    const tomos_dense* refine; /* may be NULL: lsqr_solve's
+                                mtx_refine_precision (--explicit-duplicates):
+                                a copy of A at higher precision (FP32, or
+                                packed read exactly) that the initial and
+                                restart passes read instead of A            */
 } tomos_lsqr_opts;
 
 typedef struct tomos_lsqr_report {

@@ -66,7 +66,7 @@ def test_errors_are_status_codes_not_exceptions():
     assert rc == C.TOMOS_ERR_INVALID
     assert b"layout" in L.tomos_last_error()
     d = C.DenseDesc()
-    d.numeric = 2  # FP16 storage has no kernel registered
+    d.numeric = 4  # native BF16 storage has no kernel registered
     d.layout = 1
     d.rows = d.cols = d.ld = 4
     rc = L.tomos_gemv(0, 1.0, ctypes.byref(d), 0, None, 0.0, None, None, 0, None)

@@ -131,6 +131,8 @@ class Dense:
             buf = torch.zeros(max(n, 1), dtype=torch.float32, device="cuda")
         elif st == NumericType.FP64:
             buf = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda")
+        elif st == NumericType.FP16:
+            buf = torch.zeros(max(n, 1), dtype=torch.float16, device="cuda")
         elif st in PACKED:
             buf = torch.zeros(max(2 * n, 2), dtype=torch.int16, device="cuda")
         else:
@@ -379,9 +381,21 @@ def combine_fp32_bf16(source, target, stream=None):
                                            _stream(stream)), "combine_fp32_bf16")
 
 
+def pack_fp16(A_fp32, P, stream=None):
+    """FP32 Dense -> native FP16 Dense of the same shape (round to nearest
+    even; tomos_pack_fp16)."""
+    C.check(C.lib().tomos_pack_fp16(_ptr(A_fp32.storage), int(A_fp32.layout), A_fp32.size[0],
+                                    A_fp32.size[1], A_fp32.ld, _ptr(P.storage), P.ld, _stream(stream)),
+            "pack_fp16")
+    return P
+
+
 def pack(A_fp32, store_type, rounded=False, stream=None):
-    """Convenience: a packed copy of an FP32 Dense with the same layout."""
+    """Convenience: a packed (or native FP16) copy of an FP32 Dense with the
+    same layout."""
     P = Dense.create_strided(None, A_fp32.layout, store_type, A_fp32.size, A_fp32.ld, rounded)
+    if NumericType(store_type) == NumericType.FP16:
+        return pack_fp16(A_fp32, P, stream=stream)
     if NumericType(store_type) == NumericType.FP32_16:
         split_fp32_16(A_fp32, P, stream=stream)
     else:
@@ -570,12 +584,15 @@ def add_precond(precond, workspace):
 def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=None,
                residual_history=None, restarts=1, stop_rule=StopRule.RELRES, inner_rtol=0.0,
                anorm_fro=0.0, warm_start=False, tier=None, profile=False, col_scale=None,
-               staged_plane=None, stream=None):
+               staged_plane=None, mtx_refine_precision=None, stream=None):
     """include/core/solver.hpp:68-78.  A: Dense or Csr on the device; b, x:
     FP32 Dense column vectors or float32 CUDA tensors.  iterations and
     residual_history, when lists, receive the reference's out-parameters.
     staged_plane: the (m x ld) int16 tensor apply_count_sketch(..., stage=True)
     filled for this A (HALF-tier iterations then skip their staging pass).
+    mtx_refine_precision: a Dense copy of A at higher precision (FP32, or
+    packed read exactly) for the initial and restart passes, e.g. beside an
+    FP16 A (the reference's --explicit-duplicates).
     Returns the solver report as a dict."""
     opts = C.LsqrOpts()
     opts.tol = float(tol)
@@ -593,6 +610,10 @@ def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=N
     opts.warm_start = 1 if warm_start else 0
     opts.inner_rtol = float(inner_rtol)
     opts.anorm_fro = float(anorm_fro)
+    refine_desc = None
+    if mtx_refine_precision is not None:
+        refine_desc = mtx_refine_precision.desc()
+        opts.refine = ctypes.addressof(refine_desc)
     opts.profile = 1 if profile else 0
     opts.col_scale = col_scale.data_ptr() if col_scale is not None else None
     if staged_plane is not None:

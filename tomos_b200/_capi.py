@@ -46,7 +46,7 @@ class LsqrOpts(ctypes.Structure):
                 ("implicit_duplicate", c_i32), ("warm_start", c_i32), ("inner_rtol", c_dbl),
                 ("anorm_fro", c_dbl), ("col_scale", c_vp), ("history", ctypes.POINTER(c_dbl)),
                 ("history_cap", c_i32), ("profile", c_i32), ("staged_plane", c_vp),
-                ("staged_ld", c_i64)]
+                ("staged_ld", c_i64), ("refine", c_vp)]
 
 
 class LsqrReport(ctypes.Structure):
@@ -72,6 +72,7 @@ class MtxInfo(ctypes.Structure):
 
 # Every symbol the header declares, with (restype, argtypes).
 SIGNATURES = {
+    "tomos_pack_fp16": (c_i32, [c_vp, c_i32, c_i64, c_i64, c_i64, c_vp, c_i64, c_vp]),
     "tomos_mtx_read_info": (c_i32, [ctypes.c_char_p, ctypes.POINTER(MtxInfo)]),
     "tomos_mtx_read_dense": (c_i32, [ctypes.c_char_p, c_i32, c_vp, c_i64]),
     "tomos_mtx_read_coo": (c_i32, [ctypes.c_char_p, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_i64)]),

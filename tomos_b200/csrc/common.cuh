@@ -219,6 +219,10 @@ __device__ __forceinline__ float load_elem<Elem::H16>(const void* p, const void*
     return half_bits_to_float(half_only_bits(h));
 }
 template <>
+__device__ __forceinline__ float load_elem<Elem::F16>(const void* p, const void*, size_t idx) {
+    return half_bits_to_float(__ldg(reinterpret_cast<const unsigned short*>(p) + idx));
+}
+template <>
 __device__ __forceinline__ float load_elem<Elem::A16>(const void* p, const void* q, size_t idx) {
     uint32_t h = __ldg(reinterpret_cast<const unsigned short*>(p) + idx);
     uint32_t r = __ldg(reinterpret_cast<const unsigned short*>(q) + idx);

@@ -157,6 +157,7 @@ tomos_status gemv_launch(const GemvLaunch& L, Elem e, bool acc64, cudaStream_t s
     switch (e) {
         case Elem::F32: return run_gemv_acc<Elem::F32>(L, acc64, st);
         case Elem::H16: return run_gemv_acc<Elem::H16>(L, acc64, st);
+        case Elem::F16: return run_gemv_acc<Elem::F16>(L, acc64, st);
         case Elem::A16: return run_gemv<Elem::A16, true>(L, st);
         case Elem::B16: return run_gemv_acc<Elem::B16>(L, acc64, st);
         case Elem::AB16: return run_gemv<Elem::AB16, true>(L, st);

@@ -793,7 +793,9 @@ struct DensePass : PassOps {
     }
     tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
                          const int* skip, cudaStream_t st) override {
-        return enqueue_dense_pass(ws, pl.e == Elem::F16 ? &staged : A, pl, p, u_in, coef, skip, st);
+        // F16 passes read the staged plane only when this solve staged one;
+        // native FP16 storage is read in place
+        return enqueue_dense_pass(ws, (stage && pl.e == Elem::F16) ? &staged : A, pl, p, u_in, coef, skip, st);
     }
     tomos_status fro2(double* out, const double* d, cudaStream_t st) override {
         bool dot;
@@ -807,6 +809,7 @@ struct DensePass : PassOps {
         switch (init_e) {
             case Elem::F32: TOMOS_FRO2(Elem::F32); break;
             case Elem::H16: TOMOS_FRO2(Elem::H16); break;
+            case Elem::F16: TOMOS_FRO2(Elem::F16); break;
             case Elem::A16: TOMOS_FRO2(Elem::A16); break;
             case Elem::B16: TOMOS_FRO2(Elem::B16); break;
             case Elem::AB16: TOMOS_FRO2(Elem::AB16); break;
@@ -826,6 +829,35 @@ struct DensePass : PassOps {
     }
     int64_t rows() override { return A->rows; }
     int64_t cols() override { return A->cols; }
+};
+
+// Iterations over A, the initial and restart passes over a second copy of
+// A at higher precision: the reference's mtx_refine_precision
+// (--explicit-duplicates; lsqr.cpp:451-473 computes the restart residual
+// u = b - A_refine x from it).  Here the whole restart pass, u and A^T u,
+// streams the refine copy (one read of it instead of a read of each), and
+// its ||A||_F feeds the backward-error rule.
+struct RefinePass : PassOps {
+    DensePass& it;
+    DensePass& re;
+    RefinePass(DensePass& a, DensePass& r) : it(a), re(r) {}
+    PassPlan plan(bool init) override {
+        PassPlan p = init ? re.plan(true) : it.plan(false);
+        p.src = init ? 1 : 0;
+        return p;
+    }
+    tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
+                         const int* skip, cudaStream_t st) override {
+        return pl.src ? re.enqueue(pl, p, u_in, coef, skip, st) : it.enqueue(pl, p, u_in, coef, skip, st);
+    }
+    tomos_status fro2(double* out, const double* d, cudaStream_t st) override { return re.fro2(out, d, st); }
+    uint64_t key() override { return it.key() ^ (re.key() * 0x9E3779B97F4A7C15ull); }
+    int64_t rows() override { return it.rows(); }
+    int64_t cols() override { return it.cols(); }
+    tomos_status prepare(cudaStream_t st) override {
+        tomos_status s = it.prepare(st);
+        return s ? s : re.prepare(st);
+    }
 };
 
 // ------------------------------------------------------------ driver
@@ -1292,6 +1324,37 @@ tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float*
         if (report) std::memset(report, 0, sizeof(*report));
         if (report) report->converged = 1;
         return TOMOS_OK;
+    }
+    if (opts->refine) {
+        const tomos_dense* Rf = opts->refine;
+        if (opts->implicit_duplicate)
+            return fail(TOMOS_ERR_INVALID,
+                        "lsqr_solve: explicit (mtx_refine_precision) and implicit duplicates are "
+                        "mutually exclusive");
+        if (!gemv_shape(Rf, TOMOS_NO_TRANSPOSE, &dot, &outer, &inner, &why))
+            return fail(TOMOS_ERR_INVALID, "lsqr_solve: mtx_refine_precision: " + why);
+        if (Rf->rows != A->rows || Rf->cols != A->cols || (!Rf->values && Rf->rows * Rf->cols > 0))
+            return fail(TOMOS_ERR_INVALID, "lsqr_solve: mtx_refine_precision must have A's size");
+        Elem re;
+        const int32_t rt = Rf->numeric == TOMOS_FP32 ? TOMOS_TIER_NATIVE : TOMOS_TIER_ACCURATE;
+        if (!resolve_elem(Rf, rt, &re, &why))
+            return fail(TOMOS_ERR_UNSUPPORTED, "lsqr_solve: mtx_refine_precision: " + why);
+        if (A->rows == 0 || A->cols == 0) {
+            if (A->cols > 0 && !opts->warm_start) cudaMemsetAsync(x, 0, sizeof(float) * A->cols, as_stream(stream));
+            if (report) std::memset(report, 0, sizeof(*report));
+            if (report) report->converged = 1;
+            return TOMOS_OK;
+        }
+        if (opts->staged_plane) return fail(TOMOS_ERR_INVALID, "lsqr_solve: staged_plane with mtx_refine_precision");
+        DensePass pa(ws, A, ie, ie), pr(ws, Rf, re, re);
+        RefinePass ops(pa, pr);
+        PassPlan a = ops.plan(true), b2 = ops.plan(false);
+        if (!a.fused || !b2.fused) {
+            const size_t sa = dense_pass_scratch(A), sr = dense_pass_scratch(Rf);
+            s = ensure_scratch(ws, sa > sr ? sa : sr);
+            if (s) return s;
+        }
+        return solve_driver(ws, ops, b, x, opts, report, stream);
     }
     DensePass ops(ws, A, ie, ze);
     if (opts->staged_plane) {

@@ -47,6 +47,7 @@ struct PassPlan {
     int gs = 1;      // ||ut||^2 partials
     int64_t qstride = 0;
     int tpw = 0;     // > 0: the tensor-core pass, k-tiles per consumer warp
+    int src = 0;     // 1: the pass reads the refine copy of A (RefinePass)
 };
 
 // One pass over A producing ut = cp*A p + cu*u_in in the workspace's u,

@@ -55,6 +55,14 @@ static bool resolve_numeric(int32_t numeric, int32_t rounded, int32_t tier, Elem
                 return true;
             }
             break;
+        case TOMOS_FP16:
+            // native IEEE fp16 storage (the reference's plain __half Dense,
+            // --explicit-duplicates): products in FP32
+            if (tier == TOMOS_TIER_AUTO || tier == TOMOS_TIER_NATIVE || tier == TOMOS_TIER_HALF) {
+                *out = Elem::F16;
+                return true;
+            }
+            break;
         case TOMOS_FP32_16:
             if (tier == TOMOS_TIER_AUTO || tier == TOMOS_TIER_HALF) {
                 *out = Elem::H16;
@@ -87,6 +95,10 @@ bool resolve_elem(const tomos_dense* A, int32_t tier, Elem* out, std::string* wh
     return resolve_numeric(A->numeric, A->rounded, tier, out, why);
 }
 bool resolve_elem_csr(const tomos_csr* A, int32_t tier, Elem* out, std::string* why) {
+    if (A->numeric == TOMOS_FP16) {
+        *why = "no CSR kernel registered for FP16 values";
+        return false;
+    }
     return resolve_numeric(A->numeric, A->rounded, tier, out, why);
 }
 
@@ -184,6 +196,18 @@ static bool shape_ok(int32_t layout, int64_t rows, int64_t cols, int64_t ld_a, i
     return true;
 }
 
+// FP32 -> IEEE fp16, round to nearest even (overflow to Inf, fp16
+// subnormals kept): the reference's __half(value) when it fills a native
+// FP16 Dense (fill_dense_from_host<__half>).
+__global__ void packhalf_kernel(const float* __restrict__ src, int64_t outer, int64_t inner, int64_t ld_src,
+                                uint16_t* __restrict__ dst, int64_t ld_dst) {
+    for (int64_t o = blockIdx.x; o < outer; o += gridDim.x) {
+        const float* s = src + (size_t)o * ld_src;
+        uint16_t* d = dst + (size_t)o * ld_dst;
+        for (int64_t i = threadIdx.x; i < inner; i += blockDim.x) d[i] = __half_as_ushort(__float2half_rn(s[i]));
+    }
+}
+
 static int pack_grid(int64_t outer) {
     int64_t g = (int64_t)sm_count() * 16;
     if (outer < g) g = outer;
@@ -247,6 +271,19 @@ tomos_status tomos_pack_fp32_bf16(const float* src, int32_t layout, int64_t rows
     packbf16_kernel<<<pack_grid(outer), 256, 0, as_stream(stream)>>>(src, outer, inner, ld_src, wh,
                                                                      wr, ld_dst, rounded);
     TOMOS_LAUNCH_CHECK("packbf16_kernel");
+    return TOMOS_OK;
+}
+
+tomos_status tomos_pack_fp16(const float* src, int32_t layout, int64_t rows, int64_t cols,
+                             int64_t ld_src, uint16_t* dst, int64_t ld_dst, void* stream) {
+    int64_t outer, inner;
+    std::string why;
+    if (!shape_ok(layout, rows, cols, ld_src, ld_dst, &outer, &inner, &why))
+        return fail(TOMOS_ERR_INVALID, "tomos_pack_fp16: " + why);
+    if (outer == 0 || inner == 0) return TOMOS_OK;
+    if (!src || !dst) return fail(TOMOS_ERR_INVALID, "tomos_pack_fp16: null pointer");
+    packhalf_kernel<<<pack_grid(outer), 256, 0, as_stream(stream)>>>(src, outer, inner, ld_src, dst, ld_dst);
+    TOMOS_LAUNCH_CHECK("packhalf_kernel");
     return TOMOS_OK;
 }
 

@@ -761,6 +761,7 @@ static tomos_status countsketch_apply(const tomos_dense* A, int32_t tier, int64_
                            : launch_rows_tma<Elem::H16, false>(A, lo, s, c, SA, ld_sa, colsq, fro2, nullptr, 0, st);
                 break;
             case Elem::A16: rs = launch_rows_tma<Elem::A16, false>(A, lo, s, c, SA, ld_sa, colsq, fro2, nullptr, 0, st); break;
+            case Elem::F16: rs = launch_rows_tma<Elem::F16, false>(A, lo, s, c, SA, ld_sa, colsq, fro2, nullptr, 0, st); break;
             case Elem::B16: rs = launch_rows_tma<Elem::B16, false>(A, lo, s, c, SA, ld_sa, colsq, fro2, nullptr, 0, st); break;
             case Elem::AB16: rs = launch_rows_tma<Elem::AB16, false>(A, lo, s, c, SA, ld_sa, colsq, fro2, nullptr, 0, st); break;
             case Elem::AB16R: rs = launch_rows_tma<Elem::AB16R, false>(A, lo, s, c, SA, ld_sa, colsq, fro2, nullptr, 0, st); break;
@@ -776,6 +777,7 @@ static tomos_status countsketch_apply(const tomos_dense* A, int32_t tier, int64_
             case Elem::F32: panels = launch_rows<Elem::F32>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
             case Elem::H16: panels = launch_rows<Elem::H16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
             case Elem::A16: panels = launch_rows<Elem::A16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
+            case Elem::F16: panels = launch_rows<Elem::F16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
             case Elem::B16: panels = launch_rows<Elem::B16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
             case Elem::AB16: panels = launch_rows<Elem::AB16>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
             case Elem::AB16R: panels = launch_rows<Elem::AB16R>(A, lo, s, c, SA, ld_sa, colsq, gx, st); break;
@@ -791,6 +793,7 @@ static tomos_status countsketch_apply(const tomos_dense* A, int32_t tier, int64_
             case Elem::F32: launch_cols<Elem::F32>(A, lo, s, c, SA, ld_sa, colsq, st); break;
             case Elem::H16: launch_cols<Elem::H16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
             case Elem::A16: launch_cols<Elem::A16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
+            case Elem::F16: launch_cols<Elem::F16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
             case Elem::B16: launch_cols<Elem::B16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
             case Elem::AB16: launch_cols<Elem::AB16>(A, lo, s, c, SA, ld_sa, colsq, st); break;
             case Elem::AB16R: launch_cols<Elem::AB16R>(A, lo, s, c, SA, ld_sa, colsq, st); break;
