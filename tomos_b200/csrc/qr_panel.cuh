@@ -48,7 +48,9 @@ typedef double HMat[kHB][kHB + 1];
 // Warp 0 runs the 32 right-looking steps on registers: lane l holds column
 // l of G, row j of R reaches the other lanes by shuffles (the other warps
 // wait at the end).
-__device__ __forceinline__ bool cta_chol(const HMat& G, HMat& R, double floor, int* okf) {
+// (Not inlined: inside the one-launch QR the kernel's register pressure
+// would otherwise put the lane's 32 values in local memory.)
+__device__ __noinline__ bool cta_chol(const HMat& G, HMat& R, double floor, int* okf) {
     const int t = threadIdx.x;
     __syncthreads();
     if (t < 32) {
@@ -62,8 +64,11 @@ __device__ __forceinline__ bool cta_chol(const HMat& G, HMat& R, double floor, i
             const double d = __shfl_sync(0xffffffffu, g[j], j);
             const bool good = d > floor && isfinite(d);
             if (!good) ok = 0;
-            const double rjj = sqrt(good ? d : 1.0);
-            const double rjl = l > j ? g[j] / rjj : (l == j ? rjj : 0.0);
+            // one reciprocal square root on the step's critical path:
+            // R(j, j) = d / sqrt(d), R(j, l) = G(j, l) / sqrt(d)
+            const double dd = good ? d : 1.0;
+            const double ri = rsqrt(dd);
+            const double rjl = l > j ? g[j] * ri : (l == j ? dd * ri : 0.0);
             R[j][l] = rjl;
             // G(i, l) -= R(j, i) R(j, l) for j < i <= l (entries below the
             // diagonal of G are never read)
@@ -144,7 +149,7 @@ __device__ __forceinline__ void cta_inv_unit_lower(const HMat& Q, HMat& Y, HMat&
 // diagonal, which dlarfg leaves as the identity (tau = 0, R_jj = alpha):
 // there s = +sign(pivot).  Warp 0 runs the 32 steps on registers: lane l
 // holds row l, row i of U reaches the other lanes by shuffles.
-__device__ __forceinline__ void cta_lu_signed(HMat& Q, double* sgn, int keep) {
+__device__ __noinline__ void cta_lu_signed(HMat& Q, double* sgn, int keep) {
     __syncthreads();
     if (threadIdx.x < 32) {
         const int l = threadIdx.x;
@@ -160,7 +165,16 @@ __device__ __forceinline__ void cta_lu_signed(HMat& Q, double* sgn, int keep) {
             if (l == 0) sgn[i] = si;
             if (l == i) q[i] = u;
             const bool below = l > i;
-            const double lm = below ? (u != 0.0 ? q[i] / u : 0.0) : 0.0;
+            // 1/u with |u| in [1, 2] (|u| = |q_ii| + 1): the hardware's
+            // approximate float reciprocal and two Newton steps in FP64 (no
+            // division, whose out-of-line path is costly in this kernel)
+            float uf;
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(uf) : "f"((float)u));
+            double ui = (double)uf;
+            ui = fma(ui, fma(-u, ui, 1.0), ui);
+            ui = fma(ui, fma(-u, ui, 1.0), ui);
+            if (u == 0.0) ui = 0.0;
+            const double lm = below ? q[i] * ui : 0.0;
             if (below) q[i] = lm;
 #pragma unroll
             for (int c = i + 1; c < kHB; ++c) {
@@ -258,15 +272,20 @@ __device__ void hr_q1(const HrArgs& H, int cta, double* hsm) {
     const int nb = H.nb;
 
     hr_reduce_gram(H.Gp, H.ngp, nb, G);
+    // D = diag(G1)^1/2 (dsc) and D^-1 (dinv, by rsqrt: no division)
+    double* dinv = dsc + kHB;
     if (t < kHB) {
         const double g = G[t][t];
-        dsc[t] = (t < nb && g > 0.0 && isfinite(g)) ? sqrt(g) : 1.0;
-        if (t < nb && !(g > 0.0 && isfinite(g))) G[t][t] = 0.0;  // forces the fallback
+        const bool ok = t < nb && g > 0.0 && isfinite(g);
+        const double ri = ok ? rsqrt(g) : 1.0;
+        dinv[t] = ri;
+        dsc[t] = ok ? g * ri : 1.0;
+        if (t < nb && !ok) G[t][t] = 0.0;  // forces the fallback
     }
     __syncthreads();
     for (int e = t; e < kHB * kHB; e += blockDim.x) {
         const int i = e >> 5, j = e & 31;
-        if (i < nb && j < nb) G[i][j] = G[i][j] / (dsc[i] * dsc[j]);
+        if (i < nb && j < nb) G[i][j] = G[i][j] * dinv[i] * dinv[j];
     }
     __syncthreads();
     cta_chol(G, R, 1e-12, &okflag);
@@ -275,7 +294,7 @@ __device__ void hr_q1(const HrArgs& H, int cta, double* hsm) {
     for (int e = t; e < kHB * kHB; e += blockDim.x) {
         const int i = e >> 5, j = e & 31;
         R[i][j] *= dsc[j];
-        X[i][j] /= dsc[i];
+        X[i][j] *= dinv[i];
     }
     __syncthreads();
     if (cta == 0) {
@@ -569,7 +588,7 @@ __global__ void __launch_bounds__(256) qr_hr_v_kernel(HrArgs H) {
     hr_v(H, blockIdx.x, gridDim.x, 0, hsm);
 }
 
-inline size_t hr_q1_smem() { return (4 * kHB * (kHB + 1) + kHB) * sizeof(double); }
+inline size_t hr_q1_smem() { return (4 * kHB * (kHB + 1) + 2 * kHB) * sizeof(double); }
 inline size_t hr_v_smem() { return (6 * kHB * (kHB + 1) + 3 * kHB + 8) * sizeof(double); }
 
 }  // namespace tomos_b200
