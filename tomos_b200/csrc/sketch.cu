@@ -243,7 +243,7 @@ __global__ void cs_col_reduce_kernel(const double* __restrict__ part, int64_t np
 constexpr int kCsWarps = 12;
 constexpr int kCsStages = 4;
 constexpr int kCsStageBytes = 4096;  // per warp and stage
-constexpr int kCsPanelCols = 1024;   // columns per work item
+constexpr int kCsPanelCols = 512;    // columns per work item
 constexpr int kCsList = 512;         // a bucket's row ids kept in shared memory
 
 struct CsRowsArgs {
