@@ -38,6 +38,7 @@ constexpr int kQrChunks = 8;     // row chunks of the W partials
 constexpr int kQrMaxChunks = 32; // ... when few column tiles leave SMs idle (one-launch QR)
 constexpr int kQrRowTile = 256;  // rows per apply tile (and per Gram partial)
 constexpr int kQrMinRowTile = 64; // ... halved down to this when tiles would leave CTAs idle
+constexpr int64_t kTrtriGemmMin = 1024; // R^{-1} levels from this block size on run as GEMMs
 constexpr int kQrPanelCtas = 128; // CTAs of the panel passes (~64 rows each)
 
 struct QrScratch {
@@ -61,6 +62,7 @@ struct QrScratch {
     double* Tb2;    // the block's T, kQrBlock x kQrBlock
     double* Wb;     // Z^T C, kQrBlock x n
     double* Pk;     // split-K partials, kGmaxSplits x kQrBlock x max(n, kQrBlock)
+    size_t pk_doubles;
     size_t bytes;
 };
 
@@ -112,6 +114,7 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
     q.flag = reinterpret_cast<int*>(take(sizeof(int) * 4));
     q.gsync = take(64);
     q.Tp = q.Vb = q.Z = q.Y = q.Tb2 = q.Wb = q.Pk = nullptr;
+    q.pk_doubles = 0;
     if (qr_blocked(n)) {
         const size_t bb = kQrBlock, nw = nn > bb ? nn : bb;
         q.Tp = reinterpret_cast<double*>(take(sizeof(double) * (bb / kHB) * kHB * kHB));
@@ -120,7 +123,8 @@ static QrScratch qr_layout(void* base, int64_t k, int64_t n) {
         q.Y = reinterpret_cast<double*>(take(sizeof(double) * bb * bb));
         q.Tb2 = reinterpret_cast<double*>(take(sizeof(double) * bb * bb));
         q.Wb = reinterpret_cast<double*>(take(sizeof(double) * bb * nn));
-        q.Pk = reinterpret_cast<double*>(take(sizeof(double) * kGmaxSplits * bb * nw));
+        q.pk_doubles = kGmaxSplits * bb * nw;
+        q.Pk = reinterpret_cast<double*>(take(sizeof(double) * q.pk_doubles));
     }
     q.bytes = off;
     return q;
@@ -710,13 +714,14 @@ __global__ void __launch_bounds__(256) trtri_level_kernel(const double* Rt, int6
 }
 
 // op(A) B products of the blocked QR (qr_gemm.cuh).  With a partial
-// buffer P, K is split over CTAs (partials summed in order) by the count
-// that wastes the least of the last wave of resident CTAs (two per SM),
-// each split keeping at least 16 k-stages.  sub: D -= op(A) B.
+// buffer P of pcap doubles, K is split over CTAs (partials summed in
+// order) by the count that wastes the least of the last wave of resident
+// CTAs (two per SM), each split keeping at least 16 k-stages and all
+// partials fitting P.  sub: D -= op(A) B.
 template <bool KMAJOR>
 static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64_t ldb, double* D,
                             int64_t ldd, int64_t M, int64_t N, int64_t K, double alpha, double beta,
-                            double* P, cudaStream_t st, int sub = 0) {
+                            double* P, size_t pcap, cudaStream_t st, int sub = 0) {
     if (M <= 0 || N <= 0) return TOMOS_OK;
     const int64_t tm = (M + kGbm - 1) / kGbm, tn = (N + kGbn - 1) / kGbn;
     int64_t splits = 1;
@@ -724,6 +729,8 @@ static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64
         const int64_t slots = 2 * (int64_t)sm_count(), tiles = tm * tn;
         int64_t kmax = K / (16 * kGbk);
         if (kmax > kGmaxSplits) kmax = kGmaxSplits;
+        const int64_t fit = (int64_t)(pcap / (size_t)(M * N));
+        if (kmax > fit) kmax = fit;
         double best = -1.0;
         for (int64_t s = 1; s <= kmax; ++s) {
             const int64_t ctas = tiles * s, waves = (ctas + slots - 1) / slots;
@@ -778,7 +785,7 @@ static tomos_status qr_block_update(double* SA, int64_t ld, int64_t k, int64_t n
     if (cb > 4096) cb = 4096;
     qr_copy_v_kernel<<<(unsigned)cb, 256, 0, st>>>(SA, ld, jb, krem, w, q.Vb, k);
     TOMOS_LAUNCH_CHECK("qr_copy_v_kernel");
-    tomos_status s = qr_gemm<true>(q.Vb, k, q.Vb, k, q.Y, w, w, w, krem, 1.0, 0.0, q.Pk, st);
+    tomos_status s = qr_gemm<true>(q.Vb, k, q.Vb, k, q.Y, w, w, w, krem, 1.0, 0.0, q.Pk, q.pk_doubles, st);
     if (s) return s;
     qr_block_t_init_kernel<<<(unsigned)((w * w + 255) / 256), 256, 0, st>>>(q.Tp, w, q.Tb2);
     TOMOS_LAUNCH_CHECK("qr_block_t_init_kernel");
@@ -790,12 +797,12 @@ static tomos_status qr_block_update(double* SA, int64_t ld, int64_t k, int64_t n
         trtri_level_kernel<<<g, 256, 0, st>>>(q.Y, w, q.Tb2, w, q.Tb, b, 1);
         TOMOS_LAUNCH_CHECK("trtri_level_kernel");
     }
-    s = qr_gemm<false>(q.Vb, k, q.Tb2, w, q.Z, k, krem, w, w, 1.0, 0.0, nullptr, st);
+    s = qr_gemm<false>(q.Vb, k, q.Tb2, w, q.Z, k, krem, w, w, 1.0, 0.0, nullptr, 0, st);
     if (s) return s;
     double* C = SA + (size_t)je * ld + jb;
-    s = qr_gemm<true>(q.Z, k, C, ld, q.Wb, w, w, nc, krem, 1.0, 0.0, q.Pk, st);
+    s = qr_gemm<true>(q.Z, k, C, ld, q.Wb, w, w, nc, krem, 1.0, 0.0, q.Pk, q.pk_doubles, st);
     if (s) return s;
-    return qr_gemm<false>(q.Vb, k, q.Wb, w, C, ld, krem, nc, w, -1.0, 1.0, nullptr, st, 1);
+    return qr_gemm<false>(q.Vb, k, q.Wb, w, C, ld, krem, nc, w, -1.0, 1.0, nullptr, 0, st, 1);
 }
 
 }  // namespace tomos_b200
@@ -951,6 +958,24 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     TOMOS_LAUNCH_CHECK("qr_trtri_diag_kernel");
     for (int64_t b = 32; b < n; b *= 2) {
         const int64_t pairs = (n - b + 2 * b - 1) / (2 * b);
+        if (b >= kTrtriGemmMin) {
+            // few, large pairs: each product a qr_gemm_kernel launch
+            //   T_p = R_IJ X_JJ  (R_IJ from the row-major copy of R),
+            //   X_IJ = -X_II T_p
+            for (int64_t p = 0; p < pairs; ++p) {
+                const int64_t I0 = 2 * b * p, J0 = I0 + b;
+                const int64_t Jn = n - J0 < b ? n - J0 : b;
+                if (Jn <= 0) continue;
+                double* Tp = q.Tb + (size_t)p * b * b;
+                tomos_status gs = qr_gemm<true>(q.Rt + (size_t)I0 * n + J0, n, SA + (size_t)J0 * ld + J0, ld,
+                                                Tp, b, b, Jn, Jn, 1.0, 0.0, q.Pk, q.pk_doubles, st);
+                if (gs) return gs;
+                gs = qr_gemm<false>(SA + (size_t)I0 * ld + I0, ld, Tp, b, SA + (size_t)J0 * ld + I0, ld, b, Jn,
+                                    b, -1.0, 0.0, q.Pk, q.pk_doubles, st);
+                if (gs) return gs;
+            }
+            continue;
+        }
         const dim3 g((unsigned)((b + 31) / 32), (unsigned)((b + 31) / 32), (unsigned)pairs);
         trtri_level_kernel<<<g, 256, 0, st>>>(q.Rt, n, SA, ld, q.Tb, b, 0);
         TOMOS_LAUNCH_CHECK("trtri_level_kernel");
