@@ -408,7 +408,7 @@ static tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cud
 }
 
 // The staged-fp16 pass on the tensor cores (rowpass_mma.cuh).
-template <int TPW>
+template <int TPW, bool BF>
 static tomos_status launch_fused_mma_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
     MmaPassParams T;
     T.f = P;
@@ -423,23 +423,37 @@ static tomos_status launch_fused_mma_t(const FusedParams& P, int* err, int grid,
     if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
     T.nstage = ns;
     const size_t smem = fused_rows_mma_smem(ns, T.pitch);
-    auto kern = fused_rows_mma_kernel<TPW>;
+    auto kern = fused_rows_mma_kernel<TPW, BF>;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kMmaThreads, smem, st>>>(T);
     TOMOS_LAUNCH_CHECK("fused_rows_mma_kernel");
     return TOMOS_OK;
 }
 
-static tomos_status launch_fused_mma(const FusedParams& P, int* err, int tpw, int grid, cudaStream_t st) {
+template <bool BF>
+static tomos_status launch_fused_mma_b(const FusedParams& P, int* err, int tpw, int grid, cudaStream_t st) {
     switch (tpw) {
-        case 1: return launch_fused_mma_t<1>(P, err, grid, st);
-        case 2: return launch_fused_mma_t<2>(P, err, grid, st);
-        case 3: return launch_fused_mma_t<3>(P, err, grid, st);
-        case 4: return launch_fused_mma_t<4>(P, err, grid, st);
-        case 5: return launch_fused_mma_t<5>(P, err, grid, st);
-        case 6: return launch_fused_mma_t<6>(P, err, grid, st);
+        case 1: return launch_fused_mma_t<1, BF>(P, err, grid, st);
+        case 2: return launch_fused_mma_t<2, BF>(P, err, grid, st);
+        case 3: return launch_fused_mma_t<3, BF>(P, err, grid, st);
+        case 4: return launch_fused_mma_t<4, BF>(P, err, grid, st);
+        case 5: return launch_fused_mma_t<5, BF>(P, err, grid, st);
+        case 6: return launch_fused_mma_t<6, BF>(P, err, grid, st);
+        case 7: return launch_fused_mma_t<7, BF>(P, err, grid, st);
+        case 8: return launch_fused_mma_t<8, BF>(P, err, grid, st);
+        case 9: return launch_fused_mma_t<9, BF>(P, err, grid, st);
+        case 10: return launch_fused_mma_t<10, BF>(P, err, grid, st);
+        case 11: return launch_fused_mma_t<11, BF>(P, err, grid, st);
         default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no tensor-core instantiation");
     }
+}
+
+// The tensor-core pass over a 16-bit plane: fp16 (the staged FP32_16
+// plane, or native FP16 storage) or bf16 (an FP32_BF16 wh plane).
+static tomos_status launch_fused_mma(Elem e, const FusedParams& P, int* err, int tpw, int grid,
+                                     cudaStream_t st) {
+    return e == Elem::B16 ? launch_fused_mma_b<true>(P, err, tpw, grid, st)
+                          : launch_fused_mma_b<false>(P, err, tpw, grid, st);
 }
 
 static bool elem_two_planes(Elem e) {
@@ -587,10 +601,11 @@ PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool
         pl.fused = true;
         pl.nch = nch;
         pl.g = g;
-        // the staged fp16 plane of an iteration: both products on the
-        // tensor cores when n fits 12 warps x kMmaMaxTpw k-tiles
+        // a 16-bit plane read at the HALF tier (the staged fp16 plane,
+        // native FP16, an FP32_BF16 wh plane): both products on the tensor
+        // cores when n fits 12 warps x kMmaMaxTpw k-tiles
         const int64_t ktiles = (A->cols + 15) / 16;
-        if (e == Elem::F16 && !pl.acc64 && ktiles <= (int64_t)kMmaWarps * kMmaMaxTpw)
+        if ((e == Elem::F16 || e == Elem::B16) && !pl.acc64 && ktiles <= (int64_t)kMmaWarps * kMmaMaxTpw)
             pl.tpw = (int)((ktiles + kMmaWarps - 1) / kMmaWarps);
         int64_t grid = sm_count();
         const int64_t min_rows_cta = 64;
@@ -637,7 +652,7 @@ tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A,
         P.sspart = ws->sspart;
         P.qstride = pl.qstride;
         P.skip = skip;
-        tomos_status ls = pl.tpw > 0 ? launch_fused_mma(P, &ws->st->pipe_err, pl.tpw, pl.grid, st)
+        tomos_status ls = pl.tpw > 0 ? launch_fused_mma(pl.e, P, &ws->st->pipe_err, pl.tpw, pl.grid, st)
                                      : launch_fused(pl.e, pl.acc64, P, &ws->st->pipe_err, pl.nch, pl.g, pl.grid, st);
         if (ls) return ls;
         ws->launches += 1;

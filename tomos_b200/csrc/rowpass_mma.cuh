@@ -51,6 +51,7 @@
 // (masking cost 5% of the pass).  Every mbarrier wait is bounded.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "common.cuh"
@@ -65,7 +66,7 @@ constexpr int kMmaProducer = kMmaWarps + 1;
 constexpr int kMmaThreads = (kMmaWarps + 2) * 32;
 constexpr int kMmaRows = 16;   // rows per stage
 constexpr int kMmaMaxStages = 12;
-constexpr int kMmaMaxTpw = 6;  // k-tiles per warp: n <= 12 * 6 * 16 = 1152
+constexpr int kMmaMaxTpw = 11; // k-tiles per warp: n <= 12 * 11 * 16 = 2112
 
 struct MmaPassParams {
     FusedParams f;
@@ -87,14 +88,34 @@ __device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t (&r)[4]) {
                  : "r"(addr));
 }
 
-// D += A B for one m16n8k16 tile (fp16 inputs, FP32 accumulators).
+// D += A B for one m16n8k16 tile (fp16 or, BF, bf16 inputs; FP32
+// accumulators).
+template <bool BF>
 __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
                                          uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-        "{%8, %9}, {%0, %1, %2, %3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    if constexpr (BF) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+            "{%8, %9}, {%0, %1, %2, %3};"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    } else {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+            "{%8, %9}, {%0, %1, %2, %3};"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    }
+}
+
+// x = hi + mid + lo exactly with bf16 parts (8 significant bits each;
+// bf16 has the FP32 exponent range, so no scaling).  Returns part k.
+__device__ __forceinline__ uint16_t split_bf16_part(float x, int k) {
+    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(hi);
+    const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
+    return __bfloat16_as_ushort(k == 0 ? hi : (k == 1 ? mid : lo));
 }
 
 __device__ __forceinline__ void named_bar_arrive(int id, int count) {
@@ -118,7 +139,10 @@ __device__ __forceinline__ uint32_t mask_pair(uint32_t v, int i0, int lim) {
     return v & ((i0 < lim ? 0x0000FFFFu : 0u) | (i0 + 1 < lim ? 0xFFFF0000u : 0u));
 }
 
-template <int TPW>
+// BF: the A plane is bf16 (an FP32_BF16 wh plane read in place) and p, ut
+// enter as three exact bf16 parts (columns 0-2 of B1 / B2) instead of the
+// scaled fp16 pair; the running exponent is not needed.
+template <int TPW, bool BF>
 __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassParams T) {
     const FusedParams& P = T.f;
     if (P.skip && *P.skip) return;
@@ -127,7 +151,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
     __shared__ __align__(8) uint64_t full[kMmaMaxStages];
     __shared__ __align__(8) uint64_t empty[kMmaMaxStages];
     __shared__ float2 red[2][kMmaWarps][kMmaRows];    // partial dots (hi, lo) per warp
-    __shared__ __align__(4) __half ub[2][2][kMmaRows];  // B2: ut_hi, ut_lo of a stage
+    __shared__ float red3[2][kMmaWarps][kMmaRows];    // BF: the third part's partial dots
+    __shared__ __align__(4) uint16_t ub[2][3][kMmaRows];  // B2: the parts of ut of a stage
     __shared__ int e_move[2];                         // the running exponent's last move
     __shared__ int e_final;                           // the running exponent at the end
     __shared__ float pmax_w[kMmaWarps + 2];
@@ -176,8 +201,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
     float pmax = 0.0f;
 #pragma unroll
     for (int w = 0; w < kMmaWarps + 2; ++w) pmax = fmaxf(pmax, pmax_w[w]);
-    // 2^sp brings max|p| to [2^13, 2^14)
-    const int sp = pmax > 0.0f ? 13 - ilogbf(pmax) : 0;
+    // 2^sp brings max|p| to [2^13, 2^14) (fp16 only)
+    const int sp = (!BF && pmax > 0.0f) ? 13 - ilogbf(pmax) : 0;
 
     if (warp == kMmaProducer) {
         // ---------------------------------------------------------- producer
@@ -236,27 +261,38 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
             named_bar_sync(1 + b, kBar);  // partials of stage t are in
             float ut = 0.0f;
             if (has) {
-                double hs = 0.0, ls = 0.0;
+                double hs = 0.0, ls = 0.0, ts = 0.0;
 #pragma unroll
                 for (int w = 0; w < kMmaWarps; ++w) {
                     const float2 v = red[b][w][lane];
                     hs += (double)v.x;
                     ls += (double)v.y;
+                    if (BF) ts += (double)red3[b][w][lane];
                 }
-                const double dot = ldexp(hs + ls * (1.0 / 2048.0), -sp);
+                const double dot = BF ? hs + ls + ts : ldexp(hs + ls * (1.0 / 2048.0), -sp);
                 ut = (float)(cp * dot + cu * (double)ucur);
                 P.u_out[i] = ut;
                 ss += (double)ut * (double)ut;
             }
-            float m = fabsf(ut);
+            int e_new = e_cur;
+            if constexpr (BF) {
+                if (lane < kMmaRows) {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            const int e_new = m > 0.0f ? max(e_cur, ilogbf(m) + 1) : e_cur;
-            if (lane < kMmaRows) {
-                __half hi = __float2half_rn(0.0f), lo = hi;
-                if (e_new > -1000) split_half(ut, 14 - e_new, hi, lo);
-                ub[b][0][lane] = hi;
-                ub[b][1][lane] = lo;
+                    for (int k = 0; k < 3; ++k) ub[b][k][lane] = split_bf16_part(ut, k);
+                }
+                e_new = 14;  // no scaling: q = the sum of D2's columns
+                e_cur = 14;
+            } else {
+                float m = fabsf(ut);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                e_new = m > 0.0f ? max(e_cur, ilogbf(m) + 1) : e_cur;
+                if (lane < kMmaRows) {
+                    __half hi = __float2half_rn(0.0f), lo = hi;
+                    if (e_new > -1000) split_half(ut, 14 - e_new, hi, lo);
+                    ub[b][0][lane] = __half_as_ushort(hi);
+                    ub[b][1][lane] = __half_as_ushort(lo);
+                }
             }
             if (lane == 0) e_move[b] = e_new - e_cur;
             e_cur = e_new;
@@ -273,7 +309,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
         // ------------------------------------------------------------ MMA
         const int g = lane >> 2, tq = lane & 3;
         // B1 fragments of this warp's k-tiles: lanes 0-3 carry p_hi, lanes
-        // 4-7 p_lo, the rest (columns 2..7 of B1) zero.
+        // 4-7 p_lo (BF: lanes 8-11 the third part), the rest zero.
+        constexpr int NPART = BF ? 3 : 2;
         uint32_t b1[TPW][2];
 #pragma unroll
         for (int tt = 0; tt < TPW; ++tt) {
@@ -281,17 +318,21 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 uint32_t v = 0;
-                if (g < 2 && kt < ktiles) {
-                    __half e2[2];
+                if (g < NPART && kt < ktiles) {
+                    uint16_t e2[2];
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const int64_t col = (int64_t)kt * 16 + 8 * h + 2 * tq + q;
                         const float x = col < n ? __ldg(P.p + col) : 0.0f;
-                        __half hi, lo;
-                        split_half(x, sp, hi, lo);
-                        e2[q] = g == 0 ? hi : lo;
+                        if constexpr (BF) {
+                            e2[q] = split_bf16_part(x, g);
+                        } else {
+                            __half hi, lo;
+                            split_half(x, sp, hi, lo);
+                            e2[q] = __half_as_ushort(g == 0 ? hi : lo);
+                        }
                     }
-                    v = pack_half2(e2[0], e2[1]);
+                    v = (uint32_t)e2[0] | ((uint32_t)e2[1] << 16);
                 }
                 b1[tt][h] = v;
             }
@@ -328,7 +369,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                     for (int q = 0; q < 4; ++q) d2[tt][q] *= f;
             }
             uint32_t bb0 = 0, bb1 = 0;
-            if (g < 2) {
+            if (g < NPART) {
                 bb0 = *reinterpret_cast<const uint32_t*>(&ub[b][g][2 * tq]);
                 bb1 = *reinterpret_cast<const uint32_t*>(&ub[b][g][2 * tq + 8]);
             }
@@ -340,7 +381,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                     if (mt < ktiles) {
                         uint32_t a[4];
                         ldsm_x4_t(st + off2 + (uint32_t)(mt * 32), a);
-                        mma16816(d2[tt], a, bb0, bb1);
+                        mma16816<BF>(d2[tt], a, bb0, bb1);
                     }
                 }
             } else if (!failed) {
@@ -356,7 +397,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                         a[1] = mask_pair(a[1], 2 * tq, rv);
                         a[2] = mask_pair(a[2], 2 * tq + 8, rv);
                         a[3] = mask_pair(a[3], 2 * tq + 8, rv);
-                        mma16816(d2[tt], a, bb0, bb1);
+                        mma16816<BF>(d2[tt], a, bb0, bb1);
                     }
                 }
             }
@@ -383,15 +424,19 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                         uint32_t a[4];
                         ldsm_x4(st + off1 + (uint32_t)(kt * 32), a);
                         if (tt & 1)
-                            mma16816(d1b, a, b1[tt][0], b1[tt][1]);
+                            mma16816<BF>(d1b, a, b1[tt][0], b1[tt][1]);
                         else
-                            mma16816(d1, a, b1[tt][0], b1[tt][1]);
+                            mma16816<BF>(d1, a, b1[tt][0], b1[tt][1]);
                     }
                 }
             }
             if (tq == 0) {
                 red[t & 1][warp][g] = make_float2(d1[0] + d1b[0], d1[1] + d1b[1]);
                 red[t & 1][warp][g + 8] = make_float2(d1[2] + d1b[2], d1[3] + d1b[3]);
+            }
+            if (BF && tq == 1) {  // column 2: the third part
+                red3[t & 1][warp][g] = d1[0] + d1b[0];
+                red3[t & 1][warp][g + 8] = d1[2] + d1b[2];
             }
             named_bar_arrive(1 + (t & 1), kBar);
             if (t > 0) product2(t - 1, prev_slot, rows_of(t - 1));
@@ -411,10 +456,18 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
 #pragma unroll
         for (int tt = 0; tt < TPW; ++tt) {
             const int mt = warp * TPW + tt;
+            // BF: column 2 (the third part) sits in the lane with tq == 1
+            const float t0 = __shfl_down_sync(0xffffffffu, d2[tt][0], 1);
+            const float t2 = __shfl_down_sync(0xffffffffu, d2[tt][2], 1);
             if (tq == 0 && mt < ktiles) {
                 const int64_t c0 = (int64_t)mt * 16 + g;
-                if (c0 < n) qout[c0] = (d2[tt][0] + d2[tt][1] * (1.0f / 2048.0f)) * qs;
-                if (c0 + 8 < n) qout[c0 + 8] = (d2[tt][2] + d2[tt][3] * (1.0f / 2048.0f)) * qs;
+                if constexpr (BF) {
+                    if (c0 < n) qout[c0] = (d2[tt][0] + d2[tt][1]) + t0;
+                    if (c0 + 8 < n) qout[c0 + 8] = (d2[tt][2] + d2[tt][3]) + t2;
+                } else {
+                    if (c0 < n) qout[c0] = (d2[tt][0] + d2[tt][1] * (1.0f / 2048.0f)) * qs;
+                    if (c0 + 8 < n) qout[c0 + 8] = (d2[tt][2] + d2[tt][3] * (1.0f / 2048.0f)) * qs;
+                }
             }
         }
     }
