@@ -44,8 +44,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--m", type=int, default=M_DEF)
-    ap.add_argument("--n", type=int, default=N_DEF)
+    ap.add_argument("--m", "--rows", dest="m", type=int, default=M_DEF)
+    ap.add_argument("--n", "--cols", dest="n", type=int, default=N_DEF)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-rows", type=int, default=200_000)
@@ -58,6 +58,18 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def max_over_ranks(values, device):
+    """Each value's maximum over the ranks of the process group (every rank
+    takes part; a single process gets its own values back)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
 
 
 def measured_peak():
@@ -240,10 +252,7 @@ def run_ours(args):
                                           args.steps, args.warmup)
         nvtx.range_pop()
     barrier()
-    if world > 1:
-        t = torch.tensor([ms_packed, ms_fp32], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_packed, ms_fp32 = t.tolist()
+    ms_packed, ms_fp32 = max_over_ranks([ms_packed, ms_fp32], "cuda")
 
     # accurate backward errors of the returned solutions (FP64, exact A):
     # eta_D of the column-scaled problem (the convergence measure) and the
@@ -297,10 +306,7 @@ def run_ours(args):
         e2e_ms, _ = time_steps(torch, e2e_step, args.e2e_steps, args.warmup)
         nvtx.range_pop()
         barrier()
-        if world > 1:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = t.item()
+        e2e_ms = max_over_ranks([e2e_ms], "cuda")[0]
         e2e = {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 4 * m * n + 4 * m,
                "d2h_bytes_per_step": 4 * n}
 
