@@ -161,6 +161,26 @@ def test_qr_ill_conditioned_panel():
     assert np.allclose(np.tril(Rinv, -1), 0) and np.all(np.isfinite(Rinv))
 
 
+@pytest.mark.parametrize("k,n", [(3000, 1600), (1700, 1700)])
+def test_qr_blocked_ill_conditioned_panel_and_square(k, n):
+    """The blocked QR (256-column blocks) with a near-duplicate column pair
+    inside its third block (one 32-column panel), which takes the Householder
+    column steps
+    and hands its T to the block's merge; square at 1700.  R is backward
+    stable and keeps LAPACK's diagonal signs before the near-duplicate."""
+    rng = np.random.default_rng(k + n)
+    SA = rng.standard_normal((k, n)) * np.logspace(0, 2, n)
+    # columns 705 and 709 share the 32-column panel at 704
+    SA[:, 709] = SA[:, 705] * (1.0 + 1e-10) + 1e-11 * np.abs(SA[:, 705]).max() * rng.standard_normal(k)
+    Rinv, R = qr_on_gpu(SA)
+    Rl = np.linalg.qr(SA, mode="r")
+    np.testing.assert_allclose(R[:, :709], Rl[:, :709], rtol=1e-8, atol=1e-9 * np.abs(Rl).max())
+    assert np.array_equal(np.sign(np.diag(R))[:709], np.sign(np.diag(Rl))[:709])
+    G = SA.T @ SA
+    assert np.abs(R.T @ R - G).max() <= 1e-12 * np.abs(G).max()
+    assert np.allclose(np.tril(Rinv, -1), 0) and np.all(np.isfinite(Rinv))
+
+
 def test_qr_rejects_wide_and_singular():
     with pytest.raises(tb.TomosError):
         qr_on_gpu(np.ones((3, 5)))
