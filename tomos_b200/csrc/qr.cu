@@ -145,12 +145,19 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
                  : "d"(a), "d"(b));
 }
 
+// Row stride (doubles) of the shared 32 x 32 tiles the trailing update reads
+// as m8n8k4 fragments (V, T, the Gram tile).  A fragment read touches word
+// 36 r + c for lane (r, c) in {0..3} x {0..3} (+ a constant); 36 = 4 mod 16
+// puts the 16 lanes of each half-warp on 16 distinct 8-byte banks, either way
+// round (a stride of 33 left up to four lanes on one bank).
+constexpr int kQrVs = kHB + 4;
+
 // Gram partials of the first panel: tile `tile` sums rows [256 t, 256 t + 256).
 // Shared tiles of the phase functions below, carved from `sm` (dynamic
 // shared memory of the calling kernel, 16-byte aligned).
 // (the trailing update's W, T^T W and T tiles plus its copy stages)
 constexpr int kQrTileSmemDoubles =
-    2 * kHB * (kQrWc + 2) + kHB * (kHB + 1) + 3 * (kHB * (kHB + 1) + kHB * (kQrWc + 2));
+    2 * kHB * (kQrWc + 2) + kHB * kQrVs + 3 * (kHB * kQrVs + kHB * (kQrWc + 2));
 
 __device__ void qr_gram_tile(const double* A, int64_t ld, int64_t k, int nb, int tile, double* Gp,
                              double* sm) {
@@ -190,7 +197,7 @@ __global__ void __launch_bounds__(kQrThreads) qr_gram_kernel(const double* A, in
 constexpr int kQrWs = kQrWc + 2;
 // Sub-tiles (32 rows of V and of C) in flight in the trailing update.
 constexpr int kQrStages = 3;
-constexpr int kQrStageDoubles = kHB * (kHB + 1) + kHB * kQrWs;
+constexpr int kQrStageDoubles = kHB * kQrVs + kHB * kQrWs;
 
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src),
@@ -210,8 +217,8 @@ __device__ __forceinline__ void cp_async_wait() {
 // past nc read as zeros.  One asynchronous copy group per call.
 __device__ __forceinline__ void qr_issue_vc(const double* A, int64_t ld, int64_t j0, int nb, int64_t nc,
                                             int64_t c0, int64_t rt, int64_t r1, double* stage) {
-    double (*Vs)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
-    double (*Cs)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * (kHB + 1));
+    double (*Vs)[kQrVs] = reinterpret_cast<double (*)[kQrVs]>(stage);
+    double (*Cs)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * kQrVs);
     const int t = threadIdx.x;
 #pragma unroll
     for (int i = 0; i < kHB * kHB / kQrThreads; ++i) {
@@ -233,7 +240,7 @@ __device__ __forceinline__ void qr_issue_vc(const double* A, int64_t ld, int64_t
 // The panel's first 32 rows of V: unit diagonal, zeros above it.
 __device__ __forceinline__ void qr_fix_v(double* stage, int64_t rt) {
     if (rt != 0) return;
-    double (*Vs)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
+    double (*Vs)[kQrVs] = reinterpret_cast<double (*)[kQrVs]>(stage);
     for (int e = threadIdx.x; e < kHB * kHB; e += kQrThreads) {
         const int r = e & 31, aa = e >> 5;
         if (r <= aa) Vs[r][aa] = r == aa ? 1.0 : 0.0;
@@ -277,8 +284,8 @@ __device__ void qr_w_part_tile(const double* A, int64_t ld, int64_t k, int64_t n
             qr_fix_v(stage, rt);
             __syncthreads();
         }
-        double (*Vt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
-        double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * (kHB + 1));
+        double (*Vt)[kQrVs] = reinterpret_cast<double (*)[kQrVs]>(stage);
+        double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * kQrVs);
 #pragma unroll
         for (int ks = 0; ks < kHB / 4; ++ks) {
             const double b = Ct[4 * ks + q][cw + g];  // B[k][c] = C(row, col)
@@ -324,9 +331,9 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
                               double* Gp_next, int ct, int rtile, int row_tile, double* sm) {
     double (*W0)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm);
     double (*Wt)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(sm + kHB * kQrWs);
-    double (*Tt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(sm + 2 * kHB * kQrWs);
-    double (*Gt)[kHB + 1] = Tt;  // the Gram tile reuses T's storage
-    double* stages = sm + 2 * kHB * kQrWs + kHB * (kHB + 1);
+    double (*Tt)[kQrVs] = reinterpret_cast<double (*)[kQrVs]>(sm + 2 * kHB * kQrWs);
+    double (*Gt)[kQrVs] = Tt;  // the Gram tile reuses T's storage
+    double* stages = sm + 2 * kHB * kQrWs + kHB * kQrVs;
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5, g = lane >> 2, q = lane & 3;
     const int cw = warp * 8;
@@ -343,30 +350,52 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
         if (i < nsub) qr_issue_vc(A, ld, j0, nb, nc, c0, r0 + (int64_t)i * kHB, r1, stages + i * kQrStageDoubles);
         else cp_async_commit();
     }
-    for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
-        const int aa = e / kQrWc, c = e % kQrWc;
+    // W: thread t sums column t % 64 of reflectors t / 64 + 4 i (i < 8), the
+    // chunk partials in order, one chunk's eight loads in flight at a time
+    {
+        constexpr int kPer = kHB * kQrWc / kQrThreads;
+        const int c = t % kQrWc, a0 = t / kQrWc;
         const int64_t col = c0 + c;
-        double part[kQrChunks];
+        double w[kPer];
 #pragma unroll
-        for (int qq = 0; qq < kQrChunks; ++qq)
-            part[qq] = (qq < nchunks && aa < nb && col < nc)
-                           ? __ldcg(Wp + ((size_t)qq * kHB + aa) * (size_t)nc + col)
-                           : 0.0;
-        double sum = 0.0;
+        for (int i = 0; i < kPer; ++i) w[i] = 0.0;
+        for (int qq = 0; qq < nchunks; ++qq) {
+            double v[kPer];
 #pragma unroll
-        for (int qq = 0; qq < kQrChunks; ++qq) sum += part[qq];
-        W0[aa][c] = sum;
+            for (int i = 0; i < kPer; ++i) {
+                const int aa = a0 + i * (kQrThreads / kQrWc);
+                v[i] = (aa < nb && col < nc) ? __ldcg(Wp + ((size_t)qq * kHB + aa) * (size_t)nc + col) : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < kPer; ++i) w[i] += v[i];
+        }
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) W0[a0 + i * (kQrThreads / kQrWc)][c] = w[i];
     }
     for (int e = t; e < kHB * kHB; e += kQrThreads) {
         const int aa = e & 31, b = e >> 5;
         Tt[aa][b] = (aa < nb && b < nb) ? __ldcg(T + (size_t)b * nb + aa) : 0.0;  // T(aa, b)
     }
     __syncthreads();
-    for (int e = t; e < kHB * kQrWc; e += kQrThreads) {
-        const int b = e / kQrWc, c = e % kQrWc;
-        double sum = 0.0;
-        for (int aa = 0; aa <= b; ++aa) sum += Tt[aa][b] * W0[aa][c];
-        Wt[b][c] = sum;
+    // T^T W on the tensor cores: warp w, all 32 rows x columns 8w..8w+7;
+    // A[b][aa] = T(aa, b) for aa <= b (T is upper triangular), B = W
+    {
+        double tw[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+        for (int ks = 0; ks < kHB / 4; ++ks) {
+            const int aa = 4 * ks + q;
+            const double bw = W0[aa][cw + g];
+#pragma unroll
+            for (int blk = 0; blk < 4; ++blk) {
+                const int b = 8 * blk + g;
+                dmma884(tw[blk][0], tw[blk][1], aa <= b ? Tt[aa][b] : 0.0, bw);
+            }
+        }
+#pragma unroll
+        for (int blk = 0; blk < 4; ++blk) {
+            Wt[8 * blk + g][cw + 2 * q] = tw[blk][0];
+            Wt[8 * blk + g][cw + 2 * q + 1] = tw[blk][1];
+        }
     }
     const bool gram = Gp_next != nullptr && ct == 0;
     // Gram tiles of warp w: rows 8 (w / 2) .., columns 8 (2 (w % 2) + {0, 1}) ..
@@ -387,8 +416,8 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
             qr_fix_v(stage, rt);
             __syncthreads();
         }
-        double (*Vt)[kHB + 1] = reinterpret_cast<double (*)[kHB + 1]>(stage);
-        double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * (kHB + 1));
+        double (*Vt)[kQrVs] = reinterpret_cast<double (*)[kQrVs]>(stage);
+        double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * kQrVs);
         double cur[8];
 #pragma unroll
         for (int blk = 0; blk < 4; ++blk) {
