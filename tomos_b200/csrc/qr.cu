@@ -250,8 +250,8 @@ __device__ __forceinline__ void qr_fix_v(double* stage, int64_t rt) {
 // W partials: Wp[chunk][a][c] = sum over the chunk's rows of V(i, a) C(i, c),
 // C the trailing columns j0 + nb + c.  A CTA: one row chunk x 64 columns,
 // 32-row sub-tiles streamed through kQrStages shared-memory stages by
-// asynchronous copies; warp w: all 32 reflectors x columns 8w..8w+7 as four
-// m8n8 FP64 tensor-core tiles, 4 rows of a sub-tile per step.
+// asynchronous copies; warp w: all 32 reflectors x columns 8w..8w+7 as two
+// m16n8 FP64 tensor-core tiles, 8 rows of a sub-tile per step.
 __device__ void qr_w_part_tile(const double* A, int64_t ld, int64_t k, int64_t n, int64_t j0, int nb,
                                int64_t chunk_rows, double* Wp, int ct, int rc, double* sm) {
     const int t = threadIdx.x;
@@ -263,7 +263,7 @@ __device__ void qr_w_part_tile(const double* A, int64_t ld, int64_t k, int64_t n
     int64_t r1 = r0 + chunk_rows;
     if (r1 > krem) r1 = krem;
     const int nsub = r1 > r0 ? (int)((r1 - r0 + kHB - 1) / kHB) : 0;
-    double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
     __syncthreads();  // a previous tile of this CTA may still read the stages
 #pragma unroll
     for (int i = 0; i < kQrStages - 1; ++i) {
@@ -287,26 +287,32 @@ __device__ void qr_w_part_tile(const double* A, int64_t ld, int64_t k, int64_t n
         double (*Vt)[kQrVs] = reinterpret_cast<double (*)[kQrVs]>(stage);
         double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * kQrVs);
 #pragma unroll
-        for (int ks = 0; ks < kHB / 4; ++ks) {
-            const double b = Ct[4 * ks + q][cw + g];  // B[k][c] = C(row, col)
+        for (int ks = 0; ks < kHB / 8; ++ks) {
+            const int k0 = 8 * ks + q;
+            const double b[2] = {Ct[k0][cw + g], Ct[k0 + 4][cw + g]};  // B[k][c] = C(row, col)
 #pragma unroll
-            for (int blk = 0; blk < 4; ++blk)
-                dmma884(acc[blk][0], acc[blk][1], Vt[4 * ks + q][8 * blk + g], b);  // A[a][k] = V(row, a)
+            for (int mb = 0; mb < 2; ++mb) {
+                const int m0 = 16 * mb + g;
+                const double a[4] = {Vt[k0][m0], Vt[k0][m0 + 8], Vt[k0 + 4][m0], Vt[k0 + 4][m0 + 8]};  // A[a][k] = V(row, a)
+                g_dmma1688(acc[mb], a, b);
+            }
         }
         __syncthreads();  // the stage is refilled two sub-tiles on
     }
     cp_async_wait<0>();
 #pragma unroll
-    for (int blk = 0; blk < 4; ++blk) {
-        const int aa = 8 * blk + g;
-        if (aa >= nb) continue;
-        double* out = Wp + ((size_t)rc * kHB + aa) * (size_t)nc;
+    for (int mb = 0; mb < 2; ++mb)
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            const int64_t col = c0 + cw + 2 * q + u;
-            if (col < nc) out[col] = acc[blk][u];
+        for (int h = 0; h < 2; ++h) {
+            const int aa = 16 * mb + 8 * h + g;
+            if (aa >= nb) continue;
+            double* out = Wp + ((size_t)rc * kHB + aa) * (size_t)nc;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int64_t col = c0 + cw + 2 * q + u;
+                if (col < nc) out[col] = acc[mb][2 * h + u];
+            }
         }
-    }
     __syncthreads();
 }
 
@@ -321,11 +327,11 @@ __global__ void __launch_bounds__(kQrThreads) qr_w_part_kernel(const double* A, 
 // C -= V (T^T W) on one tile of 256 rows x 64 trailing columns, W the
 // fixed-order sum of the chunk partials.  The 32-row sub-tiles of V and C
 // stream through kQrStages shared-memory stages by asynchronous copies;
-// warp w: the 32 rows of a sub-tile x columns 8w..8w+7 as four m8n8 FP64
+// warp w: the 32 rows of a sub-tile x columns 8w..8w+7 as two m16n8 FP64
 // tensor-core tiles (C the accumulator, A = -V, B = T^T W).  Tiles holding
 // the next panel's columns (column tile 0) then write that panel's Gram
 // partial over their rows below the current panel (rows j0 + nb on),
-// again on the tensor cores.
+// again on the tensor cores (warp w: one 16 x 8 tile of the 32 x 32 Gram).
 __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64_t j0, int nb,
                               int nchunks, const double* Wp, const double* T, int nb_next,
                               double* Gp_next, int ct, int rtile, int row_tile, double* sm) {
@@ -398,9 +404,9 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
         }
     }
     const bool gram = Gp_next != nullptr && ct == 0;
-    // Gram tiles of warp w: rows 8 (w / 2) .., columns 8 (2 (w % 2) + {0, 1}) ..
-    const int gab = warp >> 1, gbb = 2 * (warp & 1);
-    double gacc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    // Gram tile of warp w: rows 16 (w / 4) .., columns 8 (w % 4) ..
+    const int gmb = warp >> 2, gnb = warp & 3;
+    double gacc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = 0; i < nsub; ++i) {
         const int ni = i + kQrStages - 1;
         if (ni < nsub)
@@ -418,6 +424,8 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
         }
         double (*Vt)[kQrVs] = reinterpret_cast<double (*)[kQrVs]>(stage);
         double (*Ct)[kQrWs] = reinterpret_cast<double (*)[kQrWs]>(stage + kHB * kQrVs);
+        // cur[2 blk + u] = C(8 blk + g, cw + 2q + u): rows 16 mb + g and
+        // 16 mb + g + 8 of m16n8 tile mb are cur[4 mb + {0, 1}], cur[4 mb + {2, 3}]
         double cur[8];
 #pragma unroll
         for (int blk = 0; blk < 4; ++blk) {
@@ -425,11 +433,15 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
             cur[2 * blk + 1] = Ct[8 * blk + g][cw + 2 * q + 1];
         }
 #pragma unroll
-        for (int ks = 0; ks < kHB / 4; ++ks) {
-            const double b = Wt[4 * ks + q][cw + g];  // B[a][c] = (T^T W)(a, col)
+        for (int ks = 0; ks < kHB / 8; ++ks) {
+            const int k0 = 8 * ks + q;
+            const double b[2] = {Wt[k0][cw + g], Wt[k0 + 4][cw + g]};  // B[a][c] = (T^T W)(a, col)
 #pragma unroll
-            for (int blk = 0; blk < 4; ++blk)
-                dmma884(cur[2 * blk], cur[2 * blk + 1], -Vt[8 * blk + g][4 * ks + q], b);  // A = -V
+            for (int mb = 0; mb < 2; ++mb) {
+                const int m0 = 16 * mb + g;
+                const double a[4] = {-Vt[m0][k0], -Vt[m0 + 8][k0], -Vt[m0][k0 + 4], -Vt[m0 + 8][k0 + 4]};  // A = -V
+                g_dmma1688(&cur[4 * mb], a, b);
+            }
         }
 #pragma unroll
         for (int blk = 0; blk < 4; ++blk) {
@@ -447,11 +459,11 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
         if (gram) {
             __syncthreads();
 #pragma unroll
-            for (int ks = 0; ks < kHB / 4; ++ks) {
-                const double a = Gt[4 * ks + q][8 * gab + g];  // A[a][r] = C(r, a)
-#pragma unroll
-                for (int bb = 0; bb < 2; ++bb)
-                    dmma884(gacc[bb][0], gacc[bb][1], a, Gt[4 * ks + q][8 * (gbb + bb) + g]);
+            for (int ks = 0; ks < kHB / 8; ++ks) {
+                const int k0 = 8 * ks + q, m0 = 16 * gmb + g;
+                const double a[4] = {Gt[k0][m0], Gt[k0][m0 + 8], Gt[k0 + 4][m0], Gt[k0 + 4][m0 + 8]};  // A[a][r] = C(r, a)
+                const double b[2] = {Gt[k0][8 * gnb + g], Gt[k0 + 4][8 * gnb + g]};
+                g_dmma1688(gacc, a, b);
             }
         }
         __syncthreads();  // the stage is refilled two sub-tiles on; Gt rewritten
@@ -459,11 +471,11 @@ __device__ void qr_apply_tile(double* A, int64_t ld, int64_t k, int64_t n, int64
     cp_async_wait<0>();
     if (gram) {
 #pragma unroll
-        for (int bb = 0; bb < 2; ++bb)
+        for (int h = 0; h < 2; ++h)
 #pragma unroll
             for (int u = 0; u < 2; ++u)
-                Gp_next[(size_t)rtile * kHB * kHB + (8 * gab + g) * kHB + 8 * (gbb + bb) + 2 * q + u] =
-                    gacc[bb][u];
+                Gp_next[(size_t)rtile * kHB * kHB + (16 * gmb + 8 * h + g) * kHB + 8 * gnb + 2 * q + u] =
+                    gacc[2 * h + u];
     }
     __syncthreads();
 }
