@@ -286,7 +286,9 @@ typedef struct tomos_lsqr_opts {
                                 mtx_refine_precision (--explicit-duplicates):
                                 a copy of A at higher precision (FP32, or
                                 packed read exactly) that the initial and
-                                restart passes read instead of A            */
+                                restart passes read instead of A; it takes
+                                precedence over implicit_duplicate
+                                (lsqr.cpp:459-473)                          */
 } tomos_lsqr_opts;
 
 typedef struct tomos_lsqr_report {

@@ -143,6 +143,30 @@ def test_explicit_duplicates_relres_restarts(orc):
     assert err[False] > 10 * err[True], err
 
 
+def test_explicit_duplicate_takes_precedence_over_implicit():
+    """With both an explicit FP32 copy and the workspace's implicit duplicate
+    set, the restart residual reads the explicit copy (lsqr.cpp:459-473
+    tests it first): the solve is the explicit-duplicate solve, bit for bit,
+    and differs from the implicit-duplicate one."""
+    rng = np.random.default_rng(11)
+    m, n = 20000, 120
+    A0 = rng.standard_normal((m, n)).astype(np.float32)
+    b = cuda((A0.astype(np.float64) @ rng.standard_normal(n)).astype(np.float32))
+    A32 = to_dense(A0, L.COL_MAJOR)
+    P = tb.pack(A32, NT.FP32_16)
+    # a refine copy that is not A: the explicit and implicit residuals differ
+    R32 = to_dense((A0 * np.float32(1.001)).astype(np.float32), L.COL_MAJOR)
+    xs = {}
+    for name, implicit, refine in (("both", True, R32), ("explicit", False, R32), ("implicit", True, None)):
+        ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32)
+        ws.use_implicit_duplicate_ = implicit
+        x = torch.zeros(n, device="cuda")
+        tb.lsqr_solve(None, P, b, x, ws, 1e-7, 40, 1e-7, restarts=3, mtx_refine_precision=refine)
+        xs[name] = x.cpu().numpy()
+    assert np.array_equal(xs["both"], xs["explicit"])
+    assert not np.array_equal(xs["both"], xs["implicit"])
+
+
 def test_explicit_duplicates_errors():
     A = np.ones((100, 10), np.float32)
     A32 = to_dense(A, L.COL_MAJOR)
@@ -154,8 +178,3 @@ def test_explicit_duplicates_errors():
     with pytest.raises(tb.TomosError) as e:
         tb.lsqr_solve(None, A16, b, x, ws, 1e-6, 10, 1e-6, mtx_refine_precision=wrong)
     assert "size" in str(e.value)
-    P = tb.pack(A32, NT.FP32_16)
-    ws.use_implicit_duplicate_ = True
-    with pytest.raises(tb.TomosError) as e:
-        tb.lsqr_solve(None, P, b, x, ws, 1e-6, 10, 1e-6, mtx_refine_precision=A32)
-    assert "mutually exclusive" in str(e.value)

@@ -1340,12 +1340,11 @@ tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float*
         if (report) report->converged = 1;
         return TOMOS_OK;
     }
+    // An explicit duplicate takes precedence over the implicit one for the
+    // restart residual, as in the reference (lsqr.cpp:459-473: the explicit
+    // branch is tested first; lsqr_registries.cpp:102-112 sets both flags).
     if (opts->refine) {
         const tomos_dense* Rf = opts->refine;
-        if (opts->implicit_duplicate)
-            return fail(TOMOS_ERR_INVALID,
-                        "lsqr_solve: explicit (mtx_refine_precision) and implicit duplicates are "
-                        "mutually exclusive");
         if (!gemv_shape(Rf, TOMOS_NO_TRANSPOSE, &dot, &outer, &inner, &why))
             return fail(TOMOS_ERR_INVALID, "lsqr_solve: mtx_refine_precision: " + why);
         if (Rf->rows != A->rows || Rf->cols != A->cols || (!Rf->values && Rf->rows * Rf->cols > 0))
