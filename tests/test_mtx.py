@@ -156,3 +156,97 @@ def test_solve_from_mtx_files(tmp_path, orc):
         assert rep["converged"] == 1
         xx = x.cpu().numpy().astype(np.float64)
         assert np.linalg.norm(xx - xo) / np.linalg.norm(xo) < 1e-4
+
+
+# ---- the parallel `array` reader: byte ranges parsed by host threads ----
+
+THREADS = [1, 2, 3, 7, 64]
+
+
+def generator_values(m, n, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((m, n)) * 10.0 ** rng.uniform(-12, 12, (m, n))
+    A.ravel()[:4] = [-0.0, 5e-324, 1.0 / 3.0, -1e308]
+    return A
+
+
+@pytest.mark.parametrize("threads", THREADS)
+def test_array_parallel_bit_exact(tmp_path, monkeypatch, threads):
+    """Every thread count gives the sequential parse bit for bit: value t of
+    the file lands at (t % m, t / m) whichever range it was parsed in."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    A = generator_values(257, 13, threads)
+    p = matlab_style(tmp_path / "p.mtx", A)
+    want = np.array([float("%1.16e" % v) for v in A.ravel(order="F")]).reshape(A.shape, order="F")
+    for layout in (tb.Layout.COL_MAJOR, tb.Layout.ROW_MAJOR):
+        got = tb.read_mtx(p, layout)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), (threads, layout)
+
+
+@pytest.mark.parametrize("threads", THREADS)
+def test_array_parallel_layout_of_text(tmp_path, monkeypatch, threads):
+    """Several values a line, tabs, blank lines, CRLF endings and trailing
+    text past the last value read as the one-value-a-line file does."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((31, 9))
+    vals = ["%.17g" % v for v in A.ravel(order="F")]
+    out, k = [], 0
+    while k < len(vals):
+        w = int(rng.integers(1, 5))
+        sep = "\t" if rng.random() < 0.3 else "  "
+        out.append(sep.join(vals[k:k + w]) + ("\r" if rng.random() < 0.5 else ""))
+        if rng.random() < 0.2:
+            out.append("")
+        k += w
+    text = "%%MatrixMarket matrix array real general\n31 9\n" + "\n".join(out) + "\n7 8 9 extra\n"
+    p = write_text(tmp_path / "w.mtx", text)
+    assert np.array_equal(tb.read_mtx(p), A)
+
+
+@pytest.mark.parametrize("threads", THREADS)
+@pytest.mark.parametrize("sym", ["symmetric", "skew-symmetric"])
+def test_array_parallel_symmetric(tmp_path, monkeypatch, threads, sym):
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    rng = np.random.default_rng(7)
+    n = 40
+    L_ = np.tril(rng.standard_normal((n, n)), 0 if sym == "symmetric" else -1)
+    stored = [L_[i, j] for j in range(n) for i in range(j if sym == "symmetric" else j + 1, n)]
+    text = f"%%MatrixMarket matrix array real {sym}\n{n} {n}\n" + "\n".join("%.17g" % v for v in stored) + "\n"
+    p = write_text(tmp_path / "s.mtx", text)
+    want = L_ + (L_.T if sym == "symmetric" else -L_.T)
+    if sym == "symmetric":
+        want[np.diag_indices(n)] = np.diag(L_)
+    got = tb.read_mtx(p)
+    assert np.array_equal(got, want)
+    assert np.array_equal(got, scipy.io.mmread(p))
+
+
+@pytest.mark.parametrize("threads", THREADS)
+def test_array_parallel_errors(tmp_path, monkeypatch, threads):
+    """A value short, or a malformed value in the middle of the file, is
+    reported whichever range holds it."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    vals = ["%.17g" % v for v in np.arange(1.0, 601.0)]
+    head = "%%MatrixMarket matrix array real general\n20 30\n"
+    short = write_text(tmp_path / "short.mtx", head + "\n".join(vals[:-1]) + "\n")
+    bad_vals = list(vals)
+    bad_vals[377] = "1.5e"
+    bad = write_text(tmp_path / "bad.mtx", head + "\n".join(bad_vals) + "\n")
+    for p in (short, bad):
+        with pytest.raises(tb.TomosError) as e:
+            tb.read_mtx(p)
+        assert e.value.code == C.TOMOS_ERR_INVALID and "truncated/malformed data" in str(e.value)
+    ok = write_text(tmp_path / "ok.mtx", head + "\n".join(vals) + "\nnot-a-number\n")
+    assert np.array_equal(tb.read_mtx(ok), np.arange(1.0, 601.0).reshape(20, 30, order="F"))
+
+
+def test_array_parallel_large_default_threads(tmp_path, monkeypatch):
+    """A ~15 MB generator file (several ranges at the default thread count)
+    reads bit-exactly."""
+    monkeypatch.delenv("TOMOS_MTX_THREADS", raising=False)
+    A = generator_values(3000, 200, 11)
+    p = matlab_style(tmp_path / "big.mtx", A)
+    want = np.array([float("%1.16e" % v) for v in A.ravel(order="F")]).reshape(A.shape, order="F")
+    got = tb.read_mtx(p)
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))

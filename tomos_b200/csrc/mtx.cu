@@ -14,12 +14,30 @@
 // Errors use the runner's wording ("could not open", "not a valid
 // MatrixMarket file", "could not read array size", "truncated/malformed
 // data").
+//
+// `array` files (the generator's format: one value per line, ~24 bytes a
+// value, 24 GB for a 1e6 x 1000 system) are parsed by host threads over a
+// read-only mapping of the file: the data section is cut into byte ranges,
+// each thread counts the tokens that start in its range, a prefix sum gives
+// every range its first value index, and each thread then parses its tokens
+// with strtod.  Value t of the file sits at a position fixed by t alone, so
+// every element is written exactly once and the result is the sequential
+// read's bit for bit.  `coordinate` files stay sequential (repeated entries
+// add in file order).  TOMOS_MTX_THREADS sets the thread count.
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
 #include <cctype>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "common.cuh"
 #include "tomos_b200.h"
@@ -153,6 +171,147 @@ tomos_status mtx_entries(MtxFile& m, const char* path, Fn&& fn) {
     return TOMOS_OK;
 }
 
+inline bool is_space(char c) { return c == ' ' || c == '\n' || c == '\t' || c == '\r' || c == '\f' || c == '\v'; }
+
+// Parses one whitespace-free token [p, e) as a double, as strtod on the
+// token alone; false if it is not entirely a number (or longer than 127
+// characters, the sequential reader's token limit).
+bool parse_token(const char* p, const char* e, double* v) {
+    const size_t n = (size_t)(e - p);
+    if (n == 0 || n > 127) return false;
+    char tok[128];
+    std::memcpy(tok, p, n);
+    tok[n] = '\0';
+    char* end = nullptr;
+    *v = std::strtod(tok, &end);
+    return end == tok + n;
+}
+
+// Host threads for n bytes of values: TOMOS_MTX_THREADS when set (1..256),
+// else one per MiB up to the hardware threads.
+int parse_threads(size_t bytes) {
+    if (const char* e = std::getenv("TOMOS_MTX_THREADS")) {
+        const long c = std::atol(e);
+        if (c >= 1) return (int)std::min(c, 256L);
+    }
+    long hw = (long)std::thread::hardware_concurrency();
+    if (hw < 1) hw = 1;
+    const long want = (long)(bytes >> 20) + 1;
+    return (int)std::max(1L, std::min(std::min(hw, want), 256L));
+}
+
+// The (row, col) of stored value t of an `array` file: column by column,
+// the whole column for general storage, rows j.. (symmetric) or j+1..
+// (skew-symmetric) of column j otherwise.
+struct ArrayPos {
+    int64_t rows, cols;
+    int32_t sym;
+    int64_t first(int64_t j) const {
+        return sym == TOMOS_MTX_GENERAL ? 0 : (sym == TOMOS_MTX_SYMMETRIC ? j : j + 1);
+    }
+    void at(int64_t t, int64_t* i, int64_t* j) const {
+        if (sym == TOMOS_MTX_GENERAL) {
+            *j = t / rows;
+            *i = t % rows;
+            return;
+        }
+        int64_t c = 0;
+        while (c < cols && t >= rows - first(c)) {
+            t -= rows - first(c);
+            ++c;
+        }
+        *j = c;
+        *i = first(c) + t;
+    }
+    void next(int64_t* i, int64_t* j) const {
+        if (++*i >= rows) {
+            ++*j;
+            *i = first(*j);
+            while (*j < cols && *i >= rows) {  // empty trailing columns of skew storage
+                ++*j;
+                *i = first(*j);
+            }
+        }
+    }
+};
+
+// The `array` values of the open file (positioned at its first value) into
+// at(i, j) (and its mirror for symmetric storage), in parallel.  Returns
+// false on a malformed token or too few values.
+template <class At>
+bool read_array_parallel(MtxFile& m, At&& at) {
+    const tomos_mtx_info& in = m.info;
+    const long off = std::ftell(m.f);
+    struct stat st;
+    if (off < 0 || fstat(fileno(m.f), &st) != 0) return false;
+    const size_t size = (size_t)st.st_size, start = (size_t)off;
+    const int64_t entries = in.entries;
+    if (entries == 0) return true;
+    if (start >= size) return false;
+    void* map = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fileno(m.f), 0);
+    if (map == MAP_FAILED) return false;
+    madvise(map, size, MADV_SEQUENTIAL);
+    const char* d = static_cast<const char*>(map);
+    const size_t bytes = size - start;
+    int nt = parse_threads(bytes);
+    std::vector<size_t> lo(nt), hi(nt);
+    for (int k = 0; k < nt; ++k) {
+        lo[k] = start + bytes * (size_t)k / (size_t)nt;
+        hi[k] = start + bytes * (size_t)(k + 1) / (size_t)nt;
+    }
+    auto starts_token = [&](size_t p) { return !is_space(d[p]) && (p == start || is_space(d[p - 1])); };
+    std::vector<int64_t> cnt(nt + 1, 0);
+    auto run = [&](auto&& body) {
+        std::vector<std::thread> th;
+        bool spawned = true;
+        for (int k = 1; k < nt && spawned; ++k) {
+            try {
+                th.emplace_back(body, k);
+            } catch (...) {
+                spawned = false;
+            }
+        }
+        const int done = (int)th.size() + 1;
+        body(0);
+        for (int k = done; k < nt; ++k) body(k);  // ranges no thread took
+        for (auto& t : th) t.join();
+    };
+    run([&](int k) {
+        int64_t c = 0;
+        for (size_t p = lo[k]; p < hi[k]; ++p) c += starts_token(p);
+        cnt[k + 1] = c;
+    });
+    for (int k = 0; k < nt; ++k) cnt[k + 1] += cnt[k];
+    bool ok = cnt[nt] >= entries;
+    std::atomic<bool> bad(false);
+    if (ok) {
+        const ArrayPos pos{in.rows, in.cols, in.symmetry};
+        run([&](int k) {
+            int64_t t = cnt[k];
+            if (t >= entries) return;
+            int64_t i, j;
+            pos.at(t, &i, &j);
+            for (size_t p = lo[k]; p < hi[k] && t < entries; ++p) {
+                if (!starts_token(p)) continue;
+                size_t e = p;
+                while (e < size && !is_space(d[e])) ++e;
+                double v;
+                if (!parse_token(d + p, d + e, &v)) {
+                    bad.store(true, std::memory_order_relaxed);
+                    return;
+                }
+                at(i, j, v);
+                ++t;
+                pos.next(&i, &j);
+                p = e;  // the loop's ++p then steps past the whitespace at e
+            }
+        });
+        ok = !bad.load();
+    }
+    munmap(map, size);
+    return ok;
+}
+
 }  // namespace
 
 extern "C" {
@@ -181,6 +340,14 @@ tomos_status tomos_mtx_read_dense(const char* path, int32_t layout, double* out,
     for (int64_t j = 0; j < in.cols; ++j)
         for (int64_t i = 0; i < in.rows; ++i) at(i, j) = 0.0;
     const int32_t sym = in.symmetry;
+    if (in.format == TOMOS_MTX_ARRAY) {
+        const bool ok = read_array_parallel(m, [&](int64_t i, int64_t j, double v) {
+            at(i, j) = v;
+            if (sym != TOMOS_MTX_GENERAL && i != j) at(j, i) = sym == TOMOS_MTX_SKEW ? -v : v;
+        });
+        if (!ok) return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': truncated/malformed data");
+        return TOMOS_OK;
+    }
     return mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
         if (in.format == TOMOS_MTX_COORDINATE) at(i, j) += v;  // repeated entries add
         else at(i, j) = v;
