@@ -250,3 +250,84 @@ def test_array_parallel_large_default_threads(tmp_path, monkeypatch):
     want = np.array([float("%1.16e" % v) for v in A.ravel(order="F")]).reshape(A.shape, order="F")
     got = tb.read_mtx(p)
     assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+def coordinate_text(rng, m, n, nnz, field, split_lines=False):
+    r = rng.integers(1, m + 1, nnz)
+    c = rng.integers(1, n + 1, nnz)
+    if field == "real":
+        vals = ["%.17g" % x for x in rng.standard_normal(nnz) * 10.0 ** rng.uniform(-5, 5, nnz)]
+    elif field == "integer":
+        vals = [str(int(x)) for x in rng.integers(-1000, 1000, nnz)]
+    else:
+        vals = [None] * nnz
+    lines = []
+    for a, b, v in zip(r, c, vals):
+        toks = [str(a), str(b)] + ([v] if v is not None else [])
+        if split_lines and rng.random() < 0.3:
+            lines.append(toks[0])
+            lines.append("  ".join(toks[1:]))
+        else:
+            lines.append("\t".join(toks) if rng.random() < 0.2 else " ".join(toks))
+    head = f"%%MatrixMarket matrix coordinate {field} general\n% comment\n{m} {n} {nnz}\n"
+    return head + "\n".join(lines) + "\n", r - 1, c - 1, vals
+
+
+@pytest.mark.parametrize("threads", THREADS)
+@pytest.mark.parametrize("field", ["real", "integer", "pattern"])
+def test_coordinate_parallel_triplets(tmp_path, monkeypatch, threads, field):
+    """General coordinate files read by every thread count give the file's
+    triplets in file order (entries whose tokens straddle two byte ranges or
+    two lines included)."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    rng = np.random.default_rng(threads)
+    text, r, c, vals = coordinate_text(rng, 70, 50, 900, field, split_lines=True)
+    p = write_text(tmp_path / "c.mtx", text)
+    gr, gc, gv = tb.read_mtx_coo(p)
+    assert np.array_equal(gr, r) and np.array_equal(gc, c)
+    want = np.ones(len(r)) if field == "pattern" else np.array([float(v) for v in vals])
+    assert np.array_equal(gv.view(np.uint64), want.view(np.uint64))
+    rp, ci, vv, size = tb.read_mtx_csr(p)
+    S = scipy.sparse.coo_matrix((want, (r, c)), shape=(70, 50)).tocsr()
+    S.sum_duplicates()
+    S.sort_indices()
+    assert size == (70, 50) and np.array_equal(rp, S.indptr) and np.array_equal(ci, S.indices)
+    np.testing.assert_allclose(vv, S.data, rtol=1e-15)
+
+
+@pytest.mark.parametrize("threads", THREADS)
+def test_coordinate_parallel_errors(tmp_path, monkeypatch, threads):
+    """The first bad entry in file order is the one reported, whichever
+    range holds it: out of the matrix (by its 1-based number), malformed,
+    or missing."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    rng = np.random.default_rng(9)
+    text, r, c, vals = coordinate_text(rng, 40, 30, 400, "real")
+    head, body = text.split("40 30 400\n")
+    lines = body.rstrip("\n").split("\n")
+
+    def with_lines(name, ls, nnz=400):
+        return write_text(tmp_path / name, head + f"40 30 {nnz}\n" + "\n".join(ls) + "\n")
+
+    out = list(lines)
+    out[250] = "41 3 1.0"
+    out[300] = "1 2 x"
+    p = with_lines("out.mtx", out)
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx_coo(p)
+    assert "entry 251 lies outside the matrix" in str(e.value)
+    mal = list(lines)
+    mal[120] = "3 4 1.0e"
+    mal[300] = "0 2 1.0"
+    p = with_lines("mal.mtx", mal)
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx_coo(p)
+    assert "truncated/malformed data" in str(e.value)
+    p = with_lines("short.mtx", lines[:-1])
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx_coo(p)
+    assert "truncated/malformed data" in str(e.value)
+    p = with_lines("idx.mtx", lines[:7] + ["3.0 4 1.0"] + lines[8:])
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx_coo(p)
+    assert "truncated/malformed data" in str(e.value)

@@ -22,8 +22,11 @@
 // every range its first value index, and each thread then parses its tokens
 // with strtod.  Value t of the file sits at a position fixed by t alone, so
 // every element is written exactly once and the result is the sequential
-// read's bit for bit.  `coordinate` files stay sequential (repeated entries
-// add in file order).  TOMOS_MTX_THREADS sets the thread count.
+// read's bit for bit.  `general` coordinate files are read the same way by
+// tomos_mtx_read_coo (entry e to slot e); into a dense matrix, and for
+// symmetric storage, coordinate files stay sequential (repeated entries add
+// in file order; mirrored entries shift the slots).  TOMOS_MTX_THREADS sets
+// the thread count.
 #include <sys/mman.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -235,33 +238,33 @@ struct ArrayPos {
     }
 };
 
-// The `array` values of the open file (positioned at its first value) into
-// at(i, j) (and its mirror for symmetric storage), in parallel.  Returns
-// false on a malformed token or too few values.
-template <class At>
-bool read_array_parallel(MtxFile& m, At&& at) {
-    const tomos_mtx_info& in = m.info;
-    const long off = std::ftell(m.f);
-    struct stat st;
-    if (off < 0 || fstat(fileno(m.f), &st) != 0) return false;
-    const size_t size = (size_t)st.st_size, start = (size_t)off;
-    const int64_t entries = in.entries;
-    if (entries == 0) return true;
-    if (start >= size) return false;
-    void* map = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fileno(m.f), 0);
-    if (map == MAP_FAILED) return false;
-    madvise(map, size, MADV_SEQUENTIAL);
-    const char* d = static_cast<const char*>(map);
-    const size_t bytes = size - start;
-    int nt = parse_threads(bytes);
-    std::vector<size_t> lo(nt), hi(nt);
-    for (int k = 0; k < nt; ++k) {
-        lo[k] = start + bytes * (size_t)k / (size_t)nt;
-        hi[k] = start + bytes * (size_t)(k + 1) / (size_t)nt;
+// The data section of an open file (positioned after its size line),
+// mapped read-only and cut into one byte range per thread, with the index
+// of the first token that starts in each range (cnt[k]; cnt[nt] = all).
+struct MappedTokens {
+    const char* d = nullptr;
+    size_t size = 0, start = 0;
+    int nt = 1;
+    std::vector<size_t> lo, hi;
+    std::vector<int64_t> cnt;
+    void* map = nullptr;
+    ~MappedTokens() {
+        if (map) munmap(map, size);
     }
-    auto starts_token = [&](size_t p) { return !is_space(d[p]) && (p == start || is_space(d[p - 1])); };
-    std::vector<int64_t> cnt(nt + 1, 0);
-    auto run = [&](auto&& body) {
+    bool starts_token(size_t p) const { return !is_space(d[p]) && (p == start || is_space(d[p - 1])); }
+    // end of the token starting at p
+    size_t token_end(size_t p) const {
+        while (p < size && !is_space(d[p])) ++p;
+        return p;
+    }
+    // start of the next token at or after p (size if none)
+    size_t next_token(size_t p) const {
+        while (p < size && is_space(d[p])) ++p;
+        return p;
+    }
+    // body(k) for every range k, on up to nt threads
+    template <class Body>
+    void run(Body&& body) const {
         std::vector<std::thread> th;
         bool spawned = true;
         for (int k = 1; k < nt && spawned; ++k) {
@@ -275,41 +278,158 @@ bool read_array_parallel(MtxFile& m, At&& at) {
         body(0);
         for (int k = done; k < nt; ++k) body(k);  // ranges no thread took
         for (auto& t : th) t.join();
-    };
-    run([&](int k) {
-        int64_t c = 0;
-        for (size_t p = lo[k]; p < hi[k]; ++p) c += starts_token(p);
-        cnt[k + 1] = c;
-    });
-    for (int k = 0; k < nt; ++k) cnt[k + 1] += cnt[k];
-    bool ok = cnt[nt] >= entries;
-    std::atomic<bool> bad(false);
-    if (ok) {
-        const ArrayPos pos{in.rows, in.cols, in.symmetry};
-        run([&](int k) {
-            int64_t t = cnt[k];
-            if (t >= entries) return;
-            int64_t i, j;
-            pos.at(t, &i, &j);
-            for (size_t p = lo[k]; p < hi[k] && t < entries; ++p) {
-                if (!starts_token(p)) continue;
-                size_t e = p;
-                while (e < size && !is_space(d[e])) ++e;
-                double v;
-                if (!parse_token(d + p, d + e, &v)) {
-                    bad.store(true, std::memory_order_relaxed);
-                    return;
-                }
-                at(i, j, v);
-                ++t;
-                pos.next(&i, &j);
-                p = e;  // the loop's ++p then steps past the whitespace at e
-            }
-        });
-        ok = !bad.load();
     }
-    munmap(map, size);
-    return ok;
+    bool open(FILE* f) {
+        const long off = std::ftell(f);
+        struct stat st;
+        if (off < 0 || fstat(fileno(f), &st) != 0) return false;
+        size = (size_t)st.st_size;
+        start = (size_t)off;
+        if (start >= size) {
+            size = 0;
+            nt = 0;
+            cnt.assign(1, 0);
+            return true;
+        }
+        map = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fileno(f), 0);
+        if (map == MAP_FAILED) {
+            map = nullptr;
+            return false;
+        }
+        madvise(map, size, MADV_SEQUENTIAL);
+        d = static_cast<const char*>(map);
+        const size_t bytes = size - start;
+        nt = parse_threads(bytes);
+        lo.resize(nt);
+        hi.resize(nt);
+        for (int k = 0; k < nt; ++k) {
+            lo[k] = start + bytes * (size_t)k / (size_t)nt;
+            hi[k] = start + bytes * (size_t)(k + 1) / (size_t)nt;
+        }
+        cnt.assign(nt + 1, 0);
+        run([&](int k) {
+            int64_t c = 0;
+            for (size_t p = lo[k]; p < hi[k]; ++p) c += starts_token(p);
+            cnt[k + 1] = c;
+        });
+        for (int k = 0; k < nt; ++k) cnt[k + 1] += cnt[k];
+        return true;
+    }
+};
+
+// The `array` values of the open file (positioned at its first value) into
+// at(i, j) (and its mirror for symmetric storage), in parallel.  Returns
+// false on a malformed token or too few values.
+template <class At>
+bool read_array_parallel(MtxFile& m, At&& at) {
+    const tomos_mtx_info& in = m.info;
+    const int64_t entries = in.entries;
+    if (entries == 0) return true;
+    MappedTokens mt;
+    if (!mt.open(m.f) || mt.cnt.back() < entries) return false;
+    std::atomic<bool> bad(false);
+    const ArrayPos pos{in.rows, in.cols, in.symmetry};
+    mt.run([&](int k) {
+        int64_t t = mt.cnt[k];
+        if (t >= entries) return;
+        int64_t i, j;
+        pos.at(t, &i, &j);
+        for (size_t p = mt.lo[k]; p < mt.hi[k] && t < entries; ++p) {
+            if (!mt.starts_token(p)) continue;
+            const size_t e = mt.token_end(p);
+            double v;
+            if (!parse_token(mt.d + p, mt.d + e, &v)) {
+                bad.store(true, std::memory_order_relaxed);
+                return;
+            }
+            at(i, j, v);
+            ++t;
+            pos.next(&i, &j);
+            p = e;  // the loop's ++p then steps past the whitespace at e
+        }
+    });
+    return !bad.load();
+}
+
+// As parse_token, for a 1-based index: a whole decimal integer token.
+bool parse_index(const char* p, const char* e, long long* v) {
+    const size_t n = (size_t)(e - p);
+    if (n == 0 || n > 127) return false;
+    char tok[128];
+    std::memcpy(tok, p, n);
+    tok[n] = '\0';
+    char* end = nullptr;
+    errno = 0;
+    *v = std::strtoll(tok, &end, 10);
+    return end == tok + n && errno == 0;
+}
+
+void atomic_min(std::atomic<int64_t>& a, int64_t v) {
+    int64_t cur = a.load(std::memory_order_relaxed);
+    while (v < cur && !a.compare_exchange_weak(cur, v, std::memory_order_relaxed)) {
+    }
+}
+
+// The entries of a `general` coordinate file (positioned at its first
+// entry), in parallel: store(e, row, col, value), 0-based, once for every
+// entry e.  An entry belongs to the range its first token starts in and is
+// read to its end, past the range if need be.  Errors name the first bad
+// entry in file order, as the sequential reader would meet it.
+template <class Store>
+tomos_status read_coord_parallel(MtxFile& m, const char* path, Store&& store) {
+    using tomos_b200::fail;
+    const tomos_mtx_info& in = m.info;
+    const int per = in.field == TOMOS_MTX_PATTERN ? 2 : 3;
+    const int64_t entries = in.entries;
+    const std::string bad = std::string("'") + path + "': truncated/malformed data";
+    if (entries == 0) return TOMOS_OK;
+    MappedTokens mt;
+    if (!mt.open(m.f)) return fail(TOMOS_ERR_INVALID, bad);
+    const int64_t have = std::min<int64_t>(entries, mt.cnt.back() / per);
+    std::atomic<int64_t> first_bad(INT64_MAX), first_out(INT64_MAX);
+    mt.run([&](int k) {
+        int64_t t = mt.cnt[k];
+        for (size_t p = mt.lo[k]; p < mt.hi[k]; ++p) {
+            if (!mt.starts_token(p)) continue;
+            if (t % per != 0) {  // inside an entry an earlier range reads
+                p = mt.token_end(p);
+                ++t;
+                continue;
+            }
+            const int64_t e = t / per;
+            if (e >= have) return;
+            size_t q = p, qe = mt.token_end(q);
+            long long i = 0, j = 0;
+            double v = 1.0;
+            bool ok = parse_index(mt.d + q, mt.d + qe, &i);
+            q = mt.next_token(qe);
+            qe = mt.token_end(q);
+            ok = ok && parse_index(mt.d + q, mt.d + qe, &j);
+            if (per == 3) {
+                q = mt.next_token(qe);
+                qe = mt.token_end(q);
+                ok = ok && parse_token(mt.d + q, mt.d + qe, &v);
+            }
+            if (!ok) {
+                atomic_min(first_bad, e);
+                return;
+            }
+            if (i < 1 || j < 1 || i > in.rows || j > in.cols) {
+                atomic_min(first_out, e);
+                return;
+            }
+            store(e, (int64_t)(i - 1), (int64_t)(j - 1), v);
+            t += per;
+            p = qe;
+        }
+    });
+    const int64_t b = first_bad.load(), o = first_out.load();
+    if (b != INT64_MAX && b <= o) return fail(TOMOS_ERR_INVALID, bad);
+    if (o != INT64_MAX)
+        return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': entry " + std::to_string(o + 1) +
+                                           " lies outside the matrix");
+    if (have < entries) return fail(TOMOS_ERR_INVALID, bad);
+    return TOMOS_OK;
 }
 
 }  // namespace
@@ -379,10 +499,26 @@ tomos_status tomos_mtx_read_coo(const char* path, int64_t cap, int64_t* rows, in
         ++k;
     };
     const int32_t sym = m.info.symmetry;
-    s = mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
-        put(i, j, v);
-        if (sym != TOMOS_MTX_GENERAL && i != j) put(j, i, sym == TOMOS_MTX_SKEW ? -v : v);
-    });
+    if (m.info.format == TOMOS_MTX_COORDINATE && sym == TOMOS_MTX_GENERAL) {
+        std::atomic<bool> full(false);
+        const bool room = rows && cols && vals;
+        s = read_coord_parallel(m, path, [&](int64_t e, int64_t i, int64_t j, double v) {
+            if (room && e < cap) {
+                rows[e] = i;
+                cols[e] = j;
+                vals[e] = v;
+            } else {
+                full.store(true, std::memory_order_relaxed);
+            }
+        });
+        k = m.info.entries;
+        over = full.load();
+    } else {
+        s = mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
+            put(i, j, v);
+            if (sym != TOMOS_MTX_GENERAL && i != j) put(j, i, sym == TOMOS_MTX_SKEW ? -v : v);
+        });
+    }
     if (s) return s;
     *count = k;
     if (over)
