@@ -331,3 +331,21 @@ def test_coordinate_parallel_errors(tmp_path, monkeypatch, threads):
     with pytest.raises(tb.TomosError) as e:
         tb.read_mtx_coo(p)
     assert "truncated/malformed data" in str(e.value)
+
+
+@pytest.mark.parametrize("threads", [1, 3, 64])
+@pytest.mark.parametrize("layout", ["F", "C"])
+def test_write_parallel_bytes(tmp_path, monkeypatch, threads, layout):
+    """The writer's blocks, formatted by any number of threads, give the
+    bytes of a sequential '%.17g' a line (more values than one block of
+    2^18, so several blocks and rounds), and read back bit for bit."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    A = generator_values(1000, 600, threads)
+    A.ravel()[5:8] = [np.inf, -np.inf, 0.0]
+    A = np.asarray(A, order=layout)
+    p = str(tmp_path / "w.mtx")
+    tb.write_mtx(p, A)
+    want = "%%MatrixMarket matrix array real general\n1000 600\n" + \
+        "".join("%.17g\n" % v for v in A.ravel(order="F"))
+    assert open(p).read() == want
+    assert np.array_equal(tb.read_mtx(p).view(np.uint64), np.asfortranarray(A).view(np.uint64))

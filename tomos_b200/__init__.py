@@ -304,9 +304,12 @@ def write_mtx(path, a, layout=None):
     a = np.asarray(a, dtype=np.float64)
     if a.ndim != 2:
         raise TomosError(C.TOMOS_ERR_INVALID, "write_mtx: a 2-D array")
-    af = np.asfortranarray(a)
-    C.check(C.lib().tomos_mtx_write_dense(_path(path), int(Layout.COL_MAJOR), a.shape[0], a.shape[1],
-                                          af.ctypes.data, max(1, a.shape[0])), "write_mtx")
+    if a.flags["C_CONTIGUOUS"] and not a.flags["F_CONTIGUOUS"]:
+        buf, lay, ld = a, Layout.ROW_MAJOR, max(1, a.shape[1])  # no copy
+    else:
+        buf, lay, ld = np.asfortranarray(a), Layout.COL_MAJOR, max(1, a.shape[0])
+    C.check(C.lib().tomos_mtx_write_dense(_path(path), int(lay), a.shape[0], a.shape[1],
+                                          buf.ctypes.data, ld), "write_mtx")
 
 
 def dense_from_mtx(path, store_type=NumericType.FP32, layout=Layout.COL_MAJOR):

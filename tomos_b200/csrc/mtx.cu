@@ -537,11 +537,45 @@ tomos_status tomos_mtx_write_dense(const char* path, int32_t layout, int64_t row
     if (!f) return fail(TOMOS_ERR_INVALID, std::string("could not open '") + (path ? path : "") + "' for writing");
     bool ok = std::fprintf(f, "%%%%MatrixMarket matrix array real general\n%lld %lld\n", (long long)rows,
                            (long long)cols) > 0;
-    for (int64_t j = 0; ok && j < cols; ++j)
-        for (int64_t i = 0; ok && i < rows; ++i) {
-            const double v = layout == TOMOS_COL_MAJOR ? a[(size_t)j * ld + i] : a[(size_t)i * ld + j];
-            ok = std::fprintf(f, "%.17g\n", v) > 0;
+    // Values in file order (column by column), "%.17g" a line: host threads
+    // format consecutive blocks of kBlock values into their own buffers,
+    // which are then written in order, so the bytes are the sequential
+    // fprintf's.
+    constexpr int64_t kBlock = 1 << 18;
+    const int64_t total = rows * cols;
+    const int nt = parse_threads((size_t)(total * 24));
+    std::vector<std::string> buf(nt);
+    auto value = [&](int64_t t) {
+        const int64_t i = t % rows, j = t / rows;
+        return layout == TOMOS_COL_MAJOR ? a[(size_t)j * ld + i] : a[(size_t)i * ld + j];
+    };
+    for (int64_t t0 = 0; ok && t0 < total; t0 += kBlock * nt) {
+        auto body = [&](int k) {
+            std::string& b = buf[k];
+            b.clear();
+            const int64_t lo = t0 + kBlock * k, hi = std::min(total, lo + kBlock);
+            char s[40];
+            for (int64_t t = lo; t < hi; ++t) {
+                const int n = std::snprintf(s, sizeof(s), "%.17g\n", value(t));
+                b.append(s, (size_t)n);
+            }
+        };
+        std::vector<std::thread> th;
+        int spawned = 1;
+        for (int k = 1; k < nt; ++k) {
+            try {
+                th.emplace_back(body, k);
+                ++spawned;
+            } catch (...) {
+                break;
+            }
         }
+        body(0);
+        for (int k = spawned; k < nt; ++k) body(k);
+        for (auto& x : th) x.join();
+        for (int k = 0; ok && k < nt; ++k)
+            ok = buf[k].empty() || std::fwrite(buf[k].data(), 1, buf[k].size(), f) == buf[k].size();
+    }
     ok = (std::fclose(f) == 0) && ok;
     if (!ok) return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': write failed");
     return TOMOS_OK;
