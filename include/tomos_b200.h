@@ -391,7 +391,10 @@ tomos_status tomos_lsqr_adjoint_grad_dense(const tomos_dense* A, int64_t K, cons
  * file's values into an m x n column-major FP64 buffer.  These read the
  * same files the same way (strtod per value) and also take `coordinate`
  * files, the integer and pattern fields and symmetric / skew-symmetric
- * storage (mirrored); complex and hermitian files are rejected. */
+ * storage (mirrored); complex and hermitian files are rejected.  Array
+ * files, general coordinate files read as triplets, and writes run on all
+ * host threads (TOMOS_MTX_THREADS in the environment sets their number);
+ * the results are the sequential ones, bit for bit. */
 enum tomos_mtx_format { TOMOS_MTX_ARRAY = 0, TOMOS_MTX_COORDINATE = 1 };
 enum tomos_mtx_field { TOMOS_MTX_REAL = 0, TOMOS_MTX_INTEGER = 1, TOMOS_MTX_PATTERN = 2 };
 enum tomos_mtx_symmetry { TOMOS_MTX_GENERAL = 0, TOMOS_MTX_SYMMETRIC = 1, TOMOS_MTX_SKEW = 2 };
