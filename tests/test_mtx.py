@@ -349,3 +349,19 @@ def test_write_parallel_bytes(tmp_path, monkeypatch, threads, layout):
         "".join("%.17g\n" % v for v in A.ravel(order="F"))
     assert open(p).read() == want
     assert np.array_equal(tb.read_mtx(p).view(np.uint64), np.asfortranarray(A).view(np.uint64))
+
+
+@pytest.mark.parametrize("threads", THREADS)
+def test_coordinate_dense_parallel_repeats(tmp_path, monkeypatch, threads):
+    """A general coordinate file read into a dense matrix: triplets parsed
+    by any number of threads, repeated positions summed in file order (the
+    sequential sum's bits)."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    rng = np.random.default_rng(21)
+    text, r, c, vals = coordinate_text(rng, 12, 9, 700, "real", split_lines=True)
+    p = write_text(tmp_path / "d.mtx", text)
+    want = np.zeros((12, 9))
+    for a, b, v in zip(r, c, vals):
+        want[a, b] += float(v)
+    got = tb.read_mtx(p)
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))

@@ -468,6 +468,27 @@ tomos_status tomos_mtx_read_dense(const char* path, int32_t layout, double* out,
         if (!ok) return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': truncated/malformed data");
         return TOMOS_OK;
     }
+    if (sym == TOMOS_MTX_GENERAL) {
+        // triplets parsed in parallel, then added in file order (repeated
+        // entries sum as the sequential read sums them)
+        std::vector<int64_t> ri, ci;
+        std::vector<double> vi;
+        try {
+            ri.resize((size_t)in.entries);
+            ci.resize((size_t)in.entries);
+            vi.resize((size_t)in.entries);
+        } catch (...) {
+            return fail(TOMOS_ERR_ALLOC, "tomos_mtx_read_dense: no host memory for the entries");
+        }
+        s = read_coord_parallel(m, path, [&](int64_t e, int64_t i, int64_t j, double v) {
+            ri[(size_t)e] = i;
+            ci[(size_t)e] = j;
+            vi[(size_t)e] = v;
+        });
+        if (s) return s;
+        for (size_t e = 0; e < vi.size(); ++e) at(ri[e], ci[e]) += vi[e];
+        return TOMOS_OK;
+    }
     return mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
         if (in.format == TOMOS_MTX_COORDINATE) at(i, j) += v;  // repeated entries add
         else at(i, j) = v;
