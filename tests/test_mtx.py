@@ -365,3 +365,44 @@ def test_coordinate_dense_parallel_repeats(tmp_path, monkeypatch, threads):
         want[a, b] += float(v)
     got = tb.read_mtx(p)
     assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.timeout(120)
+@pytest.mark.parametrize("kind", ["array", "coordinate"])
+def test_pipe_reads_sequentially(tmp_path, kind):
+    """A file that cannot be mapped (a named pipe) is read by the
+    sequential reader, with the same result (one open of the pipe: the C
+    entries are called directly)."""
+    import ctypes
+    import threading
+    if kind == "array":
+        A = generator_values(50, 7, 3)
+        text = "%%MatrixMarket matrix array real general\n50 7\n" + \
+            "".join("%1.16e\n" % v for v in A.ravel(order="F"))
+    else:
+        text, r, c, vals = coordinate_text(np.random.default_rng(4), 30, 20, 200, "real")
+    assert len(text) < 60000  # fits the pipe's buffer: the writer never waits on the reader
+    fifo = str(tmp_path / "pipe.mtx")
+    os.mkfifo(fifo)
+
+    def serve():
+        with open(fifo, "w") as f:
+            f.write(text)
+
+    th = threading.Thread(target=serve, daemon=True)
+    th.start()
+    if kind == "array":
+        want = np.array([float("%1.16e" % v) for v in A.ravel(order="F")]).reshape(A.shape, order="F")
+        out = np.zeros((50, 7), order="F")
+        C.check(C.lib().tomos_mtx_read_dense(os.fsencode(fifo), int(tb.Layout.COL_MAJOR), out.ctypes.data, 50))
+        assert np.array_equal(out.view(np.uint64), want.view(np.uint64))
+    else:
+        rr = np.zeros(200, np.int64)
+        cc = np.zeros(200, np.int64)
+        vv = np.zeros(200)
+        cnt = ctypes.c_int64(0)
+        C.check(C.lib().tomos_mtx_read_coo(os.fsencode(fifo), 200, rr.ctypes.data, cc.ctypes.data,
+                                           vv.ctypes.data, ctypes.byref(cnt)))
+        assert cnt.value == 200 and np.array_equal(rr, r) and np.array_equal(cc, c)
+        assert np.array_equal(vv, np.array([float(v) for v in vals]))
+    th.join(timeout=30)

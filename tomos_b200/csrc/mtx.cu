@@ -282,7 +282,7 @@ struct MappedTokens {
     bool open(FILE* f) {
         const long off = std::ftell(f);
         struct stat st;
-        if (off < 0 || fstat(fileno(f), &st) != 0) return false;
+        if (off < 0 || fstat(fileno(f), &st) != 0 || !S_ISREG(st.st_mode)) return false;
         size = (size_t)st.st_size;
         start = (size_t)off;
         if (start >= size) {
@@ -319,14 +319,18 @@ struct MappedTokens {
 
 // The `array` values of the open file (positioned at its first value) into
 // at(i, j) (and its mirror for symmetric storage), in parallel.  Returns
-// false on a malformed token or too few values.
+// kParsed, kMalformed (a malformed token or too few values) or kNoMap (not
+// a regular file that maps: the caller reads it sequentially; the file
+// position is untouched).
+enum { kParsed = 0, kMalformed = 1, kNoMap = 2 };
 template <class At>
-bool read_array_parallel(MtxFile& m, At&& at) {
+int read_array_parallel(MtxFile& m, At&& at) {
     const tomos_mtx_info& in = m.info;
     const int64_t entries = in.entries;
-    if (entries == 0) return true;
+    if (entries == 0) return kParsed;
     MappedTokens mt;
-    if (!mt.open(m.f) || mt.cnt.back() < entries) return false;
+    if (!mt.open(m.f)) return kNoMap;
+    if (mt.cnt.back() < entries) return kMalformed;
     std::atomic<bool> bad(false);
     const ArrayPos pos{in.rows, in.cols, in.symmetry};
     mt.run([&](int k) {
@@ -348,7 +352,7 @@ bool read_array_parallel(MtxFile& m, At&& at) {
             p = e;  // the loop's ++p then steps past the whitespace at e
         }
     });
-    return !bad.load();
+    return bad.load() ? kMalformed : kParsed;
 }
 
 // As parse_token, for a 1-based index: a whole decimal integer token.
@@ -376,7 +380,7 @@ void atomic_min(std::atomic<int64_t>& a, int64_t v) {
 // read to its end, past the range if need be.  Errors name the first bad
 // entry in file order, as the sequential reader would meet it.
 template <class Store>
-tomos_status read_coord_parallel(MtxFile& m, const char* path, Store&& store) {
+tomos_status read_coord_parallel(MtxFile& m, const char* path, bool* nomap, Store&& store) {
     using tomos_b200::fail;
     const tomos_mtx_info& in = m.info;
     const int per = in.field == TOMOS_MTX_PATTERN ? 2 : 3;
@@ -384,7 +388,8 @@ tomos_status read_coord_parallel(MtxFile& m, const char* path, Store&& store) {
     const std::string bad = std::string("'") + path + "': truncated/malformed data";
     if (entries == 0) return TOMOS_OK;
     MappedTokens mt;
-    if (!mt.open(m.f)) return fail(TOMOS_ERR_INVALID, bad);
+    *nomap = !mt.open(m.f);
+    if (*nomap) return TOMOS_OK;  // the caller reads the file sequentially
     const int64_t have = std::min<int64_t>(entries, mt.cnt.back() / per);
     std::atomic<int64_t> first_bad(INT64_MAX), first_out(INT64_MAX);
     mt.run([&](int k) {
@@ -460,15 +465,16 @@ tomos_status tomos_mtx_read_dense(const char* path, int32_t layout, double* out,
     for (int64_t j = 0; j < in.cols; ++j)
         for (int64_t i = 0; i < in.rows; ++i) at(i, j) = 0.0;
     const int32_t sym = in.symmetry;
+    // in parallel where the file maps; otherwise (a pipe, say) sequentially
+    // below, from the same file position
     if (in.format == TOMOS_MTX_ARRAY) {
-        const bool ok = read_array_parallel(m, [&](int64_t i, int64_t j, double v) {
+        const int r = read_array_parallel(m, [&](int64_t i, int64_t j, double v) {
             at(i, j) = v;
             if (sym != TOMOS_MTX_GENERAL && i != j) at(j, i) = sym == TOMOS_MTX_SKEW ? -v : v;
         });
-        if (!ok) return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': truncated/malformed data");
-        return TOMOS_OK;
-    }
-    if (sym == TOMOS_MTX_GENERAL) {
+        if (r == kMalformed) return fail(TOMOS_ERR_INVALID, std::string("'") + path + "': truncated/malformed data");
+        if (r == kParsed) return TOMOS_OK;
+    } else if (sym == TOMOS_MTX_GENERAL) {
         // triplets parsed in parallel, then added in file order (repeated
         // entries sum as the sequential read sums them)
         std::vector<int64_t> ri, ci;
@@ -480,14 +486,17 @@ tomos_status tomos_mtx_read_dense(const char* path, int32_t layout, double* out,
         } catch (...) {
             return fail(TOMOS_ERR_ALLOC, "tomos_mtx_read_dense: no host memory for the entries");
         }
-        s = read_coord_parallel(m, path, [&](int64_t e, int64_t i, int64_t j, double v) {
+        bool nomap = false;
+        s = read_coord_parallel(m, path, &nomap, [&](int64_t e, int64_t i, int64_t j, double v) {
             ri[(size_t)e] = i;
             ci[(size_t)e] = j;
             vi[(size_t)e] = v;
         });
         if (s) return s;
-        for (size_t e = 0; e < vi.size(); ++e) at(ri[e], ci[e]) += vi[e];
-        return TOMOS_OK;
+        if (!nomap) {
+            for (size_t e = 0; e < vi.size(); ++e) at(ri[e], ci[e]) += vi[e];
+            return TOMOS_OK;
+        }
     }
     return mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
         if (in.format == TOMOS_MTX_COORDINATE) at(i, j) += v;  // repeated entries add
@@ -520,10 +529,11 @@ tomos_status tomos_mtx_read_coo(const char* path, int64_t cap, int64_t* rows, in
         ++k;
     };
     const int32_t sym = m.info.symmetry;
+    bool nomap = true;
     if (m.info.format == TOMOS_MTX_COORDINATE && sym == TOMOS_MTX_GENERAL) {
         std::atomic<bool> full(false);
         const bool room = rows && cols && vals;
-        s = read_coord_parallel(m, path, [&](int64_t e, int64_t i, int64_t j, double v) {
+        s = read_coord_parallel(m, path, &nomap, [&](int64_t e, int64_t i, int64_t j, double v) {
             if (room && e < cap) {
                 rows[e] = i;
                 cols[e] = j;
@@ -532,9 +542,12 @@ tomos_status tomos_mtx_read_coo(const char* path, int64_t cap, int64_t* rows, in
                 full.store(true, std::memory_order_relaxed);
             }
         });
-        k = m.info.entries;
-        over = full.load();
-    } else {
+        if (!nomap) {
+            k = m.info.entries;
+            over = full.load();
+        }
+    }
+    if (nomap) {
         s = mtx_entries(m, path, [&](int64_t i, int64_t j, double v) {
             put(i, j, v);
             if (sym != TOMOS_MTX_GENERAL && i != j) put(j, i, sym == TOMOS_MTX_SKEW ? -v : v);
