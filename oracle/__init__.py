@@ -28,10 +28,26 @@ BUCKET_SEED = 0x12345678ABCDEF00
 SIGN_SEED = 0xF00DD00D42BABE55
 
 
+# Where the reference's sources are looked for: TOMOS_REF_SRC, else the
+# checkout this build recipe was written against.
+REF_SRC_DEFAULT = "/root/reference"
+
+
+def ref_src():
+    """The reference source tree, or None when it is not on this machine."""
+    d = os.environ.get("TOMOS_REF_SRC") or REF_SRC_DEFAULT
+    return d if os.path.isdir(os.path.join(d, "src")) else None
+
+
 def build(ref=None):
-    """Builds liboracle.so (and the reference CPU library when its sources exist)."""
-    target = ["all"] if ref is None else (["oracle", "ref"] if ref else ["oracle"])
-    subprocess.run(["make", "-s", "-j8", *target], cwd=HERE, check=True)
+    """Builds liboracle.so, and the reference CPU library when its sources
+    exist (ref=None: when found; ref=True: required; ref=False: never)."""
+    src = ref_src()
+    if ref and not src:
+        raise FileNotFoundError("reference sources not found (set TOMOS_REF_SRC)")
+    target = ["oracle", "ref"] if (src and ref is not False) else ["oracle"]
+    args = [f"REF={src}"] if src else []
+    subprocess.run(["make", "-s", "-j8", *args, *target], cwd=HERE, check=True)
 
 
 def _P(a):

@@ -406,3 +406,80 @@ def test_pipe_reads_sequentially(tmp_path, kind):
         assert cnt.value == 200 and np.array_equal(rr, r) and np.array_equal(cc, c)
         assert np.array_equal(vv, np.array([float(v) for v in vals]))
     th.join(timeout=30)
+
+
+EMPTY_DATA = [
+    ("array", "%%MatrixMarket matrix array real general\n3 2\n"),
+    ("array", "%%MatrixMarket matrix array real general\n3 2"),
+    ("general", "%%MatrixMarket matrix coordinate real general\n3 3 2\n"),
+    ("general", "%%MatrixMarket matrix coordinate real general\n3 3 2"),
+    ("general", "%%MatrixMarket matrix coordinate real general\n3 3 2\n\n  \n"),
+    ("pattern", "%%MatrixMarket matrix coordinate pattern general\n4 4 3\n"),
+]
+
+
+@pytest.mark.parametrize("threads", [1, 64])
+@pytest.mark.parametrize("kind,text", EMPTY_DATA)
+def test_empty_data_section(tmp_path, monkeypatch, threads, kind, text):
+    """A size line promising values or entries with nothing after it is
+    'truncated/malformed data' for every reader (dense, COO, CSR), at any
+    thread count -- never a crash."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    p = write_text(tmp_path / "e.mtx", text)
+    readers = [tb.read_mtx] if kind == "array" else [tb.read_mtx, tb.read_mtx_coo, tb.read_mtx_csr]
+    for rd in readers:
+        with pytest.raises(tb.TomosError) as e:
+            rd(p)
+        assert "truncated/malformed data" in str(e.value)
+
+
+@pytest.mark.timeout(120)
+@pytest.mark.parametrize("kind", ["array", "coordinate"])
+def test_long_token_rejected_by_both_readers(tmp_path, kind):
+    """A token longer than 127 characters is malformed whether the file is
+    mapped (parallel reader) or read from a pipe (sequential reader)."""
+    import ctypes
+    import threading
+    long_num = "1." + "0" * 200
+    if kind == "array":
+        text = "%%MatrixMarket matrix array real general\n2 1\n" + long_num + "\n2.0\n"
+    else:
+        text = "%%MatrixMarket matrix coordinate real general\n2 2 2\n1 1 " + long_num + "\n2 2 1.0\n"
+    p = write_text(tmp_path / "long.mtx", text)
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx(p)
+    assert "truncated/malformed data" in str(e.value)
+    fifo = str(tmp_path / "long_pipe.mtx")
+    os.mkfifo(fifo)
+
+    def serve():
+        with open(fifo, "w") as f:
+            f.write(text)
+
+    th = threading.Thread(target=serve, daemon=True)
+    th.start()
+    if kind == "array":
+        out = np.zeros((2, 1), order="F")
+        rc = C.lib().tomos_mtx_read_dense(os.fsencode(fifo), int(tb.Layout.COL_MAJOR), out.ctypes.data, 2)
+    else:
+        rr = np.zeros(2, np.int64)
+        cc = np.zeros(2, np.int64)
+        vv = np.zeros(2)
+        cnt = ctypes.c_int64(0)
+        rc = C.lib().tomos_mtx_read_coo(os.fsencode(fifo), 2, rr.ctypes.data, cc.ctypes.data,
+                                        vv.ctypes.data, ctypes.byref(cnt))
+    th.join(timeout=30)
+    assert rc != 0
+    assert "truncated/malformed data" in C.lib().tomos_last_error().decode()
+
+
+@pytest.mark.parametrize("threads", [1, 64])
+def test_long_index_token_rejected(tmp_path, monkeypatch, threads):
+    """An index token of 128+ digits is malformed in both readers (the
+    sequential reader no longer reads a prefix of it)."""
+    monkeypatch.setenv("TOMOS_MTX_THREADS", str(threads))
+    text = "%%MatrixMarket matrix coordinate real symmetric\n2 2 1\n" + "0" * 140 + "1 1 1.0\n"
+    p = write_text(tmp_path / "li.mtx", text)
+    with pytest.raises(tb.TomosError) as e:
+        tb.read_mtx(p)
+    assert "truncated/malformed data" in str(e.value)

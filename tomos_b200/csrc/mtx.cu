@@ -135,13 +135,34 @@ tomos_status mtx_open(const char* path, MtxFile& m) {
 bool read_value(FILE* f, double* v) {
     char tok[128];
     if (std::fscanf(f, "%127s", tok) != 1) return false;
+    // a token of 127 characters may have been cut: if more of it follows,
+    // reject it, as the mapped reader rejects tokens over 127 characters
+    if (std::strlen(tok) == 127) {
+        const int c = std::fgetc(f);
+        if (c != EOF) std::ungetc(c, f);
+        if (c != EOF && !std::isspace(c)) return false;
+    }
     errno = 0;
     char* end = nullptr;
     *v = std::strtod(tok, &end);
     return end && *end == '\0' && end != tok;
 }
 
-bool read_index(FILE* f, long long* v) { return std::fscanf(f, "%lld", v) == 1; }
+// A whole index token, as the mapped reader's parse_index: a decimal
+// integer of at most 127 characters followed by whitespace or the end.
+bool read_index(FILE* f, long long* v) {
+    char tok[128];
+    if (std::fscanf(f, "%127s", tok) != 1) return false;
+    if (std::strlen(tok) == 127) {
+        const int c = std::fgetc(f);
+        if (c != EOF) std::ungetc(c, f);
+        if (c != EOF && !std::isspace(c)) return false;
+    }
+    errno = 0;
+    char* end = nullptr;
+    *v = std::strtoll(tok, &end, 10);
+    return end && *end == '\0' && end != tok && errno == 0;
+}
 
 // Visits every stored entry as (row, col, value), 0-based; symmetric parts
 // are emitted once here (the callers mirror them).
@@ -265,6 +286,7 @@ struct MappedTokens {
     // body(k) for every range k, on up to nt threads
     template <class Body>
     void run(Body&& body) const {
+        if (nt < 1) return;  // an empty data section has no ranges
         std::vector<std::thread> th;
         bool spawned = true;
         for (int k = 1; k < nt && spawned; ++k) {
@@ -391,6 +413,9 @@ tomos_status read_coord_parallel(MtxFile& m, const char* path, bool* nomap, Stor
     *nomap = !mt.open(m.f);
     if (*nomap) return TOMOS_OK;  // the caller reads the file sequentially
     const int64_t have = std::min<int64_t>(entries, mt.cnt.back() / per);
+    // no complete entry at all (a data section that is empty or ends at the
+    // size line): nothing to parse, and too few entries
+    if (mt.nt < 1 || have < 1) return fail(TOMOS_ERR_INVALID, bad);
     std::atomic<int64_t> first_bad(INT64_MAX), first_out(INT64_MAX);
     mt.run([&](int k) {
         int64_t t = mt.cnt[k];
