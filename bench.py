@@ -159,7 +159,7 @@ def gpu_solve(tb, torch, A, b, s):
                                                 with_colsq=True)
     if ev:
         ev[1].record()
-    Rinv = tb.generate_sketch_qr_precond(SA)
+    Rinv = tb.generate_sketch_qr_precond(SA, copy=False)
     if ev:
         ev[2].record()
     d, anorm = tb.column_scale(colsq)
@@ -169,7 +169,7 @@ def gpu_solve(tb, torch, A, b, s):
         ws = tb.create_lsqr_workspace(None, (m, n), tb.NumericType.FP32, tb.NumericType.FP64)
         gpu_solve.ws[(m, n)] = ws
     tb.add_precond(Rinv, ws)
-    x = torch.zeros(n, device="cuda")
+    x = torch.empty(n, device="cuda")  # the solve zeroes x
     rep = tb.lsqr_solve(None, A, b, x, ws, TOL, 200, 0.0, restarts=8,
                         stop_rule=tb.StopRule.BACKWARD, inner_rtol=2e-3 if packed else 0.0,
                         anorm_fro=anorm, col_scale=d, staged_plane=plane,

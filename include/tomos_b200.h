@@ -219,6 +219,15 @@ tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64
                                          double* colsq, void* scratch,
                                          size_t scratch_bytes, void* stream);
 
+/* The column scale of the BACKWARD stopping rule from column sums of
+ * squares (tomos_countsketch_apply's colsq, device, n doubles): d_j =
+ * sqrt(colsq_j), 1 for an empty column, and ||A D^{-1}||_F = sqrt(number of
+ * non-empty columns) in *anorm (device, one double).  On the device, no
+ * host round trip.  No reference counterpart (the reference stops on
+ * |phi_bar| / ||b|| only, lsqr.cpp:418-425). */
+tomos_status tomos_column_scale(const double* colsq, int64_t n, double* d, double* anorm,
+                                void* stream);
+
 /* ------------------------------------------------------------- sketch QR */
 
 /* FP64 Householder QR of the k x n (k >= n) column-major SA, then the
@@ -282,6 +291,12 @@ typedef struct tomos_lsqr_opts {
                                 it instead of staging their own copy. The
                                 caller keeps it equal to A's wh plane.      */
     int64_t staged_ld;
+    const double* anorm_fro_dev; /* device, may be NULL: ||A||_F (or
+                                ||A D^{-1}||_F) as one device double, e.g.
+                                from tomos_column_scale; read on the device,
+                                so the solve needs no host round trip before
+                                its first pass.  Takes precedence over
+                                anorm_fro.                                   */
     const tomos_dense* refine; /* may be NULL: lsqr_solve's
                                 mtx_refine_precision (--explicit-duplicates):
                                 a copy of A at higher precision (FP32, or
@@ -289,6 +304,14 @@ typedef struct tomos_lsqr_opts {
                                 restart passes read instead of A; it takes
                                 precedence over implicit_duplicate
                                 (lsqr.cpp:459-473)                          */
+    double inner_eta_factor; /* BACKWARD rule: an inner cycle also ends once
+                                its estimate |phi_bar| / (||A|| ||x|| + ||b||)
+                                is below tol times this (0 = 1).  Below 1 with
+                                refinement (inner iterations on a 16-bit
+                                plane), it leaves room for the plane's
+                                perturbation, so that the cycle's exact
+                                residual meets tol and no further cycle
+                                (and exact pass) is needed.                  */
 } tomos_lsqr_opts;
 
 typedef struct tomos_lsqr_report {

@@ -179,6 +179,37 @@ def test_prestaged_plane_same_solve():
                       staged_plane=plane[:, 1:])
 
 
+@pytest.mark.parametrize("zeros", [False, True])
+@pytest.mark.parametrize("numeric,rounded", [(NT.FP32, False), (NT.FP32_16, False),
+                                             (NT.FP32_BF16, False), (NT.FP32_BF16, True)])
+@pytest.mark.parametrize("n", [1000, 300])
+def test_exact_pass_residual(orc, numeric, rounded, zeros, n):
+    """The exact (FP64-summing) pass behind the restart residuals and the
+    backward-error entry: with b = fl32(A x) for the exactly decoded A, the
+    residual is the rounding of b alone, so one element decoded one unit
+    off at any bit would swamp it.  Covers FP32_16 control words below and
+    above the fp16 range and, with zeros, the saturated words (signed
+    zeros) that take the conversion-pipe path."""
+    rng = np.random.default_rng(n + (7 if zeros else 0))
+    m = 6000
+    A0 = rng.standard_normal((m, n)) * 10.0 ** rng.uniform(-3, 3, n)
+    pick = rng.random((m, n))
+    A0 = np.where(pick < 0.01, A0 * 1e-6, A0)                 # control words below fp16 range
+    A0 = np.where((pick >= 0.01) & (pick < 0.015), A0 * 1e4, A0)  # and above it
+    if zeros:
+        A0 = np.where((pick >= 0.015) & (pick < 0.017), 0.0, A0)
+    A0 = A0.astype(np.float32)
+    A = to_dense(A0, L.ROW_MAJOR, numeric, pad=(-n) % 8, rounded=rounded)
+    Ae = decoded(orc, A, tb.Tier.ACCURATE)
+    x = rng.standard_normal(n).astype(np.float32)
+    b = (Ae @ x.astype(np.float64)).astype(np.float32)
+    r = b.astype(np.float64) - Ae @ x.astype(np.float64)
+    ws = tb.create_lsqr_workspace(None, A.size, NT.FP32)
+    rep = tb.backward_error(A, cuda(b), cuda(x), ws)
+    np.testing.assert_allclose(rep["rnorm"], np.linalg.norm(r), rtol=1e-6)
+    np.testing.assert_allclose(rep["arnorm"], np.linalg.norm(Ae.T @ r), rtol=2e-3)
+
+
 def test_backward_error_entry(orc):
     A0, b = scaled_problem(5000, 60, 8)
     A = to_dense(A0, L.ROW_MAJOR)

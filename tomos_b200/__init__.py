@@ -140,6 +140,14 @@ class Dense:
         return cls(st, layout, size, ld, buf, rounded)
 
     @classmethod
+    def _empty_f64(cls, layout, size):
+        """An FP64 Dense whose values the caller's kernel writes in full (no
+        zero fill)."""
+        outer, inner = cls._outer_inner(layout, size)
+        buf = torch.empty(max(inner * outer, 1), dtype=torch.float64, device="cuda")
+        return cls(NumericType.FP64, layout, size, inner, buf)
+
+    @classmethod
     def from_tensor(cls, t, layout=Layout.COL_MAJOR, store_type=NumericType.FP32, lead_dim=None):
         """Copies a logical (rows x cols) tensor into a new Dense of this layout."""
         t = torch.as_tensor(t)
@@ -477,9 +485,10 @@ def apply_count_sketch(A, s, tier=Tier.AUTO, bucket_seed=CS_BUCKET_SEED, sign_se
     if stage:
         return _count_sketch_stage(A, s, bucket_seed, sign_seed, with_colsq, stream)
     n = A.size[1]
-    SA = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (s, n))
-    fro2 = torch.zeros(1, dtype=torch.float64, device="cuda")
-    colsq = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda") if with_colsq else None
+    # every output is written in full by the sketch
+    SA = Dense._empty_f64(Layout.COL_MAJOR, (s, n))
+    fro2 = torch.empty(1, dtype=torch.float64, device="cuda")
+    colsq = torch.empty(max(n, 1), dtype=torch.float64, device="cuda") if with_colsq else None
     m = A.size[0]
     nb = C.lib().tomos_countsketch_scratch_bytes(m, n, s)
     scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
@@ -498,9 +507,9 @@ def _count_sketch_stage(A, s, bucket_seed, sign_seed, with_colsq, stream):
     m, n = A.size
     ldp = (n + 7) // 8 * 8
     plane = torch.empty((max(m, 1), ldp), dtype=torch.int16, device="cuda")
-    SA = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (s, n))
-    fro2 = torch.zeros(1, dtype=torch.float64, device="cuda")
-    colsq = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda") if with_colsq else None
+    SA = Dense._empty_f64(Layout.COL_MAJOR, (s, n))
+    fro2 = torch.empty(1, dtype=torch.float64, device="cuda")
+    colsq = torch.empty(max(n, 1), dtype=torch.float64, device="cuda") if with_colsq else None
     nb = C.lib().tomos_countsketch_scratch_bytes(m, n, s)
     scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
     d = A.desc()
@@ -513,10 +522,12 @@ def _count_sketch_stage(A, s, bucket_seed, sign_seed, with_colsq, stream):
     return SA, fro2, plane
 
 
-def generate_sketch_qr_precond(sketched, R_out=None, stream=None):
+def generate_sketch_qr_precond(sketched, R_out=None, copy=True, stream=None):
     """FP64 Householder QR of the k x n column-major sketched matrix; on
     return its leading n x n block holds R^{-1} (sketch_qr.hpp:19).
-    Returns (Rinv Dense view copy, R tensor or None)."""
+    Returns R^{-1} as an n x n Dense: a copy of that block, or with
+    copy=False a view of it (leading dimension k, no device copy; it
+    shares the sketched matrix's storage)."""
     if sketched.numeric != NumericType.FP64 or sketched.layout != Layout.COL_MAJOR:
         raise TomosError(C.TOMOS_ERR_INVALID, "generate_sketch_qr_precond: FP64 column-major input")
     k, n = sketched.size
@@ -529,6 +540,8 @@ def generate_sketch_qr_precond(sketched, R_out=None, stream=None):
     C.check(C.lib().tomos_sketch_qr_precond_f64(k, n, _ptr(sketched.storage), sketched.ld,
                                                 _ptr(R_out), _ptr(scratch), nb, _stream(stream)),
             "generate_sketch_qr_precond")
+    if not copy:
+        return Dense(NumericType.FP64, Layout.COL_MAJOR, (n, n), sketched.ld, sketched.storage)
     Rinv = Dense.create_strided(None, Layout.COL_MAJOR, NumericType.FP64, (n, n))
     Rinv.view()[...] = sketched.view()[:n, :n]
     return Rinv
@@ -587,7 +600,7 @@ def add_precond(precond, workspace):
 def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=None,
                residual_history=None, restarts=1, stop_rule=StopRule.RELRES, inner_rtol=0.0,
                anorm_fro=0.0, warm_start=False, tier=None, profile=False, col_scale=None,
-               staged_plane=None, mtx_refine_precision=None, stream=None):
+               staged_plane=None, mtx_refine_precision=None, inner_eta_factor=0.0, stream=None):
     """include/core/solver.hpp:68-78.  A: Dense or Csr on the device; b, x:
     FP32 Dense column vectors or float32 CUDA tensors.  iterations and
     residual_history, when lists, receive the reference's out-parameters.
@@ -612,7 +625,12 @@ def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=N
     opts.implicit_duplicate = 1 if workspace.use_implicit_duplicate_ else 0
     opts.warm_start = 1 if warm_start else 0
     opts.inner_rtol = float(inner_rtol)
-    opts.anorm_fro = float(anorm_fro)
+    opts.inner_eta_factor = float(inner_eta_factor)
+    if isinstance(anorm_fro, torch.Tensor):  # a device value (column_scale)
+        opts.anorm_fro_dev = anorm_fro.data_ptr()
+        opts.anorm_fro = 0.0
+    else:
+        opts.anorm_fro = float(anorm_fro)
     refine_desc = None
     if mtx_refine_precision is not None:
         refine_desc = mtx_refine_precision.desc()
@@ -690,10 +708,14 @@ def lsqr_adjoint_grad(A, B, X, Lam, want_grad_a=True, stream=None):
     return gA, gB.t()
 
 
-def column_scale(colsq):
+def column_scale(colsq, stream=None):
     """D = column norms from column sums of squares (zero columns -> 1), and
-    ||A D^{-1}||_F for it."""
-    d = torch.sqrt(colsq.double())
-    nz = d > 0
-    d = torch.where(nz, d, torch.ones_like(d))
-    return d, float(torch.sqrt(nz.sum().double()).item())
+    ||A D^{-1}||_F for it, both computed on the device (tomos_column_scale):
+    returns (d, anorm) with anorm a one-element float64 CUDA tensor, which
+    lsqr_solve takes as anorm_fro without a host round trip."""
+    n = colsq.numel()
+    d = torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
+    an = torch.empty(1, dtype=torch.float64, device="cuda")
+    C.check(C.lib().tomos_column_scale(_ptr(colsq), n, _ptr(d), _ptr(an), _stream(stream)),
+            "column_scale")
+    return d[:n], an

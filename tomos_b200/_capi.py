@@ -46,7 +46,8 @@ class LsqrOpts(ctypes.Structure):
                 ("implicit_duplicate", c_i32), ("warm_start", c_i32), ("inner_rtol", c_dbl),
                 ("anorm_fro", c_dbl), ("col_scale", c_vp), ("history", ctypes.POINTER(c_dbl)),
                 ("history_cap", c_i32), ("profile", c_i32), ("staged_plane", c_vp),
-                ("staged_ld", c_i64), ("refine", c_vp)]
+                ("staged_ld", c_i64), ("anorm_fro_dev", c_vp), ("refine", c_vp),
+                ("inner_eta_factor", c_dbl)]
 
 
 class LsqrReport(ctypes.Structure):
@@ -106,6 +107,7 @@ SIGNATURES = {
                                             c_vp, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
     "tomos_sketch_qr_scratch_bytes": (c_sz, [c_i64, c_i64]),
     "tomos_sketch_qr_precond_f64": (c_i32, [c_i64, c_i64, c_vp, c_i64, c_vp, c_vp, c_sz, c_vp]),
+    "tomos_column_scale": (c_i32, [c_vp, c_i64, c_vp, c_vp, c_vp]),
     "tomos_workspace_create": (c_i32, [c_i64, c_i64, c_i32, c_i32, ctypes.POINTER(c_vp)]),
     "tomos_workspace_destroy": (c_i32, [c_vp]),
     "tomos_workspace_add_precond": (c_i32, [c_vp, ctypes.POINTER(DenseDesc)]),

@@ -138,6 +138,28 @@ struct ChunkDecoder<Elem::F16> {
     }
 };
 
+// Both elements of one wh word and its wr word, exact for control-0
+// words: for those wh is the fp16 value of the rounded top of the float,
+// so its exact conversion to FP32 has zeros in bits 13..0, and the float's
+// bits are those plus mant_lo (wr >> 2) minus the round flag (wr bit 0)
+// at bit 14 -- the borrow undoes a carry of the rounding into the
+// exponent, and never reaches the sign (the exponent is >= 113).
+// Control-1 elements come out wrong and are redone by the caller.
+__device__ __forceinline__ float2 decode_pair_fp32_16(uint32_t w, uint32_t r) {
+    const float2 hv = h2f2(w);
+    const uint32_t s = r >> 2;
+    const uint32_t lo0 = s & 0x3FFFu, fl0 = (r << 14) & 0x4000u;
+    const uint32_t lo1 = r >> 18, fl1 = s & 0x4000u;
+    return make_float2(__uint_as_float(__float_as_uint(hv.x) + lo0 - fl0),
+                       __uint_as_float(__float_as_uint(hv.y) + lo1 - fl1));
+}
+
+// Both elements of a word pair through the full exact decode.
+__device__ __forceinline__ float2 decode_pair_fp32_16_exact(uint32_t w, uint32_t r) {
+    return make_float2(decode_fp32_16_exact_nb(w & 0xFFFFu, r & 0xFFFFu),
+                       decode_fp32_16_exact_nb(w >> 16, r >> 16));
+}
+
 // FP32_16 wh + wr, exact.
 template <>
 struct ChunkDecoder<Elem::A16> {

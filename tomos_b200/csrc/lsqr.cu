@@ -81,6 +81,20 @@ __global__ void fro2_partial_kernel(const void* hi, const void* lo, int64_t oute
     if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
+// ||b|| from its partials, and ||A||_F (from a device value, from
+// ||A||_F^2, or left as the host set it) into the solver state.
+__global__ void __launch_bounds__(256) state_norms_kernel(const double* __restrict__ bpart, int64_t np,
+                                                          const double* anorm_dev, const double* fro2,
+                                                          LsqrDev* st) {
+    __shared__ double sm[32];
+    const double bn = sqrt(block_sum_array(bpart, np, sm));
+    if (threadIdx.x != 0) return;
+    st->rhsnorm = bn;
+    st->bnorm = bn;
+    if (anorm_dev) st->anorm_fro = *anorm_dev;
+    else if (fro2) st->anorm_fro = sqrt(*fro2);
+}
+
 __global__ void fill_f32_kernel(float* p, int64_t n, float v) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
@@ -112,6 +126,22 @@ __global__ void precond_copy_kernel(const void* R, int numeric, int layout, int6
         Rcm[(size_t)j * n + i] = v;
         Rrm[(size_t)i * n + j] = v;
     }
+}
+
+// d_j = sqrt(colsq_j) (1 for an empty column) and ||A D^{-1}||_F =
+// sqrt(#non-empty columns), one block.
+__global__ void __launch_bounds__(256) column_scale_kernel(const double* __restrict__ colsq, int64_t n,
+                                                           double* __restrict__ d, double* __restrict__ anorm) {
+    __shared__ double sm[32];
+    double cnt = 0.0;
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const double c = colsq[j];
+        const bool nz = c > 0.0;
+        d[j] = nz ? sqrt(c) : 1.0;
+        cnt += nz ? 1.0 : 0.0;
+    }
+    cnt = block_sum(cnt, sm);
+    if (threadIdx.x == 0) *anorm = sqrt(cnt);
 }
 
 // ------------------------------------------------------------- n-side
@@ -326,7 +356,7 @@ __global__ void __launch_bounds__(256) nside_finish_kernel(NSide S) {
     } else {
         const double den = st->anorm_fro * xn + st->bnorm;
         const double eta1 = den > 0.0 ? fabs(g.phi_bar) / den : 0.0;
-        if (eta1 <= st->tol) stop = 1;
+        if (eta1 <= st->inner_tol) stop = 1;
         if (st->inner_rtol > 0.0 && fabs(g.phi_bar) <= st->inner_rtol * st->beta_init) stop = 1;
     }
     if (alpha == 0.0 || beta == 0.0) {
@@ -932,35 +962,19 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     s = ops.prepare(st);
     if (s) return s;
 
-    // ||b|| and, for the backward-error rule, ||A||_F.
-    sumsq_partial_kernel<<<ws->gs_max, 256, 0, st>>>(b, m, nullptr, ws->bpart);
-    TOMOS_LAUNCH_CHECK("sumsq_partial_kernel");
-    sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, ws->scal + 2);
-    TOMOS_LAUNCH_CHECK("sum_to_scalar_kernel");
-    ws->launches += 2;
-    double anorm = o->anorm_fro;
+    // ||b|| and, for the backward-error rule, ||A||_F go into the device
+    // state by a kernel (no host round trip before the first pass).
     int extra_passes = 0;
     const double* dsc = o->stop_rule == TOMOS_STOP_BACKWARD ? o->col_scale : nullptr;
-    if (o->stop_rule == TOMOS_STOP_BACKWARD && !(anorm > 0.0)) {
-        s = ops.fro2(ws->scal + 3, dsc, st);
-        if (s) return s;
-        extra_passes = 1;
-        ws->launches += 2;
-    }
-    double hostsc[4];
-    TOMOS_CUDA_TRY(cudaMemcpyAsync(hostsc, ws->scal, sizeof(hostsc), cudaMemcpyDeviceToHost, st));
-    TOMOS_CUDA_TRY(cudaStreamSynchronize(st));
-    const double bnorm = std::sqrt(hostsc[2]);
-    if (o->stop_rule == TOMOS_STOP_BACKWARD && !(anorm > 0.0)) anorm = std::sqrt(hostsc[3]);
+    const bool need_fro = o->stop_rule == TOMOS_STOP_BACKWARD && !o->anorm_fro_dev && !(o->anorm_fro > 0.0);
 
     LsqrDev init_state;
     std::memset(&init_state, 0, sizeof(init_state));
-    init_state.rhsnorm = bnorm;
-    init_state.bnorm = bnorm;
-    init_state.anorm_fro = anorm;
+    init_state.anorm_fro = o->anorm_fro;
     init_state.tol = o->tol;
     init_state.max_relres = o->max_relres;
     init_state.inner_rtol = o->stop_rule == TOMOS_STOP_BACKWARD ? o->inner_rtol : 0.0;
+    init_state.inner_tol = o->tol * (o->inner_eta_factor > 0.0 ? o->inner_eta_factor : 1.0);
     init_state.max_iters = max_iters;
     init_state.stop_rule = o->stop_rule;
     init_state.history = ws->hist;
@@ -970,6 +984,18 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     const double coef_init[2] = {-1.0, 1.0};
     TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->coef_init, coef_init, sizeof(coef_init),
                                    cudaMemcpyHostToDevice, st));
+    sumsq_partial_kernel<<<ws->gs_max, 256, 0, st>>>(b, m, nullptr, ws->bpart);
+    TOMOS_LAUNCH_CHECK("sumsq_partial_kernel");
+    ws->launches += 2;
+    if (need_fro) {
+        s = ops.fro2(ws->scal + 3, dsc, st);
+        if (s) return s;
+        extra_passes = 1;
+        ws->launches += 2;
+    }
+    state_norms_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, o->anorm_fro_dev,
+                                          need_fro ? ws->scal + 3 : nullptr, ws->st);
+    TOMOS_LAUNCH_CHECK("state_norms_kernel");
 
     PassPlan pl_init = ops.plan(true);
     PassPlan pl_iter = ops.plan(false);
@@ -1145,6 +1171,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_fence, st));
     TOMOS_CUDA_TRY(cudaStreamWaitEvent(us, ws->ev_fence, 0));
 
+    const double anorm = H.anorm_fro, bnorm = H.bnorm;
     R.iterations = H.iter;
     R.restarts_used = restarts_used;
     R.converged = converged ? 1 : 0;
@@ -1273,6 +1300,14 @@ tomos_status tomos_workspace_create(int64_t m, int64_t n, int32_t value_type,
     std::memset(ws->st_host, 0, sizeof(LsqrDev));
     cudaMemset(ws->st, 0, sizeof(LsqrDev));
     *out = ws;
+    return TOMOS_OK;
+}
+
+tomos_status tomos_column_scale(const double* colsq, int64_t n, double* d, double* anorm, void* stream) {
+    if (n < 0) return fail(TOMOS_ERR_INVALID, "column_scale: negative n");
+    if (!anorm || (n > 0 && (!colsq || !d))) return fail(TOMOS_ERR_INVALID, "column_scale: null pointer");
+    column_scale_kernel<<<1, 256, 0, as_stream(stream)>>>(colsq, n, d, anorm);
+    TOMOS_LAUNCH_CHECK("column_scale_kernel");
     return TOMOS_OK;
 }
 

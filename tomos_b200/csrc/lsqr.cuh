@@ -22,6 +22,7 @@ struct LsqrDev {
     double arnorm;       // ||A^T r|| from the last restart pass
     double anorm_fro, bnorm;
     double tol, max_relres, inner_rtol;
+    double inner_tol;    // BACKWARD rule: inner cycles end at eta1 <= this
     double* history;     // device, |phi_bar|/||b|| per iteration
     int iter;            // completed iterations, all restarts
     int iter_restart;    // completed iterations in this restart

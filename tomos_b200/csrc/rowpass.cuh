@@ -104,10 +104,12 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
     constexpr int VEC = ChunkElems<E>::value;
     constexpr int HV = VEC / 2;
     if constexpr (E == Elem::A16) {
-        // Chunks in which no lane of the warp holds a control-1 word (most)
-        // take the normal-range formula; the others the branch-free exact
-        // decode -- the choice is uniform over the warp.
-        const unsigned am = __activemask();
+        // Control-0 words (all but ~0.35 % of the bench matrix) decode as
+        // the fp16 conversion of wh plus mant_lo minus the round flag at
+        // bit 14, both added to the converted bits (decode_pair_fp32_16):
+        // five operations an element.  Words with a control bit are redone
+        // by the exact decode, one word at a time and only where a lane of
+        // the warp holds one.
 #pragma unroll
         for (int k = 0; k < NCH; ++k) {
             const bool lv = (live >> k) & 1u;
@@ -117,22 +119,31 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
                 r = lds128(lrow + coff[k]);
             }
             float f[8];
-            if (__any_sync(am, ((h.x | h.y | h.z | h.w) & 0x00010001u) != 0u)) {
-                ChunkDecoder<E>::decode(h, r, f);
-            } else {
-                const uint32_t wh[4] = {h.x, h.y, h.z, h.w};
-                const uint32_t wr[4] = {r.x, r.y, r.z, r.w};
+            {
+                const float2 p0 = decode_pair_fp32_16(h.x, r.x), p1 = decode_pair_fp32_16(h.y, r.y);
+                const float2 p2 = decode_pair_fp32_16(h.z, r.z), p3 = decode_pair_fp32_16(h.w, r.w);
+                f[0] = p0.x; f[1] = p0.y; f[2] = p1.x; f[3] = p1.y;
+                f[4] = p2.x; f[5] = p2.y; f[6] = p3.x; f[7] = p3.y;
+            }
+            // one bit per element with a control bit (bits 0..3: low
+            // halves of words x..w, bits 16..19: high halves); a loop, so
+            // the rare fix is a branch and not predicated code every warp
+            // runs
+            uint32_t flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
+                             ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
+            while (flags) {
+                const int bit = __ffs(flags) - 1;
+                flags &= flags - 1;
+                const int wi = bit & 3, hi = bit >> 4;   // word, half
+                const uint32_t ww = wi == 0 ? h.x : wi == 1 ? h.y : wi == 2 ? h.z : h.w;
+                const uint32_t rw = wi == 0 ? r.x : wi == 1 ? r.y : wi == 2 ? r.z : r.w;
+                const float v = decode_fp32_16_exact_nb((ww >> (hi * 16)) & 0xFFFFu, (rw >> (hi * 16)) & 0xFFFFu);
+                const int q = 2 * wi + hi;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const uint32_t hh = (wh[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
-                    const uint32_t rr = (wr[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
-                    const uint32_t mag = ((hh & 0x7FFEu) << 13) + 0x38000000u + (rr >> 2) - ((rr & 1u) << 14);
-                    f[q] = __uint_as_float(((hh & 0x8000u) << 16) | mag);
-                }
+                for (int e = 0; e < 8; ++e) f[e] = e == q ? v : f[e];
             }
 #pragma unroll
-            for (int e = 0; e < HV; ++e)
-                a[k * HV + e] = lv ? make_float2(f[2 * e], f[2 * e + 1]) : make_float2(0.0f, 0.0f);
+            for (int e = 0; e < HV; ++e) a[k * HV + e] = make_float2(f[2 * e], f[2 * e + 1]);
         }
     } else if constexpr (E == Elem::H16) {
         uint4 h[NCH];
