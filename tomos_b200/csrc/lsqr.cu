@@ -498,7 +498,7 @@ static int fused_nch_max(Elem e, bool acc64) {
 
 // Consumer warps of a pass (RowWarps).
 static int fused_warps(Elem e, bool acc64) {
-    return (acc64 && !elem_two_planes(e)) ? 8 : 12;
+    return !acc64 ? 12 : (elem_two_planes(e) ? 16 : 8);
 }
 
 // Warps per row a pass may split a row over (divisors of its consumer
@@ -506,9 +506,10 @@ static int fused_warps(Elem e, bool acc64) {
 static const int* fused_g_list(Elem e, bool acc64, int* count) {
     static const int g12[] = {2, 3, 4, 6, 12};
     static const int g8[] = {2, 4, 8};
-    const bool eight = fused_warps(e, acc64) == 8;
-    *count = eight ? 3 : 5;
-    return eight ? g8 : g12;
+    static const int g16[] = {2, 4, 8, 16};
+    const int w = fused_warps(e, acc64);
+    *count = w == 8 ? 3 : (w == 16 ? 4 : 5);
+    return w == 8 ? g8 : (w == 16 ? g16 : g12);
 }
 
 // (nch, g) pairs with an instantiation: one warp per row with 1..NCHMAX
@@ -535,6 +536,14 @@ static tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int 
                 case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
                 case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
                 case 8: return launch_fused_t<E, NMAX, 8, ACC64>(P, err, grid, st);
+                default: break;
+            }
+        } else if constexpr (RowWarps<E, ACC64>::value == 16) {
+            switch (g) {
+                case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
+                case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
+                case 8: return launch_fused_t<E, NMAX, 8, ACC64>(P, err, grid, st);
+                case 16: return launch_fused_t<E, NMAX, 16, ACC64>(P, err, grid, st);
                 default: break;
             }
         } else {

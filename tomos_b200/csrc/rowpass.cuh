@@ -64,16 +64,16 @@ struct RowPlanes;
 // columns) to hide their latency.
 template <Elem E, bool ACC64>
 struct RowWarps {
-    static constexpr int value = (ACC64 && RowPlanes<E>::value == 1) ? 8 : 12;
+    static constexpr int value = !ACC64 ? 12 : (RowPlanes<E>::value == 1 ? 8 : 16);
 };
-constexpr int kRowWarps = 12;  // the widest configuration (shared arrays)
+constexpr int kRowWarps = 16;  // the widest configuration (shared arrays)
 
 // 16-byte chunks a lane takes per row part at most (a warp covers 32 x
 // that x VEC columns).
 template <Elem E, bool ACC64>
 struct RowNchMax {
     static constexpr int base = (E == Elem::F32) ? 8 : 4;
-    static constexpr int value = (ACC64 && RowWarps<E, ACC64>::value == 12) ? base / 2 : base;
+    static constexpr int value = (ACC64 && RowPlanes<E>::value == 2) ? base / 2 : base;
 };
 constexpr int kRowMaxStages = 12;
 constexpr size_t kRowSmemBudget = 200 * 1024;
