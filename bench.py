@@ -142,40 +142,19 @@ class ClockSampler:
 # --------------------------------------------------------------------- GPU
 
 def gpu_solve(tb, torch, A, b, s):
-    """One step: sketch (+ column norms) -> QR -> R^{-1} -> LSQR until the
-    backward error of the column-scaled problem is <= 1e-6.  Returns (x, report)."""
-    packed = A.numeric in (tb.NumericType.FP32_16, tb.NumericType.FP32_BF16)
+    """One step: the library's sketch-preconditioned LSQR pipeline
+    (tomos_b200.sketch_lsqr: sketch (+ column norms) -> QR -> R^{-1} ->
+    LSQR until the backward error of the column-scaled problem is <= 1e-6).
+    Returns (x, report)."""
     m, n = A.size
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if gpu_solve.profile else None
-    if ev:
-        ev[0].record()
-    plane = None
-    if A.numeric == tb.NumericType.FP32_16:
-        # the sketch pass also writes the fp16 plane the HALF-tier iterations read
-        SA, fro2, colsq, plane = tb.apply_count_sketch(A, s, tier=tb.Tier.HALF, with_colsq=True,
-                                                       stage=True)
-    else:
-        SA, fro2, colsq = tb.apply_count_sketch(A, s, tier=tb.Tier.HALF if packed else tb.Tier.AUTO,
-                                                with_colsq=True)
-    if ev:
-        ev[1].record()
-    Rinv = tb.generate_sketch_qr_precond(SA, copy=False)
-    if ev:
-        ev[2].record()
-    d, anorm = tb.column_scale(colsq)
-    gpu_solve.last_scale = d
     ws = gpu_solve.ws.get((m, n))
     if ws is None:
         ws = tb.create_lsqr_workspace(None, (m, n), tb.NumericType.FP32, tb.NumericType.FP64)
         gpu_solve.ws[(m, n)] = ws
-    tb.add_precond(Rinv, ws)
-    x = torch.empty(n, device="cuda")  # the solve zeroes x
-    rep = tb.lsqr_solve(None, A, b, x, ws, TOL, 200, 0.0, restarts=8,
-                        stop_rule=tb.StopRule.BACKWARD, inner_rtol=2e-3 if packed else 0.0,
-                        anorm_fro=anorm, col_scale=d, staged_plane=plane,
-                        profile=gpu_solve.profile)
+    x, rep, d = tb.sketch_lsqr(A, b, s, tol=TOL, workspace=ws, profile=gpu_solve.profile, events=ev)
+    gpu_solve.last_scale = d
     if ev:
-        ev[3].record()
         torch.cuda.synchronize()
         rep = dict(rep)
         rep["phase_ms"] = {"sketch": ev[0].elapsed_time(ev[1]), "qr": ev[1].elapsed_time(ev[2]),
@@ -258,12 +237,41 @@ def run_ours(args):
     # eta_D of the column-scaled problem (the convergence measure) and the
     # plain normwise eta
     ws_be = tb.create_lsqr_workspace(None, (m, n), tb.NumericType.FP32)
-    d_exact = gpu_solve.last_scale  # column norms from the last FP32-storage sketch
+    d_exact = torch.zeros(n, dtype=torch.float64, device="cuda")  # exact column norms, FP64
+    for r0 in range(0, m, 1 << 17):
+        d_exact += (A32[r0:r0 + (1 << 17)].double() ** 2).sum(dim=0)
+    d_exact = torch.sqrt(d_exact)
     be_p = tb.backward_error(Ap, b, xp, ws_be, col_scale=d_exact)["backward_error"]
     be_f = tb.backward_error(Af, b, xf, ws_be, col_scale=d_exact)["backward_error"]
     be_p_plain = tb.backward_error(Ap, b, xp, ws_be)["backward_error"]
     be_f_plain = tb.backward_error(Af, b, xf, ws_be)["backward_error"]
     rel_x = float(torch.linalg.norm((xp - xt).double()) / torch.linalg.norm(xt.double()))
+    # forward error against the FP64 least-squares solution (Householder QR
+    # of A in FP64, torch on the device), weighted by the column norms D --
+    # what eta_D <= 1e-6 bounds (x_true is off the LS solution by the noise,
+    # and the small columns' components are not determined to 1e-6 unweighted)
+    A64 = A32.double()
+    x_ls = torch.linalg.lstsq(A64, b.double().unsqueeze(1)).solution.squeeze(1)
+    del A64
+    fe_p = float(torch.linalg.norm(d_exact * (xp.double() - x_ls)) / torch.linalg.norm(d_exact * x_ls))
+    fe_f = float(torch.linalg.norm(d_exact * (xf.double() - x_ls)) / torch.linalg.norm(d_exact * x_ls))
+    torch.cuda.empty_cache()
+
+    # the standalone GEMV / GEMV^T (tomos_gemv, the registry's mv_apply
+    # entry) on the same matrix, y = A x and y = A^T x, per storage tier:
+    # algorithmic bytes (elements read once, x, y) / CUDA-event time
+    gemv = {}
+    xv = torch.randn(n, device="cuda")
+    uv = torch.randn(m, device="cuda")
+    for name, A, tier, eb in (("fp32", Af, tb.Tier.AUTO, 4), ("fp32_16_half", Ap, tb.Tier.HALF, 2),
+                              ("fp32_16_accurate", Ap, tb.Tier.ACCURATE, 4)):
+        for tr, xin, yout in ((tb.TransposeType.NO_TRANSPOSE, xv, uv), (tb.TransposeType.TRANSPOSE, uv, xv)):
+            f = (lambda A=A, tr=tr, xin=xin, yout=yout, tier=tier:
+                 tb.mv_apply(tb.Device.CUDA, tr, 1.0, A, xin, 0.0, yout, tier=tier))
+            ms_g, _ = time_steps(torch, f, 5, 2)
+            gb = (eb * m * n + 4.0 * (m + n)) / (ms_g * 1e-3) / 1e9
+            gemv[f"{name}_{'t' if tr == tb.TransposeType.TRANSPOSE else 'n'}"] = {
+                "ms": ms_g, "gbs": gb, "frac_of_measured_hbm": gb / measured_peak()[0]}
 
     # roofline of the dominant kernel (the fused pass over the wh plane):
     # one profiled solve times every pass with CUDA events on its stream.
@@ -316,7 +324,7 @@ def run_ours(args):
                              count_launches(torch, lambda: gpu_solve(tb, torch, Af, b, s)))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference(args, m, n)
+        cpu = cpu_reference(args, m, n, hostA.numpy(), hostb.numpy())
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms_packed, "unit": "ms", "n_gpus": world,
@@ -334,13 +342,17 @@ def run_ours(args):
                            "fp32_restarts": rep_f["restarts_used"]},
             "backward_error": {"measure": "eta_D: backward error of (A D^-1, b, D x), D = column norms",
                                "packed": be_p, "fp32": be_f, "packed_plain_eta": be_p_plain,
-                               "fp32_plain_eta": be_f_plain, "x_rel_err_vs_xtrue": rel_x},
+                               "fp32_plain_eta": be_f_plain, "x_rel_err_vs_xtrue": rel_x,
+                               "x_rel_err_D_vs_fp64_ls": {"packed": fe_p, "fp32": fe_f,
+                                                          "measure": "||D (x - x_LS)|| / ||D x_LS||, "
+                                                                     "x_LS by FP64 Householder QR"}},
             "phase_ms": {"packed": prof_p.get("phase_ms"), "fp32": prof_f.get("phase_ms"),
                          "packed_restart_pass_ms": init_ms,
                          "note": "one profiled solve each (passes timed one by one)"},
             "gemv_gbs": {"fused_pass_fp32_16_half": ach, "fused_pass_fp32": ach_f,
                          "fused_pass_fp32_16_exact_fp64acc": ach_init,
-                         "pass_ms_half": pass_ms, "pass_ms_fp32": pass_ms_f},
+                         "pass_ms_half": pass_ms, "pass_ms_fp32": pass_ms_f,
+                         "standalone": gemv},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
                          "kernel": "fused_rows_mma_kernel (staged fp16 plane, tensor cores; one LSQR "
@@ -360,61 +372,107 @@ def run_ours(args):
 
 # --------------------------------------------------------------------- CPU
 
-def cpu_reference(args, m, n, seed=0):
-    """The reference's own CPU path (oracle/_ref: its lsqr_solve, hash
-    CountSketch and LAPACK sketch QR) on a row sample of the workload,
-    extrapolated linearly in m to the full problem.  Test/baseline
-    infrastructure: the product never calls it."""
+def _eta_d_blocks(A, b, d, x, blk=100_000):
+    """eta_D of x (FP64, row blocks of the float32 host matrix A)."""
+    x = np.asarray(x, np.float64)
+    r2 = b2 = 0.0
+    atr = np.zeros(A.shape[1])
+    for r0 in range(0, A.shape[0], blk):
+        Ab = A[r0:r0 + blk].astype(np.float64)
+        bb = b[r0:r0 + blk].astype(np.float64)
+        r = bb - Ab @ x
+        r2 += float(r @ r)
+        b2 += float(bb @ bb)
+        atr += Ab.T @ r
+    an = math.sqrt(float(np.count_nonzero(d > 0)))
+    dd = np.where(d > 0, d, 1.0)
+    rn = math.sqrt(r2)
+    e1 = rn / (an * float(np.linalg.norm(dd * x)) + math.sqrt(b2))
+    e2 = float(np.linalg.norm(atr / dd)) / (an * rn) if rn > 0 else 0.0
+    return min(e1, e2)
+
+
+def cpu_reference(args, m, n, A_host, b_host, steps=1):
+    """The reference's own CPU path (oracle/_ref, built from its sources) on
+    the whole workload -- the same A and b as the GPU arm, copied to the
+    host: its hash CountSketch (countsketch_apply_impl<float>, one thread),
+    its FP64 sketch QR (generate_sketch_qr_precond: dgeqrf + dtrtri) and its
+    lsqr_solve (FP32, OpenBLAS sgemv on all host threads), each timed around
+    the reference's own call alone (copies into its Dense objects and the
+    workspace creation are outside).  The reference's LSQR stops on
+    |phi_bar|/||b|| only, so its iteration count is the smallest k whose
+    returned x meets the same eta_D <= 1e-6 (FP64, exact column norms) the
+    GPU arm stops on, found by untimed runs; each timed solve then does
+    exactly k iterations.  Test/baseline infrastructure: the product never
+    calls it."""
     import ctypes
     import oracle
     if not oracle.ref_available():
         return {"value": None, "unavailable": "reference CPU build missing"}
     R = oracle.ref()
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
-    ms = min(args.cpu_rows, m)
-    rng = np.random.default_rng(seed)
-    u = rng.uniform(-3, 3, n)
-    A = np.asfortranarray((rng.standard_normal((ms, n)) * 10.0 ** u).astype(np.float32))
-    xt = rng.standard_normal(n)
-    b = (A.astype(np.float64) @ xt + 1e-8 * rng.standard_normal(ms)).astype(np.float32)
     s = 4 * n
-    A64 = np.asfortranarray(A.astype(np.float64))
-    SA = np.zeros((s, n), np.float64, order="F")
-    t0 = time.perf_counter()
-    R.ref_countsketch_apply_f64(ms, n, P(A64), ms, s, P(SA), s)
-    t_sketch = time.perf_counter() - t0
-    W = SA.copy(order="F")
-    t0 = time.perf_counter()
-    rc = R.ref_sketch_qr_f64(s, n, P(W))
-    t_qr = time.perf_counter() - t0
-    Rinv = np.asfortranarray(np.triu(W[:n, :n]).astype(np.float32))
-    # its own LSQR to a tight tolerance, timed; the iteration at which the
-    # normwise backward error first reaches 1e-6 is read off its residual
-    # history (||r_k|| = |phi_bar_k|).
-    iters_cap = 60
-    x = np.zeros(n, np.float32)
+    A_cm = np.asfortranarray(A_host)            # the reference is column-major
+    b32 = np.ascontiguousarray(b_host, np.float32)
+    d = np.zeros(n)
+    for r0 in range(0, m, 100_000):
+        d += (A_host[r0:r0 + 100_000].astype(np.float64) ** 2).sum(axis=0)
+    d = np.sqrt(d)
+    sec = ctypes.c_double(0.0)
     it = ctypes.c_int(0)
-    hist = np.zeros(iters_cap + 2)
-    t0 = time.perf_counter()
-    R.ref_lsqr_solve_f32(ms, n, P(A), P(b), P(x), P(Rinv), 1e-12, iters_cap, 1e-12, 1,
+
+    def sketch_qr():
+        SA32 = np.zeros((s, n), np.float32, order="F")
+        t0 = time.perf_counter()
+        R.ref_countsketch_apply_f32(m, n, P(A_cm), m, s, P(SA32), s)
+        ts = time.perf_counter() - t0
+        SA = np.asfortranarray(SA32.astype(np.float64))
+        rc = R.ref_sketch_qr_f64_timed(s, n, P(SA), ctypes.byref(sec))
+        return ts, sec.value, rc, np.asfortranarray(np.triu(SA[:n, :n]).astype(np.float32))
+
+    def lsqr(k):
+        x = np.zeros(n, np.float32)
+        R.ref_lsqr_solve_f32_timed(m, n, P(A_cm), P(b32), P(x), P(Rinv), 0.0, k, 0.0, 1,
+                                   ctypes.byref(it), ctypes.byref(sec))
+        return x, sec.value
+
+    ts, tq, rc, Rinv = sketch_qr()
+    # iterations to eta_D <= 1e-6: estimate from one long run's |phi_bar|
+    # history, then confirm with untimed runs of k iterations
+    cap = 60
+    hist = np.zeros(cap + 2)
+    xl = np.zeros(n, np.float32)
+    R.ref_lsqr_solve_f32(m, n, P(A_cm), P(b32), P(xl), P(Rinv), 0.0, cap, 0.0, 1,
                          ctypes.byref(it), P(hist))
-    t_lsqr = time.perf_counter() - t0
-    k = max(1, it.value)
-    t_iter = t_lsqr / k
-    bn = float(np.linalg.norm(b.astype(np.float64)))
-    an = float(np.linalg.norm(A.astype(np.float64)))
-    xn = float(np.linalg.norm(x.astype(np.float64)))
-    eta_k = hist[:k] * bn / (an * xn + bn)
-    hit = np.flatnonzero(eta_k <= TOL)
-    k_needed = int(hit[0]) + 1 if hit.size else k
-    scale = m / ms
-    total_s = t_sketch * scale + t_qr + k_needed * t_iter * scale
-    return {"value": total_s * 1e3, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"{ms}x{n} row sample of the workload on the reference's CPU lsqr_solve "
-                      f"(FP32, OpenBLAS) with its sketch QR; sketch and per-iteration time "
-                      f"extrapolated x{scale:g} in m; {k_needed} iterations to eta<=1e-6",
-            "extrapolated": True, "sketch_s": t_sketch, "qr_s": t_qr, "iter_s": t_iter,
-            "iterations": k_needed, "qr_rc": int(rc)}
+    bn = float(np.linalg.norm(b32.astype(np.float64)))
+    an = math.sqrt(float(np.count_nonzero(d > 0)))
+    est = hist[:it.value] * bn / (an * float(np.linalg.norm(d * xl)) + bn)
+    hit = np.flatnonzero(est <= TOL)
+    k = int(hit[0]) + 1 if hit.size else it.value
+    eta = _eta_d_blocks(A_host, b32, d, lsqr(k)[0])
+    while eta > TOL and k < cap:
+        k += 1
+        eta = _eta_d_blocks(A_host, b32, d, lsqr(k)[0])
+    while k > 1:
+        e_prev = _eta_d_blocks(A_host, b32, d, lsqr(k - 1)[0])
+        if e_prev > TOL:
+            break
+        k, eta = k - 1, e_prev
+    totals, parts = [], None
+    for _ in range(max(1, steps)):
+        ts, tq, rc, Rinv = sketch_qr()
+        _, tl = lsqr(k)
+        totals.append(ts + tq + tl)
+        parts = (ts, tq, tl)
+    threads = os.environ.get("OPENBLAS_NUM_THREADS") or str(os.cpu_count())
+    return {"value": float(np.mean(totals)) * 1e3, "unit": "ms", "cores": int(threads),
+            "kind": "reference",
+            "sample": f"the whole {m}x{n} workload (same A, b as the GPU arm) on the reference's CPU "
+                      f"path: CountSketch s={s} (one thread), FP64 sketch QR, lsqr_solve FP32 with "
+                      f"OpenBLAS on {threads} threads, {k} iterations (the first k whose x has "
+                      f"eta_D <= 1e-6: {eta:.2e}); each call timed alone, mean of {len(totals)}",
+            "extrapolated": False, "same_config": True, "sketch_s": parts[0], "qr_s": parts[1],
+            "lsqr_s": parts[2], "iterations": k, "eta_D": eta, "qr_rc": int(rc)}
 
 
 def run_reference(args):
@@ -422,17 +480,27 @@ def run_reference(args):
     if rank != 0:
         return
     m, n = args.m, args.n
-    vals = []
-    last = None
-    for _ in range(max(1, args.steps)):
-        last = cpu_reference(args, m, n)
-        if last.get("value") is None:
-            print(json.dumps({"impl": "reference", "unavailable": last.get("unavailable")}))
-            return
-        vals.append(last["value"])
-    v = float(np.mean(vals))
-    cpu = dict(last)
-    cpu["value"] = v
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build missing"}))
+        return
+    # the same seeded workload as the GPU arm (generated on the device, then
+    # copied to the host once; the reference runs on the host cores only;
+    # without a GPU, torch's CPU generator draws another matrix of the same
+    # distribution)
+    import torch
+    from tomos_b200 import problems
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    A32, _, b = problems.dense_scaled(m, n, seed=args.seed, device=dev)
+    Ah, bh = A32.cpu().numpy(), b.cpu().numpy()
+    del A32, b
+    if dev == "cuda":
+        torch.cuda.empty_cache()
+    cpu = cpu_reference(args, m, n, Ah, bh, steps=args.steps)
+    if cpu.get("value") is None:
+        print(json.dumps({"impl": "reference", "unavailable": cpu.get("unavailable")}))
+        return
+    v = cpu["value"]
     line = {"metric": METRIC, "value": v, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",

@@ -104,6 +104,9 @@ def ref():
         R.ref_mv_f32.argtypes = [_i32, _dbl, _sz, _sz, _vp, _vp, _dbl, _vp]
         R.ref_sketch_qr_f64.argtypes = [_sz, _sz, _vp]
         R.ref_lsqr_solve_f32.argtypes = [_sz, _sz, _vp, _vp, _vp, _vp, _dbl, _i32, _dbl, _i32, _vp, _vp]
+        R.ref_lsqr_solve_f32_timed.argtypes = [_sz, _sz, _vp, _vp, _vp, _vp, _dbl, _i32, _dbl, _i32,
+                                               _vp, _vp]
+        R.ref_sketch_qr_f64_timed.argtypes = [_sz, _sz, _vp, _vp]
         R.ref_lsqr_iterate_f32.argtypes = [_sz, _sz, _vp, _vp, _vp, _vp, _i32]
         _ref = R
     return _ref
@@ -234,6 +237,46 @@ def lstsq_f64(A, b):
     b = np.asarray(b, np.float64)
     Q, R = np.linalg.qr(A)
     return np.linalg.solve(R, Q.T @ b)
+
+
+def lstsq_f64_blocks(blocks, n):
+    """FP64 least-squares solution of a tall problem given as row blocks
+    (A_k, b_k), by Householder QR of [A b] one block at a time (TSQR): the
+    R of [R_prev; A_k b_k] is carried, so only one block is in memory.
+    Returns (x, ||r||) with ||r|| = |R[n, n]|, the least-squares residual.
+    Same solution as lstsq_f64 on the stacked rows."""
+    R = np.zeros((0, n + 1))
+    for A, b in blocks:
+        blk = np.empty((A.shape[0], n + 1))
+        blk[:, :n] = A
+        blk[:, n] = b
+        R = np.linalg.qr(np.vstack([R, blk]), mode="r")
+        R = R[: n + 1]
+    x = np.linalg.solve(np.triu(R[:n, :n]), R[:n, n])
+    rn = abs(R[n, n]) if R.shape[0] > n else 0.0
+    return x, rn
+
+
+def residual_norms_blocks(blocks, x, d=None):
+    """FP64 ||b - A x||, ||D^{-1} A^T (b - A x)||, ||A D^{-1}||_F^2 and ||b||
+    over row blocks (the pieces of eta and eta_D, accumulated exactly in
+    FP64 without holding A)."""
+    x = np.asarray(x, np.float64)
+    r2 = b2 = 0.0
+    atr = None
+    fro = None
+    for A, b in blocks:
+        A = np.asarray(A, np.float64)
+        r = np.asarray(b, np.float64) - A @ x
+        r2 += float(r @ r)
+        b2 += float(np.asarray(b, np.float64) @ np.asarray(b, np.float64))
+        t = A.T @ r
+        atr = t if atr is None else atr + t
+        c = (A * A).sum(axis=0)
+        fro = c if fro is None else fro + c
+    if d is None:
+        d = np.ones_like(fro)
+    return np.sqrt(r2), float(np.linalg.norm(atr / d)), float((fro / d ** 2).sum()), np.sqrt(b2)
 
 
 def backward_error(A, b, x):

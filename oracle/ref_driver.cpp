@@ -9,6 +9,7 @@
 //
 // Functions return 0 on success and -1 if the reference threw.
 
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -179,6 +180,61 @@ int ref_lsqr_solve_f32(size_t m, size_t n, const float* A, const float* b,
         if (iterations) *iterations = its;
         if (history)
             for (size_t i = 0; i < hist.size(); ++i) history[i] = hist[i];
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// ref_lsqr_solve_f32 with the setup (copies into the reference's Dense
+// objects, workspace creation, add_precond) outside the timed region:
+// *seconds receives the wall time of the lsqr_solve call alone.
+int ref_lsqr_solve_f32_timed(size_t m, size_t n, const float* A, const float* b, float* x,
+                             const float* Rinv, double tol, int max_iters, double max_relres,
+                             int restarts, int* iterations, double* seconds) {
+    try {
+        Context ctx(Device::CPU);
+        Dense dA = Dense::create_strided(ctx, Layout::COL_MAJOR, NumericType::FP32, {m, n});
+        fill_colmajor(dA, A, m, n);
+        Dense db = Dense::create_strided(ctx, Layout::COL_MAJOR, NumericType::FP32, {m, 1});
+        fill_colmajor(db, b, m, 1);
+        Dense dx = Dense::create_strided(ctx, Layout::COL_MAJOR, NumericType::FP32, {n, 1});
+        Dense dR = Dense::create_strided(ctx, Layout::COL_MAJOR, NumericType::FP32, {n, n});
+        Workspace ws = create_lsqr_workspace(ctx, {m, n}, NumericType::FP32);
+        if (Rinv) {
+            fill_colmajor(dR, Rinv, n, n);
+            add_precond(dR, ws);
+        }
+        int its = 0;
+        const auto t0 = std::chrono::steady_clock::now();
+        lsqr_solve(ctx, dA, db, dx, ws, tol, max_iters, max_relres, &its, nullptr, restarts);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+        read_colmajor(dx, x, n, 1);
+        if (iterations) *iterations = its;
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// ref_sketch_qr_f64 with the copies in and out of the reference's Dense
+// outside the timed region: *seconds receives the wall time of
+// generate_sketch_qr_precond alone.
+int ref_sketch_qr_f64_timed(size_t k, size_t n, double* SA, double* seconds) {
+    try {
+        Context ctx(Device::CPU);
+        Dense d = Dense::create_strided(ctx, Layout::COL_MAJOR, NumericType::FP64, {k, n});
+        auto v = as_strided_view<double>(d);
+        for (size_t j = 0; j < n; ++j)
+            for (size_t i = 0; i < k; ++i) v.values_[i + j * v.lead_dim_] = SA[i + j * k];
+        Sparse S = Sparse::create_csr(ctx, NumericType::FP64, IntType::INT32, {k, k}, k);
+        const auto t0 = std::chrono::steady_clock::now();
+        generate_sketch_qr_precond(S, d);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+        for (size_t j = 0; j < n; ++j)
+            for (size_t i = 0; i < k; ++i) SA[i + j * k] = v.values_[i + j * v.lead_dim_];
         return 0;
     } catch (const std::exception&) {
         return -1;

@@ -1,4 +1,7 @@
-"""The full-size parity configurations besides the benchmark's own:
+"""The full-size parity configurations:
+
+* the benchmark's own 1,000,000 x 1000 (FP32_16 and FP32 storage) against
+  the FP64 Householder-QR oracle of the whole problem on the host;
 
 * 4,000,000 x 2000 in FP32_BF16 storage (32 GB packed): bf16 iterations with
   FP32 accumulation and exact restarts as the residual refinement (at most
@@ -55,6 +58,54 @@ def solve(A, b, s, restarts, inner_rtol, sketch_tier=tb.Tier.AUTO):
                         stop_rule=tb.StopRule.BACKWARD, inner_rtol=inner_rtol, anorm_fro=an,
                         col_scale=d)
     return x, rep, d
+
+
+@pytest.mark.timeout(900)
+def test_config2_packed_and_fp32_1e6x1000(orc):
+    """Config 2, the benchmark's own workload, at full size (1,000,000 x
+    1000, A = G diag(10^u), u ~ U(-3, 3), b = A x_true + 1e-8 noise,
+    s = 4000): FP32_16 packed and FP32 storage through the library's
+    pipeline (tomos_b200.sketch_lsqr) to eta_D <= 1e-6, checked against the
+    FP64 oracle on the host:
+      * eta_D of the returned x from an independent FP64 residual of the
+        whole problem (D = the exact column norms);
+      * the D-weighted forward error ||D (x - x_o)|| / ||D x_o|| against the
+        least-squares solution x_o of FP64 Householder QR of [A b] (TSQR
+        over row blocks of 100,000).  eta_D measures A's perturbation in
+        ||A D^{-1}||_F = sqrt(n), so the forward error it allows is about
+        kappa_2(A D^{-1}) sqrt(n) eta_D, with kappa_2 ~ 1.07 for this
+        matrix: at eta_D <= 1e-6 the bound asserted is 2 sqrt(n) 1e-6."""
+    m, n, s = 1_000_000, 1000, 4000
+    A32, xt, b = problems.dense_scaled(m, n, seed=0)
+    Af = tb.Dense(NT.FP32, L.ROW_MAJOR, (m, n), n, A32.view(-1))
+    Ap = tb.pack(Af, NT.FP32_16)
+    got = {}
+    for name, A in (("fp32_16", Ap), ("fp32", Af)):
+        x, rep, _ = tb.sketch_lsqr(A, b, s)
+        torch.cuda.synchronize()
+        assert rep["converged"] == 1, (name, rep)
+        got[name] = (x.cpu().numpy().astype(np.float64), rep)
+    del Ap
+    Ah = A32.cpu().numpy()
+    bh = b.cpu().numpy()
+    blk = 100_000
+
+    def blocks():
+        for r0 in range(0, m, blk):
+            yield Ah[r0:r0 + blk], bh[r0:r0 + blk]
+
+    d = np.sqrt(sum((a.astype(np.float64) ** 2).sum(axis=0) for a, _ in blocks()))
+    xo, _ = orc.lstsq_f64_blocks(blocks(), n)
+    for name, (x, rep) in got.items():
+        rn, atr, fro, bn = orc.residual_norms_blocks(blocks(), x, d)
+        an = np.sqrt(fro)
+        eta = min(rn / (an * np.linalg.norm(d * x) + bn), atr / (an * rn))
+        fe = np.linalg.norm(d * (x - xo)) / np.linalg.norm(d * xo)
+        print(f"config 2 {name}: eta_D {eta:.3e} (solver {rep['backward_error']:.3e}), "
+              f"D-weighted forward error vs FP64 QR {fe:.3e}, {rep['iterations']} iterations")
+        assert eta <= 1.05e-6, (name, eta)
+        assert abs(eta - rep["backward_error"]) <= 0.05 * eta
+        assert fe <= 2.0 * np.sqrt(n) * 1e-6, (name, fe)
 
 
 def test_config3_bf16_refinement_4e6x2000(orc):

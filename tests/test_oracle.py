@@ -191,3 +191,21 @@ def test_oracle_against_reference_library(orc):
     x2, i2, _ = orc.ref_lsqr_f32(A, bb)
     assert abs(i1 - i2) <= 1
     assert np.linalg.norm(x1 - x2) / np.linalg.norm(x2) < 1e-5
+
+
+def test_blocked_lstsq_and_residuals_match_dense(orc):
+    """The row-block oracle (TSQR of [A b] by Householder QR, FP64 residual
+    pieces) agrees with the dense oracle on a problem held whole."""
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((4000, 30)) * 10.0 ** rng.uniform(-3, 3, 30)
+    b = rng.standard_normal(4000)
+    blocks = [(A[i:i + 650], b[i:i + 650]) for i in range(0, 4000, 650)]
+    x, rn = orc.lstsq_f64_blocks(blocks, 30)
+    xo = orc.lstsq_f64(A, b)
+    assert np.linalg.norm(x - xo) <= 1e-12 * np.linalg.norm(xo)
+    assert abs(rn - np.linalg.norm(b - A @ xo)) <= 1e-10 * rn
+    d = np.linalg.norm(A, axis=0)
+    r2, atr, fro, bn = orc.residual_norms_blocks(blocks, xo, d)
+    an = np.sqrt(fro)
+    eta = min(r2 / (an * np.linalg.norm(d * xo) + bn), atr / (an * r2))
+    assert abs(eta - orc.backward_error_scaled(A, b, xo)) <= 1e-10 * max(eta, 1e-300) + 1e-15

@@ -719,3 +719,55 @@ def column_scale(colsq, stream=None):
     C.check(C.lib().tomos_column_scale(_ptr(colsq), n, _ptr(d), _ptr(an), _stream(stream)),
             "column_scale")
     return d[:n], an
+
+
+def sketch_lsqr(A, b, s, tol=1e-6, max_iters=200, restarts=8, inner_rtol=None, workspace=None,
+                x=None, profile=False, events=None, stream=None):
+    """The sketch-preconditioned LSQR pipeline of the reference's runner
+    (lsqr_precision_runner.cu:588-656: sketch, generate_sketch_qr_precond,
+    add_precond, lsqr_solve) with the BACKWARD stopping rule on the
+    column-scaled problem:
+
+      hash CountSketch SA = S A (s rows) with the column sums of squares --
+      for a row-major FP32_16 A the same pass writes the fp16 plane its
+      HALF-tier iterations read -- then the FP64 sketch QR and R^{-1}, the
+      column scale D on the device, and LSQR until eta_D <= tol, packed
+      storage refined by exact restart passes.
+
+    Returns (x, report, d).  workspace: an (m, n) FP32/FP64 workspace to
+    reuse (created when None).  inner_rtol: the refinement cycles' residual
+    reduction (default 2e-3 for packed storage, none for FP32).  events:
+    four torch.cuda.Event recorded at the start, after the sketch, after
+    the QR and after the solve (phase timing)."""
+    m, n = A.size
+    packed = A.numeric in PACKED
+    plane = None
+    if events:
+        events[0].record()
+    if (isinstance(A, Dense) and A.numeric == NumericType.FP32_16 and A.layout == Layout.ROW_MAJOR
+            and (A.ld * 2) % 16 == 0):
+        SA, _, colsq, plane = apply_count_sketch(A, s, tier=Tier.HALF, with_colsq=True, stage=True,
+                                                 stream=stream)
+    else:
+        SA, _, colsq = apply_count_sketch(A, s, tier=Tier.HALF if packed else Tier.AUTO,
+                                          with_colsq=True, stream=stream)
+    if events:
+        events[1].record()
+    Rinv = generate_sketch_qr_precond(SA, copy=False, stream=stream)
+    if events:
+        events[2].record()
+    d, anorm = column_scale(colsq, stream=stream)
+    ws = workspace
+    if ws is None:
+        ws = create_lsqr_workspace(None, (m, n), NumericType.FP32, NumericType.FP64)
+    add_precond(Rinv, ws)
+    if x is None:
+        x = torch.empty(n, dtype=torch.float32, device="cuda")  # the solve zeroes x
+    if inner_rtol is None:
+        inner_rtol = 2e-3 if packed else 0.0
+    rep = lsqr_solve(None, A, b, x, ws, tol, max_iters, 0.0, restarts=restarts,
+                     stop_rule=StopRule.BACKWARD, inner_rtol=inner_rtol, anorm_fro=anorm,
+                     col_scale=d, staged_plane=plane, profile=profile, stream=stream)
+    if events:
+        events[3].record()
+    return x, rep, d

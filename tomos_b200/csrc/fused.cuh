@@ -38,7 +38,8 @@ struct FusedParams {
     const float* p;        // n
     const float* u_in;     // m
     float* u_out;          // m (may alias u_in)
-    const double* coef;    // [cp, cu]
+    const double* coef;    // device [cp, cu], or NULL: the host values cp, cu
+    double cp, cu;
     float* qpart;          // gridDim.x x qstride
     double* sspart;        // gridDim.x
     int64_t qstride;

@@ -207,7 +207,9 @@ size_t gemv_scratch_bytes_max(const tomos_dense* A, int32_t trans) {
     int64_t outer, inner;
     std::string why;
     if (!gemv_shape(A, trans, &dot, &outer, &inner, &why) || dot) return 0;
-    return (size_t)line_sum_chunks(outer) * (size_t)inner * 8;
+    const size_t generic = (size_t)line_sum_chunks(outer) * (size_t)inner * 8;
+    const size_t rowpass = rowpass_gemv_scratch_bytes(inner);
+    return generic > rowpass ? generic : rowpass;
 }
 
 tomos_status gemv_dispatch(int32_t trans, double alpha, const tomos_dense* A, int32_t tier,
@@ -238,6 +240,9 @@ tomos_status gemv_dispatch(int32_t trans, double alpha, const tomos_dense* A, in
     L.beta = beta;
     L.scratch = scratch;
     L.scratch_bytes = scratch_bytes;
+    bool used = false;
+    tomos_status rs = rowpass_gemv(L, e, st, &used);
+    if (used) return rs;
     return gemv_launch(L, e, elem_is_exact(e), st);
 }
 

@@ -35,6 +35,11 @@ size_t gemv_scratch_bytes_max(const tomos_dense* A, int32_t trans);
 
 tomos_status gemv_launch(const GemvLaunch& L, Elem e, bool acc64, cudaStream_t st);
 
+// The product through the row pass (rowpass_gemv.cu) when A's lines fit
+// it; *used false (nothing launched) otherwise.
+tomos_status rowpass_gemv(const GemvLaunch& L, Elem e, cudaStream_t st, bool* used);
+size_t rowpass_gemv_scratch_bytes(int64_t inner);
+
 tomos_status gemv_dispatch(int32_t trans, double alpha, const tomos_dense* A, int32_t tier,
                            const float* x, double beta, float* y, void* scratch,
                            size_t scratch_bytes, cudaStream_t st);

@@ -33,6 +33,7 @@
 #include "gemv.cuh"
 #include "lsqr.cuh"
 #include "rowpass.cuh"
+#include "rowpass_launch.cuh"
 #include "rowpass_mma.cuh"
 
 namespace tomos_b200 {
@@ -415,28 +416,6 @@ static tomos_status ensure_history(tomos_workspace* ws, int cap) {
 
 // ------------------------------------------------------------ A passes
 
-template <Elem E, int NCH, int G, bool ACC64>
-static tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
-    constexpr int ESZ = (E == Elem::F32) ? 4 : 2;
-    constexpr int CW = RowWarps<E, ACC64>::value;
-    constexpr int RS = CW / G;
-    RowPassParams T;
-    T.f = P;
-    T.err = err;
-    T.copy_bytes = (int)((((int64_t)P.n * ESZ) + 15) / 16 * 16);
-    const size_t stage = (size_t)RS * T.copy_bytes * RowPlanes<E>::value;
-    int ns = (int)(kRowSmemBudget / stage);
-    if (ns > kRowMaxStages) ns = kRowMaxStages;
-    if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
-    T.nstage = ns;
-    const size_t smem = fused_rows_smem<E, NCH, ACC64>(ns, RS, T.copy_bytes);
-    auto kern = fused_rows_kernel<E, NCH, G, ACC64>;
-    TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<grid, (CW + 1) * 32, smem, st>>>(T);
-    TOMOS_LAUNCH_CHECK("fused_rows_kernel");
-    return TOMOS_OK;
-}
-
 // The staged-fp16 pass on the tensor cores (rowpass_mma.cuh).
 template <int TPW, bool BF>
 static tomos_status launch_fused_mma_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
@@ -486,102 +465,6 @@ static tomos_status launch_fused_mma(Elem e, const FusedParams& P, int* err, int
                           : launch_fused_mma_b<false>(P, err, tpw, grid, st);
 }
 
-static bool elem_two_planes(Elem e) {
-    return e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R;
-}
-
-// 16-byte chunks a lane takes per row part at most (RowNchMax).
-static int fused_nch_max(Elem e, bool acc64) {
-    const int base = (e == Elem::F32) ? 8 : 4;
-    return (acc64 && elem_two_planes(e)) ? base / 2 : base;
-}
-
-// Consumer warps of a pass (RowWarps).
-static int fused_warps(Elem e, bool acc64) {
-    return !acc64 ? 12 : (elem_two_planes(e) ? 16 : 8);
-}
-
-// Warps per row a pass may split a row over (divisors of its consumer
-// warps).
-static const int* fused_g_list(Elem e, bool acc64, int* count) {
-    static const int g12[] = {2, 3, 4, 6, 12};
-    static const int g8[] = {2, 4, 8};
-    static const int g16[] = {2, 4, 8, 16};
-    const int w = fused_warps(e, acc64);
-    *count = w == 8 ? 3 : (w == 16 ? 4 : 5);
-    return w == 8 ? g8 : (w == 16 ? g16 : g12);
-}
-
-// (nch, g) pairs with an instantiation: one warp per row with 1..NCHMAX
-// chunks per lane, or G warps per row (fused_g_list) at NCHMAX.
-template <Elem E, bool ACC64>
-static tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int g, int grid,
-                                   cudaStream_t st) {
-    constexpr int NMAX = RowNchMax<E, ACC64>::value;
-    if (g == 1) {
-        switch (nch) {
-            case 1: return launch_fused_t<E, 1, 1, ACC64>(P, err, grid, st);
-            case 2: return launch_fused_t<E, 2, 1, ACC64>(P, err, grid, st);
-            case 4:
-                if constexpr (NMAX >= 4) return launch_fused_t<E, 4, 1, ACC64>(P, err, grid, st);
-                break;
-            case 8:
-                if constexpr (NMAX == 8) return launch_fused_t<E, 8, 1, ACC64>(P, err, grid, st);
-                break;
-            default: break;
-        }
-    } else if (nch == NMAX) {
-        if constexpr (RowWarps<E, ACC64>::value == 8) {
-            switch (g) {
-                case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
-                case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
-                case 8: return launch_fused_t<E, NMAX, 8, ACC64>(P, err, grid, st);
-                default: break;
-            }
-        } else if constexpr (RowWarps<E, ACC64>::value == 16) {
-            switch (g) {
-                case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
-                case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
-                case 8: return launch_fused_t<E, NMAX, 8, ACC64>(P, err, grid, st);
-                case 16: return launch_fused_t<E, NMAX, 16, ACC64>(P, err, grid, st);
-                default: break;
-            }
-        } else {
-            switch (g) {
-                case 2: return launch_fused_t<E, NMAX, 2, ACC64>(P, err, grid, st);
-                case 3: return launch_fused_t<E, NMAX, 3, ACC64>(P, err, grid, st);
-                case 4: return launch_fused_t<E, NMAX, 4, ACC64>(P, err, grid, st);
-                case 6: return launch_fused_t<E, NMAX, 6, ACC64>(P, err, grid, st);
-                case 12: return launch_fused_t<E, NMAX, 12, ACC64>(P, err, grid, st);
-                default: break;
-            }
-        }
-    }
-    return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
-}
-
-static tomos_status launch_fused(Elem e, bool acc64, const FusedParams& P, int* err, int nch,
-                                 int g, int grid, cudaStream_t st) {
-    switch (e) {
-        case Elem::F32:
-            return acc64 ? launch_fused_e<Elem::F32, true>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::F32, false>(P, err, nch, g, grid, st);
-        case Elem::H16:
-            return acc64 ? launch_fused_e<Elem::H16, true>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::H16, false>(P, err, nch, g, grid, st);
-        case Elem::B16:
-            return acc64 ? launch_fused_e<Elem::B16, true>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::B16, false>(P, err, nch, g, grid, st);
-        case Elem::F16:
-            return acc64 ? launch_fused_e<Elem::F16, true>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::F16, false>(P, err, nch, g, grid, st);
-        case Elem::A16: return launch_fused_e<Elem::A16, true>(P, err, nch, g, grid, st);
-        case Elem::AB16: return launch_fused_e<Elem::AB16, true>(P, err, nch, g, grid, st);
-        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true>(P, err, nch, g, grid, st);
-        default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: element type");
-    }
-}
-
 // wh plane of a row-major FP32_16 A -> IEEE fp16 words with the
 // fp32_16_half_only values (fp32_16_pack.hpp:553-571), rows of ldh words;
 // a block per row, a thread per 16-byte chunk.  Control-bit words are
@@ -609,34 +492,11 @@ PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool
     PassPlan pl;
     pl.e = e;
     pl.acc64 = acc64 || elem_is_exact(e);
-    const int vec = (e == Elem::F32) ? 4 : 8;
-    const int wbytes = (e == Elem::F32) ? 4 : 2;
-    bool ok = A->layout == TOMOS_ROW_MAJOR && ((A->ld * wbytes) % 16 == 0) &&
-              (reinterpret_cast<uintptr_t>(A->values) % 16 == 0);
-    if (ok && elem_is_exact(e))
-        ok = reinterpret_cast<uintptr_t>(dense_lo_plane(A)) % 16 == 0;
     int nch = 0, g = 1;
-    const int nmax = fused_nch_max(e, pl.acc64);
-    for (int c : {1, 2, 4, 8}) {
-        if (c > nmax) break;
-        if ((int64_t)32 * c * vec >= A->cols) {
-            nch = c;
-            break;
-        }
-    }
-    if (nch == 0) {
-        int ng = 0;
-        const int* gl = fused_g_list(e, pl.acc64, &ng);
-        for (int q = 0; q < ng; ++q) {
-            const int gg = gl[q];
-            if ((int64_t)gg * 32 * nmax * vec >= A->cols) {
-                nch = nmax;
-                g = gg;
-                break;
-            }
-        }
-    }
-    if (ok && nch > 0 && A->cols > 0) {
+    const bool ok = A->layout == TOMOS_ROW_MAJOR && A->cols > 0 &&
+                    plan_row_lines(e, pl.acc64, A->cols, A->ld, A->values,
+                                   elem_is_exact(e) ? dense_lo_plane(A) : nullptr, &nch, &g);
+    if (ok) {
         pl.fused = true;
         pl.nch = nch;
         pl.g = g;
@@ -646,12 +506,7 @@ PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool
         const int64_t ktiles = (A->cols + 15) / 16;
         if ((e == Elem::F16 || e == Elem::B16) && !pl.acc64 && ktiles <= (int64_t)kMmaWarps * kMmaMaxTpw)
             pl.tpw = (int)((ktiles + kMmaWarps - 1) / kMmaWarps);
-        int64_t grid = sm_count();
-        const int64_t min_rows_cta = 64;
-        const int64_t gr = (A->rows + min_rows_cta - 1) / min_rows_cta;
-        if (grid > gr) grid = gr;
-        if (grid < 1) grid = 1;
-        pl.grid = (int)grid;
+        pl.grid = row_pass_grid(A->rows);
         pl.gq = pl.grid;
         pl.gs = pl.grid;
         pl.qstride = ws->qstride;

@@ -83,12 +83,24 @@ struct RowPlanes {
     static constexpr int value = (E == Elem::A16 || E == Elem::AB16 || E == Elem::AB16R) ? 2 : 1;
 };
 
+// What one launch of fused_rows_kernel computes.
+enum RowMode : int {
+    kRowBoth = 0,  // the LSQR pass: ut = cp A p + cu u, partials of A^T ut and ||ut||^2
+    kRowDot = 1,   // ut = cp A p + cu u only (a product whose lines are dots)
+    kRowAxpy = 2,  // partials of A^T (cu u) only (a product that sums lines)
+};
+
 struct RowPassParams {
     FusedParams f;
     int* err;        // set nonzero on a pipeline timeout
     int nstage;
     int copy_bytes;  // bytes copied per row and plane (16-byte multiple)
+    double* qpart64; // kRowAxpy with ACC64: FP64 partials (gridDim.x x qstride)
 };
+
+// kRowAxpy with ACC64 sums FP32 products over this many rows of a warp,
+// then adds them into FP64 accumulators.
+constexpr int kRowPromote = 8;
 
 __device__ __forceinline__ uint4 lds128(const uint8_t* p) {
     return *reinterpret_cast<const uint4*>(p);
@@ -146,23 +158,32 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
             for (int e = 0; e < HV; ++e) a[k * HV + e] = make_float2(f[2 * e], f[2 * e + 1]);
         }
     } else if constexpr (E == Elem::H16) {
-        uint4 h[NCH];
-        uint32_t any = 0;
+        // wh words without a control bit are fp16 values: plain
+        // conversions; the elements with one (rare) are redone by a loop,
+        // as in the exact decode above.
 #pragma unroll
         for (int k = 0; k < NCH; ++k) {
-            h[k] = (live >> k) & 1u ? lds128(hrow + coff[k]) : make_uint4(0, 0, 0, 0);
-            any |= h[k].x | h[k].y | h[k].z | h[k].w;
-        }
-        if (any & 0x00010001u) {
+            const uint4 h = (live >> k) & 1u ? lds128(hrow + coff[k]) : make_uint4(0, 0, 0, 0);
+            float f[8];
+            {
+                const float2 p0 = h2f2(h.x), p1 = h2f2(h.y), p2 = h2f2(h.z), p3 = h2f2(h.w);
+                f[0] = p0.x; f[1] = p0.y; f[2] = p1.x; f[3] = p1.y;
+                f[4] = p2.x; f[5] = p2.y; f[6] = p3.x; f[7] = p3.y;
+            }
+            uint32_t flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
+                             ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
+            while (flags) {
+                const int bit = __ffs(flags) - 1;
+                flags &= flags - 1;
+                const int wi = bit & 3, hi = bit >> 4;
+                const uint32_t ww = wi == 0 ? h.x : wi == 1 ? h.y : wi == 2 ? h.z : h.w;
+                const float v = half_bits_to_float(half_only_bits((ww >> (hi * 16)) & 0xFFFFu));
+                const int q = 2 * wi + hi;
 #pragma unroll
-            for (int k = 0; k < NCH; ++k) fix_half_chunk(h[k]);
-        }
+                for (int e = 0; e < 8; ++e) f[e] = e == q ? v : f[e];
+            }
 #pragma unroll
-        for (int k = 0; k < NCH; ++k) {
-            a[k * 4 + 0] = h2f2(h[k].x);
-            a[k * 4 + 1] = h2f2(h[k].y);
-            a[k * 4 + 2] = h2f2(h[k].z);
-            a[k * 4 + 3] = h2f2(h[k].w);
+            for (int e = 0; e < 4; ++e) a[k * 4 + e] = make_float2(f[2 * e], f[2 * e + 1]);
         }
     } else {
 #pragma unroll
@@ -193,9 +214,15 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
     }
 }
 
-template <Elem E, int NCH, int G, bool ACC64>
+template <Elem E, int NCH, int G, bool ACC64, int MODE>
 __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused_rows_kernel(RowPassParams T) {
     constexpr int CW = RowWarps<E, ACC64>::value;  // consumer warps
+    constexpr bool DOT = MODE != kRowAxpy;         // forms the row dots
+    constexpr bool AXPY = MODE != kRowDot;         // accumulates A^T ut
+    // FP64 p and per-element FP64 products: the exact LSQR passes.  The
+    // standalone FP64 tiers (kRowDot, kRowAxpy with ACC64) form FP32
+    // products over short runs and sum those in FP64.
+    constexpr bool P64 = ACC64 && MODE == kRowBoth;
     constexpr int NTHREADS = (CW + 1) * 32;
     static_assert(CW % G == 0, "G divides the consumer warps");
     const FusedParams& P = T.f;
@@ -242,6 +269,11 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
     float2 acc[PER / 2];
 #pragma unroll
     for (int j = 0; j < PER / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
+    // kRowAxpy with ACC64: FP64 sums of the FP32 run sums held in acc
+    constexpr int NACC64 = (AXPY && ACC64 && MODE != kRowBoth) ? PER : 1;
+    double acc64[NACC64];
+#pragma unroll
+    for (int j = 0; j < NACC64; ++j) acc64[j] = 0.0;
     double ss = 0.0;
     const int rg = warp / G;    // row of the stage
     const int part = warp % G;  // column part of the row
@@ -297,15 +329,17 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         }
     } else {
         // --------------------------------------------------------- consumers
-        const double cp = P.coef[0];
-        const double cu = P.coef[1];
+        const double cp = P.coef ? P.coef[0] : P.cp;
+        const double cu = P.coef ? P.coef[1] : P.cu;
+        // a product with cu == 0 never reads u (it may hold NaN)
+        const bool use_u = MODE == kRowBoth || cu != 0.0;
         const int64_t n = P.n;
         const int64_t nchunks = (n + VEC - 1) / VEC;
         int coff[NCH];
         uint32_t live = 0;
-        // p for this lane's columns: FP32 pairs, or FP64 for ACC64
-        using PT = typename std::conditional<ACC64, double, float2>::type;
-        PT pv[ACC64 ? PER : PER / 2];
+        // p for this lane's columns: FP32 pairs, or FP64 for P64
+        using PT = typename std::conditional<P64, double, float2>::type;
+        PT pv[P64 ? PER : PER / 2];
         // The lane holding the row's last, partly filled chunk zeroes the
         // elements from zero_from on (the copy's tail past column n-1).
         int zero_from = PER;
@@ -318,9 +352,9 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
 #pragma unroll
             for (int e = 0; e < VEC; e += 2) {
                 const int64_t col = c * VEC + e;
-                const float x0 = col < n ? __ldg(P.p + col) : 0.0f;
-                const float x1 = col + 1 < n ? __ldg(P.p + col + 1) : 0.0f;
-                if constexpr (ACC64) {
+                const float x0 = (DOT && col < n) ? __ldg(P.p + col) : 0.0f;
+                const float x1 = (DOT && col + 1 < n) ? __ldg(P.p + col + 1) : 0.0f;
+                if constexpr (P64) {
                     pv[k * VEC + e] = (double)x0;
                     pv[k * VEC + e + 1] = (double)x1;
                 } else {
@@ -328,10 +362,11 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                 }
             }
         }
+
         bool failed = false;
         // u of this warp's row, fetched two tiles ahead
         float ua = 0.f, ub = 0.f;
-        {
+        if (use_u) {
             const int64_t a0 = r0 + rg, b0 = r0 + RS + rg;
             if (a0 < r1) ua = __ldg(P.u_in + a0);
             if (b0 < r1) ub = __ldg(P.u_in + b0);
@@ -343,7 +378,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
             const bool has = i < r1;
             const float ucur = ua;
             ua = ub;
-            ub = (i + 2 * RS < r1) ? __ldg(P.u_in + i + 2 * RS) : 0.0f;
+            ub = (use_u && i + 2 * RS < r1) ? __ldg(P.u_in + i + 2 * RS) : 0.0f;
             if (!failed && !mbar_wait(&full[s], ph)) {
                 atomicExch(T.err, 3);
                 abort_flag = 1;
@@ -372,8 +407,10 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                 ph ^= 1u;
             }
 
-            double dsum;
-            if constexpr (ACC64) {
+            double dsum = 0.0;
+            if constexpr (!DOT) {
+                // no dot: ut = cu u
+            } else if constexpr (P64) {
                 double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
 #pragma unroll
                 for (int j = 0; j < PER / 2; j += 2) {
@@ -393,12 +430,20 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                     d0 = __ffma2_rn(a[j], pv[j], d0);
                     d1 = __ffma2_rn(a[j + 1], pv[j + 1], d1);
                 }
-                float d = (d0.x + d1.x) + (d0.y + d1.y);
+                if constexpr (ACC64) {
+                    // FP32 products summed over the lane's run, then FP64
+                    double dd = ((double)d0.x + (double)d1.x) + ((double)d0.y + (double)d1.y);
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-                dsum = (double)d;
+                    for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(0xffffffffu, dd, o);
+                    dsum = dd;
+                } else {
+                    float d = (d0.x + d1.x) + (d0.y + d1.y);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+                    dsum = (double)d;
+                }
             }
-            if constexpr (G > 1) {
+            if constexpr (DOT && G > 1) {
                 // partial dots of the row's G parts, summed in part order
                 if (lane == 0) xdot[t & 1][warp] = dsum;
                 named_bar_sync(1 + rg, G * 32);
@@ -407,20 +452,67 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                 for (int g = 0; g < G; ++g) tot += xdot[t & 1][rg * G + g];
                 dsum = tot;
             }
-            const float ut = has ? (float)(cp * dsum + cu * (double)ucur) : 0.0f;
-            if (lane == 0 && part == 0 && has) {
-                P.u_out[i] = ut;
-                ss += (double)ut * (double)ut;
+            float ut;
+            if constexpr (DOT)
+                ut = has ? (float)(cp * dsum + (use_u ? cu * (double)ucur : 0.0)) : 0.0f;
+            else
+                ut = has ? (float)(cu * (double)ucur) : 0.0f;
+            if constexpr (DOT) {
+                if (lane == 0 && part == 0 && has) {
+                    P.u_out[i] = ut;
+                    if constexpr (MODE == kRowBoth) ss += (double)ut * (double)ut;
+                }
             }
-            const float2 ut2 = make_float2(ut, ut);
+            if constexpr (AXPY) {
+                const float2 ut2 = make_float2(ut, ut);
 #pragma unroll
-            for (int j = 0; j < PER / 2; ++j) acc[j] = __ffma2_rn(a[j], ut2, acc[j]);
+                for (int j = 0; j < PER / 2; ++j) acc[j] = __ffma2_rn(a[j], ut2, acc[j]);
+                if constexpr (ACC64 && MODE != kRowBoth) {
+                    if ((t + 1) % kRowPromote == 0) {
+#pragma unroll
+                        for (int j = 0; j < PER / 2; ++j) {
+                            acc64[2 * j] += (double)acc[j].x;
+                            acc64[2 * j + 1] += (double)acc[j].y;
+                            acc[j] = make_float2(0.0f, 0.0f);
+                        }
+                    }
+                }
+            }
+        }
+        if constexpr (AXPY && ACC64 && MODE != kRowBoth) {
+#pragma unroll
+            for (int j = 0; j < PER / 2; ++j) {
+                acc64[2 * j] += (double)acc[j].x;
+                acc64[2 * j + 1] += (double)acc[j].y;
+            }
         }
     }
 
+    if constexpr (MODE == kRowDot) return;  // u_out is all a dot product writes
     // Epilogue: the producer waited for every copy it issued, so the stage
     // memory can hold the cross-warp reduction.
     __syncthreads();
+    if constexpr (NACC64 > 1) {
+        double* red64 = reinterpret_cast<double*>(smem);
+        if (warp < CW) {
+#pragma unroll
+            for (int k = 0; k < NCH; ++k)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e)
+                    red64[(size_t)warp * WCOLS + (k * 32 + lane) * VEC + e] = acc64[k * VEC + e];
+        }
+        __syncthreads();
+        double* qout64 = T.qpart64 + (size_t)blockIdx.x * P.qstride;
+        for (int64_t j = threadIdx.x; j < P.n; j += NTHREADS) {
+            const int g = (int)(j / WCOLS);
+            const int loc = (int)(j % WCOLS);
+            double sum = 0.0;
+#pragma unroll
+            for (int r = 0; r < RS; ++r) sum += red64[(size_t)(r * G + g) * WCOLS + loc];
+            qout64[j] = sum;
+        }
+        return;
+    }
     float* red = reinterpret_cast<float*>(smem);
     if (warp < CW) {
 #pragma unroll
@@ -444,7 +536,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         for (int r = 0; r < RS; ++r) sum += red[(size_t)(r * G + g) * WCOLS + loc];
         qout[j] = sum;
     }
-    if (threadIdx.x == 0) {
+    if (MODE == kRowBoth && threadIdx.x == 0) {
         double sum = 0.0;
 #pragma unroll
         for (int w = 0; w < CW; ++w) sum += ssw[w];
@@ -454,11 +546,12 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
 
 // Dynamic shared memory of one launch: the stage ring, at least the
 // cross-warp reduction buffer.
-template <Elem E, int NCH, bool ACC64>
+template <Elem E, int NCH, bool ACC64, int MODE>
 inline size_t fused_rows_smem(int nstage, int rows_per_stage, int copy_bytes) {
     constexpr int VEC = ChunkElems<E>::value;
     const size_t ring = (size_t)nstage * rows_per_stage * copy_bytes * RowPlanes<E>::value;
-    const size_t red = (size_t)RowWarps<E, ACC64>::value * NCH * 32 * VEC * sizeof(float);
+    const size_t esz = (ACC64 && MODE == kRowAxpy) ? sizeof(double) : sizeof(float);
+    const size_t red = (size_t)RowWarps<E, ACC64>::value * NCH * 32 * VEC * esz;
     return ring > red ? ring : red;
 }
 

@@ -22,8 +22,8 @@ with FP64 accumulation.
 import torch
 
 
-def _gen(seed):
-    g = torch.Generator(device="cuda")
+def _gen(seed, device="cuda"):
+    g = torch.Generator(device=device)
     g.manual_seed(int(seed))
     return g
 
@@ -38,23 +38,24 @@ def dense_gaussian(m, n, seed=0, noise=1e-6, layout="row"):
     return A, x, b
 
 
-def dense_scaled(m, n, seed=0, noise=1e-8, decades=3.0, block_rows=1 << 17, out=None):
+def dense_scaled(m, n, seed=0, noise=1e-8, decades=3.0, block_rows=1 << 17, out=None, device="cuda"):
     """A = G diag(10^u) (m x n float32 row-major), x_true, b.
 
     Generated in row blocks of block_rows; `out` may be a preallocated
-    (m, n) float32 CUDA tensor to fill."""
-    g = _gen(seed)
-    u = (torch.rand(n, generator=g, device="cuda", dtype=torch.float64) * 2.0 - 1.0) * decades
+    (m, n) float32 tensor to fill.  device="cpu" draws from torch's CPU
+    generator instead (other values for the same seed)."""
+    g = _gen(seed, device)
+    u = (torch.rand(n, generator=g, device=device, dtype=torch.float64) * 2.0 - 1.0) * decades
     scale = torch.pow(10.0, u)
-    x = torch.randn(n, generator=g, device="cuda", dtype=torch.float32)
-    A = out if out is not None else torch.empty(m, n, device="cuda", dtype=torch.float32)
-    b = torch.empty(m, device="cuda", dtype=torch.float32)
+    x = torch.randn(n, generator=g, device=device, dtype=torch.float32)
+    A = out if out is not None else torch.empty(m, n, device=device, dtype=torch.float32)
+    b = torch.empty(m, device=device, dtype=torch.float32)
     xd = x.double()
     for r0 in range(0, m, block_rows):
         r1 = min(m, r0 + block_rows)
-        blk = torch.randn(r1 - r0, n, generator=g, device="cuda", dtype=torch.float64) * scale
+        blk = torch.randn(r1 - r0, n, generator=g, device=device, dtype=torch.float64) * scale
         A[r0:r1] = blk.float()
-        e = torch.randn(r1 - r0, generator=g, device="cuda", dtype=torch.float64)
+        e = torch.randn(r1 - r0, generator=g, device=device, dtype=torch.float64)
         b[r0:r1] = (A[r0:r1].double() @ xd + noise * e).float()
         del blk
     return A, x, b
