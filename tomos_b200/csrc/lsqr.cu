@@ -416,6 +416,29 @@ static tomos_status ensure_history(tomos_workspace* ws, int cap) {
 
 // ------------------------------------------------------------ A passes
 
+// The LSQR pass (kRowBoth) for every element type and FP64 flag.
+static tomos_status launch_fused(Elem e, bool acc64, const FusedParams& P, int* err, int nch,
+                                 int g, int grid, cudaStream_t st) {
+    switch (e) {
+        case Elem::F32:
+            return acc64 ? launch_fused_e<Elem::F32, true, kRowBoth>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::F32, false, kRowBoth>(P, err, nch, g, grid, st);
+        case Elem::H16:
+            return acc64 ? launch_fused_e<Elem::H16, true, kRowBoth>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::H16, false, kRowBoth>(P, err, nch, g, grid, st);
+        case Elem::B16:
+            return acc64 ? launch_fused_e<Elem::B16, true, kRowBoth>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::B16, false, kRowBoth>(P, err, nch, g, grid, st);
+        case Elem::F16:
+            return acc64 ? launch_fused_e<Elem::F16, true, kRowBoth>(P, err, nch, g, grid, st)
+                         : launch_fused_e<Elem::F16, false, kRowBoth>(P, err, nch, g, grid, st);
+        case Elem::A16: return launch_fused_e<Elem::A16, true, kRowBoth>(P, err, nch, g, grid, st);
+        case Elem::AB16: return launch_fused_e<Elem::AB16, true, kRowBoth>(P, err, nch, g, grid, st);
+        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true, kRowBoth>(P, err, nch, g, grid, st);
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: element type");
+    }
+}
+
 // The staged-fp16 pass on the tensor cores (rowpass_mma.cuh).
 template <int TPW, bool BF>
 static tomos_status launch_fused_mma_t(const FusedParams& P, int* err, int grid, cudaStream_t st) {
@@ -427,7 +450,7 @@ static tomos_status launch_fused_mma_t(const FusedParams& P, int* err, int grid,
     // bank conflicts
     T.pitch = ((T.cb / 16) % 2 == 1) ? T.cb : T.cb + 16;
     const size_t stage = (size_t)kMmaRows * T.pitch;
-    int ns = (int)((kRowSmemBudget - 64) / stage);
+    int ns = (int)((kMmaSmemBudget - 64) / stage);
     if (ns > kMmaMaxStages) ns = kMmaMaxStages;
     if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
     T.nstage = ns;

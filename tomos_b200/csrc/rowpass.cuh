@@ -64,7 +64,8 @@ struct RowPlanes;
 // columns) to hide their latency.
 template <Elem E, bool ACC64>
 struct RowWarps {
-    static constexpr int value = !ACC64 ? 12 : (RowPlanes<E>::value == 1 ? 8 : 16);
+    static constexpr int value = !ACC64 ? ((E == Elem::F16 || E == Elem::B16) ? 16 : 12)
+                                        : (RowPlanes<E>::value == 1 ? 8 : 16);
 };
 constexpr int kRowWarps = 16;  // the widest configuration (shared arrays)
 
@@ -76,7 +77,12 @@ struct RowNchMax {
     static constexpr int value = (ACC64 && RowPlanes<E>::value == 2) ? base / 2 : base;
 };
 constexpr int kRowMaxStages = 12;
-constexpr size_t kRowSmemBudget = 200 * 1024;
+constexpr size_t kRowSmemBudget = 216 * 1024;
+// Bytes a bulk copy of one plane of a stage aims at: each copy carries a
+// fixed cost beside its bytes (measured about a microsecond a stage for
+// 24-48 KB copies), so stages of one tile of short 16-bit rows would bound
+// the pass below the memory rate.
+constexpr size_t kRowCopyTarget = 48 * 1024;
 
 template <Elem E>
 struct RowPlanes {
@@ -95,8 +101,43 @@ struct RowPassParams {
     int* err;        // set nonzero on a pipeline timeout
     int nstage;
     int copy_bytes;  // bytes copied per row and plane (16-byte multiple)
+    int tiles_per_stage;  // row tiles (CW / G rows each) a stage holds
     double* qpart64; // kRowAxpy with ACC64: FP64 partials (gridDim.x x qstride)
+    int corr_offset; // FP32_16 HALF sums of lines: byte offset of the n-float
+                     // column corrections in dynamic shared memory
 };
+
+// The control words of one lane's row part (NCH chunks of 8 wh words, as
+// loaded; elements from zero_from on lie past the row and are skipped):
+// for each, d = fp32_16_half_only value - its plain fp16 conversion.  With
+// p, returns sum d * p[col] (the correction of the lane's dot); with corr,
+// adds d * ut to corr[col] (shared memory) and returns 0.  A loop over the
+// flagged elements only, so a lane without one passes through at once.
+template <int NCH>
+__device__ __forceinline__ float h16_corrections(const uint4 (&hk)[NCH], int part, int lane, int zero_from,
+                                                 const float* p, float ut, float* corr) {
+    float dsum = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NCH; ++k) {
+        const uint4 h = hk[k];
+        uint32_t flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
+                         ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
+        while (flags) {
+            const int bit = __ffs(flags) - 1;
+            flags &= flags - 1;
+            const int wi = bit & 3, hi = bit >> 4;
+            const int q = 2 * wi + hi;  // element of the chunk
+            if (k * 8 + q >= zero_from) continue;
+            const uint32_t ww = wi == 0 ? h.x : wi == 1 ? h.y : wi == 2 ? h.z : h.w;
+            const uint32_t hb = (ww >> (hi * 16)) & 0xFFFFu;
+            const float d = half_bits_to_float(half_only_bits(hb)) - half_bits_to_float(hb);
+            const int64_t col = ((int64_t)part * 32 * NCH + (int64_t)k * 32 + lane) * 8 + q;
+            if (p) dsum += d * __ldg(p + col);
+            if (corr) atomicAdd(&corr[col], d * ut);
+        }
+    }
+    return dsum;
+}
 
 // kRowAxpy with ACC64 sums FP32 products over this many rows of a warp,
 // then adds them into FP64 accumulators.
@@ -223,6 +264,12 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
     // standalone FP64 tiers (kRowDot, kRowAxpy with ACC64) form FP32
     // products over short runs and sum those in FP64.
     constexpr bool P64 = ACC64 && MODE == kRowBoth;
+    // FP32_16 wh words in a standalone product: every word converted as an
+    // fp16 value, and the rare control words corrected afterwards by the
+    // difference between their fp32_16_half_only value and that conversion
+    // (into the lane's dot, or into a per-CTA column buffer in shared
+    // memory), so the warp never waits on a per-element fix.
+    constexpr bool HCORR = E == Elem::H16 && MODE != kRowBoth;
     constexpr int NTHREADS = (CW + 1) * 32;
     static_assert(CW % G == 0, "G divides the consumer warps");
     const FusedParams& P = T.f;
@@ -230,7 +277,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
     constexpr int VEC = ChunkElems<E>::value;
     constexpr int PER = NCH * VEC;      // columns per lane
     constexpr int WCOLS = 32 * PER;     // columns per consumer warp
-    constexpr int RS = CW / G;          // rows per stage
+    constexpr int RS = CW / G;          // rows per tile (one per row group of warps)
     constexpr int PLANES = RowPlanes<E>::value;
     constexpr int ESZ = (E == Elem::F32) ? 4 : 2;
     static_assert(PER % 4 == 0, "pairs of pairs");
@@ -246,7 +293,10 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
     const int warp = threadIdx.x >> 5;
     const int nstage = T.nstage;
     const int cb = T.copy_bytes;
-    const size_t plane_bytes = (size_t)RS * cb;
+    // A stage holds tps row tiles: each bulk copy then moves tps times a
+    // tile's bytes (a copy carries a fixed cost beside its bytes).
+    const int tps = T.tiles_per_stage;
+    const size_t plane_bytes = (size_t)RS * tps * cb;
     const size_t stage_bytes = plane_bytes * PLANES;
 
     const int64_t rows_per_cta = (P.m + gridDim.x - 1) / gridDim.x;
@@ -254,7 +304,8 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
     int64_t r1 = r0 + rows_per_cta;
     if (r1 > P.m) r1 = P.m;
     const int64_t nrows = r1 > r0 ? r1 - r0 : 0;
-    const int ntiles = (int)((nrows + RS - 1) / RS);
+    const int ntiles = (int)((nrows + RS - 1) / RS);               // row tiles
+    const int nstages_total = (int)((nrows + RS * tps - 1) / (RS * tps));  // stage loads
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < nstage; ++s) {
@@ -264,6 +315,11 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         abort_flag = 0;
         fence_barrier_init();
     }
+    // column corrections of the control words (HCORR sums of lines), after
+    // everything else in dynamic shared memory
+    float* corr = reinterpret_cast<float*>(smem + T.corr_offset);
+    if constexpr (HCORR && AXPY)
+        for (int64_t j = threadIdx.x; j < P.n; j += NTHREADS) corr[j] = 0.0f;
     __syncthreads();
 
     float2 acc[PER / 2];
@@ -285,14 +341,14 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
             int issued = 0;
             int s = 0;
             uint32_t ph = 0;
-            for (int t = 0; t < ntiles; ++t) {
+            for (int t = 0; t < nstages_total; ++t) {
                 if (!mbar_wait(&empty[s], ph ^ 1u)) {
                     atomicExch(T.err, 1);
                     break;
                 }
                 if (*(volatile int*)&abort_flag) break;
-                const int64_t i0 = r0 + (int64_t)t * RS;
-                const int rows = (int)((r1 - i0) < RS ? (r1 - i0) : RS);
+                const int64_t i0 = r0 + (int64_t)t * RS * tps;
+                const int rows = (int)((r1 - i0) < RS * tps ? (r1 - i0) : RS * tps);
                 uint8_t* st = smem + (size_t)s * stage_bytes;
                 mbar_expect_tx(&full[s], (uint32_t)(rows * cb * PLANES));
                 if (contiguous) {
@@ -373,20 +429,38 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         }
         int s = 0;
         uint32_t ph = 0;
+        int sub = 0;  // row tile within the stage
         for (int t = 0; t < ntiles; ++t) {
             const int64_t i = r0 + (int64_t)t * RS + rg;
             const bool has = i < r1;
             const float ucur = ua;
             ua = ub;
             ub = (use_u && i + 2 * RS < r1) ? __ldg(P.u_in + i + 2 * RS) : 0.0f;
-            if (!failed && !mbar_wait(&full[s], ph)) {
+            if (sub == 0 && !failed && !mbar_wait(&full[s], ph)) {
                 atomicExch(T.err, 3);
                 abort_flag = 1;
                 failed = true;
             }
-            const uint8_t* hrow = smem + (size_t)s * stage_bytes + (size_t)rg * cb;
+            const uint8_t* hrow = smem + (size_t)s * stage_bytes + (size_t)(sub * RS + rg) * cb;
             float2 a[PER / 2];
-            if (has && !failed) {
+            uint4 hk[HCORR ? NCH : 1];
+            if (HCORR && has && !failed) {
+#pragma unroll
+                for (int k = 0; k < NCH; ++k) {
+                    hk[k] = (live >> k) & 1u ? lds128(hrow + coff[k]) : make_uint4(0, 0, 0, 0);
+                    a[k * 4 + 0] = h2f2(hk[k].x);
+                    a[k * 4 + 1] = h2f2(hk[k].y);
+                    a[k * 4 + 2] = h2f2(hk[k].z);
+                    a[k * 4 + 3] = h2f2(hk[k].w);
+                }
+                if (zero_from < PER) {
+#pragma unroll
+                    for (int e = 0; e < PER; e += 2) {
+                        if (e >= zero_from) a[e / 2].x = 0.0f;
+                        if (e + 1 >= zero_from) a[e / 2].y = 0.0f;
+                    }
+                }
+            } else if (has && !failed) {
                 decode_row<E, NCH>(hrow, hrow + plane_bytes, coff, live, a);
                 if (zero_from < PER) {
 #pragma unroll
@@ -399,12 +473,16 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
 #pragma unroll
                 for (int e = 0; e < PER / 2; ++e) a[e] = make_float2(0.0f, 0.0f);
             }
-            // The stage may be refilled once every consumer warp holds its row.
-            __syncwarp();
-            if (lane == 0 && !failed) mbar_arrive(&empty[s]);
-            if (++s == nstage) {
-                s = 0;
-                ph ^= 1u;
+            // The stage may be refilled once every consumer warp holds its
+            // row of the stage's last tile (or of the CTA's last tile).
+            if (++sub == tps || t + 1 == ntiles) {
+                __syncwarp();
+                if (lane == 0 && !failed) mbar_arrive(&empty[s]);
+                sub = 0;
+                if (++s == nstage) {
+                    s = 0;
+                    ph ^= 1u;
+                }
             }
 
             double dsum = 0.0;
@@ -429,6 +507,9 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                 for (int j = 0; j < PER / 2; j += 2) {
                     d0 = __ffma2_rn(a[j], pv[j], d0);
                     d1 = __ffma2_rn(a[j + 1], pv[j + 1], d1);
+                }
+                if constexpr (HCORR) {
+                    if (has && !failed) d0.x += h16_corrections<NCH>(hk, part, lane, zero_from, P.p, 0.0f, nullptr);
                 }
                 if constexpr (ACC64) {
                     // FP32 products summed over the lane's run, then FP64
@@ -467,6 +548,9 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                 const float2 ut2 = make_float2(ut, ut);
 #pragma unroll
                 for (int j = 0; j < PER / 2; ++j) acc[j] = __ffma2_rn(a[j], ut2, acc[j]);
+                if constexpr (HCORR) {
+                    if (has && !failed) h16_corrections<NCH>(hk, part, lane, zero_from, nullptr, ut, corr);
+                }
                 if constexpr (ACC64 && MODE != kRowBoth) {
                     if ((t + 1) % kRowPromote == 0) {
 #pragma unroll
@@ -534,6 +618,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         float sum = 0.0f;
 #pragma unroll
         for (int r = 0; r < RS; ++r) sum += red[(size_t)(r * G + g) * WCOLS + loc];
+        if constexpr (HCORR) sum += corr[j];
         qout[j] = sum;
     }
     if (MODE == kRowBoth && threadIdx.x == 0) {
@@ -552,7 +637,14 @@ inline size_t fused_rows_smem(int nstage, int rows_per_stage, int copy_bytes) {
     const size_t ring = (size_t)nstage * rows_per_stage * copy_bytes * RowPlanes<E>::value;
     const size_t esz = (ACC64 && MODE == kRowAxpy) ? sizeof(double) : sizeof(float);
     const size_t red = (size_t)RowWarps<E, ACC64>::value * NCH * 32 * VEC * esz;
-    return ring > red ? ring : red;
+    const size_t body = ring > red ? ring : red;
+    return (body + 15) / 16 * 16;
+}
+
+// Bytes of the column-correction buffer (FP32_16 HALF sums of lines).
+template <Elem E, int MODE>
+inline size_t fused_rows_corr_bytes(int64_t n) {
+    return (E == Elem::H16 && MODE == kRowAxpy) ? (size_t)((n * 4 + 15) / 16 * 16) : 0;
 }
 
 }  // namespace tomos_b200

@@ -23,12 +23,23 @@ inline tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cud
     T.err = err;
     T.qpart64 = qpart64;
     T.copy_bytes = (int)((((int64_t)P.n * ESZ) + 15) / 16 * 16);
-    const size_t stage = (size_t)RS * T.copy_bytes * RowPlanes<E>::value;
-    int ns = (int)(kRowSmemBudget / stage);
+    const size_t tile = (size_t)RS * T.copy_bytes * RowPlanes<E>::value;
+    const size_t corr = fused_rows_corr_bytes<E, MODE>(P.n);
+    const size_t budget = kRowSmemBudget - corr;
+    // tiles per stage: enough that a copy moves about kRowCopyTarget bytes
+    // a plane, while the ring still holds two stages
+    int tps = (int)((kRowCopyTarget + (size_t)RS * T.copy_bytes - 1) / ((size_t)RS * T.copy_bytes));
+    while (tps > 1 && 2 * tile * tps > budget) --tps;
+    if (tps < 1) tps = 1;
+    T.tiles_per_stage = tps;
+    const size_t stage = tile * tps;
+    int ns = (int)(budget / stage);
     if (ns > kRowMaxStages) ns = kRowMaxStages;
     if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
     T.nstage = ns;
-    const size_t smem = fused_rows_smem<E, NCH, ACC64, MODE>(ns, RS, T.copy_bytes);
+    const size_t body = fused_rows_smem<E, NCH, ACC64, MODE>(ns, RS * tps, T.copy_bytes);
+    T.corr_offset = (int)body;
+    const size_t smem = body + corr;
     auto kern = fused_rows_kernel<E, NCH, G, ACC64, MODE>;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, (CW + 1) * 32, smem, st>>>(T);
@@ -48,7 +59,7 @@ inline int fused_nch_max(Elem e, bool acc64) {
 
 // Consumer warps of a pass (RowWarps).
 inline int fused_warps(Elem e, bool acc64) {
-    return !acc64 ? 12 : (elem_two_planes(e) ? 16 : 8);
+    return !acc64 ? ((e == Elem::F16 || e == Elem::B16) ? 16 : 12) : (elem_two_planes(e) ? 16 : 8);
 }
 
 // Warps per row a pass may split a row over (divisors of its consumer
@@ -95,7 +106,8 @@ inline bool plan_row_lines(Elem e, bool acc64, int64_t inner, int64_t ld, const 
     if (nch == 0) return false;
     const int64_t rows_per_stage = fused_warps(e, acc64) / g;
     const int64_t stage = rows_per_stage * ((inner * wbytes + 15) / 16 * 16) * (elem_two_planes(e) ? 2 : 1);
-    if (2 * stage > (int64_t)kRowSmemBudget) return false;
+    const int64_t corr = e == Elem::H16 ? inner * 4 + 16 : 0;  // a sum of lines' corrections
+    if (2 * stage + corr > (int64_t)kRowSmemBudget) return false;
     *nch_out = nch;
     *g_out = g;
     return true;
@@ -155,29 +167,6 @@ inline tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int 
         }
     }
     return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: no instantiation");
-}
-
-// The LSQR pass (kRowBoth) for every element type and FP64 flag.
-inline tomos_status launch_fused(Elem e, bool acc64, const FusedParams& P, int* err, int nch,
-                                 int g, int grid, cudaStream_t st) {
-    switch (e) {
-        case Elem::F32:
-            return acc64 ? launch_fused_e<Elem::F32, true, kRowBoth>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::F32, false, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::H16:
-            return acc64 ? launch_fused_e<Elem::H16, true, kRowBoth>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::H16, false, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::B16:
-            return acc64 ? launch_fused_e<Elem::B16, true, kRowBoth>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::B16, false, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::F16:
-            return acc64 ? launch_fused_e<Elem::F16, true, kRowBoth>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::F16, false, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::A16: return launch_fused_e<Elem::A16, true, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::AB16: return launch_fused_e<Elem::AB16, true, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true, kRowBoth>(P, err, nch, g, grid, st);
-        default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: element type");
-    }
 }
 
 }  // namespace tomos_b200

@@ -66,6 +66,7 @@ constexpr int kMmaProducer = kMmaWarps + 1;
 constexpr int kMmaThreads = (kMmaWarps + 2) * 32;
 constexpr int kMmaRows = 16;   // rows per stage
 constexpr int kMmaMaxStages = 12;
+constexpr size_t kMmaSmemBudget = 200 * 1024;  // the tensor-core pass's stage ring
 constexpr int kMmaMaxTpw = 11; // k-tiles per warp: n <= 12 * 11 * 16 = 2112
 
 struct MmaPassParams {
