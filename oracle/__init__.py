@@ -45,7 +45,7 @@ def build(ref=None):
     src = ref_src()
     if ref and not src:
         raise FileNotFoundError("reference sources not found (set TOMOS_REF_SRC)")
-    target = ["oracle", "ref"] if (src and ref is not False) else ["oracle"]
+    target = ["oracle", "ref", "ref_b200"] if (src and ref is not False) else ["oracle"]
     args = [f"REF={src}"] if src else []
     subprocess.run(["make", "-s", "-j8", *args, *target], cwd=HERE, check=True)
 

@@ -181,6 +181,35 @@ def test_qr_blocked_ill_conditioned_panel_and_square(k, n):
     assert np.allclose(np.tril(Rinv, -1), 0) and np.all(np.isfinite(Rinv))
 
 
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("wide", ["0", "3"])
+def test_qr_panel_and_wide_paths(wide):
+    """Up to 2048 columns a well-conditioned sketch is factored at once
+    (Gram on the tensor cores, blocked Cholesky, Householder reconstruction
+    of the signs; TOMOS_QR_WIDE=3 requires that path from one column, so a
+    fallback would fail the test); TOMOS_QR_WIDE=0 keeps the 32-column panel
+    path.  Both give LAPACK's R.  Run in a child process, as the switch is
+    read once per process."""
+    import subprocess
+    import sys
+    code = (
+        "import numpy as np, sys\n"
+        "sys.path.insert(0, %r)\n"
+        "from test_gpu_sketch_qr import qr_on_gpu\n"
+        "for k, n in ((4000, 1000), (300, 37), (64, 64), (8000, 2000), (5000, 1537)):\n"
+        "    rng = np.random.default_rng(k)\n"
+        "    SA = rng.standard_normal((k, n)) * np.logspace(0, 4, n)\n"
+        "    Rinv, R = qr_on_gpu(SA)\n"
+        "    Rl = np.linalg.qr(SA, mode='r')\n"
+        "    np.testing.assert_allclose(R, Rl, rtol=1e-8, atol=1e-9 * np.abs(Rl).max())\n"
+        "    Q = SA @ Rinv\n"
+        "    np.testing.assert_allclose(Q.T @ Q, np.eye(n), atol=1e-8)\n"
+        "print('ok')\n" % os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, TOMOS_QR_WIDE=wide)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=280)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-3000:]
+
+
 def test_qr_rejects_wide_and_singular():
     with pytest.raises(tb.TomosError):
         qr_on_gpu(np.ones((3, 5)))

@@ -21,6 +21,7 @@
 // R^{-1} is then formed recursively: 32 x 32 diagonal blocks by back
 // substitution, then levels of X_IJ = -X_II R_IJ X_JJ with doubling block
 // size, each two batched FP64 products.
+#include <cmath>
 #include <cstdlib>
 #include <string>
 
@@ -846,6 +847,499 @@ static tomos_status qr_block_update(double* SA, int64_t ld, int64_t k, int64_t n
     return qr_gemm<false>(q.Vb, k, q.Wb, w, C, ld, krem, nc, w, -1.0, 1.0, nullptr, 0, st, 1);
 }
 
+// X (n x n, column-major, leading dimension ldx) = R^{-1} for the upper
+// triangular R given row-major in Rt: zeros below the diagonal, 32 x 32
+// diagonal blocks by back substitution, then levels X_IJ = -X_II R_IJ X_JJ
+// of doubling block size (batched tiles, or two GEMMs a pair from
+// kTrtriGemmMin on).  Tb holds one level's products; P (pcap doubles) the
+// GEMMs' split-K partials.
+static tomos_status trtri_rt(const double* Rt, int64_t n, double* X, int64_t ldx, double* Tb, double* P,
+                             size_t pcap, cudaStream_t st) {
+    const int64_t nbk = (n + 31) / 32;
+    qr_zero_lower_kernel<<<(unsigned)((n * n + 255) / 256 < 4096 ? (n * n + 255) / 256 : 4096), 256, 0,
+                           st>>>(X, ldx, n);
+    TOMOS_LAUNCH_CHECK("qr_zero_lower_kernel");
+    qr_trtri_diag_kernel<<<(unsigned)nbk, 32, 0, st>>>(Rt, n, X, ldx);
+    TOMOS_LAUNCH_CHECK("qr_trtri_diag_kernel");
+    for (int64_t b = 32; b < n; b *= 2) {
+        const int64_t pairs = (n - b + 2 * b - 1) / (2 * b);
+        if (b >= kTrtriGemmMin) {
+            // few, large pairs: each product a qr_gemm_kernel launch
+            //   T_p = R_IJ X_JJ  (R_IJ from the row-major copy of R),
+            //   X_IJ = -X_II T_p
+            for (int64_t p = 0; p < pairs; ++p) {
+                const int64_t I0 = 2 * b * p, J0 = I0 + b;
+                const int64_t Jn = n - J0 < b ? n - J0 : b;
+                if (Jn <= 0) continue;
+                double* Tp = Tb + (size_t)p * b * b;
+                tomos_status gs = qr_gemm<true>(Rt + (size_t)I0 * n + J0, n, X + (size_t)J0 * ldx + J0, ldx,
+                                                Tp, b, b, Jn, Jn, 1.0, 0.0, P, pcap, st);
+                if (gs) return gs;
+                gs = qr_gemm<false>(X + (size_t)I0 * ldx + I0, ldx, Tp, b, X + (size_t)J0 * ldx + I0, ldx, b, Jn,
+                                    b, -1.0, 0.0, P, pcap, st);
+                if (gs) return gs;
+            }
+            continue;
+        }
+        const dim3 g((unsigned)((b + 31) / 32), (unsigned)((b + 31) / 32), (unsigned)pairs);
+        trtri_level_kernel<<<g, 256, 0, st>>>(Rt, n, X, ldx, Tb, b, 0);
+        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
+        trtri_level_kernel<<<g, 256, 0, st>>>(Rt, n, X, ldx, Tb, b, 1);
+        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
+    }
+    return TOMOS_OK;
+}
+
+
+// ------------------------------------------------------------ wide path
+//
+// For sketches of up to kQrWideMaxN columns, the factorisation is formed
+// from the whole sketch at once instead of 32-column panels (whose chains
+// leave most SMs waiting at grid barriers):
+//   G = SA^T SA                          (FP64 tensor-core GEMM)
+//   D^-1 G D^-1 = U^T U, d_j = G_jj^1/2 (blocked Cholesky; R = U D is SA's
+//                                        R with a positive diagonal)
+//   R^-1 = D^-1 U^-1                     (trtri_rt)
+//   Q_top = SA[0:n, :] R^-1, and the LU factorisation without pivoting
+//   Q_top - S = L U' with s_j = -sign of the pivot: the Householder
+//   reconstruction of the panel path applied to all n columns, whose S is
+//   the sign LAPACK's dgeqr2 gives row j of R (R_h = S R, R_h^-1 = R^-1 S).
+// It is Cholesky QR once, so it is used only when kappa_F(U) =
+// ||U||_F ||U^-1||_F = sqrt(n) ||U^-1||_F is at most kQrWideMaxKappa (R then
+// agrees with the Householder R to about kappa * 1e-16) and every Cholesky
+// pivot is above kQrWideFloor; otherwise the panel path factors SA, which
+// the wide path leaves untouched until it has passed both checks.
+//
+// The two n x n factorisations run in one cooperative launch each
+// (fact_kernel): right-looking in 32-column blocks, one grid barrier a
+// block.  CTA 0 updates the next diagonal block first and factors it
+// (cta_chol / cta_lu_signed, and its inverses) while the other CTAs apply
+// the current block to the rest of the trailing matrix in 32 x 32 tiles.
+
+constexpr int64_t kQrWideMaxN = 2048;
+constexpr double kQrWideMaxKappa = 1e6;
+constexpr double kQrWideFloor = 1e-10;
+
+struct WideScratch {
+    double* G;     // n x n column-major: SA^T SA, equilibrated, then Q_top
+    double* Ur;    // n x n row-major: U
+    double* X;     // n x n column-major: U^-1, then R^-1
+    double* d;     // n: column norms of SA
+    double* sgn;   // n: S
+    double* Xd;    // 2 x 2 x 32 x 32: a diagonal block's inverse factors (by block parity)
+    double* kap;   // ||U^-1||_F^2
+    double* Tb;    // trtri level products
+    double* P;     // GEMM split-K partials
+    size_t pcap;
+    int* flag;     // [0] a Cholesky pivot failed or d_j == 0
+    GridSync* gs;
+    size_t bytes;
+};
+
+static WideScratch wide_layout(void* base, int64_t n) {
+    WideScratch w;
+    char* p = static_cast<char*>(base);
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        char* r = p ? p + off : nullptr;
+        off += a256(b);
+        return r;
+    };
+    const size_t nn = n > 0 ? (size_t)n : 1;
+    w.G = reinterpret_cast<double*>(take(sizeof(double) * nn * nn));
+    w.Ur = reinterpret_cast<double*>(take(sizeof(double) * nn * nn));
+    w.X = reinterpret_cast<double*>(take(sizeof(double) * nn * nn));
+    w.d = reinterpret_cast<double*>(take(sizeof(double) * nn));
+    w.sgn = reinterpret_cast<double*>(take(sizeof(double) * nn));
+    w.Xd = reinterpret_cast<double*>(take(sizeof(double) * 4 * kHB * kHB));
+    w.kap = reinterpret_cast<double*>(take(sizeof(double) * 2));
+    size_t tb = 1;
+    for (int64_t b = 32; b < n; b *= 2) {
+        const size_t pairs = (size_t)((n - b + 2 * b - 1) / (2 * b));
+        if (pairs * b * b > tb) tb = pairs * b * b;
+    }
+    w.Tb = reinterpret_cast<double*>(take(sizeof(double) * tb));
+    w.pcap = 4 * nn * nn;
+    w.P = reinterpret_cast<double*>(take(sizeof(double) * w.pcap));
+    w.flag = reinterpret_cast<int*>(take(sizeof(int) * 4));
+    w.gs = reinterpret_cast<GridSync*>(take(sizeof(GridSync)));
+    w.bytes = off;
+    return w;
+}
+
+// d_j = G_jj^1/2 (flag[0] set when a column of SA is zero or not finite).
+__global__ void wide_colnorm_kernel(const double* G, int64_t n, double* d, int* flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double gi = G[i * n + i];
+        const bool ok = gi > 0.0 && isfinite(gi);
+        if (!ok) atomicOr(flag, 1);
+        d[i] = ok ? sqrt(gi) : 1.0;
+    }
+}
+
+// The upper half of D^-1 G D^-1 in place (d from wide_colnorm_kernel, so no
+// thread reads a diagonal entry another one rescales).
+__global__ void wide_equilibrate_kernel(double* G, int64_t n, const double* d) {
+    const int64_t total = n * n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, j = e / n;
+        if (i <= j) G[e] /= d[i] * d[j];
+    }
+}
+
+// ||X||_F^2 of the n x n column-major X (one block).
+__global__ void wide_fro2_kernel(const double* X, int64_t n, double* out) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int64_t e = threadIdx.x; e < n * n; e += blockDim.x) s += X[e] * X[e];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sm[w];
+        *out = t;
+    }
+}
+
+// X <- D^-1 X (rows scaled: U^-1 -> R^-1).
+__global__ void wide_row_scale_kernel(double* X, int64_t n, const double* d) {
+    const int64_t total = n * n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+        X[e] /= d[e % n];
+}
+
+// The outputs: R_h^-1 = R^-1 S in the leading n x n block of SA (zeros
+// below the diagonal) and, when asked, R_h = S U D (column-major, ld n).
+__global__ void wide_output_kernel(const double* X, const double* Ur, const double* d, const double* sgn,
+                                   int64_t n, double* SA, int64_t ld, double* R) {
+    const int64_t total = n * n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, j = e / n;
+        SA[(size_t)j * ld + i] = i <= j ? X[e] * sgn[j] : 0.0;
+        if (R) R[e] = i <= j ? sgn[i] * Ur[(size_t)i * n + j] * d[j] : 0.0;
+    }
+}
+
+struct FactArgs {
+    double* M;      // n x n column-major (ld n), updated in place
+    int64_t n;
+    int mode;       // 0: Cholesky of the upper half (U to Ur); 1: signed LU (signs to sgn)
+    double* Ur;
+    double* Xd;
+    double* sgn;
+    int64_t keep;   // LU: the column dlarfg leaves as the identity, or -1
+    double floor;
+    int* fail;
+    GridSync* gs;
+};
+
+constexpr int kFactSmemMats = 6;
+
+// X = R^{-1} for an upper triangular 32 x 32 R in shared memory: lane c of
+// warp 0 solves R x = e_c by back substitution on registers (rows of R are
+// broadcast reads), two partial sums a row; the other warps wait at the end.
+__device__ __forceinline__ void warp_inv_upper(const HMat& R, HMat& X, double* dinv) {
+    const int t = threadIdx.x;
+    if (t < kHB) dinv[t] = 1.0 / R[t][t];
+    __syncthreads();
+    if (t < kHB) {
+        const int c = t;
+        double x[kHB];
+#pragma unroll
+        for (int i = kHB - 1; i >= 0; --i) {
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int k = i + 1; k < kHB; k += 2) {
+                s0 = fma(R[i][k], x[k], s0);
+                if (k + 1 < kHB) s1 = fma(R[i][k + 1], x[k + 1], s1);
+            }
+            const double v = ((i == c ? 1.0 : 0.0) - (s0 + s1)) * dinv[i];
+            x[i] = i > c ? 0.0 : v;
+        }
+#pragma unroll
+        for (int i = 0; i < kHB; ++i) X[i][c] = x[i];
+    }
+    __syncthreads();
+}
+
+// Y = L^{-1} for the unit lower triangular L held strictly below the
+// diagonal of Q: lane c of warp 0 solves L y = e_c by forward substitution.
+__device__ __forceinline__ void warp_inv_unit_lower(const HMat& Q, HMat& Y) {
+    const int t = threadIdx.x;
+    if (t < kHB) {
+        const int c = t;
+        double y[kHB];
+#pragma unroll
+        for (int i = 0; i < kHB; ++i) {
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < i; k += 2) {
+                s0 = fma(Q[i][k], y[k], s0);
+                if (k + 1 < i) s1 = fma(Q[i][k + 1], y[k + 1], s1);
+            }
+            const double v = (i == c ? 1.0 : 0.0) - (s0 + s1);
+            y[i] = i < c ? 0.0 : v;
+        }
+#pragma unroll
+        for (int i = 0; i < kHB; ++i) Y[i][c] = y[i];
+    }
+    __syncthreads();
+}
+
+// Factor the diagonal block of block column p (M's block already holds
+// every earlier update): Cholesky U_pp (to Ur) and X = U_pp^-1, or the
+// signed LU L\U of the block with X = U^-1, Y = L^-1; X (and Y) to
+// Xd[p & 1] as row-major 32 x 32.
+__device__ void fact_diag(const FactArgs& a, int64_t p, double* sm) {
+    HMat& B = *reinterpret_cast<HMat*>(sm);
+    HMat& R = *reinterpret_cast<HMat*>(sm + 1 * kHB * (kHB + 1));
+    HMat& X = *reinterpret_cast<HMat*>(sm + 2 * kHB * (kHB + 1));
+    HMat& Y = *reinterpret_cast<HMat*>(sm + 3 * kHB * (kHB + 1));
+    __shared__ int okf;
+    __shared__ double sg[kHB];
+    const int t = threadIdx.x;
+    const int64_t n = a.n, jb = p * kHB;
+    const int nb = (int)(n - jb < kHB ? n - jb : kHB);
+    __syncthreads();
+    for (int e = t; e < kHB * kHB; e += blockDim.x) {
+        const int r = e & 31, c = e >> 5;
+        B[r][c] = (r < nb && c < nb) ? __ldcg(a.M + (size_t)(jb + c) * n + jb + r) : (r == c ? 1.0 : 0.0);
+    }
+    double* xd = a.Xd + (size_t)(p & 1) * 2 * kHB * kHB;
+    __shared__ double dinv[kHB];
+    if (a.mode == 0) {
+        const bool ok = cta_chol(B, R, a.floor, &okf);
+        if (!ok && t == 0) atomicExch(a.fail, 1);
+        warp_inv_upper(R, X, dinv);
+        for (int e = t; e < kHB * kHB; e += blockDim.x) {
+            const int r = e >> 5, c = e & 31;
+            if (r < nb && c < nb) a.Ur[(size_t)(jb + r) * n + jb + c] = r <= c ? R[r][c] : 0.0;
+            xd[e] = X[r][c];
+        }
+    } else {
+        const int64_t kk = a.keep - jb;
+        cta_lu_signed(B, sg, (kk >= 0 && kk < nb) ? (int)kk : -1);
+        for (int e = t; e < kHB * kHB; e += blockDim.x) {
+            const int r = e >> 5, c = e & 31;
+            R[r][c] = r <= c ? B[r][c] : 0.0;
+        }
+        if (t < nb) a.sgn[jb + t] = sg[t];
+        __syncthreads();
+        warp_inv_upper(R, X, dinv);
+        warp_inv_unit_lower(B, Y);
+        for (int e = t; e < kHB * kHB; e += blockDim.x) {
+            const int r = e >> 5, c = e & 31;
+            xd[e] = X[r][c];
+            xd[kHB * kHB + e] = Y[r][c];
+        }
+    }
+    __syncthreads();
+}
+
+// C = A^T B (TA) or A B over the CTA, 32 x 32 shared tiles.
+template <bool TA>
+__device__ __forceinline__ void fact_mm(const HMat& A, const HMat& B, HMat& C) {
+    const int t = threadIdx.x;
+    const int i = t & 31, j0 = (t >> 5) * 4;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < kHB; ++k) {
+        const double x = TA ? A[k][i] : A[i][k];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s[q] += x * B[k][j0 + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) C[i][j0 + q] = s[q];
+}
+
+// Trailing tile `tau` of block column p: Cholesky tiles (I <= J) in rows,
+// LU tiles (I, J) row by row; tile 0 is the next diagonal block.
+__device__ void fact_tile(const FactArgs& a, int64_t p, int64_t tau, double* sm) {
+    HMat& A1 = *reinterpret_cast<HMat*>(sm);
+    HMat& P1 = *reinterpret_cast<HMat*>(sm + 1 * kHB * (kHB + 1));
+    HMat& A2 = *reinterpret_cast<HMat*>(sm + 2 * kHB * (kHB + 1));
+    HMat& P2 = *reinterpret_cast<HMat*>(sm + 3 * kHB * (kHB + 1));
+    HMat& F1 = *reinterpret_cast<HMat*>(sm + 4 * kHB * (kHB + 1));
+    HMat& F2 = *reinterpret_cast<HMat*>(sm + 5 * kHB * (kHB + 1));
+    const int t = threadIdx.x;
+    const int64_t n = a.n, jb = p * kHB, t0 = jb + kHB;
+    const int64_t nt = (n - t0 + kHB - 1) / kHB;
+    int64_t I, J;
+    if (a.mode == 0) {
+        I = 0;
+        int64_t rest = tau;
+        while (rest >= nt - I) {
+            rest -= nt - I;
+            ++I;
+        }
+        J = I + rest;
+    } else {
+        I = tau / nt;
+        J = tau % nt;
+    }
+    const int64_t I0 = t0 + I * kHB, J0 = t0 + J * kHB;
+    const int wI = (int)(n - I0 < kHB ? n - I0 : kHB), wJ = (int)(n - J0 < kHB ? n - J0 : kHB);
+    const double* xd = a.Xd + (size_t)(p & 1) * 2 * kHB * kHB;
+    __syncthreads();
+    for (int e = t; e < kHB * kHB; e += blockDim.x) {
+        const int r = e & 31, c = e >> 5;
+        F1[r][c] = __ldcg(xd + r * kHB + c);
+        if (a.mode == 0) {
+            // row panel of G: A1 = G[jb.., I cols], A2 = G[jb.., J cols]
+            A1[r][c] = c < wI ? __ldcg(a.M + (size_t)(I0 + c) * n + jb + r) : 0.0;
+            A2[r][c] = c < wJ ? __ldcg(a.M + (size_t)(J0 + c) * n + jb + r) : 0.0;
+        } else {
+            F2[r][c] = __ldcg(xd + kHB * kHB + r * kHB + c);
+            // A1 = M[I rows, panel cols], A2 = M[panel rows, J cols]
+            A1[r][c] = r < wI ? __ldcg(a.M + (size_t)(jb + c) * n + I0 + r) : 0.0;
+            A2[r][c] = c < wJ ? __ldcg(a.M + (size_t)(J0 + c) * n + jb + r) : 0.0;
+        }
+    }
+    __syncthreads();
+    if (a.mode == 0) {
+        fact_mm<true>(F1, A1, P1);   // U_pI = X^T G_pI
+        if (I != J) fact_mm<true>(F1, A2, P2);  // U_pJ
+        __syncthreads();
+        const HMat& PJ = I != J ? P2 : P1;
+        fact_mm<true>(P1, PJ, A1);   // U_pI^T U_pJ
+        if (I == J)
+            for (int e = t; e < kHB * kHB; e += blockDim.x) {
+                const int r = e >> 5, c = e & 31;
+                if (c < wJ) a.Ur[(size_t)(jb + r) * n + J0 + c] = P1[r][c];
+            }
+    } else {
+        fact_mm<false>(A1, F1, P1);  // L_Ip = M_Ip U_pp^-1
+        fact_mm<false>(F2, A2, P2);  // U_pJ = L_pp^-1 M_pJ
+        __syncthreads();
+        fact_mm<false>(P1, P2, A1);  // L_Ip U_pJ
+    }
+    __syncthreads();
+    for (int e = t; e < kHB * kHB; e += blockDim.x) {
+        const int r = e & 31, c = e >> 5;
+        if (r < wI && c < wJ) a.M[(size_t)(J0 + c) * n + I0 + r] -= A1[r][c];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kQrThreads, 1) fact_kernel(FactArgs a) {
+    extern __shared__ __align__(16) double fsm[];
+    __shared__ int sflag;
+    unsigned int gen = 0;
+    const int64_t n = a.n;
+    const int64_t np = (n + kHB - 1) / kHB;
+    const int64_t G = gridDim.x;
+    if (blockIdx.x == 0) fact_diag(a, 0, fsm);
+    if (!grid_sync(a.gs, gen, &sflag)) return;
+    for (int64_t p = 0; p + 1 < np; ++p) {
+        const int64_t t0 = (p + 1) * kHB;
+        const int64_t nt = (n - t0 + kHB - 1) / kHB;
+        const int64_t ntiles = a.mode == 0 ? nt * (nt + 1) / 2 : nt * nt;
+        if (blockIdx.x == 0) {
+            fact_tile(a, p, 0, fsm);
+            fact_diag(a, p + 1, fsm);
+            if (G == 1)
+                for (int64_t tau = 1; tau < ntiles; ++tau) fact_tile(a, p, tau, fsm);
+        } else {
+            for (int64_t tau = blockIdx.x; tau < ntiles; tau += G - 1) fact_tile(a, p, tau, fsm);
+        }
+        if (!grid_sync(a.gs, gen, &sflag)) return;
+    }
+}
+
+// One cooperative launch of fact_kernel (one CTA per SM).
+static tomos_status launch_fact(const FactArgs& fa, GridSync* gs, cudaStream_t st) {
+    const size_t smem = sizeof(double) * kFactSmemMats * kHB * (kHB + 1);
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(fact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TOMOS_CUDA_TRY(cudaMemsetAsync(gs, 0, sizeof(GridSync), st));
+    FactArgs a = fa;
+    void* args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)fact_kernel, dim3((unsigned)sm_count()),
+                                                dim3(kQrThreads), args, smem, st);
+    if (e != cudaSuccess) return cuda_fail(e, "sketch_qr: cooperative launch (wide path)");
+    return TOMOS_OK;
+}
+
+// The wide path (see above).  *done false: SA untouched, the panel path
+// must factor it (not used for this size, a failed pivot, or kappa above
+// kQrWideMaxKappa).
+static tomos_status qr_wide(int64_t k, int64_t n, double* SA, int64_t ld, double* R, const WideScratch& w,
+                            cudaStream_t st, bool* done) {
+    *done = false;
+    TOMOS_CUDA_TRY(cudaMemsetAsync(w.flag, 0, sizeof(int) * 4, st));
+    tomos_status s = qr_gemm<true>(SA, ld, SA, ld, w.G, n, n, n, k, 1.0, 0.0, w.P, w.pcap, st);
+    if (s) return s;
+    const unsigned eb = (unsigned)((n * n + 255) / 256 < 4096 ? (n * n + 255) / 256 : 4096);
+    wide_colnorm_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(w.G, n, w.d, w.flag);
+    TOMOS_LAUNCH_CHECK("wide_colnorm_kernel");
+    wide_equilibrate_kernel<<<eb, 256, 0, st>>>(w.G, n, w.d);
+    TOMOS_LAUNCH_CHECK("wide_equilibrate_kernel");
+    FactArgs fa;
+    fa.M = w.G;
+    fa.n = n;
+    fa.mode = 0;
+    fa.Ur = w.Ur;
+    fa.Xd = w.Xd;
+    fa.sgn = w.sgn;
+    fa.keep = -1;
+    fa.floor = kQrWideFloor;
+    fa.fail = w.flag;
+    fa.gs = w.gs;
+    s = launch_fact(fa, w.gs, st);
+    if (s) return s;
+    s = trtri_rt(w.Ur, n, w.X, n, w.Tb, w.P, w.pcap, st);
+    if (s) return s;
+    wide_fro2_kernel<<<1, 1024, 0, st>>>(w.X, n, w.kap);
+    TOMOS_LAUNCH_CHECK("wide_fro2_kernel");
+    int flag = 0;
+    double kap2 = 0.0;
+    GridSync gsh{};
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(&flag, w.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(&kap2, w.kap, sizeof(double), cudaMemcpyDeviceToHost, st));
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(&gsh, w.gs, sizeof(gsh), cudaMemcpyDeviceToHost, st));
+    TOMOS_CUDA_TRY(cudaStreamSynchronize(st));
+    if (gsh.err) return fail(TOMOS_ERR_CUDA, "sketch_qr: a bounded grid barrier wait expired");
+    const double kappa = std::sqrt((double)n * kap2);
+    if (flag || !(kappa <= kQrWideMaxKappa)) return TOMOS_OK;  // the panel path takes over
+    wide_row_scale_kernel<<<eb, 256, 0, st>>>(w.X, n, w.d);
+    TOMOS_LAUNCH_CHECK("wide_row_scale_kernel");
+    // Q_top = SA[0:n, :] R^-1 into G (no longer needed), then its signed LU
+    s = qr_gemm<false>(SA, ld, w.X, n, w.G, n, n, n, n, 1.0, 0.0, w.P, w.pcap, st);
+    if (s) return s;
+    fa.mode = 1;
+    fa.keep = k == n ? n - 1 : -1;
+    s = launch_fact(fa, w.gs, st);
+    if (s) return s;
+    wide_output_kernel<<<eb, 256, 0, st>>>(w.X, w.Ur, w.d, w.sgn, n, SA, ld, R);
+    TOMOS_LAUNCH_CHECK("wide_output_kernel");
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(&gsh, w.gs, sizeof(gsh), cudaMemcpyDeviceToHost, st));
+    TOMOS_CUDA_TRY(cudaStreamSynchronize(st));
+    if (gsh.err) return fail(TOMOS_ERR_CUDA, "sketch_qr: a bounded grid barrier wait expired");
+    *done = true;
+    return TOMOS_OK;
+}
+
+// Whether the wide path is tried: n from 64 to kQrWideMaxN columns.
+// TOMOS_QR_WIDE=0 turns it off, =1 tries it at every size up to the max,
+// =3 requires it there (a sketch it refuses is then an error; for tests).
+static int qr_wide_mode() {
+    static int mode = -1;
+    if (mode < 0) {
+        const char* e = std::getenv("TOMOS_QR_WIDE");
+        mode = e ? std::atoi(e) : 2;
+    }
+    return mode;
+}
+
+static bool qr_wide_used(int64_t n) {
+    const int mode = qr_wide_mode();
+    if (mode == 0 || n > kQrWideMaxN) return false;
+    return mode == 1 || mode == 3 ? n >= 1 : n >= 64;
+}
+
 }  // namespace tomos_b200
 
 using namespace tomos_b200;
@@ -854,7 +1348,8 @@ extern "C" {
 
 size_t tomos_sketch_qr_scratch_bytes(int64_t k, int64_t n) {
     if (k < 0 || n < 0) return 0;
-    return qr_layout(nullptr, k, n).bytes;
+    const size_t panel = qr_layout(nullptr, k, n).bytes;
+    return qr_wide_used(n) ? panel + wide_layout(nullptr, n).bytes : panel;
 }
 
 tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64_t ld, double* R,
@@ -872,6 +1367,15 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
                     "sketch_qr: scratch too small (need " + std::to_string(need.bytes) + " bytes)");
     QrScratch q = qr_layout(scratch, k, n);
     cudaStream_t st = as_stream(stream);
+    if (qr_wide_used(n) && scratch_bytes >= need.bytes + wide_layout(nullptr, n).bytes) {
+        bool done = false;
+        tomos_status ws = qr_wide(k, n, SA, ld, R,
+                                  wide_layout(static_cast<char*>(scratch) + need.bytes, n), st, &done);
+        if (ws) return ws;
+        if (done) return TOMOS_OK;
+        if (qr_wide_mode() == 3)
+            return fail(TOMOS_ERR_NUMERIC, "sketch_qr: the wide path refused this sketch (TOMOS_QR_WIDE=3)");
+    }
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_hr_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)hr_v_smem()));
     TOMOS_CUDA_TRY(cudaMemsetAsync(q.flag, 0, sizeof(int) * 4, st));
@@ -991,39 +1495,7 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     if (flag)
         return fail(TOMOS_ERR_NUMERIC,
                     "generate_sketch_qr_precond: trtri failed -- R is singular.");
-    const int64_t nbk = (n + 31) / 32;
-    qr_zero_lower_kernel<<<(unsigned)((n * n + 255) / 256 < 4096 ? (n * n + 255) / 256 : 4096), 256, 0,
-                           st>>>(SA, ld, n);
-    TOMOS_LAUNCH_CHECK("qr_zero_lower_kernel");
-    qr_trtri_diag_kernel<<<(unsigned)nbk, 32, 0, st>>>(q.Rt, n, SA, ld);
-    TOMOS_LAUNCH_CHECK("qr_trtri_diag_kernel");
-    for (int64_t b = 32; b < n; b *= 2) {
-        const int64_t pairs = (n - b + 2 * b - 1) / (2 * b);
-        if (b >= kTrtriGemmMin) {
-            // few, large pairs: each product a qr_gemm_kernel launch
-            //   T_p = R_IJ X_JJ  (R_IJ from the row-major copy of R),
-            //   X_IJ = -X_II T_p
-            for (int64_t p = 0; p < pairs; ++p) {
-                const int64_t I0 = 2 * b * p, J0 = I0 + b;
-                const int64_t Jn = n - J0 < b ? n - J0 : b;
-                if (Jn <= 0) continue;
-                double* Tp = q.Tb + (size_t)p * b * b;
-                tomos_status gs = qr_gemm<true>(q.Rt + (size_t)I0 * n + J0, n, SA + (size_t)J0 * ld + J0, ld,
-                                                Tp, b, b, Jn, Jn, 1.0, 0.0, q.Pk, q.pk_doubles, st);
-                if (gs) return gs;
-                gs = qr_gemm<false>(SA + (size_t)I0 * ld + I0, ld, Tp, b, SA + (size_t)J0 * ld + I0, ld, b, Jn,
-                                    b, -1.0, 0.0, q.Pk, q.pk_doubles, st);
-                if (gs) return gs;
-            }
-            continue;
-        }
-        const dim3 g((unsigned)((b + 31) / 32), (unsigned)((b + 31) / 32), (unsigned)pairs);
-        trtri_level_kernel<<<g, 256, 0, st>>>(q.Rt, n, SA, ld, q.Tb, b, 0);
-        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
-        trtri_level_kernel<<<g, 256, 0, st>>>(q.Rt, n, SA, ld, q.Tb, b, 1);
-        TOMOS_LAUNCH_CHECK("trtri_level_kernel");
-    }
-    return TOMOS_OK;
+    return trtri_rt(q.Rt, n, SA, ld, q.Tb, q.Pk, q.pk_doubles, st);
 }
 
 }  // extern "C"

@@ -103,19 +103,16 @@ struct RowPassParams {
     int copy_bytes;  // bytes copied per row and plane (16-byte multiple)
     int tiles_per_stage;  // row tiles (CW / G rows each) a stage holds
     double* qpart64; // kRowAxpy with ACC64: FP64 partials (gridDim.x x qstride)
-    int corr_offset; // FP32_16 HALF sums of lines: byte offset of the n-float
-                     // column corrections in dynamic shared memory
 };
 
 // The control words of one lane's row part (NCH chunks of 8 wh words, as
 // loaded; elements from zero_from on lie past the row and are skipped):
-// for each, d = fp32_16_half_only value - its plain fp16 conversion.  With
-// p, returns sum d * p[col] (the correction of the lane's dot); with corr,
-// adds d * ut to corr[col] (shared memory) and returns 0.  A loop over the
-// flagged elements only, so a lane without one passes through at once.
+// returns sum d * p[col] with d = fp32_16_half_only value - its plain fp16
+// conversion (the correction of the lane's dot).  A loop over the flagged
+// elements only, so a lane without one passes through at once.
 template <int NCH>
 __device__ __forceinline__ float h16_corrections(const uint4 (&hk)[NCH], int part, int lane, int zero_from,
-                                                 const float* p, float ut, float* corr) {
+                                                 const float* p) {
     float dsum = 0.0f;
 #pragma unroll
     for (int k = 0; k < NCH; ++k) {
@@ -132,8 +129,7 @@ __device__ __forceinline__ float h16_corrections(const uint4 (&hk)[NCH], int par
             const uint32_t hb = (ww >> (hi * 16)) & 0xFFFFu;
             const float d = half_bits_to_float(half_only_bits(hb)) - half_bits_to_float(hb);
             const int64_t col = ((int64_t)part * 32 * NCH + (int64_t)k * 32 + lane) * 8 + q;
-            if (p) dsum += d * __ldg(p + col);
-            if (corr) atomicAdd(&corr[col], d * ut);
+            dsum += d * __ldg(p + col);
         }
     }
     return dsum;
@@ -264,12 +260,11 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
     // standalone FP64 tiers (kRowDot, kRowAxpy with ACC64) form FP32
     // products over short runs and sum those in FP64.
     constexpr bool P64 = ACC64 && MODE == kRowBoth;
-    // FP32_16 wh words in a standalone product: every word converted as an
-    // fp16 value, and the rare control words corrected afterwards by the
-    // difference between their fp32_16_half_only value and that conversion
-    // (into the lane's dot, or into a per-CTA column buffer in shared
-    // memory), so the warp never waits on a per-element fix.
-    constexpr bool HCORR = E == Elem::H16 && MODE != kRowBoth;
+    // FP32_16 wh words in a standalone dot product: every word converted as
+    // an fp16 value, and the rare control words corrected afterwards by the
+    // difference between their fp32_16_half_only value and that conversion,
+    // added to the lane's own partial dot (so the sum keeps its fixed order).
+    constexpr bool HCORR = E == Elem::H16 && MODE == kRowDot;
     constexpr int NTHREADS = (CW + 1) * 32;
     static_assert(CW % G == 0, "G divides the consumer warps");
     const FusedParams& P = T.f;
@@ -315,11 +310,6 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         abort_flag = 0;
         fence_barrier_init();
     }
-    // column corrections of the control words (HCORR sums of lines), after
-    // everything else in dynamic shared memory
-    float* corr = reinterpret_cast<float*>(smem + T.corr_offset);
-    if constexpr (HCORR && AXPY)
-        for (int64_t j = threadIdx.x; j < P.n; j += NTHREADS) corr[j] = 0.0f;
     __syncthreads();
 
     float2 acc[PER / 2];
@@ -509,7 +499,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                     d1 = __ffma2_rn(a[j + 1], pv[j + 1], d1);
                 }
                 if constexpr (HCORR) {
-                    if (has && !failed) d0.x += h16_corrections<NCH>(hk, part, lane, zero_from, P.p, 0.0f, nullptr);
+                    if (has && !failed) d0.x += h16_corrections<NCH>(hk, part, lane, zero_from, P.p);
                 }
                 if constexpr (ACC64) {
                     // FP32 products summed over the lane's run, then FP64
@@ -548,9 +538,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                 const float2 ut2 = make_float2(ut, ut);
 #pragma unroll
                 for (int j = 0; j < PER / 2; ++j) acc[j] = __ffma2_rn(a[j], ut2, acc[j]);
-                if constexpr (HCORR) {
-                    if (has && !failed) h16_corrections<NCH>(hk, part, lane, zero_from, nullptr, ut, corr);
-                }
+
                 if constexpr (ACC64 && MODE != kRowBoth) {
                     if ((t + 1) % kRowPromote == 0) {
 #pragma unroll
@@ -618,7 +606,6 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         float sum = 0.0f;
 #pragma unroll
         for (int r = 0; r < RS; ++r) sum += red[(size_t)(r * G + g) * WCOLS + loc];
-        if constexpr (HCORR) sum += corr[j];
         qout[j] = sum;
     }
     if (MODE == kRowBoth && threadIdx.x == 0) {
@@ -637,14 +624,7 @@ inline size_t fused_rows_smem(int nstage, int rows_per_stage, int copy_bytes) {
     const size_t ring = (size_t)nstage * rows_per_stage * copy_bytes * RowPlanes<E>::value;
     const size_t esz = (ACC64 && MODE == kRowAxpy) ? sizeof(double) : sizeof(float);
     const size_t red = (size_t)RowWarps<E, ACC64>::value * NCH * 32 * VEC * esz;
-    const size_t body = ring > red ? ring : red;
-    return (body + 15) / 16 * 16;
-}
-
-// Bytes of the column-correction buffer (FP32_16 HALF sums of lines).
-template <Elem E, int MODE>
-inline size_t fused_rows_corr_bytes(int64_t n) {
-    return (E == Elem::H16 && MODE == kRowAxpy) ? (size_t)((n * 4 + 15) / 16 * 16) : 0;
+    return ring > red ? ring : red;
 }
 
 }  // namespace tomos_b200

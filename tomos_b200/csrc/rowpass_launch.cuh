@@ -24,8 +24,7 @@ inline tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cud
     T.qpart64 = qpart64;
     T.copy_bytes = (int)((((int64_t)P.n * ESZ) + 15) / 16 * 16);
     const size_t tile = (size_t)RS * T.copy_bytes * RowPlanes<E>::value;
-    const size_t corr = fused_rows_corr_bytes<E, MODE>(P.n);
-    const size_t budget = kRowSmemBudget - corr;
+    const size_t budget = kRowSmemBudget;
     // tiles per stage: enough that a copy moves about kRowCopyTarget bytes
     // a plane, while the ring still holds two stages
     int tps = (int)((kRowCopyTarget + (size_t)RS * T.copy_bytes - 1) / ((size_t)RS * T.copy_bytes));
@@ -37,9 +36,7 @@ inline tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cud
     if (ns > kRowMaxStages) ns = kRowMaxStages;
     if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
     T.nstage = ns;
-    const size_t body = fused_rows_smem<E, NCH, ACC64, MODE>(ns, RS * tps, T.copy_bytes);
-    T.corr_offset = (int)body;
-    const size_t smem = body + corr;
+    const size_t smem = fused_rows_smem<E, NCH, ACC64, MODE>(ns, RS * tps, T.copy_bytes);
     auto kern = fused_rows_kernel<E, NCH, G, ACC64, MODE>;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, (CW + 1) * 32, smem, st>>>(T);
@@ -106,8 +103,7 @@ inline bool plan_row_lines(Elem e, bool acc64, int64_t inner, int64_t ld, const 
     if (nch == 0) return false;
     const int64_t rows_per_stage = fused_warps(e, acc64) / g;
     const int64_t stage = rows_per_stage * ((inner * wbytes + 15) / 16 * 16) * (elem_two_planes(e) ? 2 : 1);
-    const int64_t corr = e == Elem::H16 ? inner * 4 + 16 : 0;  // a sum of lines' corrections
-    if (2 * stage + corr > (int64_t)kRowSmemBudget) return false;
+    if (2 * stage > (int64_t)kRowSmemBudget) return false;
     *nch_out = nch;
     *g_out = g;
     return true;
