@@ -17,8 +17,12 @@ the same problem is timed beside it (fp32_ms, speedup_vs_fp32).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Multi-GPU runs are replicas (one independent problem per rank, the row
-sharding of LSQR is not built); timing is the max over ranks.
+Multi-GPU runs (torchrun, one process per GPU) solve ONE problem of
+N x 1,000,000 rows, row-sharded: rank r holds rows [r m, (r + 1) m) (drawn
+by the counter-based generator, so each rank makes only its own rows), the
+sketches are summed over the ranks, and every LSQR pass ends with one NCCL
+all-reduce of n + 1 doubles (A^T u and ||u||^2).  Per-GPU work is fixed as N
+grows (weak scaling); timing is the max over ranks.
 """
 import argparse
 import json
@@ -152,7 +156,8 @@ def gpu_solve(tb, torch, A, b, s):
     if ws is None:
         ws = tb.create_lsqr_workspace(None, (m, n), tb.NumericType.FP32, tb.NumericType.FP64)
         gpu_solve.ws[(m, n)] = ws
-    x, rep, d = tb.sketch_lsqr(A, b, s, tol=TOL, workspace=ws, profile=gpu_solve.profile, events=ev)
+    x, rep, d = tb.sketch_lsqr(A, b, s, tol=TOL, workspace=ws, profile=gpu_solve.profile, events=ev,
+                               comm=gpu_solve.comm, row0=gpu_solve.row0)
     gpu_solve.last_scale = d
     if ev:
         torch.cuda.synchronize()
@@ -165,6 +170,76 @@ def gpu_solve(tb, torch, A, b, s):
 gpu_solve.ws = {}
 gpu_solve.profile = False
 gpu_solve.last_scale = None
+gpu_solve.comm = None
+gpu_solve.row0 = 0
+
+
+def shard_problem(torch, problems, row0, m, n, seed, blk=1 << 16):
+    """Rows [row0, row0 + m) of the counter-based problem A = G diag(10^u),
+    b = A x_true + noise (problems.ctr_scaled_rows), generated block by
+    block into one (m, n) float32 tensor.  Returns (A, x_true, b)."""
+    params = problems.ctr_scaled_params(n, seed)
+    A = torch.empty((m, n), dtype=torch.float32, device="cuda")
+    b = torch.empty(m, dtype=torch.float32, device="cuda")
+    for r0 in range(0, m, blk):
+        r1 = min(m, r0 + blk)
+        Ab, bb = problems.ctr_scaled_rows(row0 + r0, row0 + r1, n, seed, params=params)
+        A[r0:r1] = Ab
+        b[r0:r1] = bb
+        del Ab, bb
+    return A, params[1].float(), b
+
+
+def allreduce_sum(torch, t):
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t)
+    return t
+
+
+def eta_rows(torch, A32, b, x, d, blk=1 << 17):
+    """Backward error of (A D^-1, b, D x) in FP64 over every rank's rows
+    (the sums over rows all-reduced): min(||r|| / (||A D^-1||_F ||D x|| +
+    ||b||), ||D^-1 A^T r|| / (||A D^-1||_F ||r||)).  d = None: D = I, the
+    plain normwise eta."""
+    m, n = A32.shape
+    x64 = x.double()
+    dd = torch.ones(n, dtype=torch.float64, device="cuda") if d is None else torch.where(d > 0, d, 1.0)
+    acc = torch.zeros(n + 3, dtype=torch.float64, device="cuda")
+    for r0 in range(0, m, blk):
+        Ab = A32[r0:r0 + blk].double()
+        bb = b[r0:r0 + blk].double()
+        r = bb - Ab @ x64
+        acc[:n] += Ab.t() @ r
+        acc[n] += r @ r
+        acc[n + 1] += bb @ bb
+        acc[n + 2] += ((Ab / dd) ** 2).sum()
+        del Ab
+    allreduce_sum(torch, acc)
+    rn, bn, fro = (float(v) for v in torch.sqrt(acc[n:]))
+    e1 = rn / (fro * float(torch.linalg.norm(dd * x64)) + bn)
+    e2 = float(torch.linalg.norm(acc[:n] / dd)) / (fro * rn) if rn > 0 else 0.0
+    return min(e1, e2)
+
+
+def ls_solution_rows(torch, A32, b, world, blk=1 << 17):
+    """The FP64 least-squares solution of the whole (row-sharded) problem:
+    Householder QR of [A | b] on the device (one rank: torch's lstsq), the
+    ranks' R factors gathered and factored again (TSQR)."""
+    import torch.distributed as dist
+    m, n = A32.shape
+    if world == 1:
+        A64 = A32.double()
+        x = torch.linalg.lstsq(A64, b.double().unsqueeze(1)).solution.squeeze(1)
+        del A64
+        return x
+    Ab = torch.cat([A32.double(), b.double().unsqueeze(1)], dim=1)
+    R = torch.linalg.qr(Ab, mode="r")[1]
+    del Ab
+    Rs = [torch.empty_like(R) for _ in range(world)]
+    dist.all_gather(Rs, R)
+    R = torch.linalg.qr(torch.cat(Rs), mode="r")[1]
+    return torch.linalg.solve_triangular(R[:n, :n], R[:n, n:], upper=True).squeeze(1)
 
 
 def count_launches(torch, fn):
@@ -206,7 +281,12 @@ def run_ours(args):
 
     m, n = args.m, args.n
     s = 4 * n
-    A32, xt, b = problems.dense_scaled(m, n, seed=args.seed + rank)
+    if world > 1:
+        # one problem of world * m rows, rank r holding rows [r m, (r + 1) m)
+        gpu_solve.comm, gpu_solve.row0 = tb.Comm(), rank * m
+        A32, xt, b = shard_problem(torch, problems, rank * m, m, n, args.seed)
+    else:
+        A32, xt, b = problems.dense_scaled(m, n, seed=args.seed)
     Af = tb.Dense(tb.NumericType.FP32, tb.Layout.ROW_MAJOR, (m, n), n, A32.view(-1))
     Ap = tb.pack(Af, tb.NumericType.FP32_16)
     torch.cuda.synchronize()
@@ -236,23 +316,26 @@ def run_ours(args):
     # accurate backward errors of the returned solutions (FP64, exact A):
     # eta_D of the column-scaled problem (the convergence measure) and the
     # plain normwise eta
-    ws_be = tb.create_lsqr_workspace(None, (m, n), tb.NumericType.FP32)
     d_exact = torch.zeros(n, dtype=torch.float64, device="cuda")  # exact column norms, FP64
     for r0 in range(0, m, 1 << 17):
         d_exact += (A32[r0:r0 + (1 << 17)].double() ** 2).sum(dim=0)
-    d_exact = torch.sqrt(d_exact)
-    be_p = tb.backward_error(Ap, b, xp, ws_be, col_scale=d_exact)["backward_error"]
-    be_f = tb.backward_error(Af, b, xf, ws_be, col_scale=d_exact)["backward_error"]
-    be_p_plain = tb.backward_error(Ap, b, xp, ws_be)["backward_error"]
-    be_f_plain = tb.backward_error(Af, b, xf, ws_be)["backward_error"]
+    d_exact = torch.sqrt(allreduce_sum(torch, d_exact))
+    if world == 1:  # the library's backward-error entry
+        ws_be = tb.create_lsqr_workspace(None, (m, n), tb.NumericType.FP32)
+        be_p = tb.backward_error(Ap, b, xp, ws_be, col_scale=d_exact)["backward_error"]
+        be_f = tb.backward_error(Af, b, xf, ws_be, col_scale=d_exact)["backward_error"]
+        be_p_plain = tb.backward_error(Ap, b, xp, ws_be)["backward_error"]
+        be_f_plain = tb.backward_error(Af, b, xf, ws_be)["backward_error"]
+        del ws_be
+    else:  # over every rank's rows, in FP64 from the FP32 values A was packed from
+        be_p, be_f = eta_rows(torch, A32, b, xp, d_exact), eta_rows(torch, A32, b, xf, d_exact)
+        be_p_plain, be_f_plain = eta_rows(torch, A32, b, xp, None), eta_rows(torch, A32, b, xf, None)
     rel_x = float(torch.linalg.norm((xp - xt).double()) / torch.linalg.norm(xt.double()))
     # forward error against the FP64 least-squares solution (Householder QR
     # of A in FP64, torch on the device), weighted by the column norms D --
     # what eta_D <= 1e-6 bounds (x_true is off the LS solution by the noise,
     # and the small columns' components are not determined to 1e-6 unweighted)
-    A64 = A32.double()
-    x_ls = torch.linalg.lstsq(A64, b.double().unsqueeze(1)).solution.squeeze(1)
-    del A64
+    x_ls = ls_solution_rows(torch, A32, b, world)
     fe_p = float(torch.linalg.norm(d_exact * (xp.double() - x_ls)) / torch.linalg.norm(d_exact * x_ls))
     fe_f = float(torch.linalg.norm(d_exact * (xf.double() - x_ls)) / torch.linalg.norm(d_exact * x_ls))
     torch.cuda.empty_cache()
@@ -331,10 +414,12 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_packed,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"dense row-major {m}x{n} G diag(10^U(-3,3)), sketch s={s}, "
+            "config": {"workload": f"dense row-major {m * world}x{n} G diag(10^U(-3,3)), sketch s={s}, "
                                    "FP32_16 packed storage, eta<=1e-6",
-                       "m": m, "n": n, "s": s, "storage": "fp32_16 (half tier + exact refinement)",
-                       "parallelism": "replicas" if world > 1 else "1 GPU",
+                       "m": m * world, "m_per_gpu": m, "n": n, "s": s,
+                       "storage": "fp32_16 (half tier + exact refinement)",
+                       "parallelism": (f"row-sharded over {world} GPUs (NCCL all-reduce of n+1 doubles "
+                                       "per pass)") if world > 1 else "1 GPU",
                        "l2": "inputs (4 GB) larger than L2 (126 MB)"},
             "fp32_ms": ms_fp32, "speedup_vs_fp32": ms_fp32 / ms_packed,
             "iterations": {"packed": rep_p["iterations"], "fp32": rep_f["iterations"],
@@ -367,6 +452,7 @@ def run_ours(args):
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
+        gpu_solve.comm.close()
         dist.destroy_process_group()
 
 

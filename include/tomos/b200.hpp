@@ -296,11 +296,10 @@ inline void lsqr_solve(Context ctx, Sparse& A, Dense& b, Dense& x, Workspace& ws
                        std::vector<double>* residual_history = nullptr, int restarts = 1,
                        Sparse* mtx_refine_precision = nullptr) {
     (void)ctx;
-    if (mtx_refine_precision)
-        throw std::runtime_error("lsqr_solve: explicit refine duplicates are not registered");
     std::vector<double> buf;
     tomos_lsqr_opts o = b200_detail::opts_for(ws, A.get_value_type(), tol, max_iters, max_relres,
                                               restarts, residual_history, buf);
+    if (mtx_refine_precision) o.refine_csr = &mtx_refine_precision->desc();
     b200_detail::check(tomos_lsqr_solve_csr(&A.desc(), static_cast<const float*>(b.data()),
                                             static_cast<float*>(x.data()), ws.handle(), &o,
                                             &ws.last_report, nullptr),

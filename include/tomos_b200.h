@@ -52,7 +52,12 @@ enum tomos_trans { TOMOS_NO_TRANSPOSE = 0, TOMOS_TRANSPOSE = 1 };
  *   AUTO     -- the reference's default rule (blas.cpp:33-53): HALF for
  *               packed A, NATIVE otherwise. */
 enum tomos_tier { TOMOS_TIER_AUTO = 0, TOMOS_TIER_NATIVE = 1, TOMOS_TIER_HALF = 2,
-                  TOMOS_TIER_ACCURATE = 3 };
+                  TOMOS_TIER_ACCURATE = 3,
+                  /* tomos_mm only: A's 16-bit values (HALF tier, or native
+                     FP16) times B rounded to the same 16-bit type -- the
+                     operands of the reference's pure_half GEMM tier
+                     (fp32_16_kernels.cpp:172-203), FP32 accumulation */
+                  TOMOS_TIER_HALF_OPERANDS = 4 };
 
 /* A strided dense matrix in device memory (non-owning; the reference's
  * StridedView, include/core/matrix.hpp:167-177).  For the packed types
@@ -163,6 +168,27 @@ tomos_status tomos_gemv_no_alloc(int32_t trans, double alpha, const tomos_dense*
                                  int32_t tier, const float* x, double beta, float* y,
                                  void* stream);
 
+/* ------------------------------------------------------------------ GEMM */
+
+/* C = alpha * op(A) op(B) + beta * C, the reference's mm_apply for a dense
+ * A (src/core/blas/blas.cpp:98-106 through dispatch::Dense::lookup_mm,
+ * dense_registries.cpp:396-405) and its FP32_16 tiers (blas.cpp:168-190,
+ * fp32_16_registries.cpp:371-455).  A: FP32, FP16 or packed storage, any
+ * layout; B and C: FP32, any layout (the reference's are column-major).
+ * Runs on the tcgen05 tensor cores with FP32 accumulation:
+ *   HALF_OPERANDS  16-bit A values x B rounded to 16 bits (pure_half
+ *                  operands), one fp16/bf16 product;
+ *   HALF / AUTO    16-bit A values x B kept to ~22 bits (the "fast" tier),
+ *                  two TF32 products;
+ *   ACCURATE / NATIVE (FP32 A)  A and B both kept to ~22 bits (the accurate
+ *                  tier), three TF32 products.
+ * An entry's error is a few units of 2^-22 times sum_l |op(A)_il op(B)_lj|
+ * plus the FP32 summation over K.  beta == 0 never reads C.  Allocates
+ * nothing; asynchronous on `stream`. */
+tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A,
+                      int32_t tier, const tomos_dense* B, double beta, tomos_dense* C,
+                      void* stream);
+
 /* CSR y = alpha * op(A) x + beta * y (cuda::mv_csr, mv_cuda_kernels.cu:
  * 2029-2058; dispatch::Sparse::lookup_mv).  FP32, FP64 and packed values.
  * The transposed product is deterministic (no atomics). */
@@ -227,6 +253,20 @@ tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64
  * |phi_bar| / ||b|| only, lsqr.cpp:418-425). */
 tomos_status tomos_column_scale(const double* colsq, int64_t n, double* d, double* anorm,
                                 void* stream);
+
+/* Row-sharded CountSketch: as tomos_countsketch_apply, for a row shard of
+ * the whole problem whose row i is row row0 + i of the whole A (the hash
+ * takes that index, so the shards' SA summed over ranks -- e.g. with
+ * tomos_comm_allreduce_f64 -- is the whole problem's SA bit for bit up to
+ * the summation order of the ranks).  plane (may be NULL): the staged fp16
+ * copy of a row-major FP32_16 shard's wh plane, as
+ * tomos_countsketch_apply_stage.  No reference counterpart (the reference
+ * runs on one GPU). */
+tomos_status tomos_countsketch_apply_shard(const tomos_dense* A, int32_t tier, int64_t s,
+                                           uint64_t bucket_seed, uint64_t sign_seed, int64_t row0,
+                                           double* SA, int64_t ld_sa, double* fro2, double* colsq,
+                                           void* plane, int64_t ld_plane, void* scratch,
+                                           size_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------- sketch QR */
 
@@ -304,6 +344,8 @@ typedef struct tomos_lsqr_opts {
                                 restart passes read instead of A; it takes
                                 precedence over implicit_duplicate
                                 (lsqr.cpp:459-473)                          */
+    struct tomos_comm* comm; /* may be NULL: the ranks of a row-sharded solve
+                                (A, b this rank's rows; x replicated)        */
     double inner_eta_factor; /* BACKWARD rule: an inner cycle also ends once
                                 its estimate |phi_bar| / (||A|| ||x|| + ||b||)
                                 is below tol times this (0 = 1).  Below 1 with
@@ -312,6 +354,14 @@ typedef struct tomos_lsqr_opts {
                                 perturbation, so that the cycle's exact
                                 residual meets tol and no further cycle
                                 (and exact pass) is needed.                  */
+    const struct tomos_csr* refine_csr; /* may be NULL: the CSR solve's
+                                mtx_refine_precision (lsqr_sparse_impl,
+                                lsqr_registries.cpp:164-183): a copy of a
+                                CSR A at higher precision (FP32 values, or
+                                packed read exactly) that the initial and
+                                restart passes read instead of A.  A dense
+                                solve rejects it, and a CSR solve rejects
+                                `refine`.                                    */
 } tomos_lsqr_opts;
 
 typedef struct tomos_lsqr_report {
@@ -342,6 +392,25 @@ typedef struct tomos_lsqr_report {
 } tomos_lsqr_report;
 
 typedef struct tomos_workspace tomos_workspace;
+
+/* ------------------------------------------------------- multi-GPU solves */
+
+/* A communicator over the ranks of a row-sharded solve (one process per
+ * GPU; NCCL over NVLink / NVSwitch).  Rank 0 makes an id
+ * (tomos_comm_unique_id), every rank receives it by its own means (a
+ * torch.distributed broadcast, MPI, a file) and calls tomos_comm_create with
+ * its device current.  Passed as tomos_lsqr_opts.comm, the solve treats A
+ * and b as rank's row shard of one problem and x as the whole solution
+ * (replicated): after every pass over A the n + 1 partial sums (A^T u and
+ * ||u||^2) are summed across ranks, once.  No reference counterpart (the
+ * reference runs on one GPU; lsqr.cpp:561-621 are the products split). */
+#define TOMOS_COMM_ID_BYTES 128
+typedef struct tomos_comm tomos_comm;
+tomos_status tomos_comm_unique_id(void* id /* TOMOS_COMM_ID_BYTES */);
+tomos_status tomos_comm_create(int32_t nranks, int32_t rank, const void* id, tomos_comm** out);
+tomos_status tomos_comm_destroy(tomos_comm* comm);
+/* buf (device, count doubles) <- its sum over the ranks, on stream. */
+tomos_status tomos_comm_allreduce_f64(tomos_comm* comm, double* buf, int64_t count, void* stream);
 
 /* create_lsqr_workspace (src/core/solver/lsqr.cpp:389-406,
  * include/core/solver.hpp:15-25): owns the device arena for the m- and

@@ -163,3 +163,105 @@ def test_csr_ragged_lsqr_iterations(orc, numeric, tier):
     assert np.linalg.norm(xx - x_ref) / np.linalg.norm(x_ref) < 1e-4
     assert np.all(xx[n - 7:] == 0.0)
     assert torch.equal(xs[0], xs[1])
+
+
+# ------------------------------------------------- FP16 values, explicit duplicates
+
+def make_fp16(rp, ci, v, m, n):
+    """A CSR of native IEEE fp16 values (the reference's __half Sparse)."""
+    return tb.Csr(NT.FP16, (m, n), cuda(rp, torch.int32), cuda(ci, torch.int32), cuda(v, torch.float16))
+
+
+def fp16_values_dense(ci, v, m, n):
+    D = np.zeros((m, n))
+    np.put_along_axis(D, ci.reshape(m, -1).astype(np.int64),
+                      v.astype(np.float16).astype(np.float64).reshape(m, -1), axis=1)
+    return D
+
+
+def test_csr_fp16_gemv():
+    """Both products over fp16 CSR values against the FP64 product of the
+    fp16 values (FP32 accumulation)."""
+    m, n = 3001, 517
+    rp, ci, v, _ = random_csr(m, n, 9, 21)
+    A = make_fp16(rp, ci, v, m, n)
+    Dd = fp16_values_dense(ci, v, m, n)
+    rng = np.random.default_rng(22)
+    for trans, M in ((tb.NO_TRANSPOSE, Dd), (tb.TRANSPOSE, Dd.T)):
+        x = rng.standard_normal(M.shape[1]).astype(np.float32)
+        y0 = rng.standard_normal(M.shape[0]).astype(np.float32)
+        y = cuda(y0)
+        tb.mv_apply(tb.Device.CUDA, trans, 1.5, A, cuda(x), 0.5, y)
+        ref = 1.5 * (M @ x) + 0.5 * y0
+        scale = 1.5 * (np.abs(M) @ np.abs(x)) + 0.5 * np.abs(y0)
+        assert np.all(np.abs(y.cpu().numpy() - ref) <= 2e-5 * scale + 1e-30)
+
+
+def test_csr_explicit_duplicates_backward_error(orc):
+    """lsqr_solve(Sparse&, ..., mtx_refine_precision): fp16 iterations (the
+    CSC gathers) with the FP32 CSR duplicate for the initial and restart
+    passes reach backward error 1e-6 of the column-scaled FP32 problem,
+    checked in FP64 on the FP32 values."""
+    m, n = 20000, 300
+    rp, ci, v, D = random_csr(m, n, 20, 23, decades=2.0)
+    rng = np.random.default_rng(24)
+    b = (D.astype(np.float64) @ rng.standard_normal(n) + 1e-8 * rng.standard_normal(m)).astype(np.float32)
+    A32 = make(rp, ci, v, m, n)
+    A16 = make_fp16(rp, ci, v, m, n)
+    SA, _, colsq = tb.apply_count_sketch(A32, 4 * n, with_colsq=True)
+    Rinv = tb.generate_sketch_qr_precond(SA)
+    d, an = tb.column_scale(colsq)
+    ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32, NT.FP64)
+    tb.add_precond(Rinv, ws)
+    xd = torch.zeros(n, device="cuda")
+    rep = tb.lsqr_solve(None, A16, cuda(b), xd, ws, 1e-6, 100, 0.0, restarts=6,
+                        stop_rule=tb.StopRule.BACKWARD, inner_rtol=1e-3, col_scale=d, anorm_fro=an,
+                        mtx_refine_precision=A32)
+    x = xd.cpu().numpy()
+    eta = orc.backward_error_scaled(D, b, x)
+    assert rep["converged"] == 1 and rep["restarts_used"] >= 2, rep
+    assert eta <= 1.05e-6, (eta, rep)
+    assert abs(rep["backward_error"] - eta) <= 0.05 * eta + 1e-9  # measured on the FP32 copy
+    xs = orc.lstsq_f64(D.astype(np.float64), b.astype(np.float64))
+    dn = np.sqrt((D.astype(np.float64) ** 2).sum(0))
+    assert np.linalg.norm(dn * (x - xs)) / np.linalg.norm(dn * xs) < 1e-4
+
+
+def test_csr_explicit_duplicates_relres_restarts(orc):
+    """Under the reference's RELRES rule the restart residual b - A_refine x
+    drives x to the FP32 system's least-squares solution; fp16 iterations
+    alone stop far from it."""
+    m, n = 20000, 200
+    rp, ci, v, D = random_csr(m, n, 16, 25, decades=0.0)
+    rng = np.random.default_rng(26)
+    b = (D.astype(np.float64) @ rng.standard_normal(n)).astype(np.float32)
+    A32 = make(rp, ci, v, m, n)
+    A16 = make_fp16(rp, ci, v, m, n)
+    xs = orc.lstsq_f64(D.astype(np.float64), b.astype(np.float64))
+    err = {}
+    for dup in (False, True):
+        ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32)
+        x = torch.zeros(n, device="cuda")
+        tb.lsqr_solve(None, A16, cuda(b), x, ws, 1e-7, 60, 1e-7, restarts=5,
+                      mtx_refine_precision=A32 if dup else None)
+        err[dup] = np.linalg.norm(x.cpu().numpy() - xs) / np.linalg.norm(xs)
+    assert err[True] < 1e-5, err
+    assert err[False] > 10 * err[True], err
+
+
+def test_csr_explicit_duplicates_errors():
+    m, n = 100, 10
+    rp, ci, v, _ = random_csr(m, n, 3, 27)
+    A16 = make_fp16(rp, ci, v, m, n)
+    ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32)
+    x = torch.zeros(n, device="cuda")
+    b = torch.ones(m, device="cuda")
+    rp2, ci2, v2, _ = random_csr(m, n - 1, 3, 28)
+    with pytest.raises(tb.TomosError) as e:  # another size
+        tb.lsqr_solve(None, A16, b, x, ws, 1e-6, 10, 1e-6, mtx_refine_precision=make(rp2, ci2, v2, m, n - 1))
+    assert "size" in str(e.value)
+    dense = tb.Dense.from_tensor(torch.ones((m, n), device="cuda"), tb.Layout.ROW_MAJOR)
+    with pytest.raises(tb.TomosError):  # a dense copy beside a CSR A
+        tb.lsqr_solve(None, A16, b, x, ws, 1e-6, 10, 1e-6, mtx_refine_precision=dense)
+    with pytest.raises(tb.TomosError):  # a CSR copy beside a dense A
+        tb.lsqr_solve(None, dense, b, x, ws, 1e-6, 10, 1e-6, mtx_refine_precision=make(rp, ci, v, m, n))

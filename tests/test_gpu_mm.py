@@ -1,0 +1,137 @@
+"""mm_apply on the tcgen05 tensor cores (tomos_mm) against FP64 products of
+the operand values each tier reads: FP32, native FP16 and packed A, every
+transpose and layout of A, B and C, ragged sizes (M, N, K not multiples of
+the 128 x BN x K-stage tiles), beta = 0 (C never read) and beta != 0, K = 0.
+
+Tolerances, per entry, relative to S = sum_l |op(A)_il| |op(B)_lj|:
+  HALF_OPERANDS  the exact product of the 16-bit operands (B rounded to
+                 fp16 / bf16 first) to 1e-5 S (FP32 accumulation);
+  HALF           A's 16-bit values times B to 1e-5 S (B split in two TF32
+                 parts, ~2^-22);
+  ACCURATE / FP32  the exact values to 1e-5 S (A and B split, ~2^-21)."""
+import numpy as np
+import pytest
+import torch
+
+import tomos_b200 as tb
+from gpu_util import to_dense, decoded
+
+pytestmark = pytest.mark.gpu
+NT = tb.NumericType
+L = tb.Layout
+T = tb.TransposeType
+
+
+def dense_f32(M, layout, pad=0):
+    return to_dense(np.ascontiguousarray(M, np.float32), layout, pad=pad)
+
+
+def values(D):
+    return D.view().double().cpu().numpy()
+
+
+def check(orc, A, A0, tier, ta, tb_, shape_b, layouts, beta, rng, bf16_ops=False):
+    """One product against FP64; returns the max error / bound ratio."""
+    lb, lc = layouts
+    if A.numeric == NT.FP32:
+        Av = A0.astype(np.float64)
+    elif A.numeric == NT.FP16:
+        Av = A.view().double().cpu().numpy()
+    else:
+        Av = decoded(orc, A, tb.Tier.HALF if tier in (tb.Tier.HALF, tb.Tier.HALF_OPERANDS) else tier)
+    opA = Av.T if ta == T.TRANSPOSE else Av
+    M, K = opA.shape
+    B0 = rng.standard_normal(shape_b).astype(np.float32)
+    B = dense_f32(B0, lb, pad=3 if beta else 0)  # strided and aligned B
+    Bv = B0.astype(np.float64)
+    if tier == tb.Tier.HALF_OPERANDS:
+        Bv = (torch.from_numpy(B0).to(torch.bfloat16 if bf16_ops else torch.float16)).double().numpy()
+    opB = Bv.T if tb_ == T.TRANSPOSE else Bv
+    assert opB.shape[0] == K
+    N = opB.shape[1]
+    C0 = rng.standard_normal((M, N)).astype(np.float32)
+    Cd = dense_f32(C0 if beta else np.full((M, N), np.nan, np.float32), lc, pad=1)
+    tb.mm_apply(tb.Device.CUDA, ta, tb_, 1.25, A, B, beta, Cd, tier=tier)
+    got = values(Cd)
+    ref = 1.25 * (opA @ opB) + (beta * C0.astype(np.float64) if beta else 0.0)
+    S = 1.25 * (np.abs(opA) @ np.abs(opB)) + (abs(beta) * np.abs(C0) if beta else 0.0)
+    err = np.abs(got - ref)
+    bound = 1e-5 * S + 1e-30
+    assert np.all(np.isfinite(got))
+    assert np.all(err <= bound), float((err / bound).max())
+    return float((err / bound).max())
+
+
+SHAPES = [(300, 17, 129), (1000, 130, 500), (128, 16, 64), (257, 1, 33), (77, 200, 1000), (5, 3, 2)]
+
+
+@pytest.mark.parametrize("M,N,K", SHAPES)
+@pytest.mark.parametrize("ta", [T.NO_TRANSPOSE, T.TRANSPOSE])
+@pytest.mark.parametrize("tb_", [T.NO_TRANSPOSE, T.TRANSPOSE])
+def test_mm_fp32(M, N, K, ta, tb_):
+    """FP32 A (the accurate TF32x3 products), column- and row-major."""
+    rng = np.random.default_rng(M * 7 + N + K)
+    A0 = (rng.standard_normal((M, K) if ta == T.NO_TRANSPOSE else (K, M)) *
+          10.0 ** rng.uniform(-2, 2, (1, K if ta == T.NO_TRANSPOSE else M))).astype(np.float32)
+    for la, lb, lc in ((L.COL_MAJOR, L.COL_MAJOR, L.COL_MAJOR), (L.ROW_MAJOR, L.ROW_MAJOR, L.ROW_MAJOR),
+                       (L.ROW_MAJOR, L.COL_MAJOR, L.ROW_MAJOR)):
+        A = dense_f32(A0, la, pad=2)
+        shape_b = (K, N) if tb_ == T.NO_TRANSPOSE else (N, K)
+        for beta in (0.0, -0.5):
+            check(None, A, A0, tb.Tier.AUTO, ta, tb_, shape_b, (lb, lc), beta, rng)
+
+
+@pytest.mark.parametrize("numeric", [NT.FP32_16, NT.FP32_BF16])
+@pytest.mark.parametrize("tier", [tb.Tier.ACCURATE, tb.Tier.HALF, tb.Tier.HALF_OPERANDS])
+@pytest.mark.parametrize("layout", [L.COL_MAJOR, L.ROW_MAJOR])
+@pytest.mark.parametrize("ta", [T.NO_TRANSPOSE, T.TRANSPOSE])
+def test_mm_packed(orc, numeric, tier, layout, ta):
+    """Packed A at each tier (values outside fp16 range included for the
+    exact tiers' control words)."""
+    M, N, K = 600, 70, 333
+    rng = np.random.default_rng(int(numeric) * 10 + int(tier))
+    shape_a = (M, K) if ta == T.NO_TRANSPOSE else (K, M)
+    A0 = (rng.standard_normal(shape_a) * np.where(rng.random(shape_a) < 0.02, 1e-6, 1.0)).astype(np.float32)
+    A = to_dense(A0, layout, numeric, pad=8)
+    for tb_ in (T.NO_TRANSPOSE, T.TRANSPOSE):
+        shape_b = (K, N) if tb_ == T.NO_TRANSPOSE else (N, K)
+        check(orc, A, A0, tier, ta, tb_, shape_b, (L.COL_MAJOR, L.COL_MAJOR), 0.5, rng,
+              bf16_ops=numeric == NT.FP32_BF16)
+
+
+@pytest.mark.parametrize("tier", [tb.Tier.AUTO, tb.Tier.HALF_OPERANDS])
+def test_mm_fp16(tier):
+    rng = np.random.default_rng(9)
+    A0 = rng.standard_normal((513, 250)).astype(np.float32)
+    A = to_dense(A0, L.ROW_MAJOR, NT.FP16, pad=6)
+    check(None, A, A0, tier, T.NO_TRANSPOSE, T.NO_TRANSPOSE, (250, 40), (L.COL_MAJOR, L.COL_MAJOR), 0.0, rng)
+
+
+def test_mm_reference_routing_and_errors(orc):
+    """mm_apply's default for packed A is the accurate tier (the reference's
+    mm_apply routing), use_workspace gives the same values; K = 0 scales C;
+    wrong shapes and FP32 A at HALF_OPERANDS are refused."""
+    rng = np.random.default_rng(3)
+    A0 = rng.standard_normal((200, 64)).astype(np.float32)
+    A = to_dense(A0, L.COL_MAJOR, NT.FP32_16)
+    B = dense_f32(rng.standard_normal((64, 20)), L.COL_MAJOR)
+    C1 = dense_f32(np.zeros((200, 20)), L.COL_MAJOR)
+    C2 = dense_f32(np.zeros((200, 20)), L.COL_MAJOR)
+    C3 = dense_f32(np.zeros((200, 20)), L.COL_MAJOR)
+    tb.mm_apply(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, A, B, 0.0, C1)
+    tb.mm_apply(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, A, B, 0.0, C2, use_workspace=True)
+    tb.mm_apply_fp32_16_ext(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, A, B, 0.0, C3)
+    assert torch.equal(C1.view(), C2.view()) and torch.equal(C1.view(), C3.view())
+    # K = 0
+    Z = dense_f32(np.zeros((200, 0)), L.COL_MAJOR)
+    Bz = dense_f32(np.zeros((0, 20)), L.COL_MAJOR, pad=1)
+    C0 = rng.standard_normal((200, 20)).astype(np.float32)
+    Cz = dense_f32(C0, L.COL_MAJOR)
+    tb.mm_apply(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, Z, Bz, 2.0, Cz)
+    np.testing.assert_array_equal(Cz.view().cpu().numpy(), (2.0 * C0.astype(np.float64)).astype(np.float32))
+    with pytest.raises(tb.TomosError):
+        tb.mm_apply(tb.Device.CUDA, T.TRANSPOSE, T.NO_TRANSPOSE, 1.0, A, B, 0.0, C1)
+    A32 = dense_f32(A0, L.COL_MAJOR)
+    with pytest.raises(tb.TomosError):
+        tb.mm_apply(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, A32, B, 0.0, C1,
+                    tier=tb.Tier.HALF_OPERANDS)

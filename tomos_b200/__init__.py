@@ -23,7 +23,7 @@ __all__ = [
     "split_fp32_16", "combine_fp32_16", "split_fp32_bf16", "combine_fp32_bf16",
     "countsketch_hash", "apply_count_sketch", "generate_sketch_qr_precond", "backward_error",
     "column_scale", "mtx_info", "read_mtx", "read_mtx_coo", "read_mtx_csr", "write_mtx",
-    "dense_from_mtx", "csr_from_mtx",
+    "dense_from_mtx", "csr_from_mtx", "sketch_lsqr", "shard_rows", "Comm", "apply_count_sketch_shard",
     "TomosError", "CS_BUCKET_SEED", "CS_SIGN_SEED", "NO_TRANSPOSE", "TRANSPOSE",
 ]
 
@@ -63,6 +63,7 @@ class Tier(enum.IntEnum):
     NATIVE = 1
     HALF = 2
     ACCURATE = 3
+    HALF_OPERANDS = 4  # mm only: 16-bit A and B operands (the pure_half tier)
 
 
 class StopRule(enum.IntEnum):
@@ -464,6 +465,42 @@ def mv_apply(dev, transpose, alpha, A, x, beta, y, compute_type=None, tier=None,
     return 0
 
 
+def mm_apply(dev, transA, transB, alpha, A, B, beta, Cm, use_workspace=False, tier=None, stream=None):
+    """C = alpha * op(A) op(B) + beta * C (include/core/blas.hpp:123-125,
+    src/core/blas/blas.cpp:98-106) on the tcgen05 tensor cores.  A: a Dense
+    (FP32, FP16 or packed); B, C (Cm): FP32 Dense.  Packed A is read
+    exactly, as the reference's mm_apply routes it (dense_registries.cpp:
+    396-405: the accurate tier, or its decode-into-scratch "workspace"
+    variant, which yields the same exact values; use_workspace therefore
+    changes nothing here).  `tier` overrides: Tier.HALF is the fast tier,
+    Tier.HALF_OPERANDS the pure_half operands."""
+    if Device(dev) != Device.CUDA:
+        raise ValueError("mm_apply: Device.CUDA only")
+    if tier is None:
+        tier = Tier.ACCURATE if A.numeric in PACKED else Tier.AUTO
+    da, db, dc = A.desc(), B.desc(), Cm.desc()
+    C.check(C.lib().tomos_mm(int(transA), int(transB), float(alpha), ctypes.byref(da), int(tier),
+                             ctypes.byref(db), float(beta), ctypes.byref(dc), _stream(stream)),
+            "mm_apply")
+    return 0
+
+
+def mm_apply_fp32_16_pure_half(dev, transA, transB, alpha, A, B, beta, Cm, stream=None):
+    """blas.hpp:185-187: 16-bit A values and B rounded to fp16 (bf16 for
+    FP32_BF16 storage), FP32 accumulation."""
+    return mm_apply(dev, transA, transB, alpha, A, B, beta, Cm, tier=Tier.HALF_OPERANDS, stream=stream)
+
+
+def mm_apply_fp32_16_fast(dev, transA, transB, alpha, A, B, beta, Cm, stream=None):
+    """blas.hpp:189-191: 16-bit A values, B to ~22 bits, FP32 accumulation."""
+    return mm_apply(dev, transA, transB, alpha, A, B, beta, Cm, tier=Tier.HALF, stream=stream)
+
+
+def mm_apply_fp32_16_ext(dev, transA, transB, alpha, A, B, beta, Cm, stream=None):
+    """blas.hpp:193-195: A exact (wh + wr), products to ~22 bits."""
+    return mm_apply(dev, transA, transB, alpha, A, B, beta, Cm, tier=Tier.ACCURATE, stream=stream)
+
+
 # ------------------------------------------------------------------ sketch
 
 def countsketch_hash(m, s, bucket_seed=CS_BUCKET_SEED, sign_seed=CS_SIGN_SEED, stream=None):
@@ -600,15 +637,17 @@ def add_precond(precond, workspace):
 def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=None,
                residual_history=None, restarts=1, stop_rule=StopRule.RELRES, inner_rtol=0.0,
                anorm_fro=0.0, warm_start=False, tier=None, profile=False, col_scale=None,
-               staged_plane=None, mtx_refine_precision=None, inner_eta_factor=0.0, stream=None):
+               staged_plane=None, mtx_refine_precision=None, inner_eta_factor=0.0, comm=None,
+               stream=None):
     """include/core/solver.hpp:68-78.  A: Dense or Csr on the device; b, x:
     FP32 Dense column vectors or float32 CUDA tensors.  iterations and
     residual_history, when lists, receive the reference's out-parameters.
     staged_plane: the (m x ld) int16 tensor apply_count_sketch(..., stage=True)
     filled for this A (HALF-tier iterations then skip their staging pass).
-    mtx_refine_precision: a Dense copy of A at higher precision (FP32, or
-    packed read exactly) for the initial and restart passes, e.g. beside an
-    FP16 A (the reference's --explicit-duplicates).
+    mtx_refine_precision: a copy of A at higher precision (FP32, or packed
+    read exactly; a Dense beside a Dense A, a Csr beside a Csr A) for the
+    initial and restart passes, e.g. beside an FP16 A (the reference's
+    --explicit-duplicates).
     Returns the solver report as a dict."""
     opts = C.LsqrOpts()
     opts.tol = float(tol)
@@ -626,6 +665,7 @@ def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=N
     opts.warm_start = 1 if warm_start else 0
     opts.inner_rtol = float(inner_rtol)
     opts.inner_eta_factor = float(inner_eta_factor)
+    opts.comm = comm.handle if comm is not None else None
     if isinstance(anorm_fro, torch.Tensor):  # a device value (column_scale)
         opts.anorm_fro_dev = anorm_fro.data_ptr()
         opts.anorm_fro = 0.0
@@ -634,7 +674,10 @@ def lsqr_solve(ctx, A, b, x, workspace, tol, max_iters, max_relres, iterations=N
     refine_desc = None
     if mtx_refine_precision is not None:
         refine_desc = mtx_refine_precision.desc()
-        opts.refine = ctypes.addressof(refine_desc)
+        if isinstance(mtx_refine_precision, Csr):
+            opts.refine_csr = ctypes.addressof(refine_desc)
+        else:
+            opts.refine = ctypes.addressof(refine_desc)
     opts.profile = 1 if profile else 0
     opts.col_scale = col_scale.data_ptr() if col_scale is not None else None
     if staged_plane is not None:
@@ -722,7 +765,7 @@ def column_scale(colsq, stream=None):
 
 
 def sketch_lsqr(A, b, s, tol=1e-6, max_iters=200, restarts=8, inner_rtol=None, workspace=None,
-                x=None, profile=False, events=None, stream=None):
+                x=None, profile=False, events=None, comm=None, row0=0, stream=None):
     """The sketch-preconditioned LSQR pipeline of the reference's runner
     (lsqr_precision_runner.cu:588-656: sketch, generate_sketch_qr_precond,
     add_precond, lsqr_solve) with the BACKWARD stopping rule on the
@@ -738,14 +781,27 @@ def sketch_lsqr(A, b, s, tol=1e-6, max_iters=200, restarts=8, inner_rtol=None, w
     reuse (created when None).  inner_rtol: the refinement cycles' residual
     reduction (default 2e-3 for packed storage, none for FP32).  events:
     four torch.cuda.Event recorded at the start, after the sketch, after
-    the QR and after the solve (phase timing)."""
+    the QR and after the solve (phase timing).  comm (a Comm): A and b are
+    this rank's rows of one problem, starting at row row0 of it; the
+    sketches are summed over the ranks (one all-reduce of SA and the column
+    sums), the QR is repeated on every rank, and the solve sums its
+    per-pass partials over the ranks (x, returned on every rank, is the
+    whole solution)."""
     m, n = A.size
     packed = A.numeric in PACKED
     plane = None
     if events:
         events[0].record()
-    if (isinstance(A, Dense) and A.numeric == NumericType.FP32_16 and A.layout == Layout.ROW_MAJOR
-            and (A.ld * 2) % 16 == 0):
+    stage = (isinstance(A, Dense) and A.numeric == NumericType.FP32_16 and A.layout == Layout.ROW_MAJOR
+             and (A.ld * 2) % 16 == 0)
+    if comm is not None:
+        if not isinstance(A, Dense):
+            raise TomosError(C.TOMOS_ERR_UNSUPPORTED, "sketch_lsqr: sharded solves take a Dense A")
+        SA, _, colsq, plane = apply_count_sketch_shard(A, s, row0, tier=Tier.HALF if packed else Tier.AUTO,
+                                                       stage=stage, stream=stream)
+        comm.allreduce_f64(SA.storage, stream=stream)
+        comm.allreduce_f64(colsq, stream=stream)
+    elif stage:
         SA, _, colsq, plane = apply_count_sketch(A, s, tier=Tier.HALF, with_colsq=True, stage=True,
                                                  stream=stream)
     else:
@@ -767,7 +823,99 @@ def sketch_lsqr(A, b, s, tol=1e-6, max_iters=200, restarts=8, inner_rtol=None, w
         inner_rtol = 2e-3 if packed else 0.0
     rep = lsqr_solve(None, A, b, x, ws, tol, max_iters, 0.0, restarts=restarts,
                      stop_rule=StopRule.BACKWARD, inner_rtol=inner_rtol, anorm_fro=anorm,
-                     col_scale=d, staged_plane=plane, profile=profile, stream=stream)
+                     col_scale=d, staged_plane=plane, profile=profile, comm=comm, stream=stream)
     if events:
         events[3].record()
     return x, rep, d
+
+
+# ------------------------------------------------------------------ row-sharded solves
+
+def shard_rows(m, rank, world):
+    """Rows [r0, r1) of an m-row problem that rank `rank` of `world` holds:
+    contiguous blocks, the first m % world ranks one row longer."""
+    base, extra = divmod(int(m), int(world))
+    r0 = rank * base + min(rank, extra)
+    return r0, r0 + base + (1 if rank < extra else 0)
+
+
+class Comm:
+    """The ranks of a row-sharded solve (tomos_comm_create; NCCL over
+    NVLink / NVSwitch).  Comm(group) takes the ranks of a torch.distributed
+    process group (rank 0's id reaches the others by a broadcast over the
+    group); Comm.single() is a one-rank communicator."""
+
+    @staticmethod
+    def exchange_id(group=None):
+        """Rank 0's communicator id (tomos_comm_unique_id), broadcast over the
+        process group; returns (id bytes, rank, world size)."""
+        import torch.distributed as dist
+        rank, world = dist.get_rank(group), dist.get_world_size(group)
+        idbuf = (ctypes.c_char * 128)()
+        if rank == 0:
+            C.check(C.lib().tomos_comm_unique_id(idbuf), "comm_unique_id")
+        obj = [bytes(idbuf) if rank == 0 else None]
+        src = 0 if group is None else dist.get_global_rank(group, 0)
+        dist.broadcast_object_list(obj, src=src, group=group)
+        return obj[0], rank, world
+
+    def __init__(self, group=None, _single=False):
+        if _single:
+            rank, world = 0, 1
+            idbuf = (ctypes.c_char * 128)()
+            C.check(C.lib().tomos_comm_unique_id(idbuf), "comm_unique_id")
+        else:
+            idb, rank, world = Comm.exchange_id(group)
+            idbuf = (ctypes.c_char * 128).from_buffer_copy(idb)
+        h = ctypes.c_void_p()
+        C.check(C.lib().tomos_comm_create(world, rank, idbuf, ctypes.byref(h)), "comm_create")
+        self._h = h
+        self.rank, self.size = rank, world
+
+    @classmethod
+    def single(cls):
+        return cls(_single=True)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def allreduce_f64(self, t, stream=None):
+        """Sum a float64 CUDA tensor across the ranks, in place."""
+        C.check(C.lib().tomos_comm_allreduce_f64(self._h, _ptr(t), t.numel(), _stream(stream)),
+                "comm_allreduce_f64")
+        return t
+
+    def close(self):
+        if self._h:
+            C.lib().tomos_comm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def apply_count_sketch_shard(A, s, row0, tier=Tier.AUTO, bucket_seed=CS_BUCKET_SEED,
+                             sign_seed=CS_SIGN_SEED, stage=False, stream=None):
+    """The CountSketch of a row shard whose row i is row row0 + i of the
+    whole problem (tomos_countsketch_apply_shard): returns (SA, fro2, colsq,
+    plane or None); summed over the ranks they are the whole problem's."""
+    m, n = A.size
+    plane = None
+    if stage:
+        ldp = (n + 7) // 8 * 8
+        plane = torch.empty((max(m, 1), ldp), dtype=torch.int16, device="cuda")
+    SA = Dense._empty_f64(Layout.COL_MAJOR, (s, n))
+    fro2 = torch.empty(1, dtype=torch.float64, device="cuda")
+    colsq = torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
+    nb = C.lib().tomos_countsketch_scratch_bytes(m, n, s)
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
+    d = A.desc()
+    C.check(C.lib().tomos_countsketch_apply_shard(
+        ctypes.byref(d), int(tier), s, bucket_seed, sign_seed, int(row0), _ptr(SA.storage), s, _ptr(fro2),
+        _ptr(colsq), _ptr(plane), plane.stride(0) if plane is not None else 0, _ptr(scratch), nb,
+        _stream(stream)), "apply_count_sketch_shard")
+    return SA, fro2, colsq[:n], plane

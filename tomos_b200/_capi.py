@@ -47,7 +47,7 @@ class LsqrOpts(ctypes.Structure):
                 ("anorm_fro", c_dbl), ("col_scale", c_vp), ("history", ctypes.POINTER(c_dbl)),
                 ("history_cap", c_i32), ("profile", c_i32), ("staged_plane", c_vp),
                 ("staged_ld", c_i64), ("anorm_fro_dev", c_vp), ("refine", c_vp),
-                ("inner_eta_factor", c_dbl)]
+                ("comm", c_vp), ("inner_eta_factor", c_dbl), ("refine_csr", c_vp)]
 
 
 class LsqrReport(ctypes.Structure):
@@ -89,6 +89,8 @@ SIGNATURES = {
     "tomos_unpack_fp32_bf16": (c_i32, [c_vp, c_vp, c_i32, c_i64, c_i64, c_i64, c_vp, c_i64,
                                        c_i32, c_vp]),
     "tomos_gemv_scratch_bytes": (c_sz, [ctypes.POINTER(DenseDesc), c_i32]),
+    "tomos_mm": (c_i32, [c_i32, c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32,
+                         ctypes.POINTER(DenseDesc), c_dbl, ctypes.POINTER(DenseDesc), c_vp]),
     "tomos_gemv": (c_i32, [c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32, c_vp, c_dbl, c_vp,
                            c_vp, c_sz, c_vp]),
     "tomos_gemv_no_alloc": (c_i32, [c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32, c_vp, c_dbl,
@@ -108,6 +110,13 @@ SIGNATURES = {
     "tomos_sketch_qr_scratch_bytes": (c_sz, [c_i64, c_i64]),
     "tomos_sketch_qr_precond_f64": (c_i32, [c_i64, c_i64, c_vp, c_i64, c_vp, c_vp, c_sz, c_vp]),
     "tomos_column_scale": (c_i32, [c_vp, c_i64, c_vp, c_vp, c_vp]),
+    "tomos_countsketch_apply_shard": (c_i32, [ctypes.POINTER(DenseDesc), c_i32, c_i64, c_u64, c_u64,
+                                              c_i64, c_vp, c_i64, c_vp, c_vp, c_vp, c_i64, c_vp, c_sz,
+                                              c_vp]),
+    "tomos_comm_unique_id": (c_i32, [c_vp]),
+    "tomos_comm_create": (c_i32, [c_i32, c_i32, c_vp, ctypes.POINTER(c_vp)]),
+    "tomos_comm_destroy": (c_i32, [c_vp]),
+    "tomos_comm_allreduce_f64": (c_i32, [c_vp, c_vp, c_i64, c_vp]),
     "tomos_workspace_create": (c_i32, [c_i64, c_i64, c_i32, c_i32, ctypes.POINTER(c_vp)]),
     "tomos_workspace_destroy": (c_i32, [c_vp]),
     "tomos_workspace_add_precond": (c_i32, [c_vp, ctypes.POINTER(DenseDesc)]),

@@ -77,7 +77,7 @@ def build(force=False, jobs=None, verbose=False):
                 f.result()
     if todo or not os.path.exists(LIB):
         tmp = LIB + ".tmp"
-        cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lnccl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}{r.stderr}")

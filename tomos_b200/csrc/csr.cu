@@ -151,6 +151,8 @@ static tomos_status launch_csr(Elem e, bool acc64, const CsrPassParams& P, int g
                                      : launch_csr_t<Elem::F32, false>(P, grid, warps, st);
         case Elem::H16: return acc64 ? launch_csr_t<Elem::H16, true>(P, grid, warps, st)
                                      : launch_csr_t<Elem::H16, false>(P, grid, warps, st);
+        case Elem::F16: return acc64 ? launch_csr_t<Elem::F16, true>(P, grid, warps, st)
+                                     : launch_csr_t<Elem::F16, false>(P, grid, warps, st);
         case Elem::B16: return acc64 ? launch_csr_t<Elem::B16, true>(P, grid, warps, st)
                                      : launch_csr_t<Elem::B16, false>(P, grid, warps, st);
         case Elem::A16: return launch_csr_t<Elem::A16, true>(P, grid, warps, st);
@@ -528,6 +530,8 @@ static tomos_status launch_rows(Elem e, bool acc64, const CsrPassParams& P, int 
                                      : launch_rows_t<Elem::F32, false>(P, lg, grid, st);
         case Elem::H16: return acc64 ? launch_rows_t<Elem::H16, true>(P, lg, grid, st)
                                      : launch_rows_t<Elem::H16, false>(P, lg, grid, st);
+        case Elem::F16: return acc64 ? launch_rows_t<Elem::F16, true>(P, lg, grid, st)
+                                     : launch_rows_t<Elem::F16, false>(P, lg, grid, st);
         case Elem::B16: return acc64 ? launch_rows_t<Elem::B16, true>(P, lg, grid, st)
                                      : launch_rows_t<Elem::B16, false>(P, lg, grid, st);
         case Elem::A16: return launch_rows_t<Elem::A16, true>(P, lg, grid, st);
@@ -626,6 +630,8 @@ static tomos_status launch_cols(Elem e, bool acc64, const CscCopy& c, int64_t n,
                                      : launch_cols_t<Elem::F32, false>(c, n, u, skip, q, st);
         case Elem::H16: return acc64 ? launch_cols_t<Elem::H16, true>(c, n, u, skip, q, st)
                                      : launch_cols_t<Elem::H16, false>(c, n, u, skip, q, st);
+        case Elem::F16: return acc64 ? launch_cols_t<Elem::F16, true>(c, n, u, skip, q, st)
+                                     : launch_cols_t<Elem::F16, false>(c, n, u, skip, q, st);
         case Elem::B16: return acc64 ? launch_cols_t<Elem::B16, true>(c, n, u, skip, q, st)
                                      : launch_cols_t<Elem::B16, false>(c, n, u, skip, q, st);
         case Elem::A16: return launch_cols_t<Elem::A16, true>(c, n, u, skip, q, st);
@@ -642,10 +648,12 @@ struct CsrPass : PassOps {
     const tomos_csr* A;
     Elem iter_e, init_e;
     bool csc = false;
+    bool allow_csc = true;  // false: the row pass only (the workspace's CSC copy serves another pass)
     CscCopy cc;
     int lg = 3;
     CsrPass(tomos_workspace* w, const tomos_csr* a, Elem ie, Elem ze) : ws(w), A(a), iter_e(ie), init_e(ze) {}
     tomos_status prepare(cudaStream_t st) override {
+        if (!allow_csc) return TOMOS_OK;
         const bool with_lo = A->numeric != TOMOS_FP32 && (elem_is_exact(iter_e) || elem_is_exact(init_e));
         const CscCopy need = csc_layout(nullptr, A, with_lo);
         if (need.bytes > ws->csc_bytes) {
@@ -762,6 +770,7 @@ tomos_status CsrPass::fro2(double* out, const double* d, cudaStream_t st) {
     switch (init_e) {
         case Elem::F32: TOMOS_CFRO(Elem::F32); break;
         case Elem::H16: TOMOS_CFRO(Elem::H16); break;
+        case Elem::F16: TOMOS_CFRO(Elem::F16); break;
         case Elem::A16: TOMOS_CFRO(Elem::A16); break;
         case Elem::B16: TOMOS_CFRO(Elem::B16); break;
         case Elem::AB16: TOMOS_CFRO(Elem::AB16); break;
@@ -944,7 +953,9 @@ tomos_status tomos_lsqr_solve_csr(const tomos_csr* A, const float* b, float* x,
                                   tomos_lsqr_report* report, void* stream) {
     std::string why;
     if (!csr_ok(A, &why)) return fail(TOMOS_ERR_INVALID, "lsqr_solve: " + why);
-    if (!opts) return fail(TOMOS_ERR_INVALID, "lsqr_solve: null options");
+    if (!opts_ok(opts, &why)) return fail(TOMOS_ERR_INVALID, "lsqr_solve: " + why);
+    if (opts->refine) return fail(TOMOS_ERR_INVALID, "lsqr_solve: a dense mtx_refine_precision for a sparse A");
+    if (opts->staged_plane) return fail(TOMOS_ERR_INVALID, "lsqr_solve: staged_plane needs a dense A");
     tomos_status s = workspace_check(ws, A->rows, A->cols);
     if (s) return s;
     if (!b || !x) return fail(TOMOS_ERR_INVALID, "lsqr_solve: null pointer");
@@ -966,6 +977,27 @@ tomos_status tomos_lsqr_solve_csr(const tomos_csr* A, const float* b, float* x,
             report->converged = 1;
         }
         return TOMOS_OK;
+    }
+    // The explicit duplicate (lsqr_sparse_impl's mtx_refine_precision,
+    // lsqr_registries.cpp:180-183): the initial and restart passes read it,
+    // exactly (FP32 values, or packed ones at the ACCURATE tier), through
+    // the row pass; the iterations keep the CSC copy of A.
+    if (opts->refine_csr) {
+        const tomos_csr* Rf = opts->refine_csr;
+        if (!csr_ok(Rf, &why)) return fail(TOMOS_ERR_INVALID, "lsqr_solve: mtx_refine_precision: " + why);
+        if (Rf->rows != A->rows || Rf->cols != A->cols)
+            return fail(TOMOS_ERR_INVALID, "lsqr_solve: mtx_refine_precision must have A's size");
+        if (Rf->nnz > 0 && (!Rf->values || !Rf->col_idxs))
+            return fail(TOMOS_ERR_INVALID, "lsqr_solve: mtx_refine_precision: null pointer");
+        Elem re;
+        const int32_t rt = (Rf->numeric == TOMOS_FP32_16 || Rf->numeric == TOMOS_FP32_BF16) ? TOMOS_TIER_ACCURATE
+                                                                                          : TOMOS_TIER_NATIVE;
+        if (!resolve_elem_csr(Rf, rt, &re, &why))
+            return fail(TOMOS_ERR_UNSUPPORTED, "lsqr_solve: mtx_refine_precision: " + why);
+        CsrPass pa(ws, A, ie, ie), pr(ws, Rf, re, re);
+        pr.allow_csc = false;
+        RefinePass ops(pa, pr);
+        return solve_driver(ws, ops, b, x, opts, report, stream);
     }
     CsrPass ops(ws, A, ie, ze);
     return solve_driver(ws, ops, b, x, opts, report, stream);
@@ -1020,6 +1052,7 @@ tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64
     switch (e) {
         case Elem::F32: TOMOS_CS_CSR(Elem::F32); break;
         case Elem::H16: TOMOS_CS_CSR(Elem::H16); break;
+        case Elem::F16: TOMOS_CS_CSR(Elem::F16); break;
         case Elem::A16: TOMOS_CS_CSR(Elem::A16); break;
         case Elem::B16: TOMOS_CS_CSR(Elem::B16); break;
         case Elem::AB16: TOMOS_CS_CSR(Elem::AB16); break;
@@ -1048,6 +1081,7 @@ tomos_status tomos_countsketch_apply_csr(const tomos_csr* A, int32_t tier, int64
         switch (e) {
             case Elem::F32: TOMOS_CSR_COLSQ(Elem::F32); break;
             case Elem::H16: TOMOS_CSR_COLSQ(Elem::H16); break;
+            case Elem::F16: TOMOS_CSR_COLSQ(Elem::F16); break;
             case Elem::A16: TOMOS_CSR_COLSQ(Elem::A16); break;
             case Elem::B16: TOMOS_CSR_COLSQ(Elem::B16); break;
             case Elem::AB16: TOMOS_CSR_COLSQ(Elem::AB16); break;

@@ -1,0 +1,693 @@
+// gemm.cu -- mm_apply: C = alpha op(A) op(B) + beta C on the 5th-generation
+// tensor cores (tcgen05.mma, accumulators in tensor memory).
+//
+// The reference's dense GEMM (blas.cpp:98-106, mm_apply; the FP32_16
+// tiers of blas.cpp:168-190 and fp32_16_registries.cpp:371-455) takes A in
+// any storage and FP32 B and C.  Here one kernel serves every storage:
+//
+//   CTA tile      128 rows of op(A) x BN columns of op(B) (BN 16..128),
+//                 the accumulator a 128-lane x BN-column FP32 tile of
+//                 tensor memory (tcgen05.alloc), one CTA per tile.
+//   producers     8 warps load op(A) and op(B) straight from global
+//                 memory (16-byte vectors along K where the lines are
+//                 K-contiguous, warp-coalesced scalar loads across lines
+//                 otherwise), decode the storage in registers, split the
+//                 values into tensor-core operands and write them as
+//                 16-byte units to a ring of shared-memory stages in the
+//                 UMMA canonical K-major layout (no swizzle).
+//   MMA warp      one thread issues 4 K-steps x terms tcgen05.mma per
+//                 stage and frees the stage with tcgen05.commit.
+//   epilogue      the producer warps read the accumulator (tcgen05.ld
+//                 32x32b) and write alpha acc + beta C.
+//
+// Operand precision per mode (the tier of the storage read):
+//   kPure16   A's 16-bit values (FP32_16 HALF tier fp16, native fp16,
+//             FP32_BF16 bf16) times B rounded to the same 16-bit type:
+//             one kind::f16 product -- the operands of the reference's
+//             pure_half tier (fp32_16_kernels.cpp:172-203), accumulated
+//             in FP32 instead of fp16.
+//   kTf32x2   the same 16-bit A values (exact in TF32) times B split as
+//             B_big + B_small (two TF32 numbers): two kind::tf32 products,
+//             B kept to about 22 bits -- the reference's "fast" tier
+//             (half decode, wide accumulation, fp32_16_kernels.cpp:113-141).
+//   kTf32x3   A exact (FP32 storage, or packed read exactly) split as
+//             A_big + A_small, B likewise: A_big B_big + A_big B_small +
+//             A_small B_big, three kind::tf32 products -- FP32-level
+//             products for the accurate tier (fp32_16_kernels.cpp:57-85).
+// Every product accumulates in FP32 in tensor memory; alpha and beta are
+// applied in FP64 in the epilogue.  The error of an entry is a few units
+// of 2^-22 times sum_l |op(A)_il| |op(B)_lj| plus FP32 summation over K.
+//
+// Every mbarrier wait is bounded (mbarrier.cuh): a wait that expires
+// records an error word and the CTA stops work, drains its MMAs (bounded
+// again), frees its tensor memory and exits; such a launch's C is
+// undefined.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <mutex>
+#include <string>
+#include <utility>
+
+#include "common.cuh"
+#include "mbarrier.cuh"
+
+namespace tomos_b200 {
+
+namespace {
+
+constexpr int kGemmM = 128;          // rows of op(A) per CTA (the MMA's M)
+constexpr int kLineBytes = 128;      // K bytes of one operand line per stage
+constexpr int kProducerWarps = 8;
+constexpr int kProducers = kProducerWarps * 32;
+constexpr int kGemmThreads = kProducers + 32;  // + the MMA warp
+constexpr int kGemmSmemBudget = 200 * 1024;
+constexpr int kMaxStages = 8;
+
+enum GemmMode : int { kPure16 = 0, kTf32x2 = 1, kTf32x3 = 2 };
+
+struct GemmArgs {
+    const void* a_hi;
+    const void* a_lo;
+    int64_t a_si, a_sl;  // op(A)(i, l) is element i * a_si + l * a_sl
+    const float* b;
+    int64_t b_sl, b_sj;  // op(B)(l, j) is element l * b_sl + j * b_sj
+    float* c;
+    int64_t c_si, c_sj;  // C(i, j) is element i * c_si + j * c_sj
+    int64_t M, N, K;
+    double alpha, beta;
+    int a_kc, b_kc;    // 1: the operand's lines run along K (else along M / N)
+    int a_vec, b_vec;  // 1: 16-byte (or 8-byte) vector loads are aligned
+    int bn;            // columns of op(B) per CTA: 16, 32, 64 or 128
+    int stages;
+    int* err;
+};
+
+template <int MODE>
+struct ModeTraits {
+    static constexpr int esz = MODE == kPure16 ? 2 : 4;  // operand bytes
+    static constexpr int epu = 16 / esz;                  // elements per 16-byte unit
+    static constexpr int kpl = kLineBytes / esz;          // K per stage
+    static constexpr int na = MODE == kTf32x3 ? 2 : 1;    // A operand tiles
+    static constexpr int nb = MODE == kPure16 ? 1 : 2;    // B operand tiles
+};
+
+// ---------------------------------------------------------------- PTX
+
+__device__ __forceinline__ uint32_t tf32_rn(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// A value and its TF32 remainder: x = big + small up to 2^-22 |x|.
+__device__ __forceinline__ void split_tf32(float x, uint32_t& big, uint32_t& small) {
+    big = tf32_rn(x);
+    small = tf32_rn(x - u2f(big));
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    // start address, leading (K-direction) and stride (MN-direction) core
+    // matrix offsets in 16-byte units; version 1 (sm_100); no swizzle.
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_issue(int kind_tf32, uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                          uint32_t acc) {
+    if (kind_tf32) {
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+            : "memory");
+    }
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+    // the load and its wait in one statement: nothing reads r before the wait
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr)
+        : "memory");
+}
+
+// ---------------------------------------------------------- element decode
+
+// A 16-bit element (raw bits h, r of the two planes) as a float.
+template <Elem E>
+__device__ __forceinline__ float decode16(uint32_t h, uint32_t r) {
+    if constexpr (E == Elem::H16) return half_bits_to_float(half_only_bits(h));
+    else if constexpr (E == Elem::F16) return half_bits_to_float(h);
+    else if constexpr (E == Elem::B16) return u2f(h << 16);
+    else if constexpr (E == Elem::A16) return decode_fp32_16_exact(h, r);
+    else if constexpr (E == Elem::AB16) return decode_fp32_bf16_exact(h, r, false);
+    else return decode_fp32_bf16_exact(h, r, true);  // AB16R
+}
+
+// The 16-bit operand bits of a HALF-tier element (fp16, or bf16 for B16).
+template <Elem E>
+__device__ __forceinline__ uint32_t bits16(uint32_t h) {
+    if constexpr (E == Elem::H16) return half_only_bits(h);
+    else return h;  // F16, B16
+}
+
+template <Elem E>
+__host__ __device__ constexpr bool two_planes() {
+    return E == Elem::A16 || E == Elem::AB16 || E == Elem::AB16R;
+}
+
+// Scalar element of op(A) (0 outside) as a float / as 16-bit operand bits.
+template <Elem E>
+__device__ __forceinline__ float a_scalar(const GemmArgs& g, int64_t i, int64_t l) {
+    if (i >= g.M || l >= g.K) return 0.0f;
+    const size_t idx = (size_t)(i * g.a_si + l * g.a_sl);
+    if constexpr (E == Elem::F32) return __ldg(static_cast<const float*>(g.a_hi) + idx);
+    else {
+        const uint32_t h = __ldg(static_cast<const unsigned short*>(g.a_hi) + idx);
+        uint32_t r = 0;
+        if constexpr (two_planes<E>()) r = __ldg(static_cast<const unsigned short*>(g.a_lo) + idx);
+        return decode16<E>(h, r);
+    }
+}
+
+template <Elem E>
+__device__ __forceinline__ uint32_t a_scalar16(const GemmArgs& g, int64_t i, int64_t l) {
+    if (i >= g.M || l >= g.K) return 0u;
+    const size_t idx = (size_t)(i * g.a_si + l * g.a_sl);
+    return bits16<E>(__ldg(static_cast<const unsigned short*>(g.a_hi) + idx));
+}
+
+__device__ __forceinline__ float b_scalar(const GemmArgs& g, int64_t l, int64_t j) {
+    if (l >= g.K || j >= g.N) return 0.0f;
+    return __ldg(g.b + (size_t)(l * g.b_sl + j * g.b_sj));
+}
+
+template <bool BF>
+__device__ __forceinline__ uint32_t to16(float x) {
+    if constexpr (BF) return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x));
+    else return (uint32_t)__half_as_ushort(__float2half_rn(x));
+}
+
+// ---------------------------------------------------------- operand tiles
+//
+// A tile holds R lines (rows of op(A), or columns of op(B)) x 128 bytes of
+// K, K-major, as 128-byte core matrices (8 lines x 16 bytes): unit (line
+// r, K chunk u of 16 bytes) at ((u * R/8 + r/8) * 8 + r % 8) * 16 bytes.
+// The MN-direction core stride (SBO) is 128 bytes, the K-direction one
+// (LBO) R/8 core matrices.  Eight consecutive lanes always write eight
+// consecutive lines of one chunk: one 128-byte shared-memory wavefront.
+// (Operands are K-major whatever their global layout: the TF32 products
+// are issued from K-major tiles only.)
+
+__device__ __forceinline__ uint32_t kmajor_off(int r, int u, int R) {
+    return (uint32_t)(((u * (R >> 3) + (r >> 3)) * 8 + (r & 7)) * 16);
+}
+
+// Writes op(A) rows [m0, m0 + 128) x K [k0, k0 + kpl) into tile(s) t0 (and
+// t1: the TF32 remainders for kTf32x3).
+template <Elem E, int MODE>
+__device__ __forceinline__ void produce_a(const GemmArgs& g, uint8_t* t0, uint8_t* t1, int64_t m0, int64_t k0,
+                                          int pt) {
+    using T = ModeTraits<MODE>;
+    constexpr int R = kGemmM;
+    constexpr int items = R * 8;
+    for (int it = pt; it < items; it += kProducers) {
+        float v[8];
+        uint32_t b16[8];
+        int r, u;  // line, 16-byte K chunk
+        uint32_t off;
+        if (g.a_kc) {
+            r = (it & 7) | ((it >> 6) << 3);
+            u = (it >> 3) & 7;
+            off = kmajor_off(r, u, R);
+            const int64_t i = m0 + r, l = k0 + (int64_t)u * T::epu;
+            const bool full = g.a_vec && i < g.M && l + T::epu <= g.K;
+            const size_t idx = (size_t)(i * g.a_si + l);
+            if constexpr (MODE == kPure16) {
+                if (full) {
+                    const uint4 h = __ldg(reinterpret_cast<const uint4*>(static_cast<const uint16_t*>(g.a_hi) + idx));
+                    const uint32_t w[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        b16[2 * e] = bits16<E>(w[e] & 0xFFFFu);
+                        b16[2 * e + 1] = bits16<E>(w[e] >> 16);
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) b16[e] = a_scalar16<E>(g, i, l + e);
+                }
+            } else if constexpr (E == Elem::F32) {
+                if (full) {
+                    const float4 f = __ldg(reinterpret_cast<const float4*>(static_cast<const float*>(g.a_hi) + idx));
+                    v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) v[e] = a_scalar<E>(g, i, l + e);
+                }
+            } else {
+                if (full) {
+                    const uint2 h = __ldg(reinterpret_cast<const uint2*>(static_cast<const uint16_t*>(g.a_hi) + idx));
+                    uint2 q = make_uint2(0u, 0u);
+                    if constexpr (two_planes<E>())
+                        q = __ldg(reinterpret_cast<const uint2*>(static_cast<const uint16_t*>(g.a_lo) + idx));
+                    v[0] = decode16<E>(h.x & 0xFFFFu, q.x & 0xFFFFu);
+                    v[1] = decode16<E>(h.x >> 16, q.x >> 16);
+                    v[2] = decode16<E>(h.y & 0xFFFFu, q.y & 0xFFFFu);
+                    v[3] = decode16<E>(h.y >> 16, q.y >> 16);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) v[e] = a_scalar<E>(g, i, l + e);
+                }
+            }
+        } else {
+            // lines strided along K (op(A) contiguous along M): consecutive
+            // lanes take consecutive lines, so each of the unit's scalar
+            // loads is one coalesced access across the warp
+            r = it % R;
+            u = it / R;
+            off = kmajor_off(r, u, R);
+            const int64_t i = m0 + r, l = k0 + (int64_t)u * T::epu;
+            if constexpr (MODE == kPure16) {
+#pragma unroll
+                for (int e = 0; e < 8; ++e) b16[e] = a_scalar16<E>(g, i, l + e);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) v[e] = a_scalar<E>(g, i, l + e);
+            }
+        }
+        (void)r;
+        (void)u;
+        if constexpr (MODE == kPure16) {
+            uint4 w;
+            w.x = b16[0] | (b16[1] << 16);
+            w.y = b16[2] | (b16[3] << 16);
+            w.z = b16[4] | (b16[5] << 16);
+            w.w = b16[6] | (b16[7] << 16);
+            *reinterpret_cast<uint4*>(t0 + off) = w;
+        } else if constexpr (MODE == kTf32x2) {
+            // 16-bit values are exact in TF32
+            *reinterpret_cast<uint4*>(t0 + off) = make_uint4(f2u(v[0]), f2u(v[1]), f2u(v[2]), f2u(v[3]));
+        } else {
+            uint32_t bg[4], sm[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) split_tf32(v[e], bg[e], sm[e]);
+            *reinterpret_cast<uint4*>(t0 + off) = make_uint4(bg[0], bg[1], bg[2], bg[3]);
+            *reinterpret_cast<uint4*>(t1 + off) = make_uint4(sm[0], sm[1], sm[2], sm[3]);
+        }
+    }
+}
+
+// Writes op(B) columns [n0, n0 + bn) x K [k0, k0 + kpl): t0 (the TF32 big
+// parts, or the 16-bit values) and t1 (TF32 remainders).
+template <int MODE, bool BF>
+__device__ __forceinline__ void produce_b(const GemmArgs& g, uint8_t* t0, uint8_t* t1, int64_t n0, int64_t k0,
+                                          int pt) {
+    using T = ModeTraits<MODE>;
+    const int R = g.bn;
+    const int items = R * 8;
+    for (int it = pt; it < items; it += kProducers) {
+        float v[8];
+        uint32_t off;
+        if (g.b_kc) {
+            const int r = (it & 7) | ((it >> 6) << 3);
+            const int u = (it >> 3) & 7;
+            off = kmajor_off(r, u, R);
+            const int64_t j = n0 + r, l = k0 + (int64_t)u * T::epu;
+            const bool full = g.b_vec && j < g.N && l + T::epu <= g.K;
+            const float* p = g.b + (size_t)(j * g.b_sj + l);
+            if (full) {
+                const float4 f = __ldg(reinterpret_cast<const float4*>(p));
+                v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+                if constexpr (T::epu == 8) {
+                    const float4 f2 = __ldg(reinterpret_cast<const float4*>(p) + 1);
+                    v[4] = f2.x; v[5] = f2.y; v[6] = f2.z; v[7] = f2.w;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < T::epu; ++e) v[e] = b_scalar(g, l + e, j);
+            }
+        } else {
+            // lines strided along K: consecutive lanes, consecutive columns
+            const int r = it % R, u = it / R;
+            off = kmajor_off(r, u, R);
+            const int64_t j = n0 + r, l = k0 + (int64_t)u * T::epu;
+#pragma unroll
+            for (int e = 0; e < T::epu; ++e) v[e] = b_scalar(g, l + e, j);
+        }
+        if constexpr (MODE == kPure16) {
+            uint4 w;
+            w.x = to16<BF>(v[0]) | (to16<BF>(v[1]) << 16);
+            w.y = to16<BF>(v[2]) | (to16<BF>(v[3]) << 16);
+            w.z = to16<BF>(v[4]) | (to16<BF>(v[5]) << 16);
+            w.w = to16<BF>(v[6]) | (to16<BF>(v[7]) << 16);
+            *reinterpret_cast<uint4*>(t0 + off) = w;
+        } else {
+            uint32_t bg[4], sm[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) split_tf32(v[e], bg[e], sm[e]);
+            *reinterpret_cast<uint4*>(t0 + off) = make_uint4(bg[0], bg[1], bg[2], bg[3]);
+            *reinterpret_cast<uint4*>(t1 + off) = make_uint4(sm[0], sm[1], sm[2], sm[3]);
+        }
+    }
+}
+
+// Descriptor of MMA K-step s (32 bytes of K: two 16-byte chunks) of a tile.
+__device__ __forceinline__ uint64_t tile_desc(uint32_t base, int s, int R) {
+    const uint32_t lbo = (uint32_t)(R >> 3) * 128u;
+    return smem_desc(base + (uint32_t)(2 * s) * lbo, lbo, 128u);
+}
+
+template <Elem E, int MODE>
+__global__ void __launch_bounds__(kGemmThreads, 1) gemm_tc_kernel(GemmArgs g) {
+    using T = ModeTraits<MODE>;
+    constexpr bool BF = (E == Elem::B16);
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int S = g.stages, BN = g.bn;
+    const uint32_t a_bytes = kGemmM * kLineBytes, b_bytes = (uint32_t)BN * kLineBytes;
+    const uint32_t stage_bytes = T::na * a_bytes + T::nb * b_bytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
+    uint64_t* empty = full + kMaxStages;
+    uint64_t* done = empty + kMaxStages;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t m0 = (int64_t)blockIdx.x * kGemmM, n0 = (int64_t)blockIdx.y * BN;
+    const int nk = (int)((g.K + T::kpl - 1) / T::kpl);
+    const uint32_t ncols = BN <= 32 ? 32u : (uint32_t)BN;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], kProducerWarps);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+    }
+    if (warp == kProducerWarps) {  // the MMA warp owns the tensor memory
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp < kProducerWarps) {
+        const int pt = threadIdx.x;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % S;
+            if (kt >= S && !mbar_wait(&empty[s], (uint32_t)((kt / S - 1) & 1))) {
+                if (lane == 0) atomicExch(g.err, 1);
+                *abort_flag = 1;
+            }
+            if (*abort_flag) break;
+            uint8_t* st = smem + (size_t)s * stage_bytes;
+            const int64_t k0 = (int64_t)kt * T::kpl;
+            produce_a<E, MODE>(g, st, st + a_bytes, m0, k0, pt);
+            uint8_t* bt = st + T::na * a_bytes;
+            produce_b<MODE, BF>(g, bt, bt + b_bytes, n0, k0, pt);
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&full[s]);
+        }
+    } else if (lane == 0) {
+        // the MMA issuer
+        uint32_t idesc = (1u << 4);  // FP32 accumulator
+        const uint32_t fmt = MODE == kPure16 ? (BF ? 1u : 0u) : 2u;
+        idesc |= fmt << 7;
+        idesc |= fmt << 10;
+        // bits 15, 16 (A, B major) stay 0: K-major operands
+        idesc |= ((uint32_t)BN >> 3) << 17;
+        idesc |= ((uint32_t)kGemmM >> 4) << 24;
+        uint32_t acc = 0;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % S;
+            if (!mbar_wait(&full[s], (uint32_t)((kt / S) & 1))) {
+                atomicExch(g.err, 2);
+                *abort_flag = 1;
+            }
+            if (*abort_flag) break;
+            tc_fence_after();
+            const uint32_t st = smem_addr(smem + (size_t)s * stage_bytes);
+            const uint32_t a0 = st, a1 = st + a_bytes;
+            const uint32_t b0 = st + T::na * a_bytes, b1 = b0 + b_bytes;
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                const uint64_t da0 = tile_desc(a0, ks, kGemmM);
+                const uint64_t db0 = tile_desc(b0, ks, BN);
+                mma_issue(MODE != kPure16, tmem, da0, db0, idesc, acc);
+                acc = 1;
+                if constexpr (MODE != kPure16) {
+                    const uint64_t db1 = tile_desc(b1, ks, BN);
+                    mma_issue(1, tmem, da0, db1, idesc, 1);
+                }
+                if constexpr (MODE == kTf32x3) {
+                    const uint64_t da1 = tile_desc(a1, ks, kGemmM);
+                    mma_issue(1, tmem, da1, db0, idesc, 1);
+                }
+            }
+            mma_commit(&empty[s]);  // frees the stage once these MMAs are done
+        }
+        mma_commit(done);  // the accumulator is complete (or the work stopped)
+    }
+
+    // epilogue: producer warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows)
+    // and half (w / 4) of the columns
+    if (warp < kProducerWarps) {
+        if (!mbar_wait(done, 0u)) {
+            if (lane == 0) atomicExch(g.err, 3);
+            *abort_flag = 1;
+        }
+        tc_fence_after();
+        const int q = warp & 3, h = warp >> 2;
+        const int64_t i = m0 + q * 32 + lane;
+        const int c_lo = h * (BN >> 1), c_hi = c_lo + (BN >> 1);
+        const bool ok = !*abort_flag;
+        for (int c = c_lo; c < c_hi; c += 8) {
+            uint32_t r[8];
+            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, r);
+            if (!ok || i >= g.M) continue;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int64_t j = n0 + c + e;
+                if (j >= g.N) break;
+                float* cp = g.c + (size_t)(i * g.c_si + j * g.c_sj);
+                double y = g.alpha * (double)u2f(r[e]);
+                if (g.beta != 0.0) y += g.beta * (double)*cp;
+                *cp = (float)y;
+            }
+        }
+    } else {
+        // the MMA warp waits for its own MMAs before freeing the memory
+        if (!mbar_wait(done, 0u) && lane == 0) atomicExch(g.err, 4);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == kProducerWarps)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// The word a bounded wait of these launches records its expiry in.
+__device__ int g_gemm_err;
+constexpr int kMaxDevices = 64;
+
+int* gemm_err_word() {
+    static std::mutex mu;
+    static int* addr[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_gemm_err) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        addr[dev] = static_cast<int*>(p);
+    }
+    return addr[dev];
+}
+
+template <int MODE>
+int stage_count(int bn) {
+    using T = ModeTraits<MODE>;
+    const int stage = T::na * kGemmM * kLineBytes + T::nb * bn * kLineBytes;
+    int s = (kGemmSmemBudget - 1024) / stage;
+    return s > kMaxStages ? kMaxStages : s;
+}
+
+template <Elem E, int MODE>
+tomos_status launch_gemm(GemmArgs& g, cudaStream_t st) {
+    using T = ModeTraits<MODE>;
+    g.stages = stage_count<MODE>(g.bn);
+    if (g.stages < 2) return fail(TOMOS_ERR_UNSUPPORTED, "mm: shared memory");
+    const size_t smem = (size_t)g.stages * (T::na * kGemmM * kLineBytes + T::nb * g.bn * kLineBytes) +
+                        (2 * kMaxStages + 1) * sizeof(uint64_t) + 16;
+    auto kern = gemm_tc_kernel<E, MODE>;
+    TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 grid((unsigned)((g.M + kGemmM - 1) / kGemmM), (unsigned)((g.N + g.bn - 1) / g.bn));
+    kern<<<grid, kGemmThreads, smem, st>>>(g);
+    TOMOS_LAUNCH_CHECK("gemm_tc_kernel");
+    return TOMOS_OK;
+}
+
+template <int MODE>
+tomos_status launch_mode(Elem e, GemmArgs& g, cudaStream_t st) {
+    switch (e) {
+        case Elem::H16: return launch_gemm<Elem::H16, MODE>(g, st);
+        case Elem::F16: return launch_gemm<Elem::F16, MODE>(g, st);
+        case Elem::B16: return launch_gemm<Elem::B16, MODE>(g, st);
+        default: return fail(TOMOS_ERR_UNSUPPORTED, "mm: element type");
+    }
+}
+
+bool two_planes_elem(Elem e) { return e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R; }
+
+// C = beta C (K == 0: op(A) op(B) is the zero matrix).
+__global__ void gemm_scale_c_kernel(float* c, int64_t M, int64_t N, int64_t si, int64_t sj, double beta) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M * N) return;
+    const int64_t i = t % M, j = t / M;
+    float* p = c + (size_t)(i * si + j * sj);
+    *p = beta == 0.0 ? 0.0f : (float)(beta * (double)*p);
+}
+
+bool strides_of(const tomos_dense* D, int32_t trans, int64_t* s_row, int64_t* s_col) {
+    // op(D)(r, c): element r * s_row + c * s_col
+    int64_t sr = D->layout == TOMOS_COL_MAJOR ? 1 : D->ld;
+    int64_t sc = D->layout == TOMOS_COL_MAJOR ? D->ld : 1;
+    if (trans == TOMOS_TRANSPOSE) std::swap(sr, sc);
+    *s_row = sr;
+    *s_col = sc;
+    return true;
+}
+
+}  // namespace
+
+}  // namespace tomos_b200
+
+using namespace tomos_b200;
+
+extern "C" {
+
+tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A, int32_t tier,
+                      const tomos_dense* B, double beta, tomos_dense* C, void* stream) {
+    if (!A || !B || !C) return fail(TOMOS_ERR_INVALID, "mm: null matrix");
+    if ((trans_a != TOMOS_NO_TRANSPOSE && trans_a != TOMOS_TRANSPOSE) ||
+        (trans_b != TOMOS_NO_TRANSPOSE && trans_b != TOMOS_TRANSPOSE))
+        return fail(TOMOS_ERR_INVALID, "mm: bad transpose");
+    if (B->numeric != TOMOS_FP32 || C->numeric != TOMOS_FP32)
+        return fail(TOMOS_ERR_UNSUPPORTED, "mm: B and C must be FP32 (dense_registries.cpp:396-405)");
+    for (const tomos_dense* D : {A, B, static_cast<const tomos_dense*>(C)}) {
+        if (D->rows < 0 || D->cols < 0) return fail(TOMOS_ERR_INVALID, "mm: negative size");
+        if (D->layout != TOMOS_ROW_MAJOR && D->layout != TOMOS_COL_MAJOR)
+            return fail(TOMOS_ERR_INVALID, "mm: bad layout");
+        const int64_t inner = D->layout == TOMOS_ROW_MAJOR ? D->cols : D->rows;
+        if (D->rows > 0 && D->cols > 0 && D->ld < inner)
+            return fail(TOMOS_ERR_INVALID, "mm: leading dimension too small");
+    }
+    const int64_t M = trans_a == TOMOS_NO_TRANSPOSE ? A->rows : A->cols;
+    const int64_t K = trans_a == TOMOS_NO_TRANSPOSE ? A->cols : A->rows;
+    const int64_t Kb = trans_b == TOMOS_NO_TRANSPOSE ? B->rows : B->cols;
+    const int64_t N = trans_b == TOMOS_NO_TRANSPOSE ? B->cols : B->rows;
+    if (Kb != K || C->rows != M || C->cols != N) return fail(TOMOS_ERR_INVALID, "mm: size mismatch");
+    // the operand tier: HALF_OPERANDS (16-bit A and B), HALF (16-bit A,
+    // ~FP32 B), exact (FP32 or ACCURATE)
+    const bool ops16 = tier == TOMOS_TIER_HALF_OPERANDS;
+    int32_t rt = tier;
+    if (ops16) rt = A->numeric == TOMOS_FP16 ? TOMOS_TIER_NATIVE : TOMOS_TIER_HALF;
+    Elem e;
+    std::string why;
+    if (!resolve_elem(A, rt, &e, &why)) return fail(TOMOS_ERR_UNSUPPORTED, "mm: " + why);
+    const bool e16 = e == Elem::H16 || e == Elem::F16 || e == Elem::B16;
+    if (ops16 && !e16) return fail(TOMOS_ERR_UNSUPPORTED, "mm: 16-bit operands need 16-bit A values");
+    if (e == Elem::F64) return fail(TOMOS_ERR_UNSUPPORTED, "mm: FP64 A");
+    cudaStream_t st = as_stream(stream);
+    if (M == 0 || N == 0) return TOMOS_OK;
+    if ((!A->values && M * K > 0) || !B->values && K * N > 0 || !C->values)
+        return fail(TOMOS_ERR_INVALID, "mm: null values");
+    int* err = gemm_err_word();
+    if (!err) return fail(TOMOS_ERR_CUDA, "mm: error word");
+
+    GemmArgs g;
+    g.a_hi = A->values;
+    g.a_lo = two_planes_elem(e) ? dense_lo_plane(A) : nullptr;
+    strides_of(A, trans_a, &g.a_si, &g.a_sl);
+    g.b = static_cast<const float*>(B->values);
+    strides_of(B, trans_b, &g.b_sl, &g.b_sj);
+    g.c = static_cast<float*>(C->values);
+    strides_of(C, TOMOS_NO_TRANSPOSE, &g.c_si, &g.c_sj);
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.alpha = alpha;
+    g.beta = beta;
+    g.err = err;
+    g.bn = N <= 16 ? 16 : N <= 32 ? 32 : N <= 64 ? 64 : 128;
+    if (K == 0) {
+        gemm_scale_c_kernel<<<(unsigned)((M * N + 255) / 256), 256, 0, st>>>(g.c, M, N, g.c_si, g.c_sj, beta);
+        TOMOS_LAUNCH_CHECK("gemm_scale_c_kernel");
+        return TOMOS_OK;
+    }
+    // one of the two strides of a dense operand is 1: lines run along K
+    // when the K stride is
+    g.a_kc = g.a_sl == 1 ? 1 : 0;
+    g.b_kc = g.b_sl == 1 ? 1 : 0;
+    // vector loads: unit stride along the line, 16-byte aligned lines
+    const int aes = e == Elem::F32 ? 4 : 2;
+    const int mode = ops16 ? kPure16 : (e16 ? kTf32x2 : kTf32x3);
+    const int aepu = mode == kPure16 ? 8 : 4;
+    const int64_t a_lstride = g.a_kc ? g.a_si : g.a_sl;
+    const uintptr_t ab = reinterpret_cast<uintptr_t>(A->values);
+    const uintptr_t al = reinterpret_cast<uintptr_t>(g.a_lo);
+    const int avb = aepu * aes;  // vector bytes
+    g.a_vec = ((g.a_kc ? g.a_sl : g.a_si) == 1) && (a_lstride * aes) % avb == 0 && ab % avb == 0 &&
+              (!g.a_lo || al % avb == 0);
+    const int64_t b_lstride = g.b_kc ? g.b_sj : g.b_sl;
+    const uintptr_t bb = reinterpret_cast<uintptr_t>(B->values);
+    g.b_vec = ((g.b_kc ? g.b_sl : g.b_sj) == 1) && (b_lstride * 4) % 16 == 0 && bb % 16 == 0;
+    switch (mode) {
+        case kPure16: return launch_mode<kPure16>(e, g, st);
+        case kTf32x2: return launch_mode<kTf32x2>(e, g, st);
+        default:
+            switch (e) {
+                case Elem::F32: return launch_gemm<Elem::F32, kTf32x3>(g, st);
+                case Elem::A16: return launch_gemm<Elem::A16, kTf32x3>(g, st);
+                case Elem::AB16: return launch_gemm<Elem::AB16, kTf32x3>(g, st);
+                case Elem::AB16R: return launch_gemm<Elem::AB16R, kTf32x3>(g, st);
+                default: return fail(TOMOS_ERR_UNSUPPORTED, "mm: element type");
+            }
+    }
+}
+
+}  // extern "C"

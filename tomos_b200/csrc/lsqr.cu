@@ -173,6 +173,7 @@ struct NSide {
     LsqrDev* st;
     const int* skip;
     const double* dscale;  // column scale D of the backward-error rule, or NULL
+    const double* qsum;    // row-sharded solves: A^T ut summed over ranks (n), else NULL
 };
 
 // Givens step of LSQR (lsqr.cpp:633-679), FP64.
@@ -202,7 +203,9 @@ __global__ void __launch_bounds__(256) nside_reduce_kernel(NSide S) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t j = (int64_t)blockIdx.x * 32 + lane;
     double q = 0.0;
-    if (j < S.n)
+    if (S.qsum)
+        q = (w == 0 && j < S.n) ? S.qsum[j] : 0.0;
+    else if (j < S.n)
         for (int c = w; c < S.gq; c += 8) q += (double)S.qpart[(size_t)c * S.qstride + j];
     smq[w][lane] = q;
     __syncthreads();
@@ -374,7 +377,7 @@ static void ws_free(tomos_workspace* ws) {
     void* ptrs[] = {ws->u,      ws->v,      ws->wt,     ws->p,    ws->qvec,   ws->t,
                     ws->vhat,   ws->qpart,  ws->sspart, ws->vpart, ws->xpart, ws->qnpart,
                     ws->scal,   ws->coef_init, ws->bpart, ws->fro2, ws->st,   ws->Rcm,
-                    ws->Rrm,    ws->hist,   ws->scratch, ws->h16, ws->adj, ws->csc};
+                    ws->Rrm,    ws->hist,   ws->scratch, ws->h16, ws->adj, ws->csc, ws->shard};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (ws->st_host) cudaFreeHost(ws->st_host);
@@ -645,6 +648,12 @@ static NSide make_nside(tomos_workspace* ws, const PassPlan& pl, float* x, bool 
     S.scal = ws->scal;
     S.st = ws->st;
     S.skip = skip;
+    S.qsum = nullptr;
+    if (ws->comm) {  // the pass's partials were folded and summed across ranks
+        S.qsum = ws->shard;
+        S.sspart = ws->shard + ws->n;
+        S.gs = 1;
+    }
     return S;
 }
 
@@ -763,35 +772,6 @@ struct DensePass : PassOps {
     int64_t cols() override { return A->cols; }
 };
 
-// Iterations over A, the initial and restart passes over a second copy of
-// A at higher precision: the reference's mtx_refine_precision
-// (--explicit-duplicates; lsqr.cpp:451-473 computes the restart residual
-// u = b - A_refine x from it).  Here the whole restart pass, u and A^T u,
-// streams the refine copy (one read of it instead of a read of each), and
-// its ||A||_F feeds the backward-error rule.
-struct RefinePass : PassOps {
-    DensePass& it;
-    DensePass& re;
-    RefinePass(DensePass& a, DensePass& r) : it(a), re(r) {}
-    PassPlan plan(bool init) override {
-        PassPlan p = init ? re.plan(true) : it.plan(false);
-        p.src = init ? 1 : 0;
-        return p;
-    }
-    tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
-                         const int* skip, cudaStream_t st) override {
-        return pl.src ? re.enqueue(pl, p, u_in, coef, skip, st) : it.enqueue(pl, p, u_in, coef, skip, st);
-    }
-    tomos_status fro2(double* out, const double* d, cudaStream_t st) override { return re.fro2(out, d, st); }
-    uint64_t key() override { return it.key() ^ (re.key() * 0x9E3779B97F4A7C15ull); }
-    int64_t rows() override { return it.rows(); }
-    int64_t cols() override { return it.cols(); }
-    tomos_status prepare(cudaStream_t st) override {
-        tomos_status s = it.prepare(st);
-        return s ? s : re.prepare(st);
-    }
-};
-
 // ------------------------------------------------------------ driver
 
 tomos_status refresh_precond(tomos_workspace* ws, cudaStream_t st) {
@@ -827,6 +807,27 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     cudaStream_t us = as_stream(user_stream);
     cudaStream_t st = ws->stream;
     const int64_t m = ops.rows(), n = ops.cols();
+    ws->comm = o->comm;
+    struct CommScope {  // the communicator belongs to this solve only
+        tomos_workspace* w;
+        ~CommScope() {
+            // A graph that captured the communicator's all-reduce must not
+            // outlive it (the caller may destroy the communicator next).
+            if (w->comm && w->graph) {
+                cudaGraphExecDestroy(w->graph);
+                w->graph = nullptr;
+                w->graph_key.clear();
+            }
+            w->comm = nullptr;
+        }
+    } comm_scope{ws};
+    // One pass over A; a row-sharded solve then sums its partials across ranks.
+    auto pass = [&](const PassPlan& pl, const float* p, const float* u_in, const double* coef,
+                    const int* skip) -> tomos_status {
+        tomos_status ps = ops.enqueue(pl, p, u_in, coef, skip, st);
+        if (ps || !ws->comm) return ps;
+        return enqueue_shard_reduce(ws, ws->comm, ws->qpart, pl.gq, pl.qstride, ws->sspart, pl.gs, skip, st);
+    };
     tomos_lsqr_report R;
     std::memset(&R, 0, sizeof(R));
 
@@ -874,13 +875,27 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     sumsq_partial_kernel<<<ws->gs_max, 256, 0, st>>>(b, m, nullptr, ws->bpart);
     TOMOS_LAUNCH_CHECK("sumsq_partial_kernel");
     ws->launches += 2;
+    const double* bsum = ws->bpart;
+    int64_t nbsum = ws->gs_max;
+    if (ws->comm) {  // ||b||^2 over every rank's rows
+        sum_to_scalar_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, ws->scal + 2);
+        TOMOS_LAUNCH_CHECK("sum_to_scalar_kernel");
+        s = comm_allreduce(ws->comm, ws->scal + 2, 1, st);
+        if (s) return s;
+        bsum = ws->scal + 2;
+        nbsum = 1;
+    }
     if (need_fro) {
         s = ops.fro2(ws->scal + 3, dsc, st);
         if (s) return s;
+        if (ws->comm) {
+            s = comm_allreduce(ws->comm, ws->scal + 3, 1, st);
+            if (s) return s;
+        }
         extra_passes = 1;
         ws->launches += 2;
     }
-    state_norms_kernel<<<1, 256, 0, st>>>(ws->bpart, ws->gs_max, o->anorm_fro_dev,
+    state_norms_kernel<<<1, 256, 0, st>>>(bsum, nbsum, o->anorm_fro_dev,
                                           need_fro ? ws->scal + 3 : nullptr, ws->st);
     TOMOS_LAUNCH_CHECK("state_norms_kernel");
 
@@ -898,7 +913,8 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
                                  reinterpret_cast<uint64_t>(x),
                                  (uint64_t)ws->has_precond,
                                  (uint64_t)n,
-                                 (uint64_t)m};
+                                 (uint64_t)m,
+                                 reinterpret_cast<uint64_t>(o->comm)};
     if (!ws->graph || ws->graph_key != key) {
         if (ws->graph) cudaGraphExecDestroy(ws->graph);
         ws->graph = nullptr;
@@ -906,7 +922,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         const int64_t before = ws->launches;
         TOMOS_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         const int* skip = &ws->st->done;
-        tomos_status cs = ops.enqueue(pl_iter, ws->p, ws->u, ws->st->coef, skip, st);
+        tomos_status cs = pass(pl_iter, ws->p, ws->u, ws->st->coef, skip);
         if (!cs) cs = enqueue_nside(ws, make_nside(ws, pl_iter, x, false, skip, dsc), st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         if (cs) {
@@ -946,7 +962,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         restarts_used = rs + 1;
         const PassPlan& pz = (rs == 0 && !o->warm_start) ? pl_iter : pl_init;
         if (o->profile) TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pa, st));
-        s = ops.enqueue(pz, x, b, ws->coef_init, nullptr, st);
+        s = pass(pz, x, b, ws->coef_init, nullptr);
         if (s) return s;
         if (o->profile) TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pb, st));
         s = enqueue_nside(ws, make_nside(ws, pz, x, true, nullptr, dsc), st);
@@ -996,7 +1012,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         while (o->profile && done_iters < max_iters) {
             const int* skip = &ws->st->done;
             TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pa, st));
-            s = ops.enqueue(pl_iter, ws->p, ws->u, ws->st->coef, skip, st);
+            s = pass(pl_iter, ws->p, ws->u, ws->st->coef, skip);
             if (s) return s;
             TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_pb, st));
             s = enqueue_nside(ws, make_nside(ws, pl_iter, x, false, skip, dsc), st);
@@ -1038,7 +1054,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     }
     // The backward-error rule reports the accurate eta of the returned x.
     if (o->stop_rule == TOMOS_STOP_BACKWARD && !converged) {
-        s = ops.enqueue(pl_init, x, b, ws->coef_init, nullptr, st);
+        s = pass(pl_init, x, b, ws->coef_init, nullptr);
         if (s) return s;
         s = enqueue_nside(ws, make_nside(ws, pl_init, x, true, nullptr, dsc), st);
         if (s) return s;
@@ -1094,7 +1110,7 @@ tomos_status workspace_check(tomos_workspace* ws, int64_t m, int64_t n) {
     return TOMOS_OK;
 }
 
-static bool opts_ok(const tomos_lsqr_opts* o, std::string* why) {
+bool opts_ok(const tomos_lsqr_opts* o, std::string* why) {
     if (!o) {
         *why = "null options";
         return false;
@@ -1172,6 +1188,7 @@ tomos_status tomos_workspace_create(int64_t m, int64_t n, int32_t value_type,
     A(alloc(&ws->bpart, (size_t)ws->gs_max));
     A(alloc(&ws->fro2, 1));
     A(alloc(&ws->st, 1));
+    A(alloc(&ws->shard, (size_t)n + 1));
     A(cudaMallocHost(reinterpret_cast<void**>(&ws->st_host), sizeof(LsqrDev)));
     A(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
     A(cudaEventCreate(&ws->ev_start));
@@ -1240,6 +1257,8 @@ tomos_status tomos_lsqr_solve_dense(const tomos_dense* A, const float* b, float*
     if (!gemv_shape(A, TOMOS_NO_TRANSPOSE, &dot, &outer, &inner, &why))
         return fail(TOMOS_ERR_INVALID, "lsqr_solve: " + why);
     if (!opts_ok(opts, &why)) return fail(TOMOS_ERR_INVALID, "lsqr_solve: " + why);
+    if (opts->refine_csr)
+        return fail(TOMOS_ERR_INVALID, "lsqr_solve: a sparse mtx_refine_precision for a dense A");
     tomos_status s = workspace_check(ws, A->rows, A->cols);
     if (s) return s;
     if (!b || !x || (!A->values && A->rows * A->cols > 0))

@@ -68,6 +68,36 @@ struct PassOps {
     virtual tomos_status prepare(cudaStream_t) { return TOMOS_OK; }
 };
 
+// Iterations over A, the initial and restart passes over a second copy of
+// A at higher precision: the reference's mtx_refine_precision
+// (--explicit-duplicates; lsqr.cpp:451-473 computes the restart residual
+// u = b - A_refine x from it).  Here the whole restart pass, u and A^T u,
+// streams the refine copy (one read of it instead of a read of each), and
+// its ||A||_F feeds the backward-error rule.  Dense (lsqr.cu) and CSR
+// (csr.cu) solves compose their passes with it.
+struct RefinePass : PassOps {
+    PassOps& it;
+    PassOps& re;
+    RefinePass(PassOps& a, PassOps& r) : it(a), re(r) {}
+    PassPlan plan(bool init) override {
+        PassPlan p = init ? re.plan(true) : it.plan(false);
+        p.src = init ? 1 : 0;
+        return p;
+    }
+    tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
+                         const int* skip, cudaStream_t st) override {
+        return pl.src ? re.enqueue(pl, p, u_in, coef, skip, st) : it.enqueue(pl, p, u_in, coef, skip, st);
+    }
+    tomos_status fro2(double* out, const double* d, cudaStream_t st) override { return re.fro2(out, d, st); }
+    uint64_t key() override { return it.key() ^ (re.key() * 0x9E3779B97F4A7C15ull); }
+    int64_t rows() override { return it.rows(); }
+    int64_t cols() override { return it.cols(); }
+    tomos_status prepare(cudaStream_t st) override {
+        tomos_status s = it.prepare(st);
+        return s ? s : re.prepare(st);
+    }
+};
+
 // Block-wide sums (every thread gets the result), fixed order.
 __device__ __forceinline__ double block_sum(double v, double* sm) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
@@ -98,6 +128,16 @@ __device__ __forceinline__ double block_sum_array(const double* part, int64_t np
 // generic two-kernel path): ut = cp A p + cu u_in into ws->u, the
 // partials of A^T ut into ws->qpart and of ||ut||^2 into ws->sspart.
 PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64);
+
+// Options every solve entry accepts (stop rule, iteration counts).
+bool opts_ok(const tomos_lsqr_opts* o, std::string* why);
+
+// Row-sharded solves (comm.cu): fold a pass's partials into ws->shard and
+// sum it across the communicator's ranks; sum any device doubles across them.
+tomos_status enqueue_shard_reduce(tomos_workspace* ws, tomos_comm* c, const float* qpart, int gq,
+                                  int64_t qstride, const double* sspart, int gs, const int* skip,
+                                  cudaStream_t st);
+tomos_status comm_allreduce(tomos_comm* c, double* buf, int64_t count, cudaStream_t st);
 tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A, const PassPlan& pl,
                                 const float* p, const float* u_in, const double* coef,
                                 const int* skip, cudaStream_t st);
@@ -155,6 +195,10 @@ struct tomos_workspace {
     // by every CSR solve and grown as needed.
     void* csc = nullptr;
     size_t csc_bytes = 0;
+    // row-sharded solves: the pass's partial sums folded to n + 1 doubles
+    // (A^T u, ||u||^2), summed across ranks (comm.cu)
+    double* shard = nullptr;
+    tomos_comm* comm = nullptr;  // the running solve's communicator (or NULL)
 
     bool has_precond = false;
     tomos_dense precond{};

@@ -95,10 +95,6 @@ bool resolve_elem(const tomos_dense* A, int32_t tier, Elem* out, std::string* wh
     return resolve_numeric(A->numeric, A->rounded, tier, out, why);
 }
 bool resolve_elem_csr(const tomos_csr* A, int32_t tier, Elem* out, std::string* why) {
-    if (A->numeric == TOMOS_FP16) {
-        *why = "no CSR kernel registered for FP16 values";
-        return false;
-    }
     return resolve_numeric(A->numeric, A->rounded, tier, out, why);
 }
 

@@ -25,14 +25,17 @@
 
 namespace tomos_b200 {
 
-__global__ void cs_hash_kernel(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed,
+// Row i of this matrix is row row0 + i of the whole problem (a row shard);
+// the hash takes the whole problem's row index.
+__global__ void cs_hash_kernel(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed, int64_t row0,
                                int32_t* __restrict__ bucket, int8_t* __restrict__ sign,
                                int32_t* __restrict__ counts) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t b = (int32_t)(splitmix64((uint64_t)i ^ bseed) % (uint64_t)s);
+        const uint64_t gi = (uint64_t)(row0 + i);
+        const int32_t b = (int32_t)(splitmix64(gi ^ bseed) % (uint64_t)s);
         bucket[i] = b;
-        sign[i] = (splitmix64((uint64_t)i ^ sseed) & 1ull) ? (int8_t)1 : (int8_t)-1;
+        sign[i] = (splitmix64(gi ^ sseed) & 1ull) ? (int8_t)1 : (int8_t)-1;
         if (counts) atomicAdd(&counts[b], 1);
     }
 }
@@ -586,12 +589,12 @@ static bool cs_grid(int64_t m, int* g) {
 
 // Steps 1-4 (shared by the dense and CSR owner sums).
 tomos_status cs_bucketize(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed, const CsScratch& c,
-                          cudaStream_t st) {
+                          cudaStream_t st, int64_t row0) {
     int g;
     cs_grid(m, &g);
     TOMOS_CUDA_TRY(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * (s + 1), st));
     TOMOS_CUDA_TRY(cudaMemsetAsync(c.cursor, 0, sizeof(int32_t) * (s + 1), st));
-    cs_hash_kernel<<<g, 256, 0, st>>>(m, s, bseed, sseed, c.bucket, c.sign, c.counts);
+    cs_hash_kernel<<<g, 256, 0, st>>>(m, s, bseed, sseed, row0, c.bucket, c.sign, c.counts);
     TOMOS_LAUNCH_CHECK("cs_hash_kernel");
     cs_scan_kernel<<<1, 1024, 0, st>>>(c.counts, s, c.offsets);
     TOMOS_LAUNCH_CHECK("cs_scan_kernel");
@@ -692,7 +695,7 @@ tomos_status tomos_countsketch_hash(int64_t m, int64_t s, uint64_t bucket_seed, 
     if (!bucket || !sign) return fail(TOMOS_ERR_INVALID, "countsketch_hash: null output");
     int g;
     cs_grid(m, &g);
-    cs_hash_kernel<<<g, 256, 0, as_stream(stream)>>>(m, s, bucket_seed, sign_seed, bucket, sign,
+    cs_hash_kernel<<<g, 256, 0, as_stream(stream)>>>(m, s, bucket_seed, sign_seed, 0, bucket, sign,
                                                      nullptr);
     TOMOS_LAUNCH_CHECK("cs_hash_kernel");
     return TOMOS_OK;
@@ -713,7 +716,7 @@ static tomos_status countsketch_apply(const tomos_dense* A, int32_t tier, int64_
                                       uint64_t bucket_seed, uint64_t sign_seed, double* SA,
                                       int64_t ld_sa, double* fro2, double* colsq, void* scratch,
                                       size_t scratch_bytes, void* stream, uint16_t* plane,
-                                      int64_t ld_plane) {
+                                      int64_t ld_plane, int64_t row0 = 0) {
     if (!A || s <= 0) return fail(TOMOS_ERR_INVALID, "countsketch_apply: need A and s > 0");
     if (A->layout != TOMOS_ROW_MAJOR && A->layout != TOMOS_COL_MAJOR)
         return fail(TOMOS_ERR_INVALID, "countsketch_apply: bad layout");
@@ -746,7 +749,7 @@ static tomos_status countsketch_apply(const tomos_dense* A, int32_t tier, int64_
         return fail(TOMOS_ERR_INVALID, "countsketch_apply: scratch too small (need " +
                                            std::to_string(need.bytes) + " bytes)");
     CsScratch c = cs_layout(scratch, m, s, cs_fro_parts(m, s), col_parts);
-    tomos_status rc = cs_bucketize(m, s, bucket_seed, sign_seed, c, st);
+    tomos_status rc = cs_bucketize(m, s, bucket_seed, sign_seed, c, st, row0);
     if (rc) return rc;
     const void* lo = (e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R) ? dense_lo_plane(A)
                                                                              : nullptr;
@@ -819,6 +822,27 @@ tomos_status tomos_countsketch_apply(const tomos_dense* A, int32_t tier, int64_t
                                      size_t scratch_bytes, void* stream) {
     return countsketch_apply(A, tier, s, bucket_seed, sign_seed, SA, ld_sa, fro2, colsq, scratch,
                              scratch_bytes, stream, nullptr, 0);
+}
+
+tomos_status tomos_countsketch_apply_shard(const tomos_dense* A, int32_t tier, int64_t s,
+                                           uint64_t bucket_seed, uint64_t sign_seed, int64_t row0,
+                                           double* SA, int64_t ld_sa, double* fro2, double* colsq,
+                                           void* plane, int64_t ld_plane, void* scratch,
+                                           size_t scratch_bytes, void* stream) {
+    if (row0 < 0) return fail(TOMOS_ERR_INVALID, "countsketch_apply_shard: negative row0");
+    if (plane) {
+        if (!A || A->numeric != TOMOS_FP32_16 || A->layout != TOMOS_ROW_MAJOR || tier != TOMOS_TIER_HALF)
+            return fail(TOMOS_ERR_INVALID,
+                        "countsketch_apply_shard: a staged plane needs a row-major FP32_16 A at the HALF tier");
+        if (reinterpret_cast<uintptr_t>(plane) % 16 != 0 || ld_plane < A->cols || ld_plane % 8 != 0)
+            return fail(TOMOS_ERR_INVALID,
+                        "countsketch_apply_shard: plane must be 16-byte aligned with ld_plane a multiple of 8 "
+                        "and >= cols");
+        if (!rows_vec_ok(A, nullptr, 2))
+            return fail(TOMOS_ERR_UNSUPPORTED, "countsketch_apply_shard: rows of A not 16-byte aligned");
+    }
+    return countsketch_apply(A, tier, s, bucket_seed, sign_seed, SA, ld_sa, fro2, colsq, scratch,
+                             scratch_bytes, stream, static_cast<uint16_t*>(plane), ld_plane, row0);
 }
 
 tomos_status tomos_countsketch_apply_stage(const tomos_dense* A, int64_t s, uint64_t bucket_seed,

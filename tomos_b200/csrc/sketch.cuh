@@ -32,6 +32,6 @@ CsScratch cs_layout(void* base, int64_t m, int64_t s, int64_t fro_parts, int64_t
 int64_t cs_col_part_rows(int64_t m, int64_t s);
 int64_t cs_fro_parts(int64_t m, int64_t s);
 tomos_status cs_bucketize(int64_t m, int64_t s, uint64_t bseed, uint64_t sseed, const CsScratch& c,
-                          cudaStream_t st);
+                          cudaStream_t st, int64_t row0 = 0);
 
 }  // namespace tomos_b200
