@@ -30,7 +30,7 @@ def values(D):
     return D.view().double().cpu().numpy()
 
 
-def check(orc, A, A0, tier, ta, tb_, shape_b, layouts, beta, rng, bf16_ops=False):
+def check(orc, A, A0, tier, ta, tb_, shape_b, layouts, beta, rng, bf16_ops=False, bpad=None):
     """One product against FP64; returns the max error / bound ratio."""
     lb, lc = layouts
     if A.numeric == NT.FP32:
@@ -42,7 +42,9 @@ def check(orc, A, A0, tier, ta, tb_, shape_b, layouts, beta, rng, bf16_ops=False
     opA = Av.T if ta == T.TRANSPOSE else Av
     M, K = opA.shape
     B0 = rng.standard_normal(shape_b).astype(np.float32)
-    B = dense_f32(B0, lb, pad=3 if beta else 0)  # strided and aligned B
+    if bpad is None:
+        bpad = 3 if beta else 0  # strided and aligned B
+    B = dense_f32(B0, lb, pad=bpad)
     Bv = B0.astype(np.float64)
     if tier == tb.Tier.HALF_OPERANDS:
         Bv = (torch.from_numpy(B0).to(torch.bfloat16 if bf16_ops else torch.float16)).double().numpy()
@@ -135,3 +137,27 @@ def test_mm_reference_routing_and_errors(orc):
     with pytest.raises(tb.TomosError):
         tb.mm_apply(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, A32, B, 0.0, C1,
                     tier=tb.Tier.HALF_OPERANDS)
+
+
+def aligned_pad(inner, mult=8):
+    return (-inner) % mult
+
+
+@pytest.mark.parametrize("numeric,tier", [(NT.FP32, tb.Tier.AUTO), (NT.FP16, tb.Tier.AUTO),
+                                          (NT.FP16, tb.Tier.HALF_OPERANDS), (NT.FP32_16, tb.Tier.ACCURATE),
+                                          (NT.FP32_16, tb.Tier.HALF), (NT.FP32_16, tb.Tier.HALF_OPERANDS),
+                                          (NT.FP32_BF16, tb.Tier.ACCURATE), (NT.FP32_BF16, tb.Tier.HALF_OPERANDS)])
+@pytest.mark.parametrize("la", [L.COL_MAJOR, L.ROW_MAJOR])
+@pytest.mark.parametrize("lb", [L.COL_MAJOR, L.ROW_MAJOR])
+@pytest.mark.parametrize("M,N,K", [(300, 50, 200), (256, 128, 256), (130, 16, 1000)])
+def test_mm_tma_pipeline(orc, numeric, tier, la, lb, M, N, K):
+    """Operands whose lines are 16-byte aligned take the TMA-fed pipeline
+    (tensor copies with zero fill at the ragged edges, converter warps)."""
+    rng = np.random.default_rng(M + N + K + int(numeric) * 3 + int(tier))
+    A0 = (rng.standard_normal((M, K)) * np.where(rng.random((M, K)) < 0.02, 1e-6, 1.0)).astype(np.float32)
+    pad = aligned_pad(K if la == L.ROW_MAJOR else M)
+    A = to_dense(A0, la, numeric, pad=pad)
+    bpad = aligned_pad(N if lb == L.ROW_MAJOR else K)
+    for beta in (0.0, 0.5):
+        check(orc, A, A0, tier, T.NO_TRANSPOSE, T.NO_TRANSPOSE, (K, N), (lb, L.COL_MAJOR), beta, rng,
+              bf16_ops=numeric == NT.FP32_BF16, bpad=bpad)

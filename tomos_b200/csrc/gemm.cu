@@ -49,6 +49,9 @@
 #include <string>
 #include <utility>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "mbarrier.cuh"
 
@@ -79,7 +82,8 @@ struct GemmArgs {
     int a_kc, b_kc;    // 1: the operand's lines run along K (else along M / N)
     int a_vec, b_vec;  // 1: 16-byte (or 8-byte) vector loads are aligned
     int bn;            // columns of op(B) per CTA: 16, 32, 64 or 128
-    int stages;
+    int stages;        // operand stages
+    int raw_stages;    // raw (copied) stages of the TMA-fed pipeline
     int* err;
 };
 
@@ -382,6 +386,90 @@ __device__ __forceinline__ uint64_t tile_desc(uint32_t base, int s, int R) {
     return smem_desc(base + (uint32_t)(2 * s) * lbo, lbo, 128u);
 }
 
+// The MMA issuer (one thread): per stage, 4 K-steps x the mode's terms,
+// then a commit that frees the stage; a final commit marks the
+// accumulator complete (or the work stopped).
+template <int MODE, bool BF>
+__device__ __forceinline__ void gemm_issue_mmas(const GemmArgs& g, uint8_t* ops, uint32_t stage_bytes,
+                                                uint32_t a_bytes, uint32_t b_bytes, uint64_t* full, uint64_t* empty,
+                                                uint64_t* done, uint32_t tmem, int nk, volatile int* abort_flag) {
+    using T = ModeTraits<MODE>;
+    const int S = g.stages, BN = g.bn;
+    uint32_t idesc = (1u << 4);  // FP32 accumulator
+    const uint32_t fmt = MODE == kPure16 ? (BF ? 1u : 0u) : 2u;
+    idesc |= fmt << 7;
+    idesc |= fmt << 10;
+    // bits 15, 16 (A, B major) stay 0: K-major operands
+    idesc |= ((uint32_t)BN >> 3) << 17;
+    idesc |= ((uint32_t)kGemmM >> 4) << 24;
+    uint32_t acc = 0;
+    for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % S;
+        if (!mbar_wait(&full[s], (uint32_t)((kt / S) & 1))) {
+            atomicExch(g.err, 2);
+            *abort_flag = 1;
+        }
+        if (*abort_flag) break;
+        tc_fence_after();
+        const uint32_t st = smem_addr(ops + (size_t)s * stage_bytes);
+        const uint32_t a0 = st, a1 = st + a_bytes;
+        const uint32_t b0 = st + T::na * a_bytes, b1 = b0 + b_bytes;
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+            const uint64_t da0 = tile_desc(a0, ks, kGemmM);
+            const uint64_t db0 = tile_desc(b0, ks, BN);
+            mma_issue(MODE != kPure16, tmem, da0, db0, idesc, acc);
+            acc = 1;
+            if constexpr (MODE != kPure16) {
+                const uint64_t db1 = tile_desc(b1, ks, BN);
+                mma_issue(1, tmem, da0, db1, idesc, 1);
+            }
+            if constexpr (MODE == kTf32x3) {
+                const uint64_t da1 = tile_desc(a1, ks, kGemmM);
+                mma_issue(1, tmem, da1, db0, idesc, 1);
+            }
+        }
+        mma_commit(&empty[s]);  // frees the stage once these MMAs are done
+    }
+    mma_commit(done);
+}
+
+// Epilogue: worker warp w (of NW) reads TMEM lanes 32 (w % 4) .. + 31
+// (rows of the tile) and every (NW / 4)-th 8-column chunk from chunk w / 4,
+// and writes alpha acc + beta C; the MMA warp (warp NW) waits for its own
+// MMAs before the memory is freed.
+template <int NW>
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, int warp, int lane, int64_t m0, int64_t n0,
+                                              uint32_t tmem, uint64_t* done, volatile int* abort_flag) {
+    const int BN = g.bn;
+    if (warp < NW) {
+        if (!mbar_wait(done, 0u)) {
+            if (lane == 0) atomicExch(g.err, 3);
+            *abort_flag = 1;
+        }
+        tc_fence_after();
+        const int q = warp & 3, h = warp >> 2;
+        const int64_t i = m0 + q * 32 + lane;
+        const bool ok = !*abort_flag;
+        for (int c = h * 8; c < BN; c += (NW / 4) * 8) {
+            uint32_t r[8];
+            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, r);
+            if (!ok || i >= g.M) continue;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int64_t j = n0 + c + e;
+                if (j >= g.N) break;
+                float* cp = g.c + (size_t)(i * g.c_si + j * g.c_sj);
+                double y = g.alpha * (double)u2f(r[e]);
+                if (g.beta != 0.0) y += g.beta * (double)*cp;
+                *cp = (float)y;
+            }
+        }
+    } else if (warp == NW) {
+        if (!mbar_wait(done, 0u) && lane == 0) atomicExch(g.err, 4);
+    }
+}
+
 template <Elem E, int MODE>
 __global__ void __launch_bounds__(kGemmThreads, 1) gemm_tc_kernel(GemmArgs g) {
     using T = ModeTraits<MODE>;
@@ -440,80 +528,353 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_tc_kernel(GemmArgs g) {
             if (lane == 0) mbar_arrive(&full[s]);
         }
     } else if (lane == 0) {
-        // the MMA issuer
-        uint32_t idesc = (1u << 4);  // FP32 accumulator
-        const uint32_t fmt = MODE == kPure16 ? (BF ? 1u : 0u) : 2u;
-        idesc |= fmt << 7;
-        idesc |= fmt << 10;
-        // bits 15, 16 (A, B major) stay 0: K-major operands
-        idesc |= ((uint32_t)BN >> 3) << 17;
-        idesc |= ((uint32_t)kGemmM >> 4) << 24;
-        uint32_t acc = 0;
-        for (int kt = 0; kt < nk; ++kt) {
-            const int s = kt % S;
-            if (!mbar_wait(&full[s], (uint32_t)((kt / S) & 1))) {
-                atomicExch(g.err, 2);
-                *abort_flag = 1;
-            }
-            if (*abort_flag) break;
-            tc_fence_after();
-            const uint32_t st = smem_addr(smem + (size_t)s * stage_bytes);
-            const uint32_t a0 = st, a1 = st + a_bytes;
-            const uint32_t b0 = st + T::na * a_bytes, b1 = b0 + b_bytes;
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-                const uint64_t da0 = tile_desc(a0, ks, kGemmM);
-                const uint64_t db0 = tile_desc(b0, ks, BN);
-                mma_issue(MODE != kPure16, tmem, da0, db0, idesc, acc);
-                acc = 1;
-                if constexpr (MODE != kPure16) {
-                    const uint64_t db1 = tile_desc(b1, ks, BN);
-                    mma_issue(1, tmem, da0, db1, idesc, 1);
-                }
-                if constexpr (MODE == kTf32x3) {
-                    const uint64_t da1 = tile_desc(a1, ks, kGemmM);
-                    mma_issue(1, tmem, da1, db0, idesc, 1);
-                }
-            }
-            mma_commit(&empty[s]);  // frees the stage once these MMAs are done
-        }
-        mma_commit(done);  // the accumulator is complete (or the work stopped)
+        gemm_issue_mmas<MODE, BF>(g, smem, stage_bytes, a_bytes, b_bytes, full, empty, done, tmem, nk, abort_flag);
     }
-
-    // epilogue: producer warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows)
-    // and half (w / 4) of the columns
-    if (warp < kProducerWarps) {
-        if (!mbar_wait(done, 0u)) {
-            if (lane == 0) atomicExch(g.err, 3);
-            *abort_flag = 1;
-        }
-        tc_fence_after();
-        const int q = warp & 3, h = warp >> 2;
-        const int64_t i = m0 + q * 32 + lane;
-        const int c_lo = h * (BN >> 1), c_hi = c_lo + (BN >> 1);
-        const bool ok = !*abort_flag;
-        for (int c = c_lo; c < c_hi; c += 8) {
-            uint32_t r[8];
-            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, r);
-            if (!ok || i >= g.M) continue;
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int64_t j = n0 + c + e;
-                if (j >= g.N) break;
-                float* cp = g.c + (size_t)(i * g.c_si + j * g.c_sj);
-                double y = g.alpha * (double)u2f(r[e]);
-                if (g.beta != 0.0) y += g.beta * (double)*cp;
-                *cp = (float)y;
-            }
-        }
-    } else {
-        // the MMA warp waits for its own MMAs before freeing the memory
-        if (!mbar_wait(done, 0u) && lane == 0) atomicExch(g.err, 4);
-    }
+    gemm_epilogue<kProducerWarps>(g, warp, lane, m0, n0, tmem, done, abort_flag);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (warp == kProducerWarps)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// ------------------------------------------------------- TMA-fed pipeline
+//
+// When the operands' lines are 16-byte aligned (base and stride), one
+// thread streams them with 2-D tensor copies (cp.async.bulk.tensor, zero
+// fill past the edges) into a ring of raw stages, and the 8 producer warps
+// become converters: raw shared memory -> decoded, split operand tiles.
+// Raw tiles of K-contiguous lines are swizzled by the copy (128-byte rows:
+// 16-byte chunk c of row r lands at chunk c ^ (r % 8); 64-byte rows: chunk
+// c ^ ((r / 2) % 4)), so eight converter lanes reading one chunk of eight
+// consecutive lines hit eight different bank groups; raw tiles of
+// M- (N-) contiguous lines are stored k-row by k-row.
+
+struct GemmMaps {
+    CUtensorMap a_hi, a_lo, b;
+};
+
+constexpr int kConvWarps = 16;                   // converter warps
+constexpr int kConv = kConvWarps * 32;
+constexpr int kTmaThreads = kConv + 64;          // + the MMA warp + the copy warp
+constexpr int kMmaWarp = kConvWarps, kCopyWarp = kConvWarps + 1;
+constexpr int kConvItems = kGemmM * 8 / kConv;   // A units a converter thread owns (2)
+
+__device__ __forceinline__ void tma2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+template <Elem E, int MODE>
+struct RawTraits {
+    using T = ModeTraits<MODE>;
+    static constexpr int es = E == Elem::F32 ? 4 : 2;               // source bytes
+    static constexpr int row = T::kpl * es;                           // bytes of a K-line
+    static constexpr int a_plane = kGemmM * row;                      // one plane of A
+    static constexpr int planes = two_planes<E>() ? 2 : 1;
+    static constexpr int a_bytes = a_plane * planes;
+};
+
+// The 16-bit HALF-tier operand bits of 8 FP32_16 / FP16 / bf16 words:
+// control-0 FP32_16 words are fp16 already, so only flagged words (bit 0,
+// about 0.35 % of them) go through half_only_bits, one at a time.
+template <Elem E>
+__device__ __forceinline__ uint4 half_operands(uint4 h) {
+    if constexpr (E == Elem::H16) {
+        uint32_t m = (h.x & 0x10001u) | ((h.y & 0x10001u) << 1) | ((h.z & 0x10001u) << 2) | ((h.w & 0x10001u) << 3);
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            const int e = b & 3, sh = b & 16;
+            uint32_t w = e == 0 ? h.x : e == 1 ? h.y : e == 2 ? h.z : h.w;
+            const uint32_t fixed = half_only_bits((w >> sh) & 0xFFFFu);
+            w = (w & ~(0xFFFFu << sh)) | (fixed << sh);
+            if (e == 0) h.x = w;
+            else if (e == 1) h.y = w;
+            else if (e == 2) h.z = w;
+            else h.w = w;
+        }
+    }
+    return h;
+}
+
+template <bool BF>
+__device__ __forceinline__ uint32_t pack16x2(float a, float b) {
+    if constexpr (BF) {
+        const __nv_bfloat162 t = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&t);
+    } else {
+        const __half2 t = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&t);
+    }
+}
+
+// Converts one raw stage into the operand tiles of one stage.  ra_off /
+// rb_off: each owned unit's byte offset in the raw tiles (first element
+// for lines strided along K), oa_off / ob_off: in the operand tiles.
+template <Elem E, int MODE, bool BF>
+__device__ __forceinline__ void convert_stage(const GemmArgs& g, const uint8_t* ra, const uint8_t* rb, uint8_t* oa0,
+                                              uint8_t* oa1, uint8_t* ob0, uint8_t* ob1, const uint32_t* ra_off,
+                                              const uint32_t* oa_off, const uint32_t* rb_off,
+                                              const uint32_t* ob_off, int nb_items) {
+    using T = ModeTraits<MODE>;
+    using RT = RawTraits<E, MODE>;
+    constexpr int R = kGemmM;
+#pragma unroll
+    for (int j = 0; j < kConvItems; ++j) {
+        const uint8_t* src = ra + ra_off[j];
+        if constexpr (MODE == kPure16) {
+            uint4 h;
+            if (g.a_kc) {
+                h = *reinterpret_cast<const uint4*>(src);
+            } else {
+                const uint16_t* c = reinterpret_cast<const uint16_t*>(src);
+                h.x = (uint32_t)c[0] | ((uint32_t)c[R] << 16);
+                h.y = (uint32_t)c[2 * R] | ((uint32_t)c[3 * R] << 16);
+                h.z = (uint32_t)c[4 * R] | ((uint32_t)c[5 * R] << 16);
+                h.w = (uint32_t)c[6 * R] | ((uint32_t)c[7 * R] << 16);
+            }
+            *reinterpret_cast<uint4*>(oa0 + oa_off[j]) = half_operands<E>(h);
+        } else {
+            float v[4];
+            if constexpr (E == Elem::F32) {
+                if (g.a_kc) {
+                    const float4 f = *reinterpret_cast<const float4*>(src);
+                    v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+                } else {
+                    const float* c = reinterpret_cast<const float*>(src);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) v[e] = c[e * R];
+                }
+            } else {
+                uint32_t hw[4], lw[4] = {0u, 0u, 0u, 0u};
+                if (g.a_kc) {
+                    const uint2 h = *reinterpret_cast<const uint2*>(src);
+                    hw[0] = h.x & 0xFFFFu; hw[1] = h.x >> 16; hw[2] = h.y & 0xFFFFu; hw[3] = h.y >> 16;
+                    if constexpr (RT::planes == 2) {
+                        const uint2 q = *reinterpret_cast<const uint2*>(src + RT::a_plane);
+                        lw[0] = q.x & 0xFFFFu; lw[1] = q.x >> 16; lw[2] = q.y & 0xFFFFu; lw[3] = q.y >> 16;
+                    }
+                } else {
+                    const uint16_t* c = reinterpret_cast<const uint16_t*>(src);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        hw[e] = c[e * R];
+                        if constexpr (RT::planes == 2) lw[e] = c[e * R + RT::a_plane / 2];
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if constexpr (E == Elem::A16) v[e] = decode_fp32_16_exact_nb(hw[e], lw[e]);
+                    else v[e] = decode16<E>(hw[e], lw[e]);
+                }
+            }
+            if constexpr (MODE == kTf32x2) {
+                *reinterpret_cast<uint4*>(oa0 + oa_off[j]) = make_uint4(f2u(v[0]), f2u(v[1]), f2u(v[2]), f2u(v[3]));
+            } else {
+                uint32_t bg[4], sm[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) split_tf32(v[e], bg[e], sm[e]);
+                *reinterpret_cast<uint4*>(oa0 + oa_off[j]) = make_uint4(bg[0], bg[1], bg[2], bg[3]);
+                *reinterpret_cast<uint4*>(oa1 + oa_off[j]) = make_uint4(sm[0], sm[1], sm[2], sm[3]);
+            }
+        }
+    }
+    const int BN = g.bn;
+#pragma unroll
+    for (int j = 0; j < kConvItems; ++j) {
+        if (j >= nb_items) break;
+        const uint8_t* src = rb + rb_off[j];
+        float v[8];
+        if (g.b_kc) {
+            if constexpr (T::epu == 8) {
+                // two 16-byte chunks of a 128-byte swizzled row: rb_off holds the
+                // first; the second is chunk c0 + 1 ^ (r % 8), kept in bits 16+
+                const float4 f0 = *reinterpret_cast<const float4*>(rb + (rb_off[j] & 0xFFFFu));
+                const float4 f1 = *reinterpret_cast<const float4*>(rb + (rb_off[j] >> 16));
+                v[0] = f0.x; v[1] = f0.y; v[2] = f0.z; v[3] = f0.w;
+                v[4] = f1.x; v[5] = f1.y; v[6] = f1.z; v[7] = f1.w;
+            } else {
+                const float4 f = *reinterpret_cast<const float4*>(src);
+                v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+            }
+        } else {
+            const float* c = reinterpret_cast<const float*>(src);
+#pragma unroll
+            for (int e = 0; e < T::epu; ++e) v[e] = c[e * BN];
+        }
+        if constexpr (MODE == kPure16) {
+            *reinterpret_cast<uint4*>(ob0 + ob_off[j]) =
+                make_uint4(pack16x2<BF>(v[0], v[1]), pack16x2<BF>(v[2], v[3]), pack16x2<BF>(v[4], v[5]),
+                           pack16x2<BF>(v[6], v[7]));
+        } else {
+            uint32_t bg[4], sm[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) split_tf32(v[e], bg[e], sm[e]);
+            *reinterpret_cast<uint4*>(ob0 + ob_off[j]) = make_uint4(bg[0], bg[1], bg[2], bg[3]);
+            *reinterpret_cast<uint4*>(ob1 + ob_off[j]) = make_uint4(sm[0], sm[1], sm[2], sm[3]);
+        }
+    }
+}
+
+// Unit (line r, 16-byte operand chunk u) of converter item `it`: eight
+// consecutive lanes take eight consecutive lines of one chunk.
+__device__ __forceinline__ void unit_of(int it, int R, bool kc, int& r, int& u) {
+    if (kc) {
+        r = (it & 7) | ((it >> 6) << 3);
+        u = (it >> 3) & 7;
+    } else {
+        r = it % R;
+        u = it / R;
+    }
+}
+
+template <Elem E, int MODE>
+__global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_kernel(GemmArgs g, const __grid_constant__ GemmMaps maps) {
+    using T = ModeTraits<MODE>;
+    using RT = RawTraits<E, MODE>;
+    constexpr bool BF = (E == Elem::B16);
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte alignment for the 128-byte swizzle of the raw tiles
+    uint8_t* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
+    const int S = g.stages, RS = g.raw_stages, BN = g.bn;
+    const uint32_t rb_bytes = (uint32_t)BN * T::kpl * 4u;
+    const uint32_t raw_bytes = RT::a_bytes + rb_bytes;
+    const uint32_t a_bytes = kGemmM * kLineBytes, b_bytes = (uint32_t)BN * kLineBytes;
+    const uint32_t stage_bytes = T::na * a_bytes + T::nb * b_bytes;
+    uint8_t* ops = smem + (size_t)RS * raw_bytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(ops + (size_t)S * stage_bytes);
+    uint64_t* empty = full + kMaxStages;
+    uint64_t* rfull = empty + kMaxStages;
+    uint64_t* rempty = rfull + kMaxStages;
+    uint64_t* done = rempty + kMaxStages;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t m0 = (int64_t)blockIdx.x * kGemmM, n0 = (int64_t)blockIdx.y * BN;
+    const int nk = (int)((g.K + T::kpl - 1) / T::kpl);
+    const uint32_t ncols = BN <= 32 ? 32u : (uint32_t)BN;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], kConvWarps);
+            mbar_init(&empty[s], 1);
+        }
+        for (int s = 0; s < RS; ++s) {
+            mbar_init(&rfull[s], 1);
+            mbar_init(&rempty[s], kConvWarps);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+    }
+    if (warp == kMmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp < kConvWarps) {
+        const int pt = threadIdx.x;
+        // the stage-invariant offsets of this thread's units
+        uint32_t ra_off[kConvItems], oa_off[kConvItems], rb_off[kConvItems], ob_off[kConvItems];
+#pragma unroll
+        for (int j = 0; j < kConvItems; ++j) {
+            int r, u;
+            unit_of(pt + kConv * j, kGemmM, g.a_kc, r, u);
+            oa_off[j] = kmajor_off(r, u, kGemmM);
+            if (!g.a_kc) ra_off[j] = (uint32_t)((u * T::epu * kGemmM + r) * RT::es);
+            else if (RT::row == 128) ra_off[j] = (uint32_t)(r * 128 + ((u ^ (r & 7)) << 4));
+            else ra_off[j] = (uint32_t)(r * 64 + ((((u >> 1) ^ ((r >> 1) & 3)) << 4) | ((u & 1) << 3)));
+        }
+        const int nb_items = (BN * 8 - pt + kConv - 1) / kConv;
+#pragma unroll
+        for (int j = 0; j < kConvItems; ++j) {
+            int r, u;
+            unit_of(pt + kConv * j, BN, g.b_kc, r, u);
+            ob_off[j] = kmajor_off(r, u, BN);
+            if (!g.b_kc) {
+                rb_off[j] = (uint32_t)((u * T::epu * BN + r) * 4);
+            } else if (T::epu == 8) {
+                const uint32_t base = (uint32_t)((u >> 2) * BN * 128 + r * 128);
+                const int c0 = 2 * (u & 3);
+                rb_off[j] = (base + ((c0 ^ (r & 7)) << 4)) | ((base + (((c0 + 1) ^ (r & 7)) << 4)) << 16);
+            } else {
+                rb_off[j] = (uint32_t)(r * 128 + ((u ^ (r & 7)) << 4));
+            }
+        }
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % S, rs = kt % RS;
+            bool ok = mbar_wait(&rfull[rs], (uint32_t)((kt / RS) & 1));
+            if (ok && kt >= S) ok = mbar_wait(&empty[s], (uint32_t)((kt / S - 1) & 1));
+            if (!ok) {
+                if (lane == 0) atomicExch(g.err, 1);
+                *abort_flag = 1;
+            }
+            if (*abort_flag) break;
+            const uint8_t* ra = smem + (size_t)rs * raw_bytes;
+            uint8_t* st = ops + (size_t)s * stage_bytes;
+            uint8_t* bt = st + T::na * a_bytes;
+            convert_stage<E, MODE, BF>(g, ra, ra + RT::a_bytes, st, st + a_bytes, bt, bt + b_bytes, ra_off, oa_off,
+                                       rb_off, ob_off, nb_items);
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&full[s]);
+                mbar_arrive(&rempty[rs]);
+            }
+        }
+    } else if (warp == kCopyWarp) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int kt = 0; kt < nk; ++kt) {
+                const int rs = kt % RS;
+                if (kt >= RS && !mbar_wait(&rempty[rs], (uint32_t)((kt / RS - 1) & 1))) {
+                    atomicExch(g.err, 5);
+                    *abort_flag = 1;
+                }
+                if (*abort_flag) break;
+                const uint32_t ra = smem_addr(smem + (size_t)rs * raw_bytes);
+                const int k0 = kt * T::kpl;
+                mbar_expect_tx(&rfull[rs], raw_bytes);
+                const int am = (int)m0, bn0 = (int)n0;
+                if (g.a_kc) {
+                    tma2d(ra, &maps.a_hi, k0, am, &rfull[rs]);
+                    if constexpr (RT::planes == 2) tma2d(ra + RT::a_plane, &maps.a_lo, k0, am, &rfull[rs]);
+                } else {
+                    tma2d(ra, &maps.a_hi, am, k0, &rfull[rs]);
+                    if constexpr (RT::planes == 2) tma2d(ra + RT::a_plane, &maps.a_lo, am, k0, &rfull[rs]);
+                }
+                const uint32_t rbs = ra + RT::a_bytes;
+                if (g.b_kc) {
+                    tma2d(rbs, &maps.b, k0, bn0, &rfull[rs]);
+                    if constexpr (T::kpl == 64) tma2d(rbs + (uint32_t)BN * 128u, &maps.b, k0 + 32, bn0, &rfull[rs]);
+                } else {
+                    tma2d(rbs, &maps.b, bn0, k0, &rfull[rs]);
+                }
+                issued = kt + 1;
+            }
+            // no copy may still be writing this CTA's memory when it exits
+            for (int kt = issued > RS ? issued - RS : 0; kt < issued; ++kt)
+                if (!mbar_wait(&rfull[kt % RS], (uint32_t)((kt / RS) & 1))) atomicExch(g.err, 6);
+        }
+    } else if (lane == 0) {
+        gemm_issue_mmas<MODE, BF>(g, ops, stage_bytes, a_bytes, b_bytes, full, empty, done, tmem, nk, abort_flag);
+    }
+    gemm_epilogue<kConvWarps>(g, warp, lane, m0, n0, tmem, done, abort_flag);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == kMmaWarp)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
@@ -546,16 +907,89 @@ int stage_count(int bn) {
     return s > kMaxStages ? kMaxStages : s;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// A 2-D map of `outer` lines of `inner` elements, line stride `stride`
+// elements; false when the copy engine cannot address it (16-byte base and
+// stride) or the driver refuses it.
+bool encode_2d(CUtensorMap* map, CUtensorMapDataType dt, int es, const void* base, int64_t inner, int64_t outer,
+               int64_t stride, uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle sw) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || !base || reinterpret_cast<uintptr_t>(base) % 16 != 0 || (stride * es) % 16 != 0) return false;
+    if (stride < inner) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)(stride * es)};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <Elem E, int MODE>
+bool make_maps(const GemmArgs& g, GemmMaps* maps) {
+    using T = ModeTraits<MODE>;
+    using RT = RawTraits<E, MODE>;
+    const CUtensorMapDataType adt = E == Elem::F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+    const CUtensorMapSwizzle ksw = RT::row == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+    const void* planes[2] = {g.a_hi, g.a_lo};
+    CUtensorMap* amaps[2] = {&maps->a_hi, &maps->a_lo};
+    for (int p = 0; p < RT::planes; ++p) {
+        const bool ok = g.a_kc ? encode_2d(amaps[p], adt, RT::es, planes[p], g.K, g.M, g.a_si, T::kpl, kGemmM, ksw)
+                               : encode_2d(amaps[p], adt, RT::es, planes[p], g.M, g.K, g.a_sl, kGemmM, T::kpl,
+                                           CU_TENSOR_MAP_SWIZZLE_NONE);
+        if (!ok) return false;
+    }
+    if (RT::planes == 1) maps->a_lo = maps->a_hi;
+    return g.b_kc ? encode_2d(&maps->b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, g.b, g.K, g.N, g.b_sj, 32, (uint32_t)g.bn,
+                              CU_TENSOR_MAP_SWIZZLE_128B)
+                  : encode_2d(&maps->b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, g.b, g.N, g.K, g.b_sl, (uint32_t)g.bn,
+                              T::kpl, CU_TENSOR_MAP_SWIZZLE_NONE);
+}
+
+constexpr int kTmaSmemBudget = 224 * 1024;
+
 template <Elem E, int MODE>
 tomos_status launch_gemm(GemmArgs& g, cudaStream_t st) {
     using T = ModeTraits<MODE>;
+    using RT = RawTraits<E, MODE>;
+    const dim3 grid((unsigned)((g.M + kGemmM - 1) / kGemmM), (unsigned)((g.N + g.bn - 1) / g.bn));
+    const size_t stage = (size_t)T::na * kGemmM * kLineBytes + (size_t)T::nb * g.bn * kLineBytes;
+    const size_t bars = (5 * kMaxStages + 1) * sizeof(uint64_t) + 16;
+    GemmMaps maps;
+    if (make_maps<E, MODE>(g, &maps)) {
+        const size_t raw = (size_t)RT::a_bytes + (size_t)g.bn * T::kpl * 4;
+        static const int pairs[][2] = {{2, 4}, {3, 3}, {2, 3}, {3, 2}, {2, 2}};
+        for (const auto& pr : pairs) {
+            const size_t smem = (size_t)pr[0] * stage + (size_t)pr[1] * raw + bars + 1024;
+            if (smem > (size_t)kTmaSmemBudget) continue;
+            g.stages = pr[0];
+            g.raw_stages = pr[1];
+            auto kern = gemm_tma_kernel<E, MODE>;
+            TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            kern<<<grid, kTmaThreads, smem, st>>>(g, maps);
+            TOMOS_LAUNCH_CHECK("gemm_tma_kernel");
+            return TOMOS_OK;
+        }
+    }
+    // direct loads (operands the copy engine cannot address)
     g.stages = stage_count<MODE>(g.bn);
+    g.raw_stages = 0;
     if (g.stages < 2) return fail(TOMOS_ERR_UNSUPPORTED, "mm: shared memory");
-    const size_t smem = (size_t)g.stages * (T::na * kGemmM * kLineBytes + T::nb * g.bn * kLineBytes) +
-                        (2 * kMaxStages + 1) * sizeof(uint64_t) + 16;
+    const size_t smem = (size_t)g.stages * stage + bars;
     auto kern = gemm_tc_kernel<E, MODE>;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const dim3 grid((unsigned)((g.M + kGemmM - 1) / kGemmM), (unsigned)((g.N + g.bn - 1) / g.bn));
     kern<<<grid, kGemmThreads, smem, st>>>(g);
     TOMOS_LAUNCH_CHECK("gemm_tc_kernel");
     return TOMOS_OK;
