@@ -242,6 +242,47 @@ def ls_solution_rows(torch, A32, b, world, blk=1 << 17):
     return torch.linalg.solve_triangular(R[:n, :n], R[:n, n:], upper=True).squeeze(1)
 
 
+def mm_numbers(tb, torch, Ap, m, n, sq=8192, rhs=16):
+    """mm_apply throughput: C = A B with the LSQR matrix (packed, row-major)
+    and `rhs` columns per tier (GB/s of A's storage read + C written), and
+    a square sq^3 product per tier from column-major operands (TF/s of
+    2 sq^3; the 16-bit-operand tier against the measured bf16 dense peak,
+    the TF32 tiers against half of it, the TF32 rate)."""
+    T, L = tb.TransposeType, tb.Layout
+    out = {}
+    B = tb.Dense.from_tensor(torch.randn(n, rhs, device="cuda"), L.COL_MAJOR)
+    C = tb.Dense.from_tensor(torch.zeros(m, rhs, device="cuda"), L.COL_MAJOR)
+    for name, tier, eb in (("half_operands", tb.Tier.HALF_OPERANDS, 2), ("half", tb.Tier.HALF, 2),
+                           ("accurate", tb.Tier.ACCURATE, 4)):
+        f = (lambda tier=tier: tb.mm_apply(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, Ap, B, 0.0, C,
+                                          tier=tier))
+        ms, _ = time_steps(torch, f, 5, 2)
+        gb = (eb * m * n + 4.0 * (m * rhs + n * rhs)) / (ms * 1e-3) / 1e9
+        out[f"rhs{rhs}_{name}"] = {"ms": ms, "gbs": gb, "frac_of_measured_hbm": gb / measured_peak()[0]}
+    del B, C
+    A32 = tb.Dense.from_tensor(torch.randn(sq, sq, device="cuda"), L.COL_MAJOR)
+    P = tb.pack(A32, tb.NumericType.FP32_16)
+    B = tb.Dense.from_tensor(torch.randn(sq, sq, device="cuda"), L.COL_MAJOR)
+    C = tb.Dense.from_tensor(torch.zeros(sq, sq, device="cuda"), L.COL_MAJOR)
+    bf16 = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("bf16_tflops") \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1590.0
+    for name, A, tier, peak in (("fp32_16_half_operands", P, tb.Tier.HALF_OPERANDS, bf16),
+                                ("fp32_16_half", P, tb.Tier.HALF, bf16 / 2),
+                                ("fp32_16_accurate", P, tb.Tier.ACCURATE, bf16 / 2),
+                                ("fp32", A32, tb.Tier.AUTO, bf16 / 2)):
+        f = (lambda A=A, tier=tier: tb.mm_apply(tb.Device.CUDA, T.NO_TRANSPOSE, T.NO_TRANSPOSE, 1.0, A, B, 0.0, C,
+                                                tier=tier))
+        ms, _ = time_steps(torch, f, 3, 2)
+        tf = 2.0 * sq ** 3 / (ms * 1e-3) / 1e12
+        out[f"sq{sq}_{name}"] = {"ms": ms, "tflops": tf, "frac_of_peak": tf / peak,
+                                 "peak_tflops": peak}
+    out["note"] = ("tensor-core products per tier: half_operands 1 fp16 MMA, half 2 TF32 MMAs, accurate / fp32 "
+                   "3 TF32 MMAs; TFLOP/s counts 2 M N K once")
+    del A32, P, B, C
+    torch.cuda.empty_cache()
+    return out
+
+
 def count_launches(torch, fn):
     """Kernels of this library (namespace tomos_b200) one call of fn launches."""
     from torch.profiler import ProfilerActivity, profile
@@ -356,6 +397,11 @@ def run_ours(args):
             gemv[f"{name}_{'t' if tr == tb.TransposeType.TRANSPOSE else 'n'}"] = {
                 "ms": ms_g, "gbs": gb, "frac_of_measured_hbm": gb / measured_peak()[0]}
 
+    # mm_apply (tomos_mm, tcgen05): the multi-RHS product of the same packed
+    # matrix with 16 columns (HBM-bound: GB/s of the storage read), and a
+    # square 8192^3 GEMM per tier (tensor-bound: 2 M N K / time)
+    mm = mm_numbers(tb, torch, Ap, m, n)
+
     # roofline of the dominant kernel (the fused pass over the wh plane):
     # one profiled solve times every pass with CUDA events on its stream.
     gpu_solve.profile = True
@@ -438,6 +484,7 @@ def run_ours(args):
                          "fused_pass_fp32_16_exact_fp64acc": ach_init,
                          "pass_ms_half": pass_ms, "pass_ms_fp32": pass_ms_f,
                          "standalone": gemv},
+            "mm": mm,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
                          "kernel": "fused_rows_mma_kernel (staged fp16 plane, tensor cores; one LSQR "
