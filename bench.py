@@ -283,6 +283,39 @@ def mm_numbers(tb, torch, Ap, m, n, sq=8192, rhs=16):
     return out
 
 
+def adjoint_numbers(tb, torch, m=200_000, n=500, K=8):
+    """The adjoint workload (lambda_k = (A^T A)^{-1} g_k, K = 8 right-hand
+    sides, A 200,000 x 500 FP32 ~ N(0,1), the sketch-QR preconditioner, CG
+    to 1e-7): all K at once (tomos_lsqr_adjoint_batch_dense: two tcgen05
+    products over A an iteration, shared) against K one-column solves (one
+    fused pass over A an iteration each).  Device time from the solver's
+    own events; achieved = the products' bytes (4 m n per product) / time."""
+    NT, L = tb.NumericType, tb.Layout
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    A32 = torch.randn(m, n, device="cuda", generator=g)
+    A = tb.Dense(NT.FP32, L.ROW_MAJOR, (m, n), n, A32.view(-1))
+    G = torch.randn(n, K, device="cuda", generator=g)
+    ws = tb.create_lsqr_workspace(None, (m, n), NT.FP32, NT.FP64)
+    SA, _, _ = tb.apply_count_sketch(A, 4 * n, with_colsq=True)
+    tb.add_precond(tb.generate_sketch_qr_precond(SA), ws)
+    for _ in range(2):  # the second of each is kept
+        _, reps = tb.lsqr_adjoint_batch(A, G, ws, tol=1e-7, max_iters=1000)
+        single = [tb.lsqr_adjoint(A, G[:, k].contiguous(), ws, tol=1e-7, max_iters=1000)[1] for k in range(K)]
+    ms_b = reps[0]["elapsed_ms"]
+    ms_s = sum(r["elapsed_ms"] for r in single)
+    products = reps[0]["half_passes"]
+    gb = products * 4.0 * m * n / (ms_b * 1e-3) / 1e9
+    del A32, ws
+    torch.cuda.empty_cache()
+    return {"workload": f"{m}x{n} FP32, {K} right-hand sides, CG to 1e-7, sketch-QR preconditioned",
+            "batched_ms": ms_b, "one_column_solves_ms": ms_s, "speedup": ms_s / ms_b,
+            "iterations": [r["iterations"] for r in reps], "products_over_A": products,
+            "achieved_gbs": gb, "frac_of_measured_hbm": gb / measured_peak()[0],
+            "note": "batched: Q = A P and W = A^T Q for all K directions by tomos_mm_ex "
+                    "(accurate TF32x3 tier, split-K for A^T Q)"}
+
+
 def count_launches(torch, fn):
     """Kernels of this library (namespace tomos_b200) one call of fn launches."""
     from torch.profiler import ProfilerActivity, profile
@@ -401,6 +434,7 @@ def run_ours(args):
     # matrix with 16 columns (HBM-bound: GB/s of the storage read), and a
     # square 8192^3 GEMM per tier (tensor-bound: 2 M N K / time)
     mm = mm_numbers(tb, torch, Ap, m, n)
+    adjoint = adjoint_numbers(tb, torch)
 
     # roofline of the dominant kernel (the fused pass over the wh plane):
     # one profiled solve times every pass with CUDA events on its stream.
@@ -485,6 +519,7 @@ def run_ours(args):
                          "pass_ms_half": pass_ms, "pass_ms_fp32": pass_ms_f,
                          "standalone": gemv},
             "mm": mm,
+            "adjoint": adjoint,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
                          "kernel": "fused_rows_mma_kernel (staged fp16 plane, tensor cores; one LSQR "

@@ -183,11 +183,25 @@ tomos_status tomos_gemv_no_alloc(int32_t trans, double alpha, const tomos_dense*
  *   ACCURATE / NATIVE (FP32 A)  A and B both kept to ~22 bits (the accurate
  *                  tier), three TF32 products.
  * An entry's error is a few units of 2^-22 times sum_l |op(A)_il op(B)_lj|
- * plus the FP32 summation over K.  beta == 0 never reads C.  Allocates
- * nothing; asynchronous on `stream`. */
+ * plus the FP32 summation over K, which one accumulator carries over the
+ * whole of K (for K in the 10^5 range prefer tomos_mm_ex below, whose split
+ * sums shorter runs).  beta == 0 never reads C.  Allocates nothing;
+ * asynchronous on `stream`. */
 tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A,
                       int32_t tier, const tomos_dense* B, double beta, tomos_dense* C,
                       void* stream);
+
+/* tomos_mm with caller scratch: a product with too few 128 x BN output tiles
+ * to fill the GPU and a long K (e.g. A^T Q with A tall, the transposed
+ * multi-right-hand-side product) splits K over CTAs, writes FP32 partial sums
+ * to `scratch` and sums them in FP64 in a fixed order (deterministic).
+ * tomos_mm_scratch_bytes gives the bytes (0: no split); with less scratch the
+ * product runs unsplit, with the same result up to summation order. */
+size_t tomos_mm_scratch_bytes(int32_t trans_a, int32_t trans_b, const tomos_dense* A,
+                              int32_t tier, const tomos_dense* B);
+tomos_status tomos_mm_ex(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A,
+                         int32_t tier, const tomos_dense* B, double beta, tomos_dense* C,
+                         void* scratch, size_t scratch_bytes, void* stream);
 
 /* CSR y = alpha * op(A) x + beta * y (cuda::mv_csr, mv_cuda_kernels.cu:
  * 2029-2058; dispatch::Sparse::lookup_mv).  FP32, FP64 and packed values.
@@ -463,6 +477,21 @@ tomos_status tomos_backward_error_dense(const tomos_dense* A, const float* b,
 tomos_status tomos_lsqr_adjoint_dense(const tomos_dense* A, const float* g, float* lambda,
                                       tomos_workspace* ws, const tomos_lsqr_opts* opts,
                                       tomos_lsqr_report* report, void* stream);
+/* K adjoints at once: Lambda_k = (A^T A)^{-1} G_k for the K columns of G
+ * (n x K column-major FP32, leading dimension ldg) into Lambda (n x K, ld
+ * ldl).  The same preconditioned CG as tomos_lsqr_adjoint_dense, one
+ * recurrence per column, sharing the products with A: every iteration
+ * forms Q = A P and W = A^T Q for all K directions with two tensor-core
+ * products (tomos_mm_ex), so A is read twice an iteration for all K
+ * columns instead of once per column.  Products at ~2^-22 relative
+ * (three TF32 terms for FP32 or exactly read packed A).  reports (K
+ * entries, may be NULL): each column's iterations, converged, relres;
+ * half_passes counts the shared products.  The workspace grows a buffer
+ * for the K columns on first use.  Synchronous on stream. */
+tomos_status tomos_lsqr_adjoint_batch_dense(const tomos_dense* A, int32_t K, const float* G,
+                                            int64_t ldg, float* Lambda, int64_t ldl,
+                                            tomos_workspace* ws, const tomos_lsqr_opts* opts,
+                                            tomos_lsqr_report* reports, void* stream);
 /* The gradients for K right-hand sides in one pass over a row-major A:
  * B (m x K), X = x*_k (n x K), Lam = lambda_k (n x K), column-major with
  * leading dimensions ldb, ldx, ldl.  gradB (m x K, ld ldgb) = A Lam;

@@ -28,8 +28,9 @@ def rel(a, b):
     return np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b)
 
 
-def gpu_grads(A0, B0, G0, numeric=NT.FP32, precond=True, tol=1e-7):
-    """Forward solves, adjoint solves and the gradient pass through the
+def gpu_grads(A0, B0, G0, numeric=NT.FP32, precond=True, tol=1e-7, batch=False):
+    """Forward solves, adjoint solves (one CG per column, or all columns at
+    once with shared products when batch) and the gradient pass through the
     C ABI; returns (X, Lam, gradA, gradB, adjoint reports)."""
     m, n = A0.shape
     K = B0.shape[1]
@@ -48,9 +49,12 @@ def gpu_grads(A0, B0, G0, numeric=NT.FP32, precond=True, tol=1e-7):
                       stop_rule=tb.StopRule.BACKWARD,
                       tier=tb.Tier.ACCURATE if numeric != NT.FP32 else None)
         X[:, k] = x
-        lam, rep = tb.lsqr_adjoint(A, cuda(G0[:, k]), ws, tol=tol, max_iters=1000)
-        Lam[:, k] = lam
-        reps.append(rep)
+        if not batch:
+            lam, rep = tb.lsqr_adjoint(A, cuda(G0[:, k]), ws, tol=tol, max_iters=1000)
+            Lam[:, k] = lam
+            reps.append(rep)
+    if batch:
+        Lam, reps = tb.lsqr_adjoint_batch(A, cuda(G0), ws, tol=tol, max_iters=1000)
     gA, gB = tb.lsqr_adjoint_grad(A, cuda(B0), X, Lam)
     return (X.cpu().numpy(), Lam.cpu().numpy(), gA.cpu().numpy(), gB.cpu().numpy(), reps)
 
@@ -137,3 +141,40 @@ def test_adjoint_zero_gradient_and_errors():
     with pytest.raises(tb.TomosError):
         tb.lsqr_adjoint_grad(Ac, cuda(B0), torch.zeros((20, 1), device="cuda"),
                              torch.zeros((20, 1), device="cuda"))
+
+
+@pytest.mark.parametrize("m,n,K", [(200_000, 500, 8), (5000, 64, 1), (3000, 40, 3)])
+def test_adjoint_batch(orc, m, n, K):
+    """All K adjoints at once (two tensor-core products over A an iteration
+    shared by the K recurrences) against the FP64 normal equations, and
+    against the one-column CG solves."""
+    A0, B0, G0 = problem(m, n, K, 11 + K)
+    X, Lam, gA, gB, reps = gpu_grads(A0, B0, G0, batch=True)
+    assert len(reps) == K and all(r["converged"] for r in reps), reps
+    assert max(r["iterations"] for r in reps) < 60
+    _, Lr, gAr, gBr = orc.lstsq_grads_f64(A0, B0, G0)
+    assert rel(Lam, Lr) < 1e-5
+    assert rel(gB, gBr) < 1e-4
+    rows = np.random.default_rng(4).choice(m, min(m, 2000), replace=False)
+    assert rel(gA[rows], gAr[rows]) < 1e-4
+    _, Lam1, _, _, reps1 = gpu_grads(A0, B0, G0)
+    assert rel(Lam, Lam1) < 1e-5
+    assert all(abs(r["iterations"] - q["iterations"]) <= 2 for r, q in zip(reps, reps1))
+
+
+@pytest.mark.parametrize("numeric", [NT.FP32_16, NT.FP32_BF16])
+def test_adjoint_batch_packed_and_plain(orc, numeric):
+    """Packed A (exact values through the accurate tensor-core tier), no
+    preconditioner, and a zero column: that column stops at once while the
+    others iterate."""
+    A0, B0, G0 = problem(4000, 60, 3, 12)
+    A0 = (A0 * 10.0 ** np.random.default_rng(7).uniform(-1, 1, 60)).astype(np.float32)
+    G0[:, 1] = 0.0
+    _, Lam, _, _, reps = gpu_grads(A0, B0, G0, numeric=numeric, batch=True)
+    _, Lr, _, _ = orc.lstsq_grads_f64(A0, B0, G0)
+    assert reps[1]["iterations"] == 0 and reps[1]["converged"] == 1
+    assert np.count_nonzero(Lam[:, 1]) == 0
+    assert rel(Lam[:, [0, 2]], Lr[:, [0, 2]]) < 1e-5
+    _, Lam_np, _, _, reps_np = gpu_grads(A0, B0, G0, precond=False, batch=True)
+    assert all(r["converged"] for r in reps_np)
+    assert rel(Lam_np[:, [0, 2]], Lr[:, [0, 2]]) < 1e-5

@@ -161,3 +161,46 @@ def test_mm_tma_pipeline(orc, numeric, tier, la, lb, M, N, K):
     for beta in (0.0, 0.5):
         check(orc, A, A0, tier, T.NO_TRANSPOSE, T.NO_TRANSPOSE, (K, N), (lb, L.COL_MAJOR), beta, rng,
               bf16_ops=numeric == NT.FP32_BF16, bpad=bpad)
+
+
+@pytest.mark.parametrize("numeric,tier", [(NT.FP32, tb.Tier.AUTO), (NT.FP32_16, tb.Tier.ACCURATE),
+                                          (NT.FP32_16, tb.Tier.HALF)])
+@pytest.mark.parametrize("beta", [0.0, 0.5])
+def test_mm_split_k(orc, numeric, tier, beta):
+    """A^T Q with a tall K (the transposed multi-right-hand-side product):
+    few output tiles, so K is split over CTAs and the FP32 partials are summed
+    in FP64 in split order; without scratch (tomos_mm) the same product runs
+    unsplit."""
+    import ctypes
+    from tomos_b200 import _capi as C
+    rng = np.random.default_rng(int(numeric) + int(tier) * 7)
+    m, n, k = 100_000, 300, 8
+    A0 = (rng.standard_normal((m, n)) * 10.0 ** rng.uniform(-1, 1, n)).astype(np.float32)
+    A = to_dense(A0, L.ROW_MAJOR, numeric)
+    da, db = A.desc(), None
+    Q = dense_f32(rng.standard_normal((m, k)), L.COL_MAJOR)
+    db = Q.desc()
+    nb = C.lib().tomos_mm_scratch_bytes(int(T.TRANSPOSE), int(T.NO_TRANSPOSE), ctypes.byref(da), int(tier),
+                                        ctypes.byref(db))
+    assert nb > 0  # the split is taken
+    check(orc, A, A0, tier, T.TRANSPOSE, T.NO_TRANSPOSE, (m, k), (L.COL_MAJOR, L.COL_MAJOR), beta, rng)
+    # unsplit (no scratch) against split: equal up to summation order
+    C0 = rng.standard_normal((n, k)).astype(np.float32)
+    Cs, Cu = dense_f32(C0, L.COL_MAJOR), dense_f32(C0, L.COL_MAJOR)
+    tb.mm_apply(tb.Device.CUDA, T.TRANSPOSE, T.NO_TRANSPOSE, 1.0, A, Q, beta, Cs, tier=tier)
+    dc = Cu.desc()
+    C.check(C.lib().tomos_mm(int(T.TRANSPOSE), int(T.NO_TRANSPOSE), 1.0, ctypes.byref(da), int(tier),
+                             ctypes.byref(db), float(beta), ctypes.byref(dc), None), "mm")
+    a, b = values(Cs), values(Cu)
+    # both within the product bound; the unsplit one sums all m rows of a
+    # column in FP32 in one accumulator, so it sits further from FP64
+    Av = A0.astype(np.float64) if numeric == NT.FP32 else decoded(
+        orc, A, tb.Tier.HALF if tier == tb.Tier.HALF else tier)
+    Qv = Q.view().double().cpu().numpy()
+    ref = Av.T @ Qv + beta * C0.astype(np.float64)
+    S = np.abs(Av.T) @ np.abs(Qv) + abs(beta) * np.abs(C0)
+    assert np.all(np.abs(a - ref) <= 1e-5 * S)
+    # unsplit: 100,000 terms in one FP32 accumulator (tomos_mm's documented
+    # summation error grows with K)
+    assert np.all(np.abs(b - ref) <= 1e-4 * S)
+    assert np.abs(a - ref).max() <= np.abs(b - ref).max()

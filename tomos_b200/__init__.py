@@ -479,8 +479,12 @@ def mm_apply(dev, transA, transB, alpha, A, B, beta, Cm, use_workspace=False, ti
     if tier is None:
         tier = Tier.ACCURATE if A.numeric in PACKED else Tier.AUTO
     da, db, dc = A.desc(), B.desc(), Cm.desc()
-    C.check(C.lib().tomos_mm(int(transA), int(transB), float(alpha), ctypes.byref(da), int(tier),
-                             ctypes.byref(db), float(beta), ctypes.byref(dc), _stream(stream)),
+    nb = C.lib().tomos_mm_scratch_bytes(int(transA), int(transB), ctypes.byref(da), int(tier),
+                                        ctypes.byref(db))
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda") if nb else None
+    C.check(C.lib().tomos_mm_ex(int(transA), int(transB), float(alpha), ctypes.byref(da), int(tier),
+                                ctypes.byref(db), float(beta), ctypes.byref(dc), _ptr(scratch), nb,
+                                _stream(stream)),
             "mm_apply")
     return 0
 
@@ -730,6 +734,29 @@ def lsqr_adjoint(A, g, workspace, tol=1e-7, max_iters=500, tier=None, stream=Non
                                              ctypes.byref(rep), _stream(stream)),
             "lsqr_adjoint")
     return lam, rep.as_dict()
+
+
+def lsqr_adjoint_batch(A, G, workspace, tol=1e-7, max_iters=500, tier=None, stream=None):
+    """Lambda = (A^T A)^{-1} G for the K columns of G (n x K float32 CUDA
+    tensor) at once (tomos_lsqr_adjoint_batch_dense: one CG recurrence per
+    column, the products with A shared, two tensor-core products an
+    iteration).  Returns (Lambda (n x K), list of K reports)."""
+    n = A.size[1]
+    K = G.shape[1]
+    opts = C.LsqrOpts()
+    opts.tol = float(tol)
+    opts.max_iters = int(max_iters)
+    opts.restarts = 1
+    opts.iter_tier = int(Tier.AUTO if tier is None else Tier(tier))
+    Gc = G.t().contiguous().float()  # column-major n x K
+    Lc = torch.empty((K, n), dtype=torch.float32, device="cuda")
+    reps = (C.LsqrReport * max(K, 1))()
+    d = A.desc()
+    C.check(C.lib().tomos_lsqr_adjoint_batch_dense(ctypes.byref(d), K, _ptr(Gc), n, _ptr(Lc), n,
+                                                   workspace.handle, ctypes.byref(opts), reps,
+                                                   _stream(stream)),
+            "lsqr_adjoint_batch")
+    return Lc.t(), [reps[k].as_dict() for k in range(K)]
 
 
 def lsqr_adjoint_grad(A, B, X, Lam, want_grad_a=True, stream=None):

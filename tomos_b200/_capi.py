@@ -91,6 +91,13 @@ SIGNATURES = {
     "tomos_gemv_scratch_bytes": (c_sz, [ctypes.POINTER(DenseDesc), c_i32]),
     "tomos_mm": (c_i32, [c_i32, c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32,
                          ctypes.POINTER(DenseDesc), c_dbl, ctypes.POINTER(DenseDesc), c_vp]),
+    "tomos_mm_ex": (c_i32, [c_i32, c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32,
+                            ctypes.POINTER(DenseDesc), c_dbl, ctypes.POINTER(DenseDesc), c_vp,
+                            ctypes.c_size_t, c_vp]),
+    "tomos_lsqr_adjoint_batch_dense": (c_i32, [ctypes.POINTER(DenseDesc), c_i32, c_vp, c_i64, c_vp, c_i64,
+                                               c_vp, ctypes.POINTER(LsqrOpts), c_vp, c_vp]),
+    "tomos_mm_scratch_bytes": (ctypes.c_size_t, [c_i32, c_i32, ctypes.POINTER(DenseDesc), c_i32,
+                                                 ctypes.POINTER(DenseDesc)]),
     "tomos_gemv": (c_i32, [c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32, c_vp, c_dbl, c_vp,
                            c_vp, c_sz, c_vp]),
     "tomos_gemv_no_alloc": (c_i32, [c_i32, c_dbl, ctypes.POINTER(DenseDesc), c_i32, c_vp, c_dbl,

@@ -3,7 +3,8 @@
 X = argmin ||A X - B|| column by column (sketch-preconditioned LSQR,
 tomos_lsqr_solve_dense), with gradients in A and B from the adjoint:
 for a loss L with G = dL/dX,
-    Lam   = (A^T A)^{-1} G        (tomos_lsqr_adjoint_dense, reusing R^{-1})
+    Lam   = (A^T A)^{-1} G        (tomos_lsqr_adjoint_batch_dense: all columns at
+                                    once, reusing R^{-1})
     dL/dB = A Lam
     dL/dA = (B - A X) Lam^T - (A Lam) X^T
 the last two in one pass over A (tomos_lsqr_adjoint_grad_dense).
@@ -11,8 +12,8 @@ the last two in one pass over A (tomos_lsqr_adjoint_grad_dense).
 import torch
 
 from . import (Dense, Layout, NumericType, StopRule, add_precond, apply_count_sketch, column_scale,
-               create_lsqr_workspace, generate_sketch_qr_precond, lsqr_adjoint, lsqr_adjoint_grad,
-               lsqr_solve)
+               create_lsqr_workspace, generate_sketch_qr_precond, lsqr_adjoint_batch,
+               lsqr_adjoint_grad, lsqr_solve)
 
 
 class LeastSquares(torch.autograd.Function):
@@ -48,11 +49,7 @@ class LeastSquares(torch.autograd.Function):
         A, B2, X = ctx.saved_tensors
         D, ws, Rinv, tol, max_iters, bshape = ctx.state
         G2 = G.reshape(X.shape[0], -1).float()
-        Lam = torch.empty_like(X)
-        for k in range(X.shape[1]):
-            lam, _ = lsqr_adjoint(D, G2[:, k].contiguous(), ws, tol=min(tol, 1e-7),
-                                  max_iters=max_iters)
-            Lam[:, k] = lam
+        Lam, _ = lsqr_adjoint_batch(D, G2, ws, tol=min(tol, 1e-7), max_iters=max_iters)
         gA, gB = lsqr_adjoint_grad(D, B2, X, Lam, want_grad_a=ctx.needs_input_grad[0])
         return gA, gB.reshape(bshape), None, None, None
 

@@ -45,6 +45,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <utility>
@@ -84,6 +85,8 @@ struct GemmArgs {
     int bn;            // columns of op(B) per CTA: 16, 32, 64 or 128
     int stages;        // operand stages
     int raw_stages;    // raw (copied) stages of the TMA-fed pipeline
+    int kt_per;        // K-tiles per split of K (blockIdx.z); all of them when unsplit
+    float* part;       // split K: FP32 partial sums [split][N][M] (NULL: write C)
     int* err;
 };
 
@@ -441,6 +444,7 @@ __device__ __forceinline__ void gemm_issue_mmas(const GemmArgs& g, uint8_t* ops,
 template <int NW>
 __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, int warp, int lane, int64_t m0, int64_t n0,
                                               uint32_t tmem, uint64_t* done, volatile int* abort_flag) {
+    float* part = g.part ? g.part + (size_t)blockIdx.z * (size_t)g.M * (size_t)g.N : nullptr;
     const int BN = g.bn;
     if (warp < NW) {
         if (!mbar_wait(done, 0u)) {
@@ -459,6 +463,10 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, int warp, int l
             for (int e = 0; e < 8; ++e) {
                 const int64_t j = n0 + c + e;
                 if (j >= g.N) break;
+                if (part) {  // split K: this split's raw sum
+                    part[(size_t)(j * g.M + i)] = u2f(r[e]);
+                    continue;
+                }
                 float* cp = g.c + (size_t)(i * g.c_si + j * g.c_sj);
                 double y = g.alpha * (double)u2f(r[e]);
                 if (g.beta != 0.0) y += g.beta * (double)*cp;
@@ -486,7 +494,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_tc_kernel(GemmArgs g) {
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t m0 = (int64_t)blockIdx.x * kGemmM, n0 = (int64_t)blockIdx.y * BN;
-    const int nk = (int)((g.K + T::kpl - 1) / T::kpl);
+    const int nk_all = (int)((g.K + T::kpl - 1) / T::kpl);
+    const int kt0 = (int)blockIdx.z * g.kt_per;  // this split's first K-tile (the host gives each >= 1)
+    const int nk = nk_all - kt0 < g.kt_per ? nk_all - kt0 : g.kt_per;
     const uint32_t ncols = BN <= 32 ? 32u : (uint32_t)BN;
 
     if (threadIdx.x == 0) {
@@ -519,7 +529,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_tc_kernel(GemmArgs g) {
             }
             if (*abort_flag) break;
             uint8_t* st = smem + (size_t)s * stage_bytes;
-            const int64_t k0 = (int64_t)kt * T::kpl;
+            const int64_t k0 = (int64_t)(kt0 + kt) * T::kpl;
             produce_a<E, MODE>(g, st, st + a_bytes, m0, k0, pt);
             uint8_t* bt = st + T::na * a_bytes;
             produce_b<MODE, BF>(g, bt, bt + b_bytes, n0, k0, pt);
@@ -733,7 +743,7 @@ __device__ __forceinline__ void unit_of(int it, int R, bool kc, int& r, int& u) 
 }
 
 template <Elem E, int MODE>
-__global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_kernel(GemmArgs g, const __grid_constant__ GemmMaps maps) {
+__global__ void __launch_bounds__(kTmaThreads, 2) gemm_tma_kernel(GemmArgs g, const __grid_constant__ GemmMaps maps) {
     using T = ModeTraits<MODE>;
     using RT = RawTraits<E, MODE>;
     constexpr bool BF = (E == Elem::B16);
@@ -756,7 +766,9 @@ __global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_kernel(GemmArgs g, co
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t m0 = (int64_t)blockIdx.x * kGemmM, n0 = (int64_t)blockIdx.y * BN;
-    const int nk = (int)((g.K + T::kpl - 1) / T::kpl);
+    const int nk_all = (int)((g.K + T::kpl - 1) / T::kpl);
+    const int kt0 = (int)blockIdx.z * g.kt_per;  // this split's first K-tile (the host gives each >= 1)
+    const int nk = nk_all - kt0 < g.kt_per ? nk_all - kt0 : g.kt_per;
     const uint32_t ncols = BN <= 32 ? 32u : (uint32_t)BN;
 
     if (threadIdx.x == 0) {
@@ -844,7 +856,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) gemm_tma_kernel(GemmArgs g, co
                 }
                 if (*abort_flag) break;
                 const uint32_t ra = smem_addr(smem + (size_t)rs * raw_bytes);
-                const int k0 = kt * T::kpl;
+                const int k0 = (kt0 + kt) * T::kpl;
                 mbar_expect_tx(&rfull[rs], raw_bytes);
                 const int am = (int)m0, bn0 = (int)n0;
                 if (g.a_kc) {
@@ -959,21 +971,31 @@ bool make_maps(const GemmArgs& g, GemmMaps* maps) {
 }
 
 constexpr int kTmaSmemBudget = 224 * 1024;
+constexpr int kTmaSmemTwo = 112 * 1024;  // two CTAs an SM (228 KB, 1 KB reserved a CTA)
 
 template <Elem E, int MODE>
 tomos_status launch_gemm(GemmArgs& g, cudaStream_t st) {
     using T = ModeTraits<MODE>;
     using RT = RawTraits<E, MODE>;
-    const dim3 grid((unsigned)((g.M + kGemmM - 1) / kGemmM), (unsigned)((g.N + g.bn - 1) / g.bn));
+    const int nk_all = (int)((g.K + T::kpl - 1) / T::kpl);
+    const dim3 grid((unsigned)((g.M + kGemmM - 1) / kGemmM), (unsigned)((g.N + g.bn - 1) / g.bn),
+                    (unsigned)((nk_all + g.kt_per - 1) / g.kt_per));
     const size_t stage = (size_t)T::na * kGemmM * kLineBytes + (size_t)T::nb * g.bn * kLineBytes;
     const size_t bars = (5 * kMaxStages + 1) * sizeof(uint64_t) + 16;
     GemmMaps maps;
     if (make_maps<E, MODE>(g, &maps)) {
         const size_t raw = (size_t)RT::a_bytes + (size_t)g.bn * T::kpl * 4;
+        // operand and raw stages: the deepest rings that fit; with many
+        // tiles, rings small enough for two CTAs an SM first, so that one
+        // CTA's pipeline fill and epilogue overlap the other's main loop
         static const int pairs[][2] = {{2, 4}, {3, 3}, {2, 3}, {3, 2}, {2, 2}};
+        const int64_t tiles = (int64_t)grid.x * grid.y * grid.z;
+        const size_t budgets[2] = {tiles >= 2 * (int64_t)sm_count() ? (size_t)kTmaSmemTwo : 0,
+                                   (size_t)kTmaSmemBudget};
+        for (int pass = 0; pass < 2; ++pass)
         for (const auto& pr : pairs) {
             const size_t smem = (size_t)pr[0] * stage + (size_t)pr[1] * raw + bars + 1024;
-            if (smem > (size_t)kTmaSmemBudget) continue;
+            if (smem > budgets[pass]) continue;
             g.stages = pr[0];
             g.raw_stages = pr[1];
             auto kern = gemm_tma_kernel<E, MODE>;
@@ -1032,17 +1054,34 @@ bool strides_of(const tomos_dense* D, int32_t trans, int64_t* s_row, int64_t* s_
 
 using namespace tomos_b200;
 
-extern "C" {
+namespace tomos_b200 {
+namespace {
 
-tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A, int32_t tier,
-                      const tomos_dense* B, double beta, tomos_dense* C, void* stream) {
+// C(i, j) = alpha sum_z part[z](i, j) + beta C(i, j), the splits summed in
+// FP64 in split order (deterministic).
+__global__ void gemm_split_reduce_kernel(const float* __restrict__ part, int splits, int64_t M, int64_t N,
+                                         double alpha, double beta, float* c, int64_t si, int64_t sj) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M * N) return;
+    const int64_t i = t % M, j = t / M;
+    double s = 0.0;
+    for (int z = 0; z < splits; ++z) s += (double)part[(size_t)z * M * N + t];
+    float* p = c + (size_t)(i * si + j * sj);
+    double y = alpha * s;
+    if (beta != 0.0) y += beta * (double)*p;
+    *p = (float)y;
+}
+
+// Validates a product and fills the launch arguments (all but the split).
+tomos_status mm_prepare(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A, int32_t tier,
+                        const tomos_dense* B, double beta, const tomos_dense* C, GemmArgs* gp, Elem* ep, int* modep) {
     if (!A || !B || !C) return fail(TOMOS_ERR_INVALID, "mm: null matrix");
     if ((trans_a != TOMOS_NO_TRANSPOSE && trans_a != TOMOS_TRANSPOSE) ||
         (trans_b != TOMOS_NO_TRANSPOSE && trans_b != TOMOS_TRANSPOSE))
         return fail(TOMOS_ERR_INVALID, "mm: bad transpose");
     if (B->numeric != TOMOS_FP32 || C->numeric != TOMOS_FP32)
         return fail(TOMOS_ERR_UNSUPPORTED, "mm: B and C must be FP32 (dense_registries.cpp:396-405)");
-    for (const tomos_dense* D : {A, B, static_cast<const tomos_dense*>(C)}) {
+    for (const tomos_dense* D : {A, B, C}) {
         if (D->rows < 0 || D->cols < 0) return fail(TOMOS_ERR_INVALID, "mm: negative size");
         if (D->layout != TOMOS_ROW_MAJOR && D->layout != TOMOS_COL_MAJOR)
             return fail(TOMOS_ERR_INVALID, "mm: bad layout");
@@ -1066,14 +1105,8 @@ tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomo
     const bool e16 = e == Elem::H16 || e == Elem::F16 || e == Elem::B16;
     if (ops16 && !e16) return fail(TOMOS_ERR_UNSUPPORTED, "mm: 16-bit operands need 16-bit A values");
     if (e == Elem::F64) return fail(TOMOS_ERR_UNSUPPORTED, "mm: FP64 A");
-    cudaStream_t st = as_stream(stream);
-    if (M == 0 || N == 0) return TOMOS_OK;
-    if ((!A->values && M * K > 0) || !B->values && K * N > 0 || !C->values)
-        return fail(TOMOS_ERR_INVALID, "mm: null values");
-    int* err = gemm_err_word();
-    if (!err) return fail(TOMOS_ERR_CUDA, "mm: error word");
-
-    GemmArgs g;
+    GemmArgs& g = *gp;
+    std::memset(&g, 0, sizeof(g));
     g.a_hi = A->values;
     g.a_lo = two_planes_elem(e) ? dense_lo_plane(A) : nullptr;
     strides_of(A, trans_a, &g.a_si, &g.a_sl);
@@ -1086,20 +1119,14 @@ tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomo
     g.K = K;
     g.alpha = alpha;
     g.beta = beta;
-    g.err = err;
     g.bn = N <= 16 ? 16 : N <= 32 ? 32 : N <= 64 ? 64 : 128;
-    if (K == 0) {
-        gemm_scale_c_kernel<<<(unsigned)((M * N + 255) / 256), 256, 0, st>>>(g.c, M, N, g.c_si, g.c_sj, beta);
-        TOMOS_LAUNCH_CHECK("gemm_scale_c_kernel");
-        return TOMOS_OK;
-    }
     // one of the two strides of a dense operand is 1: lines run along K
     // when the K stride is
     g.a_kc = g.a_sl == 1 ? 1 : 0;
     g.b_kc = g.b_sl == 1 ? 1 : 0;
+    const int mode = ops16 ? kPure16 : (e16 ? kTf32x2 : kTf32x3);
     // vector loads: unit stride along the line, 16-byte aligned lines
     const int aes = e == Elem::F32 ? 4 : 2;
-    const int mode = ops16 ? kPure16 : (e16 ? kTf32x2 : kTf32x3);
     const int aepu = mode == kPure16 ? 8 : 4;
     const int64_t a_lstride = g.a_kc ? g.a_si : g.a_sl;
     const uintptr_t ab = reinterpret_cast<uintptr_t>(A->values);
@@ -1110,18 +1137,106 @@ tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomo
     const int64_t b_lstride = g.b_kc ? g.b_sj : g.b_sl;
     const uintptr_t bb = reinterpret_cast<uintptr_t>(B->values);
     g.b_vec = ((g.b_kc ? g.b_sl : g.b_sj) == 1) && (b_lstride * 4) % 16 == 0 && bb % 16 == 0;
+    g.kt_per = 1 << 30;
+    *ep = e;
+    *modep = mode;
+    return TOMOS_OK;
+}
+
+// Splits of K for products with too few output tiles to fill the SMs
+// (e.g. A^T Q with a tall K): at least one CTA an SM, and runs of at most 16
+// K-tiles (512 TF32 / 1024 16-bit terms) in one FP32 accumulator -- a
+// coherent sum such as the diagonal of A^T A loses ~u x run length
+// relative in FP32, so long K is cut into short runs that are summed in
+// FP64.  Each split has at least 4 K-tiles.
+int split_count(const GemmArgs& g, int mode, int* kt_per) {
+    const int kpl = mode == kPure16 ? 64 : 32;
+    const int64_t nk_all = (g.K + kpl - 1) / kpl;
+    const int64_t tiles = ((g.M + kGemmM - 1) / kGemmM) * ((g.N + g.bn - 1) / g.bn);
+    int64_t splits = 1;
+    if (tiles < sm_count() / 2 && nk_all >= 16) {
+        splits = sm_count() / tiles;
+        const int64_t runs = (nk_all + 15) / 16;
+        if (splits < runs) splits = runs;
+        if (splits > nk_all / 4) splits = nk_all / 4;
+        if (splits < 1) splits = 1;
+    }
+    const int64_t per = (nk_all + splits - 1) / splits;
+    *kt_per = (int)per;
+    return (int)((nk_all + per - 1) / per);
+}
+
+}  // namespace
+}  // namespace tomos_b200
+
+extern "C" {
+
+size_t tomos_mm_scratch_bytes(int32_t trans_a, int32_t trans_b, const tomos_dense* A, int32_t tier,
+                              const tomos_dense* B) {
+    if (!A || !B) return 0;
+    tomos_dense C{TOMOS_FP32, TOMOS_COL_MAJOR, trans_a == TOMOS_NO_TRANSPOSE ? A->rows : A->cols,
+                  trans_b == TOMOS_NO_TRANSPOSE ? B->cols : B->rows, 0, nullptr, nullptr, 0, 0};
+    C.ld = C.rows > 0 ? C.rows : 1;
+    GemmArgs g;
+    Elem e;
+    int mode;
+    if (mm_prepare(trans_a, trans_b, 1.0, A, tier, B, 0.0, &C, &g, &e, &mode) != TOMOS_OK) return 0;
+    if (g.M == 0 || g.N == 0 || g.K == 0) return 0;
+    int per;
+    const int splits = split_count(g, mode, &per);
+    return splits > 1 ? (size_t)splits * (size_t)g.M * (size_t)g.N * sizeof(float) : 0;
+}
+
+tomos_status tomos_mm_ex(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A, int32_t tier,
+                         const tomos_dense* B, double beta, tomos_dense* C, void* scratch, size_t scratch_bytes,
+                         void* stream) {
+    GemmArgs g;
+    Elem e;
+    int mode;
+    tomos_status s = mm_prepare(trans_a, trans_b, alpha, A, tier, B, beta, C, &g, &e, &mode);
+    if (s) return s;
+    cudaStream_t st = as_stream(stream);
+    if (g.M == 0 || g.N == 0) return TOMOS_OK;
+    if ((!A->values && g.M * g.K > 0) || (!B->values && g.K * g.N > 0) || !C->values)
+        return fail(TOMOS_ERR_INVALID, "mm: null values");
+    g.err = gemm_err_word();
+    if (!g.err) return fail(TOMOS_ERR_CUDA, "mm: error word");
+    if (g.K == 0) {
+        gemm_scale_c_kernel<<<(unsigned)((g.M * g.N + 255) / 256), 256, 0, st>>>(g.c, g.M, g.N, g.c_si, g.c_sj,
+                                                                                 beta);
+        TOMOS_LAUNCH_CHECK("gemm_scale_c_kernel");
+        return TOMOS_OK;
+    }
+    int splits = split_count(g, mode, &g.kt_per);
+    const size_t need = (size_t)splits * (size_t)g.M * (size_t)g.N * sizeof(float);
+    if (splits > 1 && (!scratch || scratch_bytes < need)) {
+        // no (or too little) scratch: one split
+        splits = 1;
+        g.kt_per = 1 << 30;
+    }
+    g.part = splits > 1 ? static_cast<float*>(scratch) : nullptr;
     switch (mode) {
-        case kPure16: return launch_mode<kPure16>(e, g, st);
-        case kTf32x2: return launch_mode<kTf32x2>(e, g, st);
+        case kPure16: s = launch_mode<kPure16>(e, g, st); break;
+        case kTf32x2: s = launch_mode<kTf32x2>(e, g, st); break;
         default:
             switch (e) {
-                case Elem::F32: return launch_gemm<Elem::F32, kTf32x3>(g, st);
-                case Elem::A16: return launch_gemm<Elem::A16, kTf32x3>(g, st);
-                case Elem::AB16: return launch_gemm<Elem::AB16, kTf32x3>(g, st);
-                case Elem::AB16R: return launch_gemm<Elem::AB16R, kTf32x3>(g, st);
+                case Elem::F32: s = launch_gemm<Elem::F32, kTf32x3>(g, st); break;
+                case Elem::A16: s = launch_gemm<Elem::A16, kTf32x3>(g, st); break;
+                case Elem::AB16: s = launch_gemm<Elem::AB16, kTf32x3>(g, st); break;
+                case Elem::AB16R: s = launch_gemm<Elem::AB16R, kTf32x3>(g, st); break;
                 default: return fail(TOMOS_ERR_UNSUPPORTED, "mm: element type");
             }
     }
+    if (s || splits == 1) return s;
+    gemm_split_reduce_kernel<<<(unsigned)((g.M * g.N + 255) / 256), 256, 0, st>>>(g.part, splits, g.M, g.N, alpha,
+                                                                                  beta, g.c, g.c_si, g.c_sj);
+    TOMOS_LAUNCH_CHECK("gemm_split_reduce_kernel");
+    return TOMOS_OK;
+}
+
+tomos_status tomos_mm(int32_t trans_a, int32_t trans_b, double alpha, const tomos_dense* A, int32_t tier,
+                      const tomos_dense* B, double beta, tomos_dense* C, void* stream) {
+    return tomos_mm_ex(trans_a, trans_b, alpha, A, tier, B, beta, C, nullptr, 0, stream);
 }
 
 }  // extern "C"

@@ -377,7 +377,7 @@ static void ws_free(tomos_workspace* ws) {
     void* ptrs[] = {ws->u,      ws->v,      ws->wt,     ws->p,    ws->qvec,   ws->t,
                     ws->vhat,   ws->qpart,  ws->sspart, ws->vpart, ws->xpart, ws->qnpart,
                     ws->scal,   ws->coef_init, ws->bpart, ws->fro2, ws->st,   ws->Rcm,
-                    ws->Rrm,    ws->hist,   ws->scratch, ws->h16, ws->adj, ws->csc, ws->shard};
+                    ws->Rrm,    ws->hist,   ws->scratch, ws->h16, ws->adj, ws->csc, ws->shard, ws->adjb};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (ws->st_host) cudaFreeHost(ws->st_host);

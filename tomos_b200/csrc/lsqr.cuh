@@ -191,6 +191,10 @@ struct tomos_workspace {
     // adjoint solve (adjoint.cu): FP64 n-vectors and its device state,
     // allocated by the first adjoint call.
     void* adj = nullptr;
+    // batched adjoint solves (adjoint_batch.cu): K columns of FP64 vectors,
+    // the products' FP32 operands and split-K scratch, grown as needed.
+    void* adjb = nullptr;
+    size_t adjb_bytes = 0;
     // column-major copy of a CSR matrix for the CSR pass (csr.cu), rebuilt
     // by every CSR solve and grown as needed.
     void* csc = nullptr;
