@@ -86,6 +86,7 @@ struct GemmArgs {
     int stages;        // operand stages
     int raw_stages;    // raw (copied) stages of the TMA-fed pipeline
     int kt_per;        // K-tiles per split of K (blockIdx.z); all of them when unsplit
+    int direct_a;      // TMA pipeline, 16-bit operands, K-contiguous A: the MMA reads A from the raw ring
     float* part;       // split K: FP32 partial sums [split][N][M] (NULL: write C)
     int* err;
 };
@@ -392,10 +393,26 @@ __device__ __forceinline__ uint64_t tile_desc(uint32_t base, int s, int R) {
 // The MMA issuer (one thread): per stage, 4 K-steps x the mode's terms,
 // then a commit that frees the stage; a final commit marks the
 // accumulator complete (or the work stopped).
+// A descriptor of K-step s (32 bytes of K) of a 128-byte-swizzled K-major
+// tile as the copy engine writes it: 8-row atoms of 128-byte rows, atoms
+// 1024 bytes apart (SBO), the step's 32 bytes at +32 s within each row
+// (layout type 2 = 128-byte swizzle; LBO unused for swizzled K-major).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t base, int s) {
+    return smem_desc(base + 32u * (uint32_t)s, 16u, 1024u) | (2ull << 61);
+}
+
+// The MMA issuer (one thread): per stage, 4 K-steps x the mode's terms,
+// then a commit that frees the stage; a final commit marks the
+// accumulator complete (or the work stopped).  raw != NULL (16-bit
+// operands, K-contiguous A): A is read straight from the raw ring the copy
+// engine filled (128-byte swizzle), and a second commit frees that raw
+// stage.
 template <int MODE, bool BF>
 __device__ __forceinline__ void gemm_issue_mmas(const GemmArgs& g, uint8_t* ops, uint32_t stage_bytes,
                                                 uint32_t a_bytes, uint32_t b_bytes, uint64_t* full, uint64_t* empty,
-                                                uint64_t* done, uint32_t tmem, int nk, volatile int* abort_flag) {
+                                                uint64_t* done, uint32_t tmem, int nk, volatile int* abort_flag,
+                                                const uint8_t* raw = nullptr, uint32_t raw_bytes = 0,
+                                                uint64_t* rempty = nullptr) {
     using T = ModeTraits<MODE>;
     const int S = g.stages, BN = g.bn;
     uint32_t idesc = (1u << 4);  // FP32 accumulator
@@ -416,10 +433,12 @@ __device__ __forceinline__ void gemm_issue_mmas(const GemmArgs& g, uint8_t* ops,
         tc_fence_after();
         const uint32_t st = smem_addr(ops + (size_t)s * stage_bytes);
         const uint32_t a0 = st, a1 = st + a_bytes;
-        const uint32_t b0 = st + T::na * a_bytes, b1 = b0 + b_bytes;
+        const uint32_t b0 = raw ? st : st + T::na * a_bytes, b1 = b0 + b_bytes;
+        const int rs = raw ? kt % g.raw_stages : 0;
+        const uint32_t ra = raw ? smem_addr(raw + (size_t)rs * raw_bytes) : 0u;
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
-            const uint64_t da0 = tile_desc(a0, ks, kGemmM);
+            const uint64_t da0 = raw ? sw128_desc(ra, ks) : tile_desc(a0, ks, kGemmM);
             const uint64_t db0 = tile_desc(b0, ks, BN);
             mma_issue(MODE != kPure16, tmem, da0, db0, idesc, acc);
             acc = 1;
@@ -433,6 +452,7 @@ __device__ __forceinline__ void gemm_issue_mmas(const GemmArgs& g, uint8_t* ops,
             }
         }
         mma_commit(&empty[s]);  // frees the stage once these MMAs are done
+        if (raw) mma_commit(&rempty[rs]);
     }
     mma_commit(done);
 }
@@ -629,12 +649,13 @@ template <Elem E, int MODE, bool BF>
 __device__ __forceinline__ void convert_stage(const GemmArgs& g, const uint8_t* ra, const uint8_t* rb, uint8_t* oa0,
                                               uint8_t* oa1, uint8_t* ob0, uint8_t* ob1, const uint32_t* ra_off,
                                               const uint32_t* oa_off, const uint32_t* rb_off,
-                                              const uint32_t* ob_off, int nb_items) {
+                                              const uint32_t* ob_off, int nb_items, bool direct) {
     using T = ModeTraits<MODE>;
     using RT = RawTraits<E, MODE>;
     constexpr int R = kGemmM;
 #pragma unroll
     for (int j = 0; j < kConvItems; ++j) {
+        if (direct) break;  // the MMA reads A from the raw ring
         const uint8_t* src = ra + ra_off[j];
         if constexpr (MODE == kPure16) {
             uint4 h;
@@ -730,6 +751,20 @@ __device__ __forceinline__ void convert_stage(const GemmArgs& g, const uint8_t* 
     }
 }
 
+// 16-bit operands read straight from the raw ring: only FP32_16's flagged
+// control words need their fp16 value, fixed in place (the order of the
+// 16-byte chunks does not matter for an elementwise fix).
+template <Elem E>
+__device__ __forceinline__ void fix_raw_a(uint8_t* ra, int pt) {
+    if constexpr (E == Elem::H16) {
+        for (int c = pt; c < kGemmM * 8; c += kConv) {
+            uint4* p = reinterpret_cast<uint4*>(ra) + c;
+            const uint4 h = *p;
+            if (((h.x | h.y | h.z | h.w) & 0x10001u) != 0u) *p = half_operands<E>(h);
+        }
+    }
+}
+
 // Unit (line r, 16-byte operand chunk u) of converter item `it`: eight
 // consecutive lanes take eight consecutive lines of one chunk.
 __device__ __forceinline__ void unit_of(int it, int R, bool kc, int& r, int& u) {
@@ -754,7 +789,9 @@ __global__ void __launch_bounds__(kTmaThreads, 2) gemm_tma_kernel(GemmArgs g, co
     const uint32_t rb_bytes = (uint32_t)BN * T::kpl * 4u;
     const uint32_t raw_bytes = RT::a_bytes + rb_bytes;
     const uint32_t a_bytes = kGemmM * kLineBytes, b_bytes = (uint32_t)BN * kLineBytes;
-    const uint32_t stage_bytes = T::na * a_bytes + T::nb * b_bytes;
+    const bool direct = g.direct_a != 0;
+    const uint32_t a_ops = direct ? 0u : T::na * a_bytes;  // A operand tiles in a stage
+    const uint32_t stage_bytes = a_ops + T::nb * b_bytes;
     uint8_t* ops = smem + (size_t)RS * raw_bytes;
     uint64_t* full = reinterpret_cast<uint64_t*>(ops + (size_t)S * stage_bytes);
     uint64_t* empty = full + kMaxStages;
@@ -778,7 +815,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2) gemm_tma_kernel(GemmArgs g, co
         }
         for (int s = 0; s < RS; ++s) {
             mbar_init(&rfull[s], 1);
-            mbar_init(&rempty[s], kConvWarps);
+            mbar_init(&rempty[s], direct ? 1 : kConvWarps);  // direct: the MMA commit frees it
         }
         mbar_init(done, 1);
         *abort_flag = 0;
@@ -833,16 +870,17 @@ __global__ void __launch_bounds__(kTmaThreads, 2) gemm_tma_kernel(GemmArgs g, co
                 *abort_flag = 1;
             }
             if (*abort_flag) break;
-            const uint8_t* ra = smem + (size_t)rs * raw_bytes;
+            uint8_t* ra = smem + (size_t)rs * raw_bytes;
             uint8_t* st = ops + (size_t)s * stage_bytes;
-            uint8_t* bt = st + T::na * a_bytes;
+            uint8_t* bt = st + a_ops;
+            if (direct) fix_raw_a<E>(ra, pt);
             convert_stage<E, MODE, BF>(g, ra, ra + RT::a_bytes, st, st + a_bytes, bt, bt + b_bytes, ra_off, oa_off,
-                                       rb_off, ob_off, nb_items);
+                                       rb_off, ob_off, nb_items, direct);
             fence_async_smem();
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(&full[s]);
-                mbar_arrive(&rempty[rs]);
+                if (!direct) mbar_arrive(&rempty[rs]);
             }
         }
     } else if (warp == kCopyWarp) {
@@ -880,7 +918,8 @@ __global__ void __launch_bounds__(kTmaThreads, 2) gemm_tma_kernel(GemmArgs g, co
                 if (!mbar_wait(&rfull[kt % RS], (uint32_t)((kt / RS) & 1))) atomicExch(g.err, 6);
         }
     } else if (lane == 0) {
-        gemm_issue_mmas<MODE, BF>(g, ops, stage_bytes, a_bytes, b_bytes, full, empty, done, tmem, nk, abort_flag);
+        gemm_issue_mmas<MODE, BF>(g, ops, stage_bytes, a_bytes, b_bytes, full, empty, done, tmem, nk, abort_flag,
+                                  direct ? smem : nullptr, raw_bytes, rempty);
     }
     gemm_epilogue<kConvWarps>(g, warp, lane, m0, n0, tmem, done, abort_flag);
     tc_fence_before();
@@ -985,6 +1024,10 @@ tomos_status launch_gemm(GemmArgs& g, cudaStream_t st) {
     GemmMaps maps;
     if (make_maps<E, MODE>(g, &maps)) {
         const size_t raw = (size_t)RT::a_bytes + (size_t)g.bn * T::kpl * 4;
+        // 16-bit operands with K-contiguous A: the copy's 128-byte-swizzled
+        // tile is the MMA's A operand, no A tile in the operand stages
+        g.direct_a = (MODE == kPure16 && g.a_kc && RT::row == 128) ? 1 : 0;
+        const size_t tstage = g.direct_a ? (size_t)T::nb * g.bn * kLineBytes : stage;
         // operand and raw stages: the deepest rings that fit; with many
         // tiles, rings small enough for two CTAs an SM first, so that one
         // CTA's pipeline fill and epilogue overlap the other's main loop
@@ -994,7 +1037,7 @@ tomos_status launch_gemm(GemmArgs& g, cudaStream_t st) {
                                    (size_t)kTmaSmemBudget};
         for (int pass = 0; pass < 2; ++pass)
         for (const auto& pr : pairs) {
-            const size_t smem = (size_t)pr[0] * stage + (size_t)pr[1] * raw + bars + 1024;
+            const size_t smem = (size_t)pr[0] * tstage + (size_t)pr[1] * raw + bars + 1024;
             if (smem > budgets[pass]) continue;
             g.stages = pr[0];
             g.raw_stages = pr[1];
@@ -1006,6 +1049,7 @@ tomos_status launch_gemm(GemmArgs& g, cudaStream_t st) {
         }
     }
     // direct loads (operands the copy engine cannot address)
+    g.direct_a = 0;
     g.stages = stage_count<MODE>(g.bn);
     g.raw_stages = 0;
     if (g.stages < 2) return fail(TOMOS_ERR_UNSUPPORTED, "mm: shared memory");
