@@ -452,13 +452,15 @@ static tomos_status launch_fused_mma_t(const FusedParams& P, int* err, int grid,
     // an odd number of 16-byte units between rows keeps ldmatrix free of
     // bank conflicts
     T.pitch = ((T.cb / 16) % 2 == 1) ? T.cb : T.cb + 16;
-    const size_t stage = (size_t)kMmaRows * T.pitch;
+    // 32-row stages where two of them fit the ring, else 16-row stages
+    const int rows = (size_t)2 * 32 * T.pitch + 64 <= kMmaSmemBudget ? 32 : 16;
+    const size_t stage = (size_t)rows * T.pitch;
     int ns = (int)((kMmaSmemBudget - 64) / stage);
     if (ns > kMmaMaxStages) ns = kMmaMaxStages;
     if (ns < 2) return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: rows too long for the stage ring");
     T.nstage = ns;
-    const size_t smem = fused_rows_mma_smem(ns, T.pitch);
-    auto kern = fused_rows_mma_kernel<TPW, BF>;
+    const size_t smem = fused_rows_mma_smem(ns, rows, T.pitch);
+    auto kern = rows == 32 ? fused_rows_mma_kernel<TPW, BF, 32> : fused_rows_mma_kernel<TPW, BF, 16>;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kMmaThreads, smem, st>>>(T);
     TOMOS_LAUNCH_CHECK("fused_rows_mma_kernel");

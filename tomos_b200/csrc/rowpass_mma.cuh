@@ -10,18 +10,20 @@
 // The CUDA-core pass converts every element and spends per-row
 // instructions on shuffles and the FP64 ut; at 2 bytes an element that
 // kept it issue-bound near two thirds of HBM bandwidth.  Here a stage is
-// 16 rows (one m16 tile) and both products are tensor-core tiles read
+// 32 rows (two m16 tiles: the per-stage barrier round trips between the
+// MMA warps and the ut warp are paid once per 32 rows, and every lane of
+// the ut warp has a row) and both products are tensor-core tiles read
 // straight from the staged rows with ldmatrix, so an element costs no
 // instruction of its own:
 //
-//   product 1   D1[16 rows x 8] = A_stage[16 x 16k] . B1[16k x 8]
+//   product 1   D1[32 rows x 8] = A_stage[32 x 16k] . B1[16k x 8]
 //               B1's columns 0 and 1 are p_hi and p_lo:
 //               p * 2^sp = p_hi + p_lo * 2^-11 (fp16 each), 2^sp putting
 //               max|p| near 2^14 -- 22 significant bits of p, exact
 //               products, FP32 sums
-//   ut          16 lanes of the ut warp: dot_i = (sum over warps of D1[i][0] +
+//   ut          32 lanes of the ut warp: dot_i = (sum over warps of D1[i][0] +
 //               D1[i][1] 2^-11) 2^-sp in FP64, ut_i as rowpass.cuh
-//   product 2   D2[16 cols x 8] += A_stage^T[16 x 16 rows] . B2[16 x 8]
+//   product 2   D2[16 cols x 8] += A_stage^T[16 x 32 rows] . B2[32 x 8]
 //               (ldmatrix.trans), B2's columns ut_hi and ut_lo split the
 //               same way against a running CTA exponent E: a stage whose
 //               max|ut| raises E first rescales every D2 by the power of
@@ -64,7 +66,7 @@ constexpr int kMmaWarps = 12;  // MMA warps; warp 12 computes ut, warp 13 copies
 constexpr int kMmaUtWarp = kMmaWarps;
 constexpr int kMmaProducer = kMmaWarps + 1;
 constexpr int kMmaThreads = (kMmaWarps + 2) * 32;
-constexpr int kMmaRows = 16;   // rows per stage
+constexpr int kMmaRows = 32;   // rows per stage at most: two m16 tiles (k = 32 for product 2)
 constexpr int kMmaMaxStages = 12;
 constexpr size_t kMmaSmemBudget = 200 * 1024;  // the tensor-core pass's stage ring
 constexpr int kMmaMaxTpw = 11; // k-tiles per warp: n <= 12 * 11 * 16 = 2112
@@ -143,7 +145,9 @@ __device__ __forceinline__ uint32_t mask_pair(uint32_t v, int i0, int lim) {
 // BF: the A plane is bf16 (an FP32_BF16 wh plane read in place) and p, ut
 // enter as three exact bf16 parts (columns 0-2 of B1 / B2) instead of the
 // scaled fp16 pair; the running exponent is not needed.
-template <int TPW, bool BF>
+// ROWS: rows per stage, 32 (two m16 tiles) where two such stages fit the
+// ring, else 16.
+template <int TPW, bool BF, int ROWS>
 __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassParams T) {
     const FusedParams& P = T.f;
     if (P.skip && *P.skip) return;
@@ -165,7 +169,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
     const int nstage = T.nstage;
     const int cb = T.cb;
     const int pitch = T.pitch;
-    const size_t stage_bytes = (size_t)kMmaRows * pitch;
+    const size_t stage_bytes = (size_t)ROWS * pitch;
     const int64_t n = P.n;
     const int ktiles = (int)((n + 15) / 16);
     constexpr int kBar = (kMmaWarps + 1) * 32;  // MMA warps + the ut warp
@@ -175,7 +179,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
     int64_t r1 = r0 + rows_per_cta;
     if (r1 > P.m) r1 = P.m;
     const int64_t nrows = r1 > r0 ? r1 - r0 : 0;
-    const int ntiles = (int)((nrows + kMmaRows - 1) / kMmaRows);
+    const int ntiles = (int)((nrows + ROWS - 1) / ROWS);
 
     // Zero the ring and its 64-byte tail (read by the last row's last
     // tile) and find max|p|.
@@ -218,8 +222,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                     break;
                 }
                 if (*(volatile int*)&abort_flag) break;
-                const int64_t i0 = r0 + (int64_t)t * kMmaRows;
-                const int rows = (int)((r1 - i0) < kMmaRows ? (r1 - i0) : kMmaRows);
+                const int64_t i0 = r0 + (int64_t)t * ROWS;
+                const int rows = (int)((r1 - i0) < ROWS ? (r1 - i0) : ROWS);
                 uint8_t* st = smem + (size_t)s * stage_bytes;
                 mbar_expect_tx(&full[s], (uint32_t)(rows * cb));
                 if (contiguous) {
@@ -251,14 +255,14 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
         const double cu = P.coef[1];
         double ss = 0.0;
         int e_cur = -1000;  // running exponent: |ut| < 2^e_cur so far
-        float unext = (lane < kMmaRows && r0 + lane < r1) ? __ldg(P.u_in + r0 + lane) : 0.0f;
+        float unext = (lane < ROWS && r0 + lane < r1) ? __ldg(P.u_in + r0 + lane) : 0.0f;  // a row a lane
         for (int t = 0; t < ntiles; ++t) {
             const int b = t & 1;
-            const int64_t i = r0 + (int64_t)t * kMmaRows + lane;
-            const bool has = lane < kMmaRows && i < r1;
+            const int64_t i = r0 + (int64_t)t * ROWS + lane;
+            const bool has = lane < ROWS && i < r1;
             const float ucur = unext;
-            const int64_t inx = i + kMmaRows;
-            unext = (lane < kMmaRows && inx < r1) ? __ldg(P.u_in + inx) : 0.0f;
+            const int64_t inx = i + ROWS;
+            unext = (lane < ROWS && inx < r1) ? __ldg(P.u_in + inx) : 0.0f;
             named_bar_sync(1 + b, kBar);  // partials of stage t are in
             float ut = 0.0f;
             if (has) {
@@ -277,10 +281,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
             }
             int e_new = e_cur;
             if constexpr (BF) {
-                if (lane < kMmaRows) {
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) ub[b][k][lane] = split_bf16_part(ut, k);
-                }
+                for (int k = 0; k < 3; ++k) ub[b][k][lane] = split_bf16_part(ut, k);
                 e_new = 14;  // no scaling: q = the sum of D2's columns
                 e_cur = 14;
             } else {
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
                 e_new = m > 0.0f ? max(e_cur, ilogbf(m) + 1) : e_cur;
-                if (lane < kMmaRows) {
+                {
                     __half hi = __float2half_rn(0.0f), lo = hi;
                     if (e_new > -1000) split_half(ut, 14 - e_new, hi, lo);
                     ub[b][0][lane] = __half_as_ushort(hi);
@@ -355,8 +357,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
         // release that stage
         // valid rows of stage tp (16 but in the CTA's last stage)
         auto rows_of = [&](int tp) {
-            const int64_t left = r1 - (r0 + (int64_t)tp * kMmaRows);
-            return left < kMmaRows ? (int)left : kMmaRows;
+            const int64_t left = r1 - (r0 + (int64_t)tp * ROWS);
+            return left < ROWS ? (int)left : ROWS;
         };
         auto product2 = [&](int tp, int sp_slot, int rv) {
             const int b = tp & 1;
@@ -369,13 +371,17 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
 #pragma unroll
                     for (int q = 0; q < 4; ++q) d2[tt][q] *= f;
             }
-            uint32_t bb0 = 0, bb1 = 0;
+            // B2 fragments of the two k16 steps (rows 0-15, 16-31)
+            uint32_t bb0 = 0, bb1 = 0, bc0 = 0, bc1 = 0;
             if (g < NPART) {
                 bb0 = *reinterpret_cast<const uint32_t*>(&ub[b][g][2 * tq]);
                 bb1 = *reinterpret_cast<const uint32_t*>(&ub[b][g][2 * tq + 8]);
+                bc0 = *reinterpret_cast<const uint32_t*>(&ub[b][g][16 + 2 * tq]);
+                bc1 = *reinterpret_cast<const uint32_t*>(&ub[b][g][16 + 2 * tq + 8]);
             }
             const uint32_t st = ring + (uint32_t)(sp_slot * stage_bytes);
-            if (!failed && rv == kMmaRows) {
+            const uint32_t st2 = st + (uint32_t)(16 * pitch);
+            if (!failed && rv == ROWS) {
 #pragma unroll
                 for (int tt = 0; tt < TPW; ++tt) {
                     const int mt = warp * TPW + tt;
@@ -383,9 +389,15 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                         uint32_t a[4];
                         ldsm_x4_t(st + off2 + (uint32_t)(mt * 32), a);
                         mma16816<BF>(d2[tt], a, bb0, bb1);
+                        if constexpr (ROWS == 32) {
+                            uint32_t c[4];
+                            ldsm_x4_t(st2 + off2 + (uint32_t)(mt * 32), c);
+                            mma16816<BF>(d2[tt], c, bc0, bc1);
+                        }
                     }
                 }
             } else if (!failed) {
+                const int rv2 = rv - 16;  // valid rows of the second k16 step
 #pragma unroll
                 for (int tt = 0; tt < TPW; ++tt) {
                     const int mt = warp * TPW + tt;
@@ -399,6 +411,14 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                         a[2] = mask_pair(a[2], 2 * tq + 8, rv);
                         a[3] = mask_pair(a[3], 2 * tq + 8, rv);
                         mma16816<BF>(d2[tt], a, bb0, bb1);
+                        if (ROWS == 32 && rv2 > 0) {
+                            ldsm_x4_t(st2 + off2 + (uint32_t)(mt * 32), a);
+                            a[0] = mask_pair(a[0], 2 * tq, rv2);
+                            a[1] = mask_pair(a[1], 2 * tq, rv2);
+                            a[2] = mask_pair(a[2], 2 * tq + 8, rv2);
+                            a[3] = mask_pair(a[3], 2 * tq + 8, rv2);
+                            mma16816<BF>(d2[tt], a, bc0, bc1);
+                        }
                     }
                 }
             }
@@ -414,10 +434,12 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                 failed = true;
             }
             const uint32_t st = ring + (uint32_t)(s * stage_bytes);
-            // product 1: this warp's partial dots of the stage's 16 rows
-            // (two accumulator sets halve the dependent chain)
+            // product 1: this warp's partial dots of the stage's 32 rows (two
+            // m16 tiles; two accumulator sets each halve the dependent chain)
             float d1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, d1b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            float d1c[4] = {0.0f, 0.0f, 0.0f, 0.0f}, d1d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             if (!failed) {
+                const uint32_t st2 = st + (uint32_t)(16 * pitch);
 #pragma unroll
                 for (int tt = 0; tt < TPW; ++tt) {
                     const int kt = warp * TPW + tt;
@@ -428,16 +450,32 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
                             mma16816<BF>(d1b, a, b1[tt][0], b1[tt][1]);
                         else
                             mma16816<BF>(d1, a, b1[tt][0], b1[tt][1]);
+                        if constexpr (ROWS == 32) {
+                            uint32_t c[4];
+                            ldsm_x4(st2 + off1 + (uint32_t)(kt * 32), c);
+                            if (tt & 1)
+                                mma16816<BF>(d1d, c, b1[tt][0], b1[tt][1]);
+                            else
+                                mma16816<BF>(d1c, c, b1[tt][0], b1[tt][1]);
+                        }
                     }
                 }
             }
             if (tq == 0) {
                 red[t & 1][warp][g] = make_float2(d1[0] + d1b[0], d1[1] + d1b[1]);
                 red[t & 1][warp][g + 8] = make_float2(d1[2] + d1b[2], d1[3] + d1b[3]);
+                if (ROWS == 32) {
+                    red[t & 1][warp][g + 16] = make_float2(d1c[0] + d1d[0], d1c[1] + d1d[1]);
+                    red[t & 1][warp][g + 24] = make_float2(d1c[2] + d1d[2], d1c[3] + d1d[3]);
+                }
             }
             if (BF && tq == 1) {  // column 2: the third part
                 red3[t & 1][warp][g] = d1[0] + d1b[0];
                 red3[t & 1][warp][g + 8] = d1[2] + d1b[2];
+                if (ROWS == 32) {
+                    red3[t & 1][warp][g + 16] = d1c[0] + d1d[0];
+                    red3[t & 1][warp][g + 24] = d1c[2] + d1d[2];
+                }
             }
             named_bar_arrive(1 + (t & 1), kBar);
             if (t > 0) product2(t - 1, prev_slot, rows_of(t - 1));
@@ -477,8 +515,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) fused_rows_mma_kernel(MmaPassP
 }
 
 // Dynamic shared memory of one launch: the stage ring and its tail.
-inline size_t fused_rows_mma_smem(int nstage, int pitch) {
-    return (size_t)nstage * kMmaRows * pitch + 64;
+inline size_t fused_rows_mma_smem(int nstage, int rows, int pitch) {
+    return (size_t)nstage * rows * pitch + 64;
 }
 
 }  // namespace tomos_b200
