@@ -295,6 +295,18 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
                                          double* R, void* scratch,
                                          size_t scratch_bytes, void* stream);
 
+/* Flags of tomos_sketch_qr_precond_ex_f64.  TOMOS_QR_ANY_SIGNS: the rows of
+ * R may carry other signs than LAPACK's (R = S R_lapack, S diagonal +-1, so
+ * R^{-1} = R_lapack^{-1} S differs by the signs of its columns).  A right-
+ * preconditioned LSQR is invariant under such S (the iterates x_k of A R^{-1}
+ * S and A R^{-1} agree in exact arithmetic), and the path that returns
+ * positive pivots skips the sign reconstruction (a second n x n
+ * factorisation). */
+#define TOMOS_QR_ANY_SIGNS 1
+tomos_status tomos_sketch_qr_precond_ex_f64(int64_t k, int64_t n, double* SA, int64_t ld,
+                                            double* R, int32_t flags, void* scratch,
+                                            size_t scratch_bytes, void* stream);
+
 /* ------------------------------------------------------------------ LSQR */
 
 /* Stopping rules.  RELRES is the reference's (lsqr.cpp:418-425, :723-729):

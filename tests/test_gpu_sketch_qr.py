@@ -215,3 +215,22 @@ def test_qr_rejects_wide_and_singular():
         qr_on_gpu(np.ones((3, 5)))
     with pytest.raises(tb.TomosError):
         qr_on_gpu(np.zeros((10, 4)))
+
+
+def test_qr_any_signs():
+    """TOMOS_QR_ANY_SIGNS: R equals LAPACK's up to the signs of its rows, so
+    R^{-1} = R_lapack^{-1} S; the preconditioned LSQR solve (sketch_lsqr
+    uses it) reaches the same solution."""
+    for k, n in ((4000, 1000), (300, 64)):
+        rng = np.random.default_rng(k + 1)
+        SA0 = rng.standard_normal((k, n)) * np.logspace(0, 4, n)
+        Rinv_l, R_l = qr_on_gpu(SA0)
+        D = tb.Dense.create_strided(None, tb.Layout.COL_MAJOR, tb.NumericType.FP64, (k, n))
+        D.view()[...] = torch.from_numpy(SA0).cuda()
+        Rout = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        Rinv = tb.generate_sketch_qr_precond(D, R_out=Rout, any_signs=True).view().cpu().numpy()
+        R = Rout.t().cpu().numpy()  # column-major n x n
+        S = np.sign(np.diag(R)) * np.sign(np.diag(R_l))
+        np.testing.assert_allclose(R, S[:, None] * R_l, rtol=1e-8, atol=1e-9 * np.abs(R_l).max())
+        np.testing.assert_allclose(Rinv, Rinv_l * S[None, :], rtol=1e-8, atol=1e-9 * np.abs(Rinv_l).max())
+        assert np.all(np.diag(R) > 0)

@@ -563,12 +563,14 @@ def _count_sketch_stage(A, s, bucket_seed, sign_seed, with_colsq, stream):
     return SA, fro2, plane
 
 
-def generate_sketch_qr_precond(sketched, R_out=None, copy=True, stream=None):
+def generate_sketch_qr_precond(sketched, R_out=None, copy=True, any_signs=False, stream=None):
     """FP64 Householder QR of the k x n column-major sketched matrix; on
     return its leading n x n block holds R^{-1} (sketch_qr.hpp:19).
     Returns R^{-1} as an n x n Dense: a copy of that block, or with
     copy=False a view of it (leading dimension k, no device copy; it
-    shares the sketched matrix's storage)."""
+    shares the sketched matrix's storage).  any_signs: R's rows may carry
+    other signs than LAPACK's (TOMOS_QR_ANY_SIGNS), which a preconditioned
+    LSQR does not see and which saves the sign reconstruction."""
     if sketched.numeric != NumericType.FP64 or sketched.layout != Layout.COL_MAJOR:
         raise TomosError(C.TOMOS_ERR_INVALID, "generate_sketch_qr_precond: FP64 column-major input")
     k, n = sketched.size
@@ -578,8 +580,9 @@ def generate_sketch_qr_precond(sketched, R_out=None, copy=True, stream=None):
                          "rows as columns (k >= n).")
     nb = C.lib().tomos_sketch_qr_scratch_bytes(k, n)
     scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
-    C.check(C.lib().tomos_sketch_qr_precond_f64(k, n, _ptr(sketched.storage), sketched.ld,
-                                                _ptr(R_out), _ptr(scratch), nb, _stream(stream)),
+    C.check(C.lib().tomos_sketch_qr_precond_ex_f64(k, n, _ptr(sketched.storage), sketched.ld, _ptr(R_out),
+                                                   C.TOMOS_QR_ANY_SIGNS if any_signs else 0, _ptr(scratch),
+                                                   nb, _stream(stream)),
             "generate_sketch_qr_precond")
     if not copy:
         return Dense(NumericType.FP64, Layout.COL_MAJOR, (n, n), sketched.ld, sketched.storage)
@@ -836,7 +839,8 @@ def sketch_lsqr(A, b, s, tol=1e-6, max_iters=200, restarts=8, inner_rtol=None, w
                                           with_colsq=True, stream=stream)
     if events:
         events[1].record()
-    Rinv = generate_sketch_qr_precond(SA, copy=False, stream=stream)
+    # R up to row signs: LSQR preconditioned by R^-1 S iterates as with R^-1
+    Rinv = generate_sketch_qr_precond(SA, copy=False, any_signs=True, stream=stream)
     if events:
         events[2].record()
     d, anorm = column_scale(colsq, stream=stream)

@@ -24,6 +24,8 @@ TOMOS_ERR_CUDA = -3
 TOMOS_ERR_ALLOC = -4
 TOMOS_ERR_NUMERIC = -5
 
+TOMOS_QR_ANY_SIGNS = 1  # tomos_sketch_qr_precond_ex_f64: R up to the signs of its rows
+
 CS_BUCKET_SEED = 0x12345678ABCDEF00
 CS_SIGN_SEED = 0xF00DD00D42BABE55
 
@@ -116,6 +118,7 @@ SIGNATURES = {
                                             c_vp, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
     "tomos_sketch_qr_scratch_bytes": (c_sz, [c_i64, c_i64]),
     "tomos_sketch_qr_precond_f64": (c_i32, [c_i64, c_i64, c_vp, c_i64, c_vp, c_vp, c_sz, c_vp]),
+    "tomos_sketch_qr_precond_ex_f64": (c_i32, [c_i64, c_i64, c_vp, c_i64, c_vp, c_i32, c_vp, c_sz, c_vp]),
     "tomos_column_scale": (c_i32, [c_vp, c_i64, c_vp, c_vp, c_vp]),
     "tomos_countsketch_apply_shard": (c_i32, [ctypes.POINTER(DenseDesc), c_i32, c_i64, c_u64, c_u64,
                                               c_i64, c_vp, c_i64, c_vp, c_vp, c_vp, c_i64, c_vp, c_sz,

@@ -988,11 +988,15 @@ __global__ void wide_equilibrate_kernel(double* G, int64_t n, const double* d) {
     }
 }
 
-// ||X||_F^2 of the n x n column-major X (one block).
-__global__ void wide_fro2_kernel(const double* X, int64_t n, double* out) {
+// ||X||_F^2 of the n x n column-major X: block b sums its contiguous
+// chunk into part[b], then one thread sums the parts in block order.
+__global__ void wide_fro2_part_kernel(const double* X, int64_t total, double* part) {
     __shared__ double sm[32];
+    const int64_t chunk = (total + gridDim.x - 1) / gridDim.x;
+    const int64_t e0 = (int64_t)blockIdx.x * chunk;
+    const int64_t e1 = e0 + chunk < total ? e0 + chunk : total;
     double s = 0.0;
-    for (int64_t e = threadIdx.x; e < n * n; e += blockDim.x) s += X[e] * X[e];
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) s += X[e] * X[e];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
@@ -1000,6 +1004,14 @@ __global__ void wide_fro2_kernel(const double* X, int64_t n, double* out) {
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sm[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void wide_fro2_sum_kernel(const double* part, int np, double* out) {
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int b = 0; b < np; ++b) t += part[b];
         *out = t;
     }
 }
@@ -1020,8 +1032,9 @@ __global__ void wide_output_kernel(const double* X, const double* Ur, const doub
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = e % n, j = e / n;
-        SA[(size_t)j * ld + i] = i <= j ? X[e] * sgn[j] : 0.0;
-        if (R) R[e] = i <= j ? sgn[i] * Ur[(size_t)i * n + j] * d[j] : 0.0;
+        const double sj = sgn ? sgn[j] : 1.0, si = sgn ? sgn[i] : 1.0;  // NULL: no signs
+        SA[(size_t)j * ld + i] = i <= j ? X[e] * sj : 0.0;
+        if (R) R[e] = i <= j ? si * Ur[(size_t)i * n + j] * d[j] : 0.0;
     }
 }
 
@@ -1266,8 +1279,12 @@ static tomos_status launch_fact(const FactArgs& fa, GridSync* gs, cudaStream_t s
 // The wide path (see above).  *done false: SA untouched, the panel path
 // must factor it (not used for this size, a failed pivot, or kappa above
 // kQrWideMaxKappa).
+// any_signs: R is returned with a positive diagonal (the Cholesky factor
+// scaled back) instead of LAPACK's row signs S, which skips Q_top and its
+// signed LU (R^-1 then differs from the LAPACK one by the signs of its
+// columns: R_h^-1 = R^-1 S).
 static tomos_status qr_wide(int64_t k, int64_t n, double* SA, int64_t ld, double* R, const WideScratch& w,
-                            cudaStream_t st, bool* done) {
+                            cudaStream_t st, bool* done, bool any_signs) {
     *done = false;
     TOMOS_CUDA_TRY(cudaMemsetAsync(w.flag, 0, sizeof(int) * 4, st));
     tomos_status s = qr_gemm<true>(SA, ld, SA, ld, w.G, n, n, n, k, 1.0, 0.0, w.P, w.pcap, st);
@@ -1292,8 +1309,14 @@ static tomos_status qr_wide(int64_t k, int64_t n, double* SA, int64_t ld, double
     if (s) return s;
     s = trtri_rt(w.Ur, n, w.X, n, w.Tb, w.P, w.pcap, st);
     if (s) return s;
-    wide_fro2_kernel<<<1, 1024, 0, st>>>(w.X, n, w.kap);
-    TOMOS_LAUNCH_CHECK("wide_fro2_kernel");
+    {
+        // the split-K partial buffer is free between the products
+        const int np = w.pcap >= 256 ? 256 : (int)w.pcap;
+        wide_fro2_part_kernel<<<np, 256, 0, st>>>(w.X, n * n, w.P);
+        TOMOS_LAUNCH_CHECK("wide_fro2_part_kernel");
+        wide_fro2_sum_kernel<<<1, 32, 0, st>>>(w.P, np, w.kap);
+        TOMOS_LAUNCH_CHECK("wide_fro2_sum_kernel");
+    }
     int flag = 0;
     double kap2 = 0.0;
     GridSync gsh{};
@@ -1306,6 +1329,12 @@ static tomos_status qr_wide(int64_t k, int64_t n, double* SA, int64_t ld, double
     if (flag || !(kappa <= kQrWideMaxKappa)) return TOMOS_OK;  // the panel path takes over
     wide_row_scale_kernel<<<eb, 256, 0, st>>>(w.X, n, w.d);
     TOMOS_LAUNCH_CHECK("wide_row_scale_kernel");
+    if (any_signs) {
+        wide_output_kernel<<<eb, 256, 0, st>>>(w.X, w.Ur, w.d, nullptr, n, SA, ld, R);
+        TOMOS_LAUNCH_CHECK("wide_output_kernel");
+        *done = true;
+        return TOMOS_OK;
+    }
     // Q_top = SA[0:n, :] R^-1 into G (no longer needed), then its signed LU
     s = qr_gemm<false>(SA, ld, w.X, n, w.G, n, n, n, n, 1.0, 0.0, w.P, w.pcap, st);
     if (s) return s;
@@ -1352,8 +1381,8 @@ size_t tomos_sketch_qr_scratch_bytes(int64_t k, int64_t n) {
     return qr_wide_used(n) ? panel + wide_layout(nullptr, n).bytes : panel;
 }
 
-tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64_t ld, double* R,
-                                         void* scratch, size_t scratch_bytes, void* stream) {
+tomos_status tomos_sketch_qr_precond_ex_f64(int64_t k, int64_t n, double* SA, int64_t ld, double* R,
+                                            int32_t flags, void* scratch, size_t scratch_bytes, void* stream) {
     if (k < n)
         return fail(TOMOS_ERR_INVALID,
                     "generate_sketch_qr_precond: sketched_mtx must have at least as many rows as "
@@ -1369,8 +1398,8 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
     cudaStream_t st = as_stream(stream);
     if (qr_wide_used(n) && scratch_bytes >= need.bytes + wide_layout(nullptr, n).bytes) {
         bool done = false;
-        tomos_status ws = qr_wide(k, n, SA, ld, R,
-                                  wide_layout(static_cast<char*>(scratch) + need.bytes, n), st, &done);
+        tomos_status ws = qr_wide(k, n, SA, ld, R, wide_layout(static_cast<char*>(scratch) + need.bytes, n),
+                                  st, &done, (flags & TOMOS_QR_ANY_SIGNS) != 0);
         if (ws) return ws;
         if (done) return TOMOS_OK;
         if (qr_wide_mode() == 3)
@@ -1496,6 +1525,11 @@ tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64
         return fail(TOMOS_ERR_NUMERIC,
                     "generate_sketch_qr_precond: trtri failed -- R is singular.");
     return trtri_rt(q.Rt, n, SA, ld, q.Tb, q.Pk, q.pk_doubles, st);
+}
+
+tomos_status tomos_sketch_qr_precond_f64(int64_t k, int64_t n, double* SA, int64_t ld, double* R,
+                                         void* scratch, size_t scratch_bytes, void* stream) {
+    return tomos_sketch_qr_precond_ex_f64(k, n, SA, ld, R, 0, scratch, scratch_bytes, stream);
 }
 
 }  // extern "C"
