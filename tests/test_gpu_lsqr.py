@@ -244,3 +244,28 @@ def test_zero_rhs_and_restarts():
     A0, b = config1(2000, 40, 2)
     x1, r1 = solve(to_dense(A0, L.ROW_MAJOR), b, max_iters=3, restarts=4)
     assert r1["iterations"] <= 12
+
+
+def test_repeated_solves_on_one_workspace():
+    """Solves that reuse a workspace (and its captured iteration graph) read
+    the column scale and x of the current call: the caller's buffers of an
+    earlier call are freed and overwritten in between (NaN-filled tensors of
+    their size take their memory), and every solve still converges with the
+    same iterations and the same x."""
+    A0, b = scaled_problem(30000, 300, 21)
+    A = to_dense(A0, L.ROW_MAJOR, NT.FP32_16, pad=4)
+    ws = tb.create_lsqr_workspace(None, A.size, NT.FP32, NT.FP64)
+    bd = cuda(b)
+    out = []
+    for _ in range(4):
+        x, rep, d = tb.sketch_lsqr(A, bd, 1200, workspace=ws)
+        out.append((x.cpu().numpy(), rep["iterations"], rep["converged"], rep["backward_error"]))
+        del x, d
+        junk = [torch.full((300,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(8)]
+        junk += [torch.full((300,), float("nan"), dtype=torch.float32, device="cuda") for _ in range(8)]
+        del junk
+    x0, it0, c0, e0 = out[0]
+    assert c0 == 1 and e0 <= 1e-6
+    for x, it, c, e in out[1:]:
+        assert c == 1 and it == it0 and e == e0
+        assert np.array_equal(x, x0)

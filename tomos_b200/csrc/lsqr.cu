@@ -115,9 +115,13 @@ __global__ void scaled_sumsq_kernel(const float* __restrict__ x, const double* _
 }
 
 // FP64 column-major and row-major copies of a dense n x n preconditioner.
+// Both copies of the preconditioner; *lower_nz (zeroed before) becomes 1
+// if any element below the diagonal is nonzero, else the n-side products
+// skip the zero triangle of the (sketch QR's upper triangular) R^{-1}.
 __global__ void precond_copy_kernel(const void* R, int numeric, int layout, int64_t ld, int64_t n,
-                                    double* Rcm, double* Rrm) {
+                                    double* Rcm, double* Rrm, double* lower_nz) {
     const int64_t total = n * n;
+    bool nz = false;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = k % n, j = k / n;  // element (i, j)
@@ -126,7 +130,9 @@ __global__ void precond_copy_kernel(const void* R, int numeric, int layout, int6
                                          : (double)static_cast<const float*>(R)[src];
         Rcm[(size_t)j * n + i] = v;
         Rrm[(size_t)i * n + j] = v;
+        nz = nz || (i > j && v != 0.0);
     }
+    if (nz) *lower_nz = 1.0;  // every writer stores the same value
 }
 
 // d_j = sqrt(colsq_j) (1 for an empty column) and ||A D^{-1}||_F =
@@ -205,8 +211,16 @@ __global__ void __launch_bounds__(256) nside_reduce_kernel(NSide S) {
     double q = 0.0;
     if (S.qsum)
         q = (w == 0 && j < S.n) ? S.qsum[j] : 0.0;
-    else if (j < S.n)
-        for (int c = w; c < S.gq; c += 8) q += (double)S.qpart[(size_t)c * S.qstride + j];
+    else if (j < S.n) {
+        double q1 = 0.0;
+        int c = w;
+        for (; c + 8 < S.gq; c += 16) {
+            q += (double)S.qpart[(size_t)c * S.qstride + j];
+            q1 += (double)S.qpart[(size_t)(c + 8) * S.qstride + j];
+        }
+        if (c < S.gq) q += (double)S.qpart[(size_t)c * S.qstride + j];
+        q += q1;
+    }
     smq[w][lane] = q;
     __syncthreads();
     if (w == 0) {
@@ -246,9 +260,16 @@ __global__ void __launch_bounds__(256) nside_precond_t_kernel(NSide S) {
     double vh2 = 0.0;
     if (j < S.n) {
         const double* col = S.Rcm + (size_t)j * S.n;
-        double z = 0.0;
-        for (int64_t i = lane; i < S.n; i += 32) z += col[i] * S.t[i];
-        z = warp_sum(z);
+        // an upper triangular M: column j ends at row j
+        const int64_t ie = S.scal[7] != 0.0 ? S.n : j + 1;
+        double z0 = 0.0, z1 = 0.0;
+        int64_t i = lane;
+        for (; i + 32 < ie; i += 64) {
+            z0 = fma(col[i], S.t[i], z0);
+            z1 = fma(col[i + 32], S.t[i + 32], z1);
+        }
+        if (i < ie) z0 = fma(col[i], S.t[i], z0);
+        double z = warp_sum(z0 + z1);
         const double vh = S.init ? z : z - beta * (double)S.v[j];
         if (lane == 0) S.vhat[j] = vh;
         vh2 = vh * vh;
@@ -282,9 +303,15 @@ __global__ void __launch_bounds__(256) nside_update_kernel(NSide S) {
         double pi;
         if (S.has_precond) {
             const double* row = S.Rrm + (size_t)i * S.n;
-            double z = 0.0;
-            for (int64_t jj = lane; jj < S.n; jj += 32) z += row[jj] * S.vhat[jj];
-            pi = warp_sum(z) * inva;
+            // an upper triangular M: row i starts at column i
+            int64_t jj = (S.scal[7] != 0.0 ? 0 : i) + lane;
+            double z0 = 0.0, z1 = 0.0;
+            for (; jj + 32 < S.n; jj += 64) {
+                z0 = fma(row[jj], S.vhat[jj], z0);
+                z1 = fma(row[jj + 32], S.vhat[jj + 32], z1);
+            }
+            if (jj < S.n) z0 = fma(row[jj], S.vhat[jj], z0);
+            pi = warp_sum(z0 + z1) * inva;
         } else {
             pi = S.vhat[i] * inva;
         }
@@ -377,7 +404,8 @@ static void ws_free(tomos_workspace* ws) {
     void* ptrs[] = {ws->u,      ws->v,      ws->wt,     ws->p,    ws->qvec,   ws->t,
                     ws->vhat,   ws->qpart,  ws->sspart, ws->vpart, ws->xpart, ws->qnpart,
                     ws->scal,   ws->coef_init, ws->bpart, ws->fro2, ws->st,   ws->Rcm,
-                    ws->Rrm,    ws->hist,   ws->scratch, ws->h16, ws->adj, ws->csc, ws->shard, ws->adjb};
+                    ws->Rrm,    ws->hist,   ws->scratch, ws->h16, ws->adj, ws->csc, ws->shard, ws->adjb,
+                    ws->xg,     ws->dscale};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (ws->st_host) cudaFreeHost(ws->st_host);
@@ -778,9 +806,10 @@ struct DensePass : PassOps {
 
 tomos_status refresh_precond(tomos_workspace* ws, cudaStream_t st) {
     if (!ws->has_precond) return TOMOS_OK;
+    TOMOS_CUDA_TRY(cudaMemsetAsync(ws->scal + 7, 0, sizeof(double), st));
     precond_copy_kernel<<<ws->gs_max, 256, 0, st>>>(ws->precond.values, ws->precond.numeric,
                                                    ws->precond.layout, ws->precond.ld, ws->n,
-                                                   ws->Rcm, ws->Rrm);
+                                                   ws->Rcm, ws->Rrm, ws->scal + 7);
     TOMOS_LAUNCH_CHECK("precond_copy_kernel");
     ws->launches += 1;
     return TOMOS_OK;
@@ -804,7 +833,7 @@ static double eta_of(const LsqrDev& s) {
     return e1 < e2 ? e1 : e2;
 }
 
-tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, float* x,
+tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, float* x_user,
                           const tomos_lsqr_opts* o, tomos_lsqr_report* rep, void* user_stream) {
     cudaStream_t us = as_stream(user_stream);
     cudaStream_t st = ws->stream;
@@ -848,14 +877,28 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     // Precondition copies (FP64, both orientations).
     s = refresh_precond(ws, st);
     if (s) return s;
-    if (!o->warm_start) TOMOS_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(float) * n, st));
+    // The solve runs on the workspace's copy of x, so the iteration graph
+    // (whose kernels hold x's address) is reused whatever buffer the
+    // caller passes; the result is copied out at the end.
+    float* x = ws->xg;
+    if (o->warm_start)
+        TOMOS_CUDA_TRY(cudaMemcpyAsync(x, x_user, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    else
+        TOMOS_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(float) * n, st));
     s = ops.prepare(st);
     if (s) return s;
 
     // ||b|| and, for the backward-error rule, ||A||_F go into the device
     // state by a kernel (no host round trip before the first pass).
     int extra_passes = 0;
-    const double* dsc = o->stop_rule == TOMOS_STOP_BACKWARD ? o->col_scale : nullptr;
+    // The column scale the n-side kernels read (the iteration graph holds
+    // its address): the workspace's copy, so a graph captured by an earlier
+    // solve never reads a caller's buffer that has since been freed.
+    const double* dsc = nullptr;
+    if (o->stop_rule == TOMOS_STOP_BACKWARD && o->col_scale) {
+        TOMOS_CUDA_TRY(cudaMemcpyAsync(ws->dscale, o->col_scale, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        dsc = ws->dscale;
+    }
     const bool need_fro = o->stop_rule == TOMOS_STOP_BACKWARD && !o->anorm_fro_dev && !(o->anorm_fro > 0.0);
 
     LsqrDev init_state;
@@ -913,6 +956,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
                                  (uint64_t)pl_iter.grid,
                                  (uint64_t)pl_iter.tpw,
                                  reinterpret_cast<uint64_t>(x),
+                                 reinterpret_cast<uint64_t>(dsc),
                                  (uint64_t)ws->has_precond,
                                  (uint64_t)n,
                                  (uint64_t)m,
@@ -1069,6 +1113,7 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
         R.backward_error = eta_of(H);
         converged = R.backward_error <= o->tol;
     }
+    TOMOS_CUDA_TRY(cudaMemcpyAsync(x_user, x, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
     TOMOS_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
     TOMOS_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
     float ms = 0.0f;
@@ -1191,6 +1236,8 @@ tomos_status tomos_workspace_create(int64_t m, int64_t n, int32_t value_type,
     A(alloc(&ws->fro2, 1));
     A(alloc(&ws->st, 1));
     A(alloc(&ws->shard, (size_t)n + 1));
+    A(alloc(&ws->xg, (size_t)n));
+    A(alloc(&ws->dscale, (size_t)n));
     A(cudaMallocHost(reinterpret_cast<void**>(&ws->st_host), sizeof(LsqrDev)));
     A(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
     A(cudaEventCreate(&ws->ev_start));

@@ -202,6 +202,11 @@ struct tomos_workspace {
     // row-sharded solves: the pass's partial sums folded to n + 1 doubles
     // (A^T u, ||u||^2), summed across ranks (comm.cu)
     double* shard = nullptr;
+    // the solution the solve iterates on (copied from / to the caller's x),
+    // so the iteration graph does not depend on the caller's buffer
+    float* xg = nullptr;
+    // the column scale of the backward-error rule (copied from the caller's)
+    double* dscale = nullptr;
     tomos_comm* comm = nullptr;  // the running solve's communicator (or NULL)
 
     bool has_precond = false;
