@@ -319,7 +319,11 @@ tomos_status tomos_sketch_qr_precond_ex_f64(int64_t k, int64_t n, double* SA, in
  *   eta_D = min( ||r|| / (||A D^{-1}||_F ||D x|| + ||b||),
  *                ||D^{-1} A^T r|| / (||A D^{-1}||_F ||r||) ),
  * which is invariant to the scaling of A's columns; with D the column
- * norms it is the backward error of the equilibrated problem. */
+ * norms it is the backward error of the equilibrated problem.  With
+ * BACKWARD at tol >= 1e-6 the accurate-tier passes form their row dots
+ * as FP32 products over runs of at most 8, summed in FP64 (a backward
+ * error of at most 4.8e-7 an element); below 1e-6, and under RELRES, as
+ * one FP64 product an element. */
 enum tomos_stop { TOMOS_STOP_RELRES = 0, TOMOS_STOP_BACKWARD = 1 };
 
 typedef struct tomos_lsqr_opts {

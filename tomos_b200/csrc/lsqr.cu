@@ -447,13 +447,17 @@ static tomos_status ensure_history(tomos_workspace* ws, int cap) {
 
 // ------------------------------------------------------------ A passes
 
-// The LSQR pass (kRowBoth) for every element type and FP64 flag.
-static tomos_status launch_fused(Elem e, bool acc64, const FusedParams& P, int* err, int nch,
-                                 int g, int grid, cudaStream_t st) {
+// The LSQR pass (kRowBoth) for every element type and FP64 flag; runs:
+// the FP64-summing passes of the FP32 and exact two-plane types form their
+// row dots as FP32 products over short runs (kRowBothRuns).
+static tomos_status launch_fused(Elem e, bool acc64, bool runs, const FusedParams& P, int* err,
+                                 int nch, int g, int grid, cudaStream_t st) {
+#define TOMOS_BOTH(EE)                                                                    \
+    (runs ? launch_fused_e<EE, true, kRowBothRuns>(P, err, nch, g, grid, st)              \
+          : launch_fused_e<EE, true, kRowBoth>(P, err, nch, g, grid, st))
     switch (e) {
         case Elem::F32:
-            return acc64 ? launch_fused_e<Elem::F32, true, kRowBoth>(P, err, nch, g, grid, st)
-                         : launch_fused_e<Elem::F32, false, kRowBoth>(P, err, nch, g, grid, st);
+            return acc64 ? TOMOS_BOTH(Elem::F32) : launch_fused_e<Elem::F32, false, kRowBoth>(P, err, nch, g, grid, st);
         case Elem::H16:
             return acc64 ? launch_fused_e<Elem::H16, true, kRowBoth>(P, err, nch, g, grid, st)
                          : launch_fused_e<Elem::H16, false, kRowBoth>(P, err, nch, g, grid, st);
@@ -463,11 +467,12 @@ static tomos_status launch_fused(Elem e, bool acc64, const FusedParams& P, int* 
         case Elem::F16:
             return acc64 ? launch_fused_e<Elem::F16, true, kRowBoth>(P, err, nch, g, grid, st)
                          : launch_fused_e<Elem::F16, false, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::A16: return launch_fused_e<Elem::A16, true, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::AB16: return launch_fused_e<Elem::AB16, true, kRowBoth>(P, err, nch, g, grid, st);
-        case Elem::AB16R: return launch_fused_e<Elem::AB16R, true, kRowBoth>(P, err, nch, g, grid, st);
+        case Elem::A16: return TOMOS_BOTH(Elem::A16);
+        case Elem::AB16: return TOMOS_BOTH(Elem::AB16);
+        case Elem::AB16R: return TOMOS_BOTH(Elem::AB16R);
         default: return fail(TOMOS_ERR_UNSUPPORTED, "fused pass: element type");
     }
+#undef TOMOS_BOTH
 }
 
 // The staged-fp16 pass on the tensor cores (rowpass_mma.cuh).
@@ -603,7 +608,8 @@ tomos_status enqueue_dense_pass(tomos_workspace* ws, const tomos_dense* A,
         P.qstride = pl.qstride;
         P.skip = skip;
         tomos_status ls = pl.tpw > 0 ? launch_fused_mma(pl.e, P, &ws->st->pipe_err, pl.tpw, pl.grid, st)
-                                     : launch_fused(pl.e, pl.acc64, P, &ws->st->pipe_err, pl.nch, pl.g, pl.grid, st);
+                                     : launch_fused(pl.e, pl.acc64, pl.runs, P, &ws->st->pipe_err, pl.nch, pl.g,
+                                                    pl.grid, st);
         if (ls) return ls;
         ws->launches += 1;
         return TOMOS_OK;
@@ -946,6 +952,13 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
 
     PassPlan pl_init = ops.plan(true);
     PassPlan pl_iter = ops.plan(false);
+    // Under the BACKWARD rule at a tolerance of 1e-6 or above, the accurate
+    // passes' dots need only a backward error below it: FP32 products over
+    // runs of at most 8, summed in FP64 (gamma_8 = 4.8e-7), the accuracy of
+    // the FP32 tier's own passes, instead of one FP64 conversion and product
+    // an element.  RELRES keeps the FP64 products: the residual of a
+    // consistent system is far below the rounding of its products.
+    if (o->stop_rule == TOMOS_STOP_BACKWARD && o->tol >= kRunsTolMin) pl_init.runs = true;
 
     // Capture (or reuse) the graph of one iteration.
     std::vector<uint64_t> key = {ops.key(),

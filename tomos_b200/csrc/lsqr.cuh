@@ -37,6 +37,9 @@ struct LsqrDev {
 };
 
 // How one pass over A is run.
+// The BACKWARD tolerance from which the accurate passes sum FP32 runs.
+constexpr double kRunsTolMin = 1e-6;
+
 struct PassPlan {
     bool fused = false;
     Elem e = Elem::F32;
@@ -49,6 +52,7 @@ struct PassPlan {
     int64_t qstride = 0;
     int tpw = 0;     // > 0: the tensor-core pass, k-tiles per consumer warp
     int src = 0;     // 1: the pass reads the refine copy of A (RefinePass)
+    bool runs = false;  // FP64-summing fused pass: dots as FP32 runs (kRowBothRuns)
 };
 
 // One pass over A producing ut = cp*A p + cu*u_in in the workspace's u,

@@ -94,6 +94,11 @@ enum RowMode : int {
     kRowBoth = 0,  // the LSQR pass: ut = cp A p + cu u, partials of A^T ut and ||ut||^2
     kRowDot = 1,   // ut = cp A p + cu u only (a product whose lines are dots)
     kRowAxpy = 2,  // partials of A^T (cu u) only (a product that sums lines)
+    kRowBothRuns = 3,  // kRowBoth with ACC64: the row dots as FP32 products
+                       // over runs of at most 8 (a lane's float2 chains),
+                       // summed in FP64, instead of one FP64 product an
+                       // element; the backward error of a dot is then at
+                       // most gamma_8 = 4.8e-7 (gamma_4 for two-plane rows)
 };
 
 struct RowPassParams {
@@ -256,9 +261,11 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
     constexpr int CW = RowWarps<E, ACC64>::value;  // consumer warps
     constexpr bool DOT = MODE != kRowAxpy;         // forms the row dots
     constexpr bool AXPY = MODE != kRowDot;         // accumulates A^T ut
-    // FP64 p and per-element FP64 products: the exact LSQR passes.  The
-    // standalone FP64 tiers (kRowDot, kRowAxpy with ACC64) form FP32
-    // products over short runs and sum those in FP64.
+    constexpr bool BOTH = MODE == kRowBoth || MODE == kRowBothRuns;  // an LSQR pass
+    // FP64 p and per-element FP64 products: the exact LSQR passes of the
+    // RELRES rule (a consistent system's residual keeps its digits).  The
+    // standalone FP64 tiers (kRowDot, kRowAxpy with ACC64) and kRowBothRuns
+    // form FP32 products over short runs and sum those in FP64.
     constexpr bool P64 = ACC64 && MODE == kRowBoth;
     // FP32_16 wh words in a standalone dot product: every word converted as
     // an fp16 value, and the rare control words corrected afterwards by the
@@ -316,7 +323,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
 #pragma unroll
     for (int j = 0; j < PER / 2; ++j) acc[j] = make_float2(0.0f, 0.0f);
     // kRowAxpy with ACC64: FP64 sums of the FP32 run sums held in acc
-    constexpr int NACC64 = (AXPY && ACC64 && MODE != kRowBoth) ? PER : 1;
+    constexpr int NACC64 = (AXPY && ACC64 && !BOTH) ? PER : 1;
     double acc64[NACC64];
 #pragma unroll
     for (int j = 0; j < NACC64; ++j) acc64[j] = 0.0;
@@ -378,7 +385,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         const double cp = P.coef ? P.coef[0] : P.cp;
         const double cu = P.coef ? P.coef[1] : P.cu;
         // a product with cu == 0 never reads u (it may hold NaN)
-        const bool use_u = MODE == kRowBoth || cu != 0.0;
+        const bool use_u = BOTH || cu != 0.0;
         const int64_t n = P.n;
         const int64_t nchunks = (n + VEC - 1) / VEC;
         int coff[NCH];
@@ -531,7 +538,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
             if constexpr (DOT) {
                 if (lane == 0 && part == 0 && has) {
                     P.u_out[i] = ut;
-                    if constexpr (MODE == kRowBoth) ss += (double)ut * (double)ut;
+                    if constexpr (BOTH) ss += (double)ut * (double)ut;
                 }
             }
             if constexpr (AXPY) {
@@ -539,7 +546,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
 #pragma unroll
                 for (int j = 0; j < PER / 2; ++j) acc[j] = __ffma2_rn(a[j], ut2, acc[j]);
 
-                if constexpr (ACC64 && MODE != kRowBoth) {
+                if constexpr (ACC64 && !BOTH) {
                     if ((t + 1) % kRowPromote == 0) {
 #pragma unroll
                         for (int j = 0; j < PER / 2; ++j) {
@@ -551,7 +558,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
                 }
             }
         }
-        if constexpr (AXPY && ACC64 && MODE != kRowBoth) {
+        if constexpr (AXPY && ACC64 && !BOTH) {
 #pragma unroll
             for (int j = 0; j < PER / 2; ++j) {
                 acc64[2 * j] += (double)acc[j].x;
@@ -608,7 +615,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused
         for (int r = 0; r < RS; ++r) sum += red[(size_t)(r * G + g) * WCOLS + loc];
         qout[j] = sum;
     }
-    if (MODE == kRowBoth && threadIdx.x == 0) {
+    if (BOTH && threadIdx.x == 0) {
         double sum = 0.0;
 #pragma unroll
         for (int w = 0; w < CW; ++w) sum += ssw[w];
