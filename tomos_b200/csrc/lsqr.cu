@@ -549,13 +549,15 @@ __global__ void __launch_bounds__(128) stage_half_kernel(const uint16_t* __restr
 // Chooses the fused pass when A is row-major with 16-byte aligned rows
 // and n fits the consumer warps (12288 columns; 8192 or 6144 for ACC64); otherwise
 // the generic two-kernel path.
-PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64) {
+PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64, bool runs) {
     PassPlan pl;
     pl.e = e;
     pl.acc64 = acc64 || elem_is_exact(e);
+    // run-summed dots: the FP32 and two-plane FP64-summing passes
+    pl.runs = runs && pl.acc64 && (e == Elem::F32 || elem_two_planes(e));
     int nch = 0, g = 1;
     const bool ok = A->layout == TOMOS_ROW_MAJOR && A->cols > 0 &&
-                    plan_row_lines(e, pl.acc64, A->cols, A->ld, A->values,
+                    plan_row_lines(e, pl.acc64 && !pl.runs, A->cols, A->ld, A->values,
                                    elem_is_exact(e) ? dense_lo_plane(A) : nullptr, &nch, &g);
     if (ok) {
         pl.fused = true;
@@ -766,7 +768,7 @@ struct DensePass : PassOps {
     }
     PassPlan plan(bool init) override {
         if (!init && stage) return plan_dense_pass(ws, &staged, Elem::F16, false);
-        return plan_dense_pass(ws, A, init ? init_e : iter_e, init);
+        return plan_dense_pass(ws, A, init ? init_e : iter_e, init, init && runs);
     }
     tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in, const double* coef,
                          const int* skip, cudaStream_t st) override {
@@ -950,15 +952,15 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
                                           need_fro ? ws->scal + 3 : nullptr, ws->st);
     TOMOS_LAUNCH_CHECK("state_norms_kernel");
 
-    PassPlan pl_init = ops.plan(true);
-    PassPlan pl_iter = ops.plan(false);
     // Under the BACKWARD rule at a tolerance of 1e-6 or above, the accurate
     // passes' dots need only a backward error below it: FP32 products over
     // runs of at most 8, summed in FP64 (gamma_8 = 4.8e-7), the accuracy of
     // the FP32 tier's own passes, instead of one FP64 conversion and product
     // an element.  RELRES keeps the FP64 products: the residual of a
     // consistent system is far below the rounding of its products.
-    if (o->stop_rule == TOMOS_STOP_BACKWARD && o->tol >= kRunsTolMin) pl_init.runs = true;
+    ops.runs = o->stop_rule == TOMOS_STOP_BACKWARD && o->tol >= kRunsTolMin;
+    PassPlan pl_init = ops.plan(true);
+    PassPlan pl_iter = ops.plan(false);
 
     // Capture (or reuse) the graph of one iteration.
     std::vector<uint64_t> key = {ops.key(),

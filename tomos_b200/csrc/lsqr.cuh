@@ -60,6 +60,8 @@ struct PassPlan {
 // rows of stride qstride).
 struct PassOps {
     virtual ~PassOps() = default;
+    // accurate (init) passes may form their dots as FP32 runs (kRowBothRuns)
+    bool runs = false;
     virtual PassPlan plan(bool init) = 0;
     virtual tomos_status enqueue(const PassPlan& pl, const float* p, const float* u_in,
                                  const double* coef, const int* skip, cudaStream_t st) = 0;
@@ -84,6 +86,8 @@ struct RefinePass : PassOps {
     PassOps& re;
     RefinePass(PassOps& a, PassOps& r) : it(a), re(r) {}
     PassPlan plan(bool init) override {
+        re.runs = runs;
+        it.runs = runs;
         PassPlan p = init ? re.plan(true) : it.plan(false);
         p.src = init ? 1 : 0;
         return p;
@@ -131,7 +135,7 @@ __device__ __forceinline__ double block_sum_array(const double* part, int64_t np
 // One pass over a dense A (the fused kernel when pl.fused, else the
 // generic two-kernel path): ut = cp A p + cu u_in into ws->u, the
 // partials of A^T ut into ws->qpart and of ||ut||^2 into ws->sspart.
-PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64);
+PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool acc64, bool runs = false);
 
 // Options every solve entry accepts (stop rule, iteration counts).
 bool opts_ok(const tomos_lsqr_opts* o, std::string* why);

@@ -54,37 +54,6 @@
 namespace tomos_b200 {
 
 template <Elem E>
-struct RowPlanes;
-
-// Consumer warps of a pass.  13 warps (with the producer) leave 128
-// registers a thread; the FP64-accumulating passes over one plane keep p
-// in FP64 and a whole row part per lane, and run 8 consumers (9 warps: up
-// to 168 registers) so that a warp still covers 1024 columns.  The exact
-// two-plane decodes are ALU-heavy and keep 12 warps (a warp covering 512
-// columns) to hide their latency.
-template <Elem E, bool ACC64>
-struct RowWarps {
-    static constexpr int value = !ACC64 ? ((E == Elem::F16 || E == Elem::B16) ? 16 : 12)
-                                        : (RowPlanes<E>::value == 1 ? 8 : 16);
-};
-constexpr int kRowWarps = 16;  // the widest configuration (shared arrays)
-
-// 16-byte chunks a lane takes per row part at most (a warp covers 32 x
-// that x VEC columns).
-template <Elem E, bool ACC64>
-struct RowNchMax {
-    static constexpr int base = (E == Elem::F32) ? 8 : 4;
-    static constexpr int value = (ACC64 && RowPlanes<E>::value == 2) ? base / 2 : base;
-};
-constexpr int kRowMaxStages = 12;
-constexpr size_t kRowSmemBudget = 216 * 1024;
-// Bytes a bulk copy of one plane of a stage aims at: each copy carries a
-// fixed cost beside its bytes (measured about a microsecond a stage for
-// 24-48 KB copies), so stages of one tile of short 16-bit rows would bound
-// the pass below the memory rate.
-constexpr size_t kRowCopyTarget = 48 * 1024;
-
-template <Elem E>
 struct RowPlanes {
     static constexpr int value = (E == Elem::A16 || E == Elem::AB16 || E == Elem::AB16R) ? 2 : 1;
 };
@@ -100,6 +69,42 @@ enum RowMode : int {
                        // element; the backward error of a dot is then at
                        // most gamma_8 = 4.8e-7 (gamma_4 for two-plane rows)
 };
+
+// Passes that hold an FP64 register per column of a lane: the LSQR pass
+// with FP64 products (p in FP64) and the FP64-accumulating A^T product.
+template <bool ACC64, int MODE>
+struct RowF64Regs {
+    static constexpr bool value = ACC64 && (MODE == kRowBoth || MODE == kRowAxpy);
+};
+
+// Consumer warps of a pass.  13 warps (with the producer) leave 128
+// registers a thread; the passes with FP64 registers per column over one
+// plane keep a whole row part per lane, and run 8 consumers (9 warps: up
+// to 168 registers) so that a warp still covers 1024 columns; over two
+// planes they keep 16 warps (a warp covering 512 columns) to hide the
+// exact decode's latency.
+template <Elem E, bool ACC64, int MODE>
+struct RowWarps {
+    static constexpr int value = !RowF64Regs<ACC64, MODE>::value
+                                     ? ((E == Elem::F16 || E == Elem::B16) ? 16 : 12)
+                                     : (RowPlanes<E>::value == 1 ? 8 : 16);
+};
+constexpr int kRowWarps = 16;  // the widest configuration (shared arrays)
+
+// 16-byte chunks a lane takes per row part at most (a warp covers 32 x
+// that x VEC columns).
+template <Elem E, bool ACC64, int MODE>
+struct RowNchMax {
+    static constexpr int base = (E == Elem::F32) ? 8 : 4;
+    static constexpr int value = (RowF64Regs<ACC64, MODE>::value && RowPlanes<E>::value == 2) ? base / 2 : base;
+};
+constexpr int kRowMaxStages = 12;
+constexpr size_t kRowSmemBudget = 216 * 1024;
+// Bytes a bulk copy of one plane of a stage aims at: each copy carries a
+// fixed cost beside its bytes (measured about a microsecond a stage for
+// 24-48 KB copies), so stages of one tile of short 16-bit rows would bound
+// the pass below the memory rate.
+constexpr size_t kRowCopyTarget = 48 * 1024;
 
 struct RowPassParams {
     FusedParams f;
@@ -257,8 +262,8 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
 }
 
 template <Elem E, int NCH, int G, bool ACC64, int MODE>
-__global__ void __launch_bounds__((RowWarps<E, ACC64>::value + 1) * 32, 1) fused_rows_kernel(RowPassParams T) {
-    constexpr int CW = RowWarps<E, ACC64>::value;  // consumer warps
+__global__ void __launch_bounds__((RowWarps<E, ACC64, MODE>::value + 1) * 32, 1) fused_rows_kernel(RowPassParams T) {
+    constexpr int CW = RowWarps<E, ACC64, MODE>::value;  // consumer warps
     constexpr bool DOT = MODE != kRowAxpy;         // forms the row dots
     constexpr bool AXPY = MODE != kRowDot;         // accumulates A^T ut
     constexpr bool BOTH = MODE == kRowBoth || MODE == kRowBothRuns;  // an LSQR pass
@@ -630,7 +635,7 @@ inline size_t fused_rows_smem(int nstage, int rows_per_stage, int copy_bytes) {
     constexpr int VEC = ChunkElems<E>::value;
     const size_t ring = (size_t)nstage * rows_per_stage * copy_bytes * RowPlanes<E>::value;
     const size_t esz = (ACC64 && MODE == kRowAxpy) ? sizeof(double) : sizeof(float);
-    const size_t red = (size_t)RowWarps<E, ACC64>::value * NCH * 32 * VEC * esz;
+    const size_t red = (size_t)RowWarps<E, ACC64, MODE>::value * NCH * 32 * VEC * esz;
     return ring > red ? ring : red;
 }
 

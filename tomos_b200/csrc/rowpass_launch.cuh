@@ -16,7 +16,7 @@ template <Elem E, int NCH, int G, bool ACC64, int MODE>
 inline tomos_status launch_fused_t(const FusedParams& P, int* err, int grid, cudaStream_t st,
                                    double* qpart64 = nullptr) {
     constexpr int ESZ = (E == Elem::F32) ? 4 : 2;
-    constexpr int CW = RowWarps<E, ACC64>::value;
+    constexpr int CW = RowWarps<E, ACC64, MODE>::value;
     constexpr int RS = CW / G;
     RowPassParams T;
     T.f = P;
@@ -48,24 +48,25 @@ inline bool elem_two_planes(Elem e) {
     return e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R;
 }
 
-// 16-byte chunks a lane takes per row part at most (RowNchMax).
-inline int fused_nch_max(Elem e, bool acc64) {
+// 16-byte chunks a lane takes per row part at most (RowNchMax); f64regs:
+// the pass holds FP64 registers per column (RowF64Regs).
+inline int fused_nch_max(Elem e, bool f64regs) {
     const int base = (e == Elem::F32) ? 8 : 4;
-    return (acc64 && elem_two_planes(e)) ? base / 2 : base;
+    return (f64regs && elem_two_planes(e)) ? base / 2 : base;
 }
 
 // Consumer warps of a pass (RowWarps).
-inline int fused_warps(Elem e, bool acc64) {
-    return !acc64 ? ((e == Elem::F16 || e == Elem::B16) ? 16 : 12) : (elem_two_planes(e) ? 16 : 8);
+inline int fused_warps(Elem e, bool f64regs) {
+    return !f64regs ? ((e == Elem::F16 || e == Elem::B16) ? 16 : 12) : (elem_two_planes(e) ? 16 : 8);
 }
 
 // Warps per row a pass may split a row over (divisors of its consumer
 // warps).
-inline const int* fused_g_list(Elem e, bool acc64, int* count) {
+inline const int* fused_g_list(Elem e, bool f64regs, int* count) {
     static const int g12[] = {2, 3, 4, 6, 12};
     static const int g8[] = {2, 4, 8};
     static const int g16[] = {2, 4, 8, 16};
-    const int w = fused_warps(e, acc64);
+    const int w = fused_warps(e, f64regs);
     *count = w == 8 ? 3 : (w == 16 ? 4 : 5);
     return w == 8 ? g8 : (w == 16 ? g16 : g12);
 }
@@ -74,14 +75,14 @@ inline const int* fused_g_list(Elem e, bool acc64, int* count) {
 // ld: chunks per lane (nch) and warps per line (g), or false when the
 // lines are not 16-byte aligned (both planes for two-plane types), too
 // long for the consumer warps, or too long for a stage ring of two.
-inline bool plan_row_lines(Elem e, bool acc64, int64_t inner, int64_t ld, const void* hi,
+inline bool plan_row_lines(Elem e, bool f64regs, int64_t inner, int64_t ld, const void* hi,
                            const void* lo, int* nch_out, int* g_out) {
     const int vec = (e == Elem::F32) ? 4 : 8;
     const int wbytes = (e == Elem::F32) ? 4 : 2;
     if (inner <= 0 || (ld * wbytes) % 16 != 0 || reinterpret_cast<uintptr_t>(hi) % 16 != 0) return false;
     if (elem_two_planes(e) && reinterpret_cast<uintptr_t>(lo) % 16 != 0) return false;
     int nch = 0, g = 1;
-    const int nmax = fused_nch_max(e, acc64);
+    const int nmax = fused_nch_max(e, f64regs);
     for (int c : {1, 2, 4, 8}) {
         if (c > nmax) break;
         if ((int64_t)32 * c * vec >= inner) {
@@ -91,7 +92,7 @@ inline bool plan_row_lines(Elem e, bool acc64, int64_t inner, int64_t ld, const 
     }
     if (nch == 0) {
         int ng = 0;
-        const int* gl = fused_g_list(e, acc64, &ng);
+        const int* gl = fused_g_list(e, f64regs, &ng);
         for (int q = 0; q < ng; ++q) {
             if ((int64_t)gl[q] * 32 * nmax * vec >= inner) {
                 nch = nmax;
@@ -101,7 +102,7 @@ inline bool plan_row_lines(Elem e, bool acc64, int64_t inner, int64_t ld, const 
         }
     }
     if (nch == 0) return false;
-    const int64_t rows_per_stage = fused_warps(e, acc64) / g;
+    const int64_t rows_per_stage = fused_warps(e, f64regs) / g;
     const int64_t stage = rows_per_stage * ((inner * wbytes + 15) / 16 * 16) * (elem_two_planes(e) ? 2 : 1);
     if (2 * stage > (int64_t)kRowSmemBudget) return false;
     *nch_out = nch;
@@ -122,7 +123,7 @@ inline int row_pass_grid(int64_t outer) {
 template <Elem E, bool ACC64, int MODE>
 inline tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int g, int grid,
                                    cudaStream_t st, double* qpart64 = nullptr) {
-    constexpr int NMAX = RowNchMax<E, ACC64>::value;
+    constexpr int NMAX = RowNchMax<E, ACC64, MODE>::value;
     if (g == 1) {
         switch (nch) {
             case 1: return launch_fused_t<E, 1, 1, ACC64, MODE>(P, err, grid, st, qpart64);
@@ -136,14 +137,14 @@ inline tomos_status launch_fused_e(const FusedParams& P, int* err, int nch, int 
             default: break;
         }
     } else if (nch == NMAX) {
-        if constexpr (RowWarps<E, ACC64>::value == 8) {
+        if constexpr (RowWarps<E, ACC64, MODE>::value == 8) {
             switch (g) {
                 case 2: return launch_fused_t<E, NMAX, 2, ACC64, MODE>(P, err, grid, st, qpart64);
                 case 4: return launch_fused_t<E, NMAX, 4, ACC64, MODE>(P, err, grid, st, qpart64);
                 case 8: return launch_fused_t<E, NMAX, 8, ACC64, MODE>(P, err, grid, st, qpart64);
                 default: break;
             }
-        } else if constexpr (RowWarps<E, ACC64>::value == 16) {
+        } else if constexpr (RowWarps<E, ACC64, MODE>::value == 16) {
             switch (g) {
                 case 2: return launch_fused_t<E, NMAX, 2, ACC64, MODE>(P, err, grid, st, qpart64);
                 case 4: return launch_fused_t<E, NMAX, 4, ACC64, MODE>(P, err, grid, st, qpart64);
