@@ -786,7 +786,14 @@ tomos_status CsrPass::fro2(double* out, const double* d, cudaStream_t st) {
 
 // CSR CountSketch owner sums: a warp per bucket accumulates its rows into
 // a warp-private dense row (shared memory, FP64; distinct columns within a
-// row need no atomics), then writes SA row b.
+// row need no atomics) in increasing row order, then the CTA writes its
+// buckets' rows of SA together.  The rows' metadata (row id, sign, extent)
+// come 32 rows at a time, a row a lane, and the next row's values are
+// loaded before the current one is added, so a row costs the shared-memory
+// update rather than a chain of dependent global loads.  The CTA's nw
+// buckets are consecutive rows of the column-major SA: for each column it
+// writes them as one run of nw doubles (SA is s x n, so writing a row of it
+// alone would touch one 8-byte word per 32-byte sector).
 template <Elem E>
 __global__ void cs_csr_kernel(const void* hi, const void* lo, const int32_t* row_ptrs,
                               const int32_t* col_idxs, int64_t n, int64_t s,
@@ -795,24 +802,68 @@ __global__ void cs_csr_kernel(const void* hi, const void* lo, const int32_t* row
     extern __shared__ __align__(16) double racc[];
     __shared__ double smf[8];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int64_t b = (int64_t)blockIdx.x * nw + w;
+    const int64_t b0 = (int64_t)blockIdx.x * nw;
+    const int64_t b = b0 + w;
     double* acc = racc + (size_t)w * n;
     double f2 = 0.0;
+    for (int64_t j = lane; j < n; j += 32) acc[j] = 0.0;
+    __syncwarp();
     if (b < s) {
-        for (int64_t j = lane; j < n; j += 32) acc[j] = 0.0;
-        __syncwarp();
         const int32_t o0 = offsets[b], o1 = offsets[b + 1];
-        for (int32_t q = o0; q < o1; ++q) {
-            const int32_t r = perm[q];
-            const double sg = (double)sign[r];
-            for (int32_t k = row_ptrs[r] + lane; k < row_ptrs[r + 1]; k += 32) {
-                const double a = load_elem<E>(hi, lo, k);
-                acc[col_idxs[k]] += sg * a;
-                f2 += a * a;
+        for (int32_t base = o0; base < o1; base += 32) {
+            // rows base .. base+31 of the bucket: a row a lane
+            int32_t rs = 0, re = 0;
+            double sgl = 0.0;
+            if (base + lane < o1) {
+                const int32_t r = perm[base + lane];
+                rs = row_ptrs[r];
+                re = row_ptrs[r + 1];
+                sgl = (double)sign[r];
             }
-            __syncwarp();
+            const int cnt = (o1 - base) < 32 ? (o1 - base) : 32;
+            // the first 32 values of the next row, loaded ahead
+            int32_t ks = __shfl_sync(0xffffffffu, rs, 0), ke = __shfl_sync(0xffffffffu, re, 0);
+            double va = 0.0;
+            int32_t ca = 0;
+            if (ks + lane < ke) {
+                va = load_elem<E>(hi, lo, ks + lane);
+                ca = col_idxs[ks + lane];
+            }
+            for (int q = 0; q < cnt; ++q) {
+                const double sg = __shfl_sync(0xffffffffu, sgl, q);
+                const int32_t cs = ks, ce = ke;
+                const double vcur = va;
+                const int32_t ccur = ca;
+                if (q + 1 < cnt) {
+                    ks = __shfl_sync(0xffffffffu, rs, q + 1);
+                    ke = __shfl_sync(0xffffffffu, re, q + 1);
+                    va = 0.0;
+                    if (ks + lane < ke) {
+                        va = load_elem<E>(hi, lo, ks + lane);
+                        ca = col_idxs[ks + lane];
+                    }
+                }
+                if (cs + lane < ce) {
+                    acc[ccur] += sg * vcur;
+                    f2 += vcur * vcur;
+                }
+                // a row longer than a warp: the rest in order
+                for (int32_t k = cs + 32 + lane; k < ce; k += 32) {
+                    const double a = load_elem<E>(hi, lo, k);
+                    acc[col_idxs[k]] += sg * a;
+                    f2 += a * a;
+                }
+                __syncwarp();
+            }
         }
-        for (int64_t j = lane; j < n; j += 32) SA[(size_t)j * ld_sa + b] = acc[j];
+    }
+    __syncthreads();
+    // the CTA's buckets b0 .. b0+nw-1 for every column j, as runs of nw doubles
+    const int nb = (int)((s - b0) < nw ? (s - b0) : nw);
+    const int tot = (int)n * nb;  // n * 8 doubles fit shared memory: no overflow
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int j = idx / nb, k = idx - j * nb;
+        SA[(size_t)j * ld_sa + b0 + k] = racc[(size_t)k * n + j];
     }
     f2 = warp_sum(f2);
     if (lane == 0) smf[w] = f2;

@@ -755,20 +755,38 @@ __global__ void __launch_bounds__(256) trtri_level_kernel(const double* Rt, int6
         }
 }
 
+// D[i, j] = D[j, i] for i > j (n x n column-major).
+__global__ void qr_mirror_lower_kernel(double* D, int64_t ldd, int64_t n) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, j = e / n;
+        if (i > j) D[(size_t)j * ldd + i] = D[(size_t)i * ldd + j];
+    }
+}
+
 // op(A) B products of the blocked QR (qr_gemm.cuh).  With a partial
 // buffer P of pcap doubles, K is split over CTAs (partials summed in
 // order) by the count that wastes the least of the last wave of resident
 // CTAs (two per SM), each split keeping at least 16 k-stages and all
-// partials fitting P.  sub: D -= op(A) B.
+// partials fitting P.  sub: D -= op(A) B.  upper (a symmetric product,
+// op(A) = B^T, square D): only the tiles that reach the diagonal or above
+// are formed, and the lower triangle is then copied from the upper
+// (qr_mirror_lower_kernel), exactly symmetric.
 template <bool KMAJOR>
 static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64_t ldb, double* D,
                             int64_t ldd, int64_t M, int64_t N, int64_t K, double alpha, double beta,
-                            double* P, size_t pcap, cudaStream_t st, int sub = 0) {
+                            double* P, size_t pcap, cudaStream_t st, int sub = 0, bool upper = false) {
     if (M <= 0 || N <= 0) return TOMOS_OK;
     const int64_t tm = (M + kGbm - 1) / kGbm, tn = (N + kGbn - 1) / kGbn;
+    int64_t active = tm * tn;
+    if (upper) {
+        active = 0;
+        for (int64_t i = 0; i < tm; ++i)
+            for (int64_t j = 0; j < tn; ++j)
+                if (i * kGbm <= j * kGbn + kGbn - 1) ++active;
+    }
     int64_t splits = 1;
     if (P) {
-        const int64_t slots = 2 * (int64_t)sm_count(), tiles = tm * tn;
+        const int64_t slots = 2 * (int64_t)sm_count(), tiles = active;
         int64_t kmax = K / (16 * kGbk);
         if (kmax > kGmaxSplits) kmax = kGmaxSplits;
         const int64_t fit = (int64_t)(pcap / (size_t)(M * N));
@@ -803,6 +821,7 @@ static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64
     g.alpha = alpha;
     g.beta = beta;
     g.sub = sub;
+    g.upper = upper ? 1 : 0;
     TOMOS_CUDA_TRY(cudaFuncSetAttribute(qr_gemm_kernel<KMAJOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kGemmSmem));
     qr_gemm_kernel<KMAJOR><<<dim3((unsigned)tm, (unsigned)tn, (unsigned)splits), 256, kGemmSmem, st>>>(g);
@@ -812,6 +831,12 @@ static tomos_status qr_gemm(const double* A, int64_t lda, const double* B, int64
         if (rb > 4096) rb = 4096;
         qr_gemm_reduce_kernel<<<(unsigned)rb, 256, 0, st>>>(P, (int)splits, M, N, alpha, beta, D, ldd);
         TOMOS_LAUNCH_CHECK("qr_gemm_reduce_kernel");
+    }
+    if (upper) {
+        const int64_t nn = M * M;
+        const unsigned mb = (unsigned)((nn + 255) / 256 < 4096 ? (nn + 255) / 256 : 4096);
+        qr_mirror_lower_kernel<<<mb, 256, 0, st>>>(D, ldd, M);
+        TOMOS_LAUNCH_CHECK("qr_mirror_lower_kernel");
     }
     return TOMOS_OK;
 }
@@ -1287,7 +1312,8 @@ static tomos_status qr_wide(int64_t k, int64_t n, double* SA, int64_t ld, double
                             cudaStream_t st, bool* done, bool any_signs) {
     *done = false;
     TOMOS_CUDA_TRY(cudaMemsetAsync(w.flag, 0, sizeof(int) * 4, st));
-    tomos_status s = qr_gemm<true>(SA, ld, SA, ld, w.G, n, n, n, k, 1.0, 0.0, w.P, w.pcap, st);
+    // the Gram S^T S: its upper triangle, mirrored
+    tomos_status s = qr_gemm<true>(SA, ld, SA, ld, w.G, n, n, n, k, 1.0, 0.0, w.P, w.pcap, st, 0, true);
     if (s) return s;
     const unsigned eb = (unsigned)((n * n + 255) / 256 < 4096 ? (n * n + 255) / 256 : 4096);
     wide_colnorm_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(w.G, n, w.d, w.flag);

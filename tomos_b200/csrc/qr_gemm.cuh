@@ -74,6 +74,7 @@ struct GemmArgs {
     int64_t M, N, K, kc;
     double alpha, beta;
     int sub;
+    int upper;  // skip the tiles wholly below the diagonal (a symmetric product's other half)
 };
 
 template <bool KMAJOR>
@@ -83,6 +84,7 @@ __global__ void __launch_bounds__(256, 2) qr_gemm_kernel(GemmArgs g) {
     const int gq = lane >> 2, qq = lane & 3;
     const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
     const int64_t m0 = (int64_t)blockIdx.x * kGbm, n0 = (int64_t)blockIdx.y * kGbn;
+    if (g.upper && m0 > n0 + kGbn - 1) return;
     const int64_t kb = (int64_t)blockIdx.z * g.kc;
     const int64_t ke = kb + g.kc < g.K ? kb + g.kc : g.K;
     const int nk = ke > kb ? (int)((ke - kb + kGbk - 1) / kGbk) : 0;
