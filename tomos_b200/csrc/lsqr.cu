@@ -180,6 +180,10 @@ struct NSide {
     const int* skip;
     const double* dscale;  // column scale D of the backward-error rule, or NULL
     const double* qsum;    // row-sharded solves: A^T ut summed over ranks (n), else NULL
+    // The iteration graph's while loop: N4 sets its condition (1: run the
+    // body again) on every path, so the loop ends once the solver stops.
+    cudaGraphConditionalHandle cond;
+    int use_cond;
 };
 
 // Givens step of LSQR (lsqr.cpp:633-679), FP64.
@@ -342,9 +346,15 @@ __global__ void __launch_bounds__(256) nside_update_kernel(NSide S) {
     }
 }
 
-// N4: one block -- state update and the stopping rule.
+// N4: one block -- state update and the stopping rule.  In the iteration
+// graph's while loop it also sets the loop's condition: 0 once the solver
+// stopped (a skipped body, the stopping rule, a breakdown or the restart's
+// max_iters iterations), so the loop runs at most max_iters + 1 bodies.
 __global__ void __launch_bounds__(256) nside_finish_kernel(NSide S) {
-    if (S.skip && *S.skip) return;
+    if (S.skip && *S.skip) {
+        if (S.use_cond && threadIdx.x == 0) cudaGraphSetConditional(S.cond, 0u);
+        return;
+    }
     __shared__ double sm[32];
     const double xn = sqrt(block_sum_array(S.xpart, S.nb3, sm));
     const double qn = S.init ? sqrt(block_sum_array(S.qnpart, S.nb1, sm)) : 0.0;
@@ -365,6 +375,7 @@ __global__ void __launch_bounds__(256) nside_finish_kernel(NSide S) {
         st->relres = st->rhsnorm > 0.0 ? beta / st->rhsnorm : 0.0;
         st->done = 0;
         st->breakdown = (alpha == 0.0 || beta == 0.0) ? 1 : 0;
+        if (S.use_cond) cudaGraphSetConditional(S.cond, 0u);  // no loop runs init passes
         return;
     }
     Givens g = givens(st->rho_bar, st->phi_bar, alpha, beta);
@@ -396,6 +407,7 @@ __global__ void __launch_bounds__(256) nside_finish_kernel(NSide S) {
     }
     if (st->iter_restart >= st->max_iters) stop = 1;
     if (stop) st->done = 1;
+    if (S.use_cond) cudaGraphSetConditional(S.cond, stop ? 0u : 1u);
 }
 
 // ------------------------------------------------------------ workspace
@@ -687,6 +699,8 @@ static NSide make_nside(tomos_workspace* ws, const PassPlan& pl, float* x, bool 
     S.st = ws->st;
     S.skip = skip;
     S.qsum = nullptr;
+    S.cond = 0;
+    S.use_cond = 0;
     if (ws->comm) {  // the pass's partials were folded and summed across ranks
         S.qsum = ws->shard;
         S.sspart = ws->shard + ws->n;
@@ -979,6 +993,64 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
     if (!ws->graph || ws->graph_key != key) {
         if (ws->graph) cudaGraphExecDestroy(ws->graph);
         ws->graph = nullptr;
+        ws->graph_loop = false;
+        // A graph whose one node is a while loop over the iteration: its
+        // condition starts at 1 at each launch and N4 sets it, so one
+        // launch runs a restart's iterations to the stopping rule with no
+        // host round trip.  Row-sharded solves (an NCCL call in the
+        // iteration) and a runtime without conditional nodes replay the
+        // plain iteration graph in batches instead.
+        if (!o->comm) {
+            const int64_t before = ws->launches;
+            cudaGraph_t g = nullptr;
+            cudaGraphConditionalHandle h = 0;
+            cudaGraphNodeParams cp = {};
+            cudaGraphNode_t node = nullptr;
+            bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+                      cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+            if (ok) {
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = h;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                ok = cudaGraphAddNode(&node, g, nullptr, 0, &cp) == cudaSuccess;
+            }
+            if (ok)
+                ok = cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                const int* skip = &ws->st->done;
+                NSide S = make_nside(ws, pl_iter, x, false, skip, dsc);
+                S.cond = h;
+                S.use_cond = 1;
+                tomos_status cs = pass(pl_iter, ws->p, ws->u, ws->st->coef, skip);
+                if (!cs) cs = enqueue_nside(ws, S, st);
+                cudaGraph_t body = nullptr;
+                const cudaError_t ce = cudaStreamEndCapture(st, &body);
+                if (cs) {
+                    cudaGraphDestroy(g);
+                    return cs;
+                }
+                ok = ce == cudaSuccess;
+            }
+            if (ok) ok = cudaGraphInstantiate(&ws->graph, g, 0) == cudaSuccess;
+            if (g) cudaGraphDestroy(g);
+            if (ok) {
+                ws->graph_loop = true;
+                ws->graph_key = key;
+                ws->graph_kernels = ws->launches - before;
+            } else {
+                cudaGetLastError();  // not sticky: fall back to the plain graph
+                if (ws->graph) cudaGraphExecDestroy(ws->graph);
+                ws->graph = nullptr;
+                ws->launches = before;
+            }
+        }
+    }
+    if (!ws->graph || ws->graph_key != key) {
+        if (ws->graph) cudaGraphExecDestroy(ws->graph);
+        ws->graph = nullptr;
+        ws->graph_loop = false;
         cudaGraph_t g = nullptr;
         const int64_t before = ws->launches;
         TOMOS_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -1086,6 +1158,14 @@ tomos_status solve_driver(tomos_workspace* ws, PassOps& ops, const float* b, flo
             R.iter_pass_count += 1;
             done_iters = H.iter_restart;
             if (H.done) break;
+        }
+        if (!o->profile && ws->graph_loop) {
+            // one launch: the device loops to the stopping rule
+            TOMOS_CUDA_TRY(cudaGraphLaunch(ws->graph, st));
+            s = sync_state(ws);
+            if (s) return s;
+            ws->launches += (int64_t)H.iter_restart * ws->graph_kernels;
+            done_iters = max_iters;
         }
         while (!o->profile && done_iters < max_iters) {
             int k = batch < max_iters - done_iters ? batch : max_iters - done_iters;

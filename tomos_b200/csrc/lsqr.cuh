@@ -227,6 +227,7 @@ struct tomos_workspace {
 
     cudaGraphExec_t graph = nullptr;
     int64_t launches = 0;        // kernels enqueued by the driver (graph replays included)
-    int64_t graph_kernels = 0;   // kernels in one replay of `graph`
+    int64_t graph_kernels = 0;   // kernels in one replay of `graph`'s iteration
+    bool graph_loop = false;     // `graph` is a device-side while loop over the iteration
     std::vector<uint64_t> graph_key;
 };
