@@ -203,6 +203,29 @@ __device__ __forceinline__ Givens givens(double rho_bar, double phi_bar, double 
     return g;
 }
 
+// sum over k = lane, lane + 32, .. < len of a[k] b[k] (the lane's share of a
+// warp's dot product over L2-resident vectors): eight independent FP64
+// chains, so a lane has sixteen loads in flight instead of two.
+__device__ __forceinline__ double strided_dot(const double* __restrict__ a, const double* __restrict__ b,
+                                              int lane, int64_t len) {
+    double z[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int64_t k = lane;
+    for (; k + 7 * 32 < len; k += 8 * 32) {
+        double av[8], bv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            av[u] = __ldg(a + k + 32 * u);
+            bv[u] = __ldg(b + k + 32 * u);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) z[u] = fma(av[u], bv[u], z[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+        if (k + 32 * u < len) z[u] = fma(__ldg(a + k + 32 * u), __ldg(b + k + 32 * u), z[u]);
+    return ((z[0] + z[1]) + (z[2] + z[3])) + ((z[4] + z[5]) + (z[6] + z[7]));
+}
+
 // N1: beta and t = A^T ut / beta (no preconditioner: vh = t - beta v).
 __global__ void __launch_bounds__(256) nside_reduce_kernel(NSide S) {
     if (S.skip && *S.skip) return;
@@ -263,17 +286,11 @@ __global__ void __launch_bounds__(256) nside_precond_t_kernel(NSide S) {
     const double beta = S.scal[0];
     double vh2 = 0.0;
     if (j < S.n) {
-        const double* col = S.Rcm + (size_t)j * S.n;
+        const double* __restrict__ col = S.Rcm + (size_t)j * S.n;
+        const double* __restrict__ tv = S.t;
         // an upper triangular M: column j ends at row j
         const int64_t ie = S.scal[7] != 0.0 ? S.n : j + 1;
-        double z0 = 0.0, z1 = 0.0;
-        int64_t i = lane;
-        for (; i + 32 < ie; i += 64) {
-            z0 = fma(col[i], S.t[i], z0);
-            z1 = fma(col[i + 32], S.t[i + 32], z1);
-        }
-        if (i < ie) z0 = fma(col[i], S.t[i], z0);
-        double z = warp_sum(z0 + z1);
+        const double z = warp_sum(strided_dot(col, tv, lane, ie));
         const double vh = S.init ? z : z - beta * (double)S.v[j];
         if (lane == 0) S.vhat[j] = vh;
         vh2 = vh * vh;
@@ -306,16 +323,11 @@ __global__ void __launch_bounds__(256) nside_update_kernel(NSide S) {
     if (i < S.n) {
         double pi;
         if (S.has_precond) {
-            const double* row = S.Rrm + (size_t)i * S.n;
+            const double* __restrict__ row = S.Rrm + (size_t)i * S.n;
+            const double* __restrict__ vh = S.vhat;
             // an upper triangular M: row i starts at column i
-            int64_t jj = (S.scal[7] != 0.0 ? 0 : i) + lane;
-            double z0 = 0.0, z1 = 0.0;
-            for (; jj + 32 < S.n; jj += 64) {
-                z0 = fma(row[jj], S.vhat[jj], z0);
-                z1 = fma(row[jj + 32], S.vhat[jj + 32], z1);
-            }
-            if (jj < S.n) z0 = fma(row[jj], S.vhat[jj], z0);
-            pi = warp_sum(z0 + z1) * inva;
+            const int64_t j0 = S.scal[7] != 0.0 ? 0 : i;
+            pi = warp_sum(strided_dot(row + j0, vh + j0, lane, S.n - j0)) * inva;
         } else {
             pi = S.vhat[i] * inva;
         }
