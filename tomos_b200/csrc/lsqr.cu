@@ -581,7 +581,7 @@ PassPlan plan_dense_pass(tomos_workspace* ws, const tomos_dense* A, Elem e, bool
     pl.runs = runs && pl.acc64 && (e == Elem::F32 || elem_two_planes(e));
     int nch = 0, g = 1;
     const bool ok = A->layout == TOMOS_ROW_MAJOR && A->cols > 0 &&
-                    plan_row_lines(e, pl.acc64 && !pl.runs, A->cols, A->ld, A->values,
+                    plan_row_lines(e, pl.acc64, pl.runs ? kRowBothRuns : kRowBoth, A->cols, A->ld, A->values,
                                    elem_is_exact(e) ? dense_lo_plane(A) : nullptr, &nch, &g);
     if (ok) {
         pl.fused = true;

@@ -78,16 +78,18 @@ struct RowF64Regs {
 };
 
 // Consumer warps of a pass.  13 warps (with the producer) leave 128
-// registers a thread; the passes with FP64 registers per column over one
-// plane keep a whole row part per lane, and run 8 consumers (9 warps: up
-// to 168 registers) so that a warp still covers 1024 columns; over two
-// planes they keep 16 warps (a warp covering 512 columns) to hide the
-// exact decode's latency.
+// registers a thread, 17 warps 96; the passes with FP64 registers per
+// column over one plane keep a whole row part per lane, and run 8
+// consumers (9 warps: up to 168 registers) so that a warp still covers
+// 1024 columns; over two planes they keep 16 warps (a warp covering 512
+// columns) to hide the exact decode's latency.  The plain 16-bit planes,
+// and FP32_16's wh plane in the standalone products, take 16 warps; the
+// LSQR pass over a wh plane keeps 12 (at 96 registers it would spill).
 template <Elem E, bool ACC64, int MODE>
 struct RowWarps {
-    static constexpr int value = !RowF64Regs<ACC64, MODE>::value
-                                     ? ((E == Elem::F16 || E == Elem::B16) ? 16 : 12)
-                                     : (RowPlanes<E>::value == 1 ? 8 : 16);
+    static constexpr bool wide16 = E == Elem::F16 || E == Elem::B16 || (E == Elem::H16 && MODE != kRowBoth);
+    static constexpr int value = !RowF64Regs<ACC64, MODE>::value ? (wide16 ? 16 : 12)
+                                                                 : (RowPlanes<E>::value == 1 ? 8 : 16);
 };
 constexpr int kRowWarps = 16;  // the widest configuration (shared arrays)
 
@@ -127,6 +129,7 @@ __device__ __forceinline__ float h16_corrections(const uint4 (&hk)[NCH], int par
 #pragma unroll
     for (int k = 0; k < NCH; ++k) {
         const uint4 h = hk[k];
+        if (!((h.x | h.y | h.z | h.w) & 0x00010001u)) continue;  // most chunks
         uint32_t flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
                          ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
         while (flags) {
@@ -217,8 +220,11 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
                 f[0] = p0.x; f[1] = p0.y; f[2] = p1.x; f[3] = p1.y;
                 f[4] = p2.x; f[5] = p2.y; f[6] = p3.x; f[7] = p3.y;
             }
-            uint32_t flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
-                             ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
+            // formed only for a chunk that has a control bit (most have none)
+            uint32_t flags = 0;
+            if ((h.x | h.y | h.z | h.w) & 0x00010001u)
+                flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
+                        ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
             while (flags) {
                 const int bit = __ffs(flags) - 1;
                 flags &= flags - 1;

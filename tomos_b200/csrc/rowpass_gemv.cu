@@ -93,8 +93,7 @@ tomos_status rowpass_gemv(const GemvLaunch& L, Elem e, cudaStream_t st, bool* us
     const bool acc64 = elem_is_exact(e);
     if (e == Elem::F64 || L.coef || L.skip) return TOMOS_OK;
     int nch = 0, g = 1;
-    // the FP64-accumulating A^T product holds FP64 registers per column
-    if (!plan_row_lines(e, acc64 && !L.dot, L.inner, L.ld, L.hi, L.lo, &nch, &g)) return TOMOS_OK;
+    if (!plan_row_lines(e, acc64, L.dot ? kRowDot : kRowAxpy, L.inner, L.ld, L.hi, L.lo, &nch, &g)) return TOMOS_OK;
     const int grid = row_pass_grid(L.outer);
     const int64_t qs = (L.inner + 31) / 32 * 32;
     if (!L.dot && (!L.scratch || L.scratch_bytes < (size_t)grid * qs * (acc64 ? 8 : 4))) return TOMOS_OK;

@@ -48,25 +48,28 @@ inline bool elem_two_planes(Elem e) {
     return e == Elem::A16 || e == Elem::AB16 || e == Elem::AB16R;
 }
 
-// 16-byte chunks a lane takes per row part at most (RowNchMax); f64regs:
-// the pass holds FP64 registers per column (RowF64Regs).
-inline int fused_nch_max(Elem e, bool f64regs) {
+// Host mirrors of RowF64Regs, RowNchMax and RowWarps for a pass of
+// element type e, FP64 flag acc64 and mode (RowMode).
+inline bool fused_f64regs(bool acc64, int mode) { return acc64 && (mode == kRowBoth || mode == kRowAxpy); }
+
+inline int fused_nch_max(Elem e, bool acc64, int mode) {
     const int base = (e == Elem::F32) ? 8 : 4;
-    return (f64regs && elem_two_planes(e)) ? base / 2 : base;
+    return (fused_f64regs(acc64, mode) && elem_two_planes(e)) ? base / 2 : base;
 }
 
-// Consumer warps of a pass (RowWarps).
-inline int fused_warps(Elem e, bool f64regs) {
-    return !f64regs ? ((e == Elem::F16 || e == Elem::B16) ? 16 : 12) : (elem_two_planes(e) ? 16 : 8);
+inline int fused_warps(Elem e, bool acc64, int mode) {
+    if (fused_f64regs(acc64, mode)) return elem_two_planes(e) ? 16 : 8;
+    const bool wide16 = e == Elem::F16 || e == Elem::B16 || (e == Elem::H16 && mode != kRowBoth);
+    return wide16 ? 16 : 12;
 }
 
 // Warps per row a pass may split a row over (divisors of its consumer
 // warps).
-inline const int* fused_g_list(Elem e, bool f64regs, int* count) {
+inline const int* fused_g_list(Elem e, bool acc64, int mode, int* count) {
     static const int g12[] = {2, 3, 4, 6, 12};
     static const int g8[] = {2, 4, 8};
     static const int g16[] = {2, 4, 8, 16};
-    const int w = fused_warps(e, f64regs);
+    const int w = fused_warps(e, acc64, mode);
     *count = w == 8 ? 3 : (w == 16 ? 4 : 5);
     return w == 8 ? g8 : (w == 16 ? g16 : g12);
 }
@@ -75,14 +78,14 @@ inline const int* fused_g_list(Elem e, bool f64regs, int* count) {
 // ld: chunks per lane (nch) and warps per line (g), or false when the
 // lines are not 16-byte aligned (both planes for two-plane types), too
 // long for the consumer warps, or too long for a stage ring of two.
-inline bool plan_row_lines(Elem e, bool f64regs, int64_t inner, int64_t ld, const void* hi,
+inline bool plan_row_lines(Elem e, bool acc64, int mode, int64_t inner, int64_t ld, const void* hi,
                            const void* lo, int* nch_out, int* g_out) {
     const int vec = (e == Elem::F32) ? 4 : 8;
     const int wbytes = (e == Elem::F32) ? 4 : 2;
     if (inner <= 0 || (ld * wbytes) % 16 != 0 || reinterpret_cast<uintptr_t>(hi) % 16 != 0) return false;
     if (elem_two_planes(e) && reinterpret_cast<uintptr_t>(lo) % 16 != 0) return false;
     int nch = 0, g = 1;
-    const int nmax = fused_nch_max(e, f64regs);
+    const int nmax = fused_nch_max(e, acc64, mode);
     for (int c : {1, 2, 4, 8}) {
         if (c > nmax) break;
         if ((int64_t)32 * c * vec >= inner) {
@@ -92,7 +95,7 @@ inline bool plan_row_lines(Elem e, bool f64regs, int64_t inner, int64_t ld, cons
     }
     if (nch == 0) {
         int ng = 0;
-        const int* gl = fused_g_list(e, f64regs, &ng);
+        const int* gl = fused_g_list(e, acc64, mode, &ng);
         for (int q = 0; q < ng; ++q) {
             if ((int64_t)gl[q] * 32 * nmax * vec >= inner) {
                 nch = nmax;
@@ -102,7 +105,7 @@ inline bool plan_row_lines(Elem e, bool f64regs, int64_t inner, int64_t ld, cons
         }
     }
     if (nch == 0) return false;
-    const int64_t rows_per_stage = fused_warps(e, f64regs) / g;
+    const int64_t rows_per_stage = fused_warps(e, acc64, mode) / g;
     const int64_t stage = rows_per_stage * ((inner * wbytes + 15) / 16 * 16) * (elem_two_planes(e) ? 2 : 1);
     if (2 * stage > (int64_t)kRowSmemBudget) return false;
     *nch_out = nch;
