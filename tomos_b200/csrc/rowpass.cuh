@@ -27,8 +27,9 @@
 // 16-byte access.
 //
 // FP32_16 wh words with the control bit set (values outside the fp16
-// range) are rare; one OR over a row's words tests for them and only then
-// takes the exact fp32_16_half_only decode.
+// range) are rare; one OR over a chunk's words tests for them, and only a
+// chunk that has one rewrites them to their fp32_16_half_only bits before
+// the fp16 conversion.
 //
 // ACC64 (the exact tiers, restart residuals, backward errors) forms every
 // product exactly and sums it in FP64, as the reference's accurate tier
@@ -117,37 +118,6 @@ struct RowPassParams {
     double* qpart64; // kRowAxpy with ACC64: FP64 partials (gridDim.x x qstride)
 };
 
-// The control words of one lane's row part (NCH chunks of 8 wh words, as
-// loaded; elements from zero_from on lie past the row and are skipped):
-// returns sum d * p[col] with d = fp32_16_half_only value - its plain fp16
-// conversion (the correction of the lane's dot).  A loop over the flagged
-// elements only, so a lane without one passes through at once.
-template <int NCH>
-__device__ __forceinline__ float h16_corrections(const uint4 (&hk)[NCH], int part, int lane, int zero_from,
-                                                 const float* p) {
-    float dsum = 0.0f;
-#pragma unroll
-    for (int k = 0; k < NCH; ++k) {
-        const uint4 h = hk[k];
-        if (!((h.x | h.y | h.z | h.w) & 0x00010001u)) continue;  // most chunks
-        uint32_t flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
-                         ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
-        while (flags) {
-            const int bit = __ffs(flags) - 1;
-            flags &= flags - 1;
-            const int wi = bit & 3, hi = bit >> 4;
-            const int q = 2 * wi + hi;  // element of the chunk
-            if (k * 8 + q >= zero_from) continue;
-            const uint32_t ww = wi == 0 ? h.x : wi == 1 ? h.y : wi == 2 ? h.z : h.w;
-            const uint32_t hb = (ww >> (hi * 16)) & 0xFFFFu;
-            const float d = half_bits_to_float(half_only_bits(hb)) - half_bits_to_float(hb);
-            const int64_t col = ((int64_t)part * 32 * NCH + (int64_t)k * 32 + lane) * 8 + q;
-            dsum += d * __ldg(p + col);
-        }
-    }
-    return dsum;
-}
-
 // kRowAxpy with ACC64 sums FP32 products over this many rows of a warp,
 // then adds them into FP64 accumulators.
 constexpr int kRowPromote = 8;
@@ -208,35 +178,17 @@ __device__ __forceinline__ void decode_row(const uint8_t* hrow, const uint8_t* l
             for (int e = 0; e < HV; ++e) a[k * HV + e] = make_float2(f[2 * e], f[2 * e + 1]);
         }
     } else if constexpr (E == Elem::H16) {
-        // wh words without a control bit are fp16 values: plain
-        // conversions; the elements with one (rare) are redone by a loop,
-        // as in the exact decode above.
+        // wh words without a control bit are fp16 values: a chunk that
+        // holds a control bit (rare) has those words rewritten to their
+        // fp32_16_half_only bits first, then every word converts as fp16.
 #pragma unroll
         for (int k = 0; k < NCH; ++k) {
-            const uint4 h = (live >> k) & 1u ? lds128(hrow + coff[k]) : make_uint4(0, 0, 0, 0);
-            float f[8];
-            {
-                const float2 p0 = h2f2(h.x), p1 = h2f2(h.y), p2 = h2f2(h.z), p3 = h2f2(h.w);
-                f[0] = p0.x; f[1] = p0.y; f[2] = p1.x; f[3] = p1.y;
-                f[4] = p2.x; f[5] = p2.y; f[6] = p3.x; f[7] = p3.y;
-            }
-            // formed only for a chunk that has a control bit (most have none)
-            uint32_t flags = 0;
-            if ((h.x | h.y | h.z | h.w) & 0x00010001u)
-                flags = (h.x & 0x00010001u) | ((h.y & 0x00010001u) << 1) |
-                        ((h.z & 0x00010001u) << 2) | ((h.w & 0x00010001u) << 3);
-            while (flags) {
-                const int bit = __ffs(flags) - 1;
-                flags &= flags - 1;
-                const int wi = bit & 3, hi = bit >> 4;
-                const uint32_t ww = wi == 0 ? h.x : wi == 1 ? h.y : wi == 2 ? h.z : h.w;
-                const float v = half_bits_to_float(half_only_bits((ww >> (hi * 16)) & 0xFFFFu));
-                const int q = 2 * wi + hi;
-#pragma unroll
-                for (int e = 0; e < 8; ++e) f[e] = e == q ? v : f[e];
-            }
-#pragma unroll
-            for (int e = 0; e < 4; ++e) a[k * 4 + e] = make_float2(f[2 * e], f[2 * e + 1]);
+            uint4 h = (live >> k) & 1u ? lds128(hrow + coff[k]) : make_uint4(0, 0, 0, 0);
+            if ((h.x | h.y | h.z | h.w) & 0x00010001u) fix_half_chunk(h);
+            a[k * 4 + 0] = h2f2(h.x);
+            a[k * 4 + 1] = h2f2(h.y);
+            a[k * 4 + 2] = h2f2(h.z);
+            a[k * 4 + 3] = h2f2(h.w);
         }
     } else {
 #pragma unroll
@@ -278,11 +230,6 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64, MODE>::value + 1) * 32, 1)
     // standalone FP64 tiers (kRowDot, kRowAxpy with ACC64) and kRowBothRuns
     // form FP32 products over short runs and sum those in FP64.
     constexpr bool P64 = ACC64 && MODE == kRowBoth;
-    // FP32_16 wh words in a standalone dot product: every word converted as
-    // an fp16 value, and the rare control words corrected afterwards by the
-    // difference between their fp32_16_half_only value and that conversion,
-    // added to the lane's own partial dot (so the sum keeps its fixed order).
-    constexpr bool HCORR = E == Elem::H16 && MODE == kRowDot;
     constexpr int NTHREADS = (CW + 1) * 32;
     static_assert(CW % G == 0, "G divides the consumer warps");
     const FusedParams& P = T.f;
@@ -451,24 +398,7 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64, MODE>::value + 1) * 32, 1)
             }
             const uint8_t* hrow = smem + (size_t)s * stage_bytes + (size_t)(sub * RS + rg) * cb;
             float2 a[PER / 2];
-            uint4 hk[HCORR ? NCH : 1];
-            if (HCORR && has && !failed) {
-#pragma unroll
-                for (int k = 0; k < NCH; ++k) {
-                    hk[k] = (live >> k) & 1u ? lds128(hrow + coff[k]) : make_uint4(0, 0, 0, 0);
-                    a[k * 4 + 0] = h2f2(hk[k].x);
-                    a[k * 4 + 1] = h2f2(hk[k].y);
-                    a[k * 4 + 2] = h2f2(hk[k].z);
-                    a[k * 4 + 3] = h2f2(hk[k].w);
-                }
-                if (zero_from < PER) {
-#pragma unroll
-                    for (int e = 0; e < PER; e += 2) {
-                        if (e >= zero_from) a[e / 2].x = 0.0f;
-                        if (e + 1 >= zero_from) a[e / 2].y = 0.0f;
-                    }
-                }
-            } else if (has && !failed) {
+            if (has && !failed) {
                 decode_row<E, NCH>(hrow, hrow + plane_bytes, coff, live, a);
                 if (zero_from < PER) {
 #pragma unroll
@@ -515,9 +445,6 @@ __global__ void __launch_bounds__((RowWarps<E, ACC64, MODE>::value + 1) * 32, 1)
                 for (int j = 0; j < PER / 2; j += 2) {
                     d0 = __ffma2_rn(a[j], pv[j], d0);
                     d1 = __ffma2_rn(a[j + 1], pv[j + 1], d1);
-                }
-                if constexpr (HCORR) {
-                    if (has && !failed) d0.x += h16_corrections<NCH>(hk, part, lane, zero_from, P.p);
                 }
                 if constexpr (ACC64) {
                     // FP32 products summed over the lane's run, then FP64
