@@ -1,12 +1,14 @@
 """Named small workloads of the library's hot kernels, for profiling one
 kernel at a time (e.g. under ncu) without the whole benchmark around it.
 
-    python -m tomos_b200.cases solve [--m M] [--n N] [--storage fp32_16|fp32] [--reps R]
+    python -m tomos_b200.cases solve [--m M] [--n N] [--storage fp32_16|fp32] [--reps R] [--profile]
     python -m tomos_b200.cases gemm  [--size S] [--tier half_operands|half|accurate] [--reps R]
     python -m tomos_b200.cases gemv  [--m M] [--n N] [--tier half|accurate|fp32] [--reps R]
 
 `solve` runs the sketch-preconditioned LSQR pipeline (sketch_lsqr) on the
-seeded dense problem A = G diag(10^u) of problems.dense_scaled; `gemm` runs
+seeded dense problem A = G diag(10^u) of problems.dense_scaled (--profile: the
+solver's profile mode, every iteration launched on its own instead of in the
+device-side graph loop, so that a profiler lists each pass); `gemm` runs
 mm_apply on S x S column-major operands (A packed FP32_16); `gemv` runs
 mv_apply both ways on the packed (or FP32) row-major matrix.  Each case
 runs `reps` times after one untimed warm-up call and prints one line."""
@@ -27,7 +29,7 @@ def _solve(a):
     ws = tb.create_lsqr_workspace(None, (a.m, a.n), tb.NumericType.FP32, tb.NumericType.FP64)
     rep = None
     for _ in range(1 + a.reps):
-        _, rep, _ = tb.sketch_lsqr(A, b, 4 * a.n, workspace=ws)
+        _, rep, _ = tb.sketch_lsqr(A, b, 4 * a.n, workspace=ws, profile=a.profile)
     torch.cuda.synchronize()
     return f"solve {a.m}x{a.n} {a.storage}: iterations {rep['iterations']}, eta_D {rep['backward_error']:.3e}"
 
@@ -73,6 +75,7 @@ def main(argv=None):
     ap.add_argument("--size", type=int, default=4096)
     ap.add_argument("--tier", default="half_operands")
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--profile", action="store_true")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
     print({"solve": _solve, "gemm": _gemm, "gemv": _gemv}[a.case](a))
